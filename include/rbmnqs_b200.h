@@ -1,0 +1,208 @@
+/*
+ * rbmnqs_b200.h -- C ABI of the B200 (sm_100a) VMC hot path for rbm-nqs.
+ *
+ * The library replaces, for one GPU, the reference's per-epoch hot path
+ *   sampler::abstract_sampler::sample()        include/sampler/abstract_sampler.hpp:74
+ *   optimizer::abstract_optimizer::optimize()   src/optimizer/abstract_optimizer.cpp:80-178
+ *   optimizer::abstract_solver::solve(...)      include/optimizer/abstract_solver.hpp:31-34
+ * together with the machine/operators work they drive (machine/rbm_base,
+ * machine/rbm_symmetry, operators/local_op, operators/aggregator).
+ *
+ * Conventions (all identical to the reference):
+ *   - complex arrays are interleaved (re, im) doubles;
+ *   - a configuration is four uint32 words, bit i of word i/32 is site i and a
+ *     set bit means sigma_i = -1               (machine/spin_state.cpp:44-50);
+ *   - the parameter vector is [v (n_vb), h (n_hidden), W (n x n_hidden,
+ *     column-major, j + n*k), Pfaffian f (n_indep x 4, column-major)]
+ *                                              (machine/rbm_base.cpp:117-131);
+ *   - samples are ordered chain-major: sample c*samples_per_chain + j.
+ * All functions return 0 on success or a negative RBMNQS_ERR_* code; the
+ * message of the last error of the calling thread is rbmnqs_last_error().
+ * No C++ exception crosses this boundary.  A handle owns one CUDA stream and
+ * all its device buffers; calls on one handle must not run concurrently.
+ */
+#ifndef RBMNQS_B200_H
+#define RBMNQS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RBMNQS_OK 0
+#define RBMNQS_ERR_ARG (-1)           /* bad argument / shape */
+#define RBMNQS_ERR_CUDA (-2)          /* CUDA runtime error */
+#define RBMNQS_ERR_UNSUPPORTED (-3)   /* configuration not supported */
+#define RBMNQS_ERR_MASSIVE_STEP (-4)  /* max|dw| > 30, abstract_optimizer.cpp:157-159 */
+#define RBMNQS_ERR_NONFINITE (-5)     /* NaN/Inf in energies or update */
+#define RBMNQS_ERR_NO_DEVICE (-6)     /* no CUDA device / kernels not loadable */
+
+typedef struct rbmnqs_model rbmnqs_model;
+typedef struct rbmnqs_handle rbmnqs_handle;
+
+/* ----------------------------------------------------------- models ---- */
+/* Kitaev honeycomb model: bond operators J_g sigma^g sigma^g on x/y/z bonds
+ * and an optional field -h sx + h sy + h sz on every site.
+ * Replaces model::kitaev (src/model/kitaev.cpp:29-50) with
+ * lattice::honeycomb (src/lattice/honeycomb.cpp); `symmetry` is the
+ * model.symmetry value used by rbm.type=symmetry (honeycomb.hpp:77-85). */
+int rbmnqs_model_kitaev(int32_t n_cells, int32_t n_cells_b, const double J[3],
+                        double h, double symmetry, rbmnqs_model** out);
+/* Toric code: J sz^4 on plaquettes, J sx^4 on stars.
+ * Replaces model::toric (src/model/toric.cpp:27-47) with
+ * lattice::toric_lattice (src/lattice/toric_lattice.cpp:57-69). */
+int rbmnqs_model_toric(int32_t n_cells, double J, double symmetry,
+                       rbmnqs_model** out);
+/* Adds the hexagon plaquette operators W_p (observables, main.cpp:645-671)
+ * as extra, separately accumulated operators. */
+int rbmnqs_model_add_hexagons(rbmnqs_model* m);
+/* Sizes: spins, Hamiltonian operators, lattice bonds, observables. */
+int rbmnqs_model_sizes(const rbmnqs_model* m, int32_t* n_sites,
+                       int32_t* n_ops, int32_t* n_bonds, int32_t* n_observables);
+/* Bond list (a, b, type) as lattice::get_bonds (bravais.hpp get_bonds). */
+int rbmnqs_model_bonds(const rbmnqs_model* m, int32_t* abt);
+/* Operator k, acts_on[6] (-1 padded) and its dense 2^k x 2^k row-major
+ * complex matrix (operators/local_op.hpp op_), for inspection and tests. */
+int rbmnqs_model_op(const rbmnqs_model* m, int32_t o, int32_t* k,
+                    int32_t* acts_on, double* mat);
+/* Symmetry permutations perm[s*n + i] = P_s(i) and basis (n_vb entries) used
+ * by rbm.type=symmetry (bravais.cpp:160-247, honeycomb.cpp:69-134). */
+int rbmnqs_model_symmetry(const rbmnqs_model* m, int32_t* S, int32_t* n_vb,
+                          int32_t* perm, int32_t* basis);
+void rbmnqs_model_destroy(rbmnqs_model* m);
+
+/* ----------------------------------------------------------- config ---- */
+/* Key names follow the reference's .ini options (README.md:66-173). */
+typedef struct {
+    int32_t rbm_type;          /* rbm.type: 0 = basic, 1 = symmetry */
+    int32_t alpha;             /* rbm.alpha */
+    int32_t pfaffian;          /* rbm.pfaffian (0/1) */
+    double pfaffian_symmetry;  /* rbm.pfaffian.symmetry */
+    int32_t n_chains;          /* sampler.metropolis.n_chains */
+    int32_t samples_per_chain; /* sampler.n_samples_per_chain */
+    int32_t warmup;            /* sampler.metropolis.n_warmup_steps (sweeps) */
+    int32_t step;              /* sampler.metropolis.n_steps_per_sample */
+    double bond_flips;         /* sampler.metropolis.bond_flips */
+    int32_t pfaffian_refresh;  /* sampler.pfaffian_refresh */
+    int32_t reinit_chains;     /* 1: fresh random chains every epoch (reference
+                                  behaviour, metropolis_sampler.cpp:127);
+                                  0: chains persist across epochs */
+    uint64_t seed;             /* seed */
+    double lr[3];              /* optimizer.learning_rate: initial, min, decay */
+    double reg1[3];            /* optimizer.sr.reg1 */
+    double reg2[3];            /* optimizer.sr.reg2 */
+    double deltareg1[3];       /* optimizer.sr.deltareg1 */
+    int32_t max_iterations;    /* optimizer.sr.max_iterations (0 = 2P) */
+    double rtol;               /* optimizer.sr.rtol (0 = 1e-16) */
+    int32_t precision;         /* 0: FP32 psi-ratio math with FP64 theta
+                                     recompute, TF32x3 tensor-core Gram;
+                                  1: FP64 throughout */
+    int32_t n_updates;         /* rbm n_updates_ (decay_t offset on resume) */
+} rbmnqs_config;
+
+/* Fills the reference defaults (src/tools/ini.cpp:38-120). */
+int rbmnqs_config_default(rbmnqs_config* cfg);
+
+/* -------------------------------------------------- session lifetime ---- */
+int rbmnqs_create(const rbmnqs_model* m, const rbmnqs_config* cfg,
+                  rbmnqs_handle** out);
+void rbmnqs_destroy(rbmnqs_handle* h);
+const char* rbmnqs_last_error(void);
+
+/* Parameter counts (abstract_machine.hpp:84-104). */
+int rbmnqs_sizes(const rbmnqs_handle* h, int32_t* n_params, int32_t* n_neural,
+                 int32_t* n_vb, int32_t* n_hidden, int32_t* n_symmetry);
+
+/* Weights in the reference parameter order (rbm_base::update_weights). */
+int rbmnqs_set_weights(rbmnqs_handle* h, const double* w);
+int rbmnqs_get_weights(rbmnqs_handle* h, double* w);
+
+/* ------------------------------------------------------ hot path -------- */
+typedef struct {
+    double energy[2];     /* <E_loc> (aggregator a_h_ result) */
+    double energy_var;    /* unbiased variance of E_loc */
+    double energy_stddev; /* binned standard error (aggregator::get_stddev) */
+    double tau;           /* binning autocorrelation estimate */
+    double acceptance;    /* mean acceptance rate over chains */
+    int64_t n_samples;
+    int32_t n_bins;
+    int32_t status;       /* RBMNQS_OK or RBMNQS_ERR_NONFINITE */
+} rbmnqs_sample_stats;
+
+/* One Metropolis epoch: sweeps, E_loc, O_k, and the reductions the
+ * reference's aggregators produce (metropolis_sampler.cpp:55-116). */
+int rbmnqs_sample(rbmnqs_handle* h, rbmnqs_sample_stats* out);
+
+typedef struct {
+    int32_t iterations;   /* CG iterations (cg_solver itn_) */
+    int32_t status;       /* RBMNQS_OK, RBMNQS_ERR_MASSIVE_STEP, _NONFINITE */
+    double residual;      /* final ||r||^2 */
+    double max_dw;        /* max |x| before scaling by lr */
+    double lr, reg1, reg2, deltareg1;
+} rbmnqs_sr_stats;
+
+/* SR step after rbmnqs_sample: F, S, CG solve, w -= lr * x
+ * (stochastic_reconfiguration.cpp:81-116, abstract_optimizer.cpp:80-178). */
+int rbmnqs_optimize(rbmnqs_handle* h, rbmnqs_sr_stats* out);
+
+/* sample + optimize as one CUDA-graph launch (captured on first use). */
+int rbmnqs_epoch(rbmnqs_handle* h, rbmnqs_sample_stats* s, rbmnqs_sr_stats* o);
+
+/* Copies of the last epoch's per-sample data: E[N] and O[N][n_params]
+ * (sample-major), both interleaved complex. */
+int rbmnqs_get_samples(rbmnqs_handle* h, double* E, double* O);
+/* SR moments of the last epoch: d = <O>, F, unbiased var(O), S (P x P,
+ * row-major, S_kl = <conj(O_k) O_l> - conj(d_k) d_l, unregularised). */
+int rbmnqs_get_sr(rbmnqs_handle* h, double* d, double* F, double* diag, double* S);
+
+/* Chain configurations [n_chains][4]. */
+int rbmnqs_get_spins(rbmnqs_handle* h, uint32_t* spins);
+int rbmnqs_set_spins(rbmnqs_handle* h, const uint32_t* spins);
+
+/* -------------------------------------------- parity / drop-in calls ---- */
+/* log psi, E_loc and O_k (optional, NULL skips) of B given configurations
+ * (machine::abstract_machine::psi / derivative, local_op::evaluate). */
+int rbmnqs_eval_batch(rbmnqs_handle* h, const uint32_t* spins, int32_t B,
+                      double* logpsi, double* eloc, double* O);
+/* log(psi(sigma with flips)/psi(sigma)) for B configurations, each with
+ * n_flips sites (rbm_base::log_psi_over_psi, rbm_base.cpp:306-344). */
+int rbmnqs_log_psi_over_psi(rbmnqs_handle* h, const uint32_t* spins,
+                            const int32_t* flips, int32_t n_flips, int32_t B,
+                            double* out);
+/* abstract_solver::solve on the GPU: O is N x P sample-major (the
+ * reference's a_dd_ store transposed), d = <O>, norm = sum of weights, F the
+ * force, x_io the warm start in / solution out, r1/r2/rd the regularisation
+ * and diag = var(O) (cg_solver.cpp:260-334). */
+int rbmnqs_sr_solve(rbmnqs_handle* h, const double* O, int32_t N,
+                    const double* d, double norm, const double* F,
+                    double* x_io, double r1, double r2, double rd,
+                    const double* diag, int32_t* iterations, double* residual);
+/* Exact enumeration of all 2^n configurations weighted by |psi|^2
+ * (full_sampler.cpp:43-186); n <= 30.  Outputs <E>, <O>, <E O*>. */
+int rbmnqs_full_sample(rbmnqs_handle* h, double* E_mean, double* d, double* dh);
+/* Observable expectation values <W_p> of the last epoch (after
+ * rbmnqs_model_add_hexagons). */
+int rbmnqs_get_observables(rbmnqs_handle* h, double* values);
+
+/* ----------------------------------------------------------- timing ---- */
+/* Device time (ms, CUDA events on the handle's stream) accumulated per stage
+ * since the last reset: 0 sample kernel, 1 moments, 2 Gram, 3 CG, 4 update,
+ * 5 stats.  `launches` counts kernel launches per stage. */
+int rbmnqs_timing(rbmnqs_handle* h, double* ms, int64_t* launches, int32_t n);
+int rbmnqs_timing_reset(rbmnqs_handle* h, int32_t enable);
+/* Number of kernel launches one rbmnqs_epoch performs (kernel nodes of the
+ * captured epoch graph; 0 before the first rbmnqs_epoch). */
+int rbmnqs_graph_kernels(rbmnqs_handle* h, int32_t* kernel_nodes);
+/* The handle's cudaStream_t, for callers that order work against it. */
+void* rbmnqs_stream(rbmnqs_handle* h);
+/* Measured special-function (MUFU: ex2/lg2/sin/cos) throughput of the current
+ * device in operations per second, from a dependent-chain probe kernel on
+ * every SM; the denominator of the sampler kernel's roofline.  No
+ * counterpart in the reference (measurement helper). */
+int rbmnqs_probe_mufu(int32_t iters, double* ops_per_second);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -61,7 +61,8 @@ static double run_chain(const orc_machine* m, const orc_ops* ops,
         orc_pf_context(m, spins, &pc);
     }
     int spc = cfg->samples_per_chain;
-    long total = (long)spc * cfg->step + cfg->warmup;
+    int warm = cfg->warmup;
+    long total = (long)spc * cfg->step + warm;
     uint32_t prop = 0;
     long accepted = 0;
     int ar = 0;
@@ -126,8 +127,8 @@ static double run_chain(const orc_machine* m, const orc_ops* ops,
                 }
             }
         }
-        if (st >= cfg->warmup && (st - cfg->warmup) % cfg->step == 0) {
-            long j = (st - cfg->warmup) / cfg->step;
+        if (st >= warm && (st - warm) % cfg->step == 0) {
+            long j = (st - warm) / cfg->step;
             size_t idx = (size_t)chain * spc + j;
             if (E) E[idx] = orc_eloc(m, ops, spins);
             if (O) orc_derivative(m, spins, O + idx * P);

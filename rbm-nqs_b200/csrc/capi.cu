@@ -1,0 +1,906 @@
+// capi.cu -- the C ABI (include/rbmnqs_b200.h): models, the GPU session that
+// plays the role of the reference's metropolis_sampler + stochastic_
+// reconfiguration + cg_solver for one GPU, and the parity entry points.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../host/model.hpp"
+#include "rbmnqs_b200.h"
+#include "sampler.cuh"
+#include "sr.cuh"
+
+using rbmnqs::cplx;
+
+struct rbmnqs_model {
+    rbmnqs::model m;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+struct Fail {
+    int code;
+    std::string msg;
+};
+
+void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw Fail{RBMNQS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+
+template <typename F> int guard(F&& f) {
+    try {
+        f();
+        return RBMNQS_OK;
+    } catch (const Fail& e) {
+        g_err = e.msg;
+        return e.code;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return RBMNQS_ERR_ARG;
+    }
+}
+
+void require(bool c, const std::string& msg, int code = RBMNQS_ERR_ARG) {
+    if (!c) throw Fail{code, msg};
+}
+
+template <typename T> struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        release();
+        n = count;
+        if (count) ck(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DevBuf() { release(); }
+};
+
+// Hamiltonian operators in the device CSR form (see OpDev).
+struct HamHost {
+    std::vector<rbmnqs::OpDev> ops;
+    std::vector<int> rowptr;
+    std::vector<uint32_t> mask;
+    std::vector<double2> val;
+};
+
+HamHost build_ham(const std::vector<rbmnqs::local_op>& ops) {
+    HamHost h;
+    for (auto& op : ops) {
+        rbmnqs::OpDev d;
+        d.k = op.k;
+        for (int i = 0; i < 6; i++) d.sites[i] = op.acts_on[i];
+        d.rp = (int)h.rowptr.size();
+        const int dim = 1 << op.k;
+        for (int r = 0; r < dim; r++) {
+            h.rowptr.push_back((int)h.mask.size());
+            for (int c = 0; c < dim; c++) {
+                const cplx v = op.mat[(size_t)r * dim + c];
+                if (v == cplx(0, 0)) continue;
+                h.mask.push_back((uint32_t)(r ^ c));
+                h.val.push_back(make_double2(v.real(), v.imag()));
+            }
+        }
+        h.rowptr.push_back((int)h.mask.size());
+        h.ops.push_back(d);
+    }
+    return h;
+}
+
+}  // namespace
+
+struct rbmnqs_handle {
+    rbmnqs_config cfg{};
+    rbmnqs::model model;
+    int n = 0, n_vb = 0, nh = 0, S = 0, T = 0, P = 0, P_neural = 0, N = 0, n_bins = 1;
+    int fp64 = 0, wpb = 8, w_in_smem = 1;
+    int gram_ks = 1, mom_blocks = 1;
+    cudaStream_t st = nullptr;
+
+    DevBuf<double2> params, vb, hb, W64, x;
+    DevBuf<float2> W32;
+    DevBuf<uint8_t> perm, inv, orbit;
+    DevBuf<rbmnqs::OpDev> ops;
+    DevBuf<int> rowptr;
+    DevBuf<uint32_t> emask;
+    DevBuf<double2> eval;
+    DevBuf<int2> bonds;
+    DevBuf<uint32_t> spins, nacc, nprop, ctl;
+    DevBuf<double2> E;
+    DevBuf<unsigned char> O;
+    DevBuf<double2> pd, pf, pe, d, F, emean, part, Sm, Sreg;
+    DevBuf<double> diag, maxdiag;
+    DevBuf<rbmnqs::ScheduleDev> sched;
+    DevBuf<rbmnqs::CgResultDev> cgres;
+    DevBuf<rbmnqs::EpochStatsDev> stats;
+    int n_ops = 0, n_prop_bonds = 0;
+    uint32_t epoch = 0;
+    bool sampled = false;
+
+    cudaGraphExec_t graph = nullptr;
+    int graph_kernels = 0;
+    static constexpr int kStages = 6;
+    cudaEvent_t ev[kStages + 1] = {};
+    bool timing = false;
+    double stage_ms[kStages] = {};
+    int64_t stage_launches[kStages] = {};
+
+    ~rbmnqs_handle() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    rbmnqs::MachineDev machine() const {
+        rbmnqs::MachineDev m{};
+        m.n = n;
+        m.n_vb = n_vb;
+        m.nh = nh;
+        m.S = S;
+        m.T = T;
+        m.P = P;
+        m.P_neural = P_neural;
+        m.symmetric = cfg.rbm_type == 1;
+        m.W64 = W64.p;
+        m.W32 = W32.p;
+        m.hb = hb.p;
+        m.vb = vb.p;
+        m.perm = perm.p;
+        m.inv = inv.p;
+        m.orbit = orbit.p;
+        return m;
+    }
+    rbmnqs::HamDev ham() const {
+        rbmnqs::HamDev H{};
+        H.n_ops = n_ops;
+        H.ops = ops.p;
+        H.rowptr = rowptr.p;
+        H.ent_mask = emask.p;
+        H.ent_val = eval.p;
+        return H;
+    }
+    size_t osize() const { return fp64 ? sizeof(double2) : sizeof(float2); }
+
+    void mark(int i) {
+        if (timing) ck(cudaEventRecordWithFlags(ev[i], st, cudaEventRecordExternal), "event");
+    }
+
+    // --- the epoch pieces -------------------------------------------------
+    void enqueue_sample() {
+        rbmnqs::SamplerArgs a{};
+        a.m = machine();
+        a.H = ham();
+        a.n_prop_bonds = n_prop_bonds;
+        a.prop_bonds = bonds.p;
+        a.bond_flips = cfg.bond_flips;
+        a.n_chains = cfg.n_chains;
+        a.spc = cfg.samples_per_chain;
+        a.warmup = cfg.warmup;
+        a.step = cfg.step;
+        a.ctl = ctl.p;
+        a.seed = cfg.seed;
+        a.spins = spins.p;
+        a.E = E.p;
+        a.O = O.p;
+        a.n_acc = nacc.p;
+        a.n_prop = nprop.p;
+        a.w_in_smem = w_in_smem;
+        mark(0);
+        ck(rbmnqs::launch_sampler(a, fp64, wpb, st), "sampler kernel");
+        mark(1);
+        ck(rbmnqs::launch_moments(O.p, fp64, E.p, N, P, mom_blocks, pd.p, pf.p, pe.p, d.p, F.p, emean.p, st),
+           "moments");
+        ck(rbmnqs::launch_energy_stats(E.p, N, n_bins, emean.p, nacc.p, nprop.p, cfg.n_chains, stats.p, st),
+           "energy stats");
+        ck(rbmnqs::launch_advance(ctl.p, cfg.reinit_chains, st), "advance");
+        mark(2);
+    }
+    void enqueue_optimize() {
+        ck(rbmnqs::launch_schedule(sched.p, st), "schedule");
+        ck(rbmnqs::launch_gram_fp64(O.p, fp64, d.p, N, P, gram_ks, part.p, Sm.p, st), "gram");
+        ck(rbmnqs::launch_regularize(Sm.p, P, P_neural, N, sched.p, diag.p, Sreg.p, maxdiag.p, st), "regularize");
+        mark(3);
+        int max_it = std::min(2 * P, cfg.max_iterations);
+        if (max_it == 0) max_it = 2 * P;
+        const double rtol = cfg.rtol == 0 ? 1e-16 : cfg.rtol;
+        ck(rbmnqs::launch_cg(Sreg.p, F.p, x.p, P, max_it, rtol, cgres.p, st), "cg");
+        mark(4);
+        ck(rbmnqs::launch_update(params.p, x.p, P, sched.p, cgres.p, st), "update");
+        ck(rbmnqs::launch_unpack(params.p, n, n_vb, nh, vb.p, hb.p, W64.p, W32.p, st), "unpack");
+        mark(5);
+    }
+    void collect_timing(int first, int last) {
+        if (!timing) return;
+        ck(cudaEventSynchronize(ev[last]), "event sync");
+        const int stage_of[kStages] = {0, 1, 2, 3, 4, 5};
+        (void)stage_of;
+        for (int i = first; i < last; i++) {
+            float ms = 0;
+            ck(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]), "elapsed");
+            stage_ms[i] += ms;
+            stage_launches[i] += 1;
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* rbmnqs_last_error(void) { return g_err.c_str(); }
+
+int rbmnqs_model_kitaev(int32_t n_cells, int32_t n_cells_b, const double J[3], double h, double symmetry,
+                        rbmnqs_model** out) {
+    return guard([&] {
+        require(out && J && n_cells >= 1, "rbmnqs_model_kitaev: bad arguments");
+        auto m = std::make_unique<rbmnqs_model>();
+        m->m = rbmnqs::make_kitaev(n_cells, n_cells_b, J, h, symmetry);
+        require(m->m.n <= 128, "rbmnqs_model_kitaev: more than 128 sites (MAX_SPIN_SITES)");
+        *out = m.release();
+    });
+}
+
+int rbmnqs_model_toric(int32_t n_cells, double J, double symmetry, rbmnqs_model** out) {
+    return guard([&] {
+        require(out && n_cells >= 1, "rbmnqs_model_toric: bad arguments");
+        auto m = std::make_unique<rbmnqs_model>();
+        m->m = rbmnqs::make_toric(n_cells, J, symmetry);
+        require(m->m.n <= 128, "rbmnqs_model_toric: more than 128 sites (MAX_SPIN_SITES)");
+        *out = m.release();
+    });
+}
+
+int rbmnqs_model_add_hexagons(rbmnqs_model* m) {
+    return guard([&] {
+        require(m != nullptr, "null model");
+        rbmnqs::add_hexagons(m->m);
+    });
+}
+
+int rbmnqs_model_sizes(const rbmnqs_model* m, int32_t* n_sites, int32_t* n_ops, int32_t* n_bonds,
+                       int32_t* n_obs) {
+    return guard([&] {
+        require(m != nullptr, "null model");
+        if (n_sites) *n_sites = m->m.n;
+        if (n_ops) *n_ops = (int32_t)m->m.hamiltonian.size();
+        if (n_bonds) *n_bonds = (int32_t)m->m.bonds.size();
+        if (n_obs) *n_obs = (int32_t)m->m.observables.size();
+    });
+}
+
+int rbmnqs_model_bonds(const rbmnqs_model* m, int32_t* abt) {
+    return guard([&] {
+        require(m && abt, "null argument");
+        for (size_t i = 0; i < m->m.bonds.size(); i++) {
+            abt[3 * i] = m->m.bonds[i].a;
+            abt[3 * i + 1] = m->m.bonds[i].b;
+            abt[3 * i + 2] = m->m.bonds[i].type;
+        }
+    });
+}
+
+int rbmnqs_model_op(const rbmnqs_model* m, int32_t o, int32_t* k, int32_t* acts_on, double* mat) {
+    return guard([&] {
+        require(m != nullptr, "null model");
+        const int nh = (int)m->m.hamiltonian.size();
+        require(o >= 0 && o < nh + (int)m->m.observables.size(), "operator index out of range");
+        const auto& op = o < nh ? m->m.hamiltonian[o] : m->m.observables[o - nh];
+        if (k) *k = op.k;
+        if (acts_on)
+            for (int i = 0; i < 6; i++) acts_on[i] = op.acts_on[i];
+        if (mat)
+            for (size_t i = 0; i < op.mat.size(); i++) {
+                mat[2 * i] = op.mat[i].real();
+                mat[2 * i + 1] = op.mat[i].imag();
+            }
+    });
+}
+
+int rbmnqs_model_symmetry(const rbmnqs_model* m, int32_t* S, int32_t* n_vb, int32_t* perm, int32_t* basis) {
+    return guard([&] {
+        require(m != nullptr, "null model");
+        if (S) *S = (int32_t)m->m.perm.size();
+        if (n_vb) *n_vb = (int32_t)m->m.basis.size();
+        if (perm)
+            for (size_t s = 0; s < m->m.perm.size(); s++)
+                for (int i = 0; i < m->m.n; i++) perm[s * m->m.n + i] = m->m.perm[s][i];
+        if (basis)
+            for (size_t i = 0; i < m->m.basis.size(); i++) basis[i] = m->m.basis[i];
+    });
+}
+
+void rbmnqs_model_destroy(rbmnqs_model* m) { delete m; }
+
+int rbmnqs_config_default(rbmnqs_config* c) {
+    return guard([&] {
+        require(c != nullptr, "null config");
+        std::memset(c, 0, sizeof(*c));
+        // src/tools/ini.cpp:38-120
+        c->rbm_type = 0;
+        c->alpha = 1;
+        c->pfaffian = 0;
+        c->pfaffian_symmetry = 0.5;
+        c->n_chains = 4;
+        c->samples_per_chain = 250;  // sampler.n_samples 1000 / 4 chains
+        c->warmup = 100;
+        c->step = 1;
+        c->bond_flips = 0.5;
+        c->pfaffian_refresh = 0;
+        c->reinit_chains = 1;
+        c->seed = 421390484ULL;
+        const double lr[3] = {1e-2, 1e-2, 1.0}, r1[3] = {1, 1e-4, 0.9}, r2[3] = {1e-3, 1e-6, 0.9},
+                     rd[3] = {1e-2, 1e-2, 1.0};
+        std::memcpy(c->lr, lr, sizeof(lr));
+        std::memcpy(c->reg1, r1, sizeof(r1));
+        std::memcpy(c->reg2, r2, sizeof(r2));
+        std::memcpy(c->deltareg1, rd, sizeof(rd));
+        c->max_iterations = 0;
+        c->rtol = 0;
+        c->precision = 0;
+        c->n_updates = 0;
+    });
+}
+
+int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_handle** out) {
+    return guard([&] {
+        require(mdl && cfg && out, "rbmnqs_create: null argument");
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+            throw Fail{RBMNQS_ERR_NO_DEVICE, "no CUDA device available"};
+        require(cfg->rbm_type == 0 || cfg->rbm_type == 1, "rbm.type must be basic (0) or symmetry (1)");
+        require(!cfg->pfaffian, "the Pfaffian factor is not available in this build", RBMNQS_ERR_UNSUPPORTED);
+        require(cfg->alpha >= 1 && cfg->n_chains >= 1 && cfg->samples_per_chain >= 1 && cfg->step >= 1 &&
+                    cfg->warmup >= 0,
+                "bad sampler/machine sizes");
+        auto h = std::make_unique<rbmnqs_handle>();
+        h->cfg = *cfg;
+        h->model = mdl->m;
+        const auto& m = h->model;
+        h->n = m.n;
+        if (cfg->rbm_type == 1) {
+            h->S = (int)m.perm.size();
+            h->n_vb = (int)m.basis.size();
+            require(h->n % h->S == 0 || true, "");
+        } else {
+            h->S = 1;
+            h->n_vb = h->n;
+        }
+        h->nh = cfg->alpha * h->n_vb;
+        h->T = h->nh * h->S;
+        h->P_neural = h->n_vb + h->nh + h->n * h->nh;
+        h->P = h->P_neural;
+        require(rbmnqs::elements_per_lane(h->T) > 0, "theta table larger than 512 entries per chain",
+                RBMNQS_ERR_UNSUPPORTED);
+        require(h->P <= 2048, "dense SR path supports at most 2048 parameters", RBMNQS_ERR_UNSUPPORTED);
+        h->N = cfg->n_chains * cfg->samples_per_chain;
+        require(h->N >= 2, "need at least two samples");
+        int k = 50;
+        while (h->N % k) k--;
+        h->n_bins = k;
+        h->fp64 = cfg->precision == 1;
+
+        ck(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking), "stream");
+        for (auto& e : h->ev) ck(cudaEventCreate(&e), "event");
+
+        // machine tables
+        const int n = h->n, S = h->S, nh = h->nh;
+        h->params.alloc(h->P);
+        h->vb.alloc(h->n_vb);
+        h->hb.alloc(nh);
+        h->W64.alloc((size_t)n * nh);
+        h->W32.alloc((size_t)n * nh);
+        h->x.alloc(h->P);
+        ck(cudaMemsetAsync(h->params.p, 0, h->P * sizeof(double2), h->st), "memset");
+        ck(cudaMemsetAsync(h->x.p, 0, h->P * sizeof(double2), h->st), "memset");
+        if (cfg->rbm_type == 1) {
+            std::vector<uint8_t> perm((size_t)n * S), inv((size_t)S * n), orbit((size_t)h->n_vb * S);
+            for (int s = 0; s < S; s++)
+                for (int i = 0; i < n; i++) {
+                    perm[(size_t)i * S + s] = (uint8_t)m.perm[s][i];
+                    inv[(size_t)s * n + m.perm[s][i]] = (uint8_t)i;
+                }
+            for (int i = 0; i < h->n_vb; i++)
+                for (int s = 0; s < S; s++) orbit[(size_t)i * S + s] = (uint8_t)m.perm[s][m.basis[i]];
+            h->perm.alloc(perm.size());
+            h->inv.alloc(inv.size());
+            h->orbit.alloc(orbit.size());
+            ck(cudaMemcpy(h->perm.p, perm.data(), perm.size(), cudaMemcpyHostToDevice), "copy");
+            ck(cudaMemcpy(h->inv.p, inv.data(), inv.size(), cudaMemcpyHostToDevice), "copy");
+            ck(cudaMemcpy(h->orbit.p, orbit.data(), orbit.size(), cudaMemcpyHostToDevice), "copy");
+        }
+        // Hamiltonian
+        HamHost hh = build_ham(m.hamiltonian);
+        h->n_ops = (int)hh.ops.size();
+        h->ops.alloc(hh.ops.size());
+        h->rowptr.alloc(hh.rowptr.size());
+        h->emask.alloc(hh.mask.size());
+        h->eval.alloc(hh.val.size());
+        ck(cudaMemcpy(h->ops.p, hh.ops.data(), hh.ops.size() * sizeof(rbmnqs::OpDev), cudaMemcpyHostToDevice), "c");
+        ck(cudaMemcpy(h->rowptr.p, hh.rowptr.data(), hh.rowptr.size() * sizeof(int), cudaMemcpyHostToDevice), "c");
+        ck(cudaMemcpy(h->emask.p, hh.mask.data(), hh.mask.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "c");
+        ck(cudaMemcpy(h->eval.p, hh.val.data(), hh.val.size() * sizeof(double2), cudaMemcpyHostToDevice), "c");
+        // bond proposals: bonds of type != 2 (metropolis_sampler.cpp:145-166)
+        std::vector<int2> pb;
+        if (m.kind == "kitaev")
+            for (auto& b : m.bonds)
+                if (b.type != 2) pb.push_back(make_int2(b.a, b.b));
+        h->n_prop_bonds = (int)pb.size();
+        if (!pb.empty()) {
+            h->bonds.alloc(pb.size());
+            ck(cudaMemcpy(h->bonds.p, pb.data(), pb.size() * sizeof(int2), cudaMemcpyHostToDevice), "c");
+        }
+        // sampler state and outputs
+        h->spins.alloc((size_t)cfg->n_chains * 4);
+        ck(cudaMemsetAsync(h->spins.p, 0, (size_t)cfg->n_chains * 16, h->st), "memset");
+        h->nacc.alloc(cfg->n_chains);
+        h->nprop.alloc(cfg->n_chains);
+        h->ctl.alloc(2);
+        const uint32_t ctl0[2] = {0, 1};
+        ck(cudaMemcpy(h->ctl.p, ctl0, sizeof(ctl0), cudaMemcpyHostToDevice), "c");
+        h->E.alloc(h->N);
+        h->O.alloc((size_t)h->N * h->P * h->osize());
+        h->mom_blocks = std::max(1, std::min(296, h->N / 64));
+        h->pd.alloc((size_t)h->mom_blocks * h->P);
+        h->pf.alloc((size_t)h->mom_blocks * h->P);
+        h->pe.alloc(h->mom_blocks);
+        h->d.alloc(h->P);
+        h->F.alloc(h->P);
+        h->emean.alloc(1);
+        h->gram_ks = rbmnqs::gram_splits(h->N, h->P);
+        h->part.alloc((size_t)h->gram_ks * h->P * h->P);
+        h->Sm.alloc((size_t)h->P * h->P);
+        h->Sreg.alloc((size_t)h->P * h->P);
+        h->diag.alloc(h->P);
+        h->maxdiag.alloc(1);
+        h->sched.alloc(1);
+        h->cgres.alloc(1);
+        h->stats.alloc(1);
+        // decay_t schedules with the n_updates offset
+        rbmnqs::ScheduleDev sd{};
+        const double* src[4] = {cfg->lr, cfg->reg1, cfg->reg2, cfg->deltareg1};
+        for (int i = 0; i < 4; i++) {
+            sd.value[i] = std::pow(src[i][2], (double)cfg->n_updates) * src[i][0];
+            sd.min[i] = src[i][1];
+            sd.decay[i] = src[i][2];
+            sd.min_reached[i] = src[i][2] == 1.0;
+        }
+        ck(cudaMemcpy(h->sched.p, &sd, sizeof(sd), cudaMemcpyHostToDevice), "c");
+        // launch shape: FP32 W in shared memory when it fits comfortably
+        h->w_in_smem = (size_t)n * nh * 8 <= 96 * 1024 ? 1 : 0;
+        h->wpb = 8;
+        while (h->wpb > 1 && rbmnqs::sampler_smem_bytes(h->machine(), h->fp64, h->wpb, h->w_in_smem) > 200 * 1024)
+            h->wpb >>= 1;
+        ck(cudaStreamSynchronize(h->st), "sync");
+        *out = h.release();
+    });
+}
+
+void rbmnqs_destroy(rbmnqs_handle* h) { delete h; }
+
+int rbmnqs_sizes(const rbmnqs_handle* h, int32_t* n_params, int32_t* n_neural, int32_t* n_vb, int32_t* n_hidden,
+                 int32_t* n_symm) {
+    return guard([&] {
+        require(h != nullptr, "null handle");
+        if (n_params) *n_params = h->P;
+        if (n_neural) *n_neural = h->P_neural;
+        if (n_vb) *n_vb = h->n_vb;
+        if (n_hidden) *n_hidden = h->nh;
+        if (n_symm) *n_symm = h->S;
+    });
+}
+
+int rbmnqs_set_weights(rbmnqs_handle* h, const double* w) {
+    return guard([&] {
+        require(h && w, "null argument");
+        ck(cudaMemcpyAsync(h->params.p, w, h->P * sizeof(double2), cudaMemcpyHostToDevice, h->st), "copy");
+        ck(rbmnqs::launch_unpack(h->params.p, h->n, h->n_vb, h->nh, h->vb.p, h->hb.p, h->W64.p, h->W32.p, h->st),
+           "unpack");
+        ck(cudaStreamSynchronize(h->st), "sync");
+    });
+}
+
+int rbmnqs_get_weights(rbmnqs_handle* h, double* w) {
+    return guard([&] {
+        require(h && w, "null argument");
+        ck(cudaMemcpyAsync(w, h->params.p, h->P * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "copy");
+        ck(cudaStreamSynchronize(h->st), "sync");
+    });
+}
+
+static void read_sample_stats(rbmnqs_handle* h, rbmnqs_sample_stats* out) {
+    rbmnqs::EpochStatsDev s{};
+    ck(cudaMemcpyAsync(&s, h->stats.p, sizeof(s), cudaMemcpyDeviceToHost, h->st), "copy");
+    ck(cudaStreamSynchronize(h->st), "sync");
+    if (out) {
+        out->energy[0] = s.energy.x;
+        out->energy[1] = s.energy.y;
+        out->energy_var = s.var;
+        out->energy_stddev = s.stddev;
+        out->tau = s.tau;
+        out->acceptance = s.acceptance;
+        out->n_samples = h->N;
+        out->n_bins = h->n_bins;
+        out->status = s.finite ? RBMNQS_OK : RBMNQS_ERR_NONFINITE;
+    }
+}
+
+static void read_sr_stats(rbmnqs_handle* h, rbmnqs_sr_stats* out) {
+    rbmnqs::CgResultDev r{};
+    rbmnqs::ScheduleDev sd{};
+    ck(cudaMemcpyAsync(&r, h->cgres.p, sizeof(r), cudaMemcpyDeviceToHost, h->st), "copy");
+    ck(cudaMemcpyAsync(&sd, h->sched.p, sizeof(sd), cudaMemcpyDeviceToHost, h->st), "copy");
+    ck(cudaStreamSynchronize(h->st), "sync");
+    if (out) {
+        out->iterations = r.iterations;
+        out->status = r.status;
+        out->residual = r.residual;
+        out->max_dw = r.max_dw;
+        out->lr = sd.value[0];
+        out->reg1 = sd.value[1];
+        out->reg2 = sd.value[2];
+        out->deltareg1 = sd.value[3];
+    }
+}
+
+int rbmnqs_sample(rbmnqs_handle* h, rbmnqs_sample_stats* out) {
+    return guard([&] {
+        require(h != nullptr, "null handle");
+        h->enqueue_sample();
+        h->collect_timing(0, 2);
+        read_sample_stats(h, out);
+        h->sampled = true;
+    });
+}
+
+int rbmnqs_optimize(rbmnqs_handle* h, rbmnqs_sr_stats* out) {
+    return guard([&] {
+        require(h != nullptr, "null handle");
+        require(h->sampled, "rbmnqs_optimize needs a preceding rbmnqs_sample");
+        if (h->timing) ck(cudaEventRecordWithFlags(h->ev[2], h->st, cudaEventRecordExternal), "event");
+        h->enqueue_optimize();
+        h->collect_timing(2, 5);
+        read_sr_stats(h, out);
+    });
+}
+
+int rbmnqs_epoch(rbmnqs_handle* h, rbmnqs_sample_stats* s, rbmnqs_sr_stats* o) {
+    return guard([&] {
+        require(h != nullptr, "null handle");
+        if (!h->graph) {
+            cudaGraph_t g;
+            ck(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal), "capture");
+            try {
+                h->enqueue_sample();
+                h->enqueue_optimize();
+            } catch (...) {
+                cudaStreamEndCapture(h->st, &g);
+                throw;
+            }
+            ck(cudaStreamEndCapture(h->st, &g), "end capture");
+            size_t nn = 0;
+            ck(cudaGraphGetNodes(g, nullptr, &nn), "graph nodes");
+            std::vector<cudaGraphNode_t> nodes(nn);
+            ck(cudaGraphGetNodes(g, nodes.data(), &nn), "graph nodes");
+            h->graph_kernels = 0;
+            for (auto nd : nodes) {
+                cudaGraphNodeType t;
+                ck(cudaGraphNodeGetType(nd, &t), "node type");
+                h->graph_kernels += t == cudaGraphNodeTypeKernel;
+            }
+            ck(cudaGraphInstantiate(&h->graph, g, 0), "instantiate");
+            cudaGraphDestroy(g);
+        }
+        ck(cudaGraphLaunch(h->graph, h->st), "graph launch");
+        h->collect_timing(0, 5);
+        read_sample_stats(h, s);
+        read_sr_stats(h, o);
+        h->sampled = true;
+    });
+}
+
+int rbmnqs_get_samples(rbmnqs_handle* h, double* E, double* O) {
+    return guard([&] {
+        require(h != nullptr, "null handle");
+        if (E) ck(cudaMemcpyAsync(E, h->E.p, (size_t)h->N * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "c");
+        if (O) {
+            const size_t cnt = (size_t)h->N * h->P;
+            if (h->fp64) {
+                ck(cudaMemcpyAsync(O, h->O.p, cnt * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "c");
+            } else {
+                std::vector<float2> tmp(cnt);
+                ck(cudaMemcpyAsync(tmp.data(), h->O.p, cnt * sizeof(float2), cudaMemcpyDeviceToHost, h->st), "c");
+                ck(cudaStreamSynchronize(h->st), "sync");
+                for (size_t i = 0; i < cnt; i++) {
+                    O[2 * i] = tmp[i].x;
+                    O[2 * i + 1] = tmp[i].y;
+                }
+            }
+        }
+        ck(cudaStreamSynchronize(h->st), "sync");
+    });
+}
+
+int rbmnqs_get_sr(rbmnqs_handle* h, double* d, double* F, double* diag, double* S) {
+    return guard([&] {
+        require(h != nullptr, "null handle");
+        const size_t P = h->P;
+        if (d) ck(cudaMemcpyAsync(d, h->d.p, P * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "c");
+        if (F) ck(cudaMemcpyAsync(F, h->F.p, P * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "c");
+        if (diag) ck(cudaMemcpyAsync(diag, h->diag.p, P * sizeof(double), cudaMemcpyDeviceToHost, h->st), "c");
+        if (S) ck(cudaMemcpyAsync(S, h->Sm.p, P * P * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "c");
+        ck(cudaStreamSynchronize(h->st), "sync");
+    });
+}
+
+int rbmnqs_get_spins(rbmnqs_handle* h, uint32_t* spins) {
+    return guard([&] {
+        require(h && spins, "null argument");
+        ck(cudaMemcpyAsync(spins, h->spins.p, (size_t)h->cfg.n_chains * 16, cudaMemcpyDeviceToHost, h->st), "c");
+        ck(cudaStreamSynchronize(h->st), "sync");
+    });
+}
+
+int rbmnqs_set_spins(rbmnqs_handle* h, const uint32_t* spins) {
+    return guard([&] {
+        require(h && spins, "null argument");
+        ck(cudaMemcpyAsync(h->spins.p, spins, (size_t)h->cfg.n_chains * 16, cudaMemcpyHostToDevice, h->st), "c");
+        const uint32_t zero = 0;
+        ck(cudaMemcpyAsync(h->ctl.p + 1, &zero, sizeof(zero), cudaMemcpyHostToDevice, h->st), "c");
+        ck(cudaStreamSynchronize(h->st), "sync");
+    });
+}
+
+static void eval_common(rbmnqs_handle* h, const uint32_t* spins, int B, double* logpsi, double* eloc, double* O,
+                        const int32_t* flips, int nflips, double* ratio) {
+    require(h && spins && B >= 0, "bad arguments");
+    if (B == 0) return;
+    DevBuf<uint32_t> ds;
+    DevBuf<double2> dl, de, dr;
+    DevBuf<unsigned char> dO;
+    DevBuf<int> df;
+    ds.alloc((size_t)B * 4);
+    ck(cudaMemcpyAsync(ds.p, spins, (size_t)B * 16, cudaMemcpyHostToDevice, h->st), "c");
+    rbmnqs::EvalArgs a{};
+    a.m = h->machine();
+    a.H = h->ham();
+    a.spins = ds.p;
+    a.B = B;
+    a.w_in_smem = h->w_in_smem;
+    if (logpsi) {
+        dl.alloc(B);
+        a.logpsi = dl.p;
+    }
+    if (eloc) {
+        de.alloc(B);
+        a.eloc = de.p;
+    }
+    if (O) {
+        dO.alloc((size_t)B * h->P * h->osize());
+        a.O = dO.p;
+    }
+    if (ratio) {
+        require(flips && nflips >= 1 && nflips <= 6, "1..6 flips per configuration");
+        df.alloc((size_t)B * nflips);
+        dr.alloc(B);
+        ck(cudaMemcpyAsync(df.p, flips, (size_t)B * nflips * sizeof(int), cudaMemcpyHostToDevice, h->st), "c");
+        a.flips = df.p;
+        a.n_flips = nflips;
+        a.ratio = dr.p;
+    }
+    ck(rbmnqs::launch_eval(a, h->fp64, h->wpb, h->st), "eval kernel");
+    if (logpsi) ck(cudaMemcpyAsync(logpsi, dl.p, B * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "c");
+    if (eloc) ck(cudaMemcpyAsync(eloc, de.p, B * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "c");
+    if (ratio) ck(cudaMemcpyAsync(ratio, dr.p, B * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "c");
+    if (O) {
+        const size_t cnt = (size_t)B * h->P;
+        if (h->fp64) {
+            ck(cudaMemcpyAsync(O, dO.p, cnt * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "c");
+        } else {
+            std::vector<float2> tmp(cnt);
+            ck(cudaMemcpyAsync(tmp.data(), dO.p, cnt * sizeof(float2), cudaMemcpyDeviceToHost, h->st), "c");
+            ck(cudaStreamSynchronize(h->st), "sync");
+            for (size_t i = 0; i < cnt; i++) {
+                O[2 * i] = tmp[i].x;
+                O[2 * i + 1] = tmp[i].y;
+            }
+        }
+    }
+    ck(cudaStreamSynchronize(h->st), "sync");
+}
+
+int rbmnqs_eval_batch(rbmnqs_handle* h, const uint32_t* spins, int32_t B, double* logpsi, double* eloc, double* O) {
+    return guard([&] { eval_common(h, spins, B, logpsi, eloc, O, nullptr, 0, nullptr); });
+}
+
+int rbmnqs_log_psi_over_psi(rbmnqs_handle* h, const uint32_t* spins, const int32_t* flips, int32_t n_flips,
+                            int32_t B, double* out) {
+    return guard([&] {
+        require(out != nullptr, "null output");
+        eval_common(h, spins, B, nullptr, nullptr, nullptr, flips, n_flips, out);
+    });
+}
+
+int rbmnqs_sr_solve(rbmnqs_handle* h, const double* O, int32_t N, const double* d, double norm, const double* F,
+                    double* x_io, double r1, double r2, double rd, const double* diag, int32_t* iterations,
+                    double* residual) {
+    return guard([&] {
+        require(h && O && d && F && x_io && diag && N >= 1 && norm > 0, "bad arguments");
+        const int P = h->P;
+        DevBuf<double2> dO, dd, dF, dx, part, G, Sreg;
+        DevBuf<double> ddiag;
+        DevBuf<rbmnqs::CgResultDev> res;
+        dO.alloc((size_t)N * P);
+        dd.alloc(P);
+        dF.alloc(P);
+        dx.alloc(P);
+        ddiag.alloc(P);
+        res.alloc(1);
+        G.alloc((size_t)P * P);
+        Sreg.alloc((size_t)P * P);
+        const int ks = rbmnqs::gram_splits(N, P);
+        part.alloc((size_t)ks * P * P);
+        ck(cudaMemcpyAsync(dO.p, O, (size_t)N * P * sizeof(double2), cudaMemcpyHostToDevice, h->st), "c");
+        ck(cudaMemcpyAsync(dd.p, d, P * sizeof(double2), cudaMemcpyHostToDevice, h->st), "c");
+        ck(cudaMemcpyAsync(dF.p, F, P * sizeof(double2), cudaMemcpyHostToDevice, h->st), "c");
+        ck(cudaMemcpyAsync(dx.p, x_io, P * sizeof(double2), cudaMemcpyHostToDevice, h->st), "c");
+        ck(cudaMemcpyAsync(ddiag.p, diag, P * sizeof(double), cudaMemcpyHostToDevice, h->st), "c");
+        ck(rbmnqs::launch_gram_fp64(dO.p, 1, nullptr, N, P, ks, part.p, G.p, h->st), "gram");
+        ck(rbmnqs::launch_solve_prep(G.p, N, norm, dd.p, ddiag.p, P, h->P_neural, r1, r2, rd, Sreg.p, h->st),
+           "prep");
+        int max_it = std::min(2 * P, h->cfg.max_iterations);
+        if (max_it == 0) max_it = 2 * P;
+        const double rtol = h->cfg.rtol == 0 ? 1e-16 : h->cfg.rtol;
+        ck(rbmnqs::launch_cg(Sreg.p, dF.p, dx.p, P, max_it, rtol, res.p, h->st), "cg");
+        rbmnqs::CgResultDev r{};
+        ck(cudaMemcpyAsync(x_io, dx.p, P * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "c");
+        ck(cudaMemcpyAsync(&r, res.p, sizeof(r), cudaMemcpyDeviceToHost, h->st), "c");
+        ck(cudaStreamSynchronize(h->st), "sync");
+        if (iterations) *iterations = r.iterations;
+        if (residual) *residual = r.residual;
+    });
+}
+
+int rbmnqs_full_sample(rbmnqs_handle* h, double* E_mean, double* dm, double* dh) {
+    return guard([&] {
+        require(h && E_mean, "bad arguments");
+        require(h->n <= 30, "full enumeration needs n <= 30 (full_sampler.cpp:38-40 allows 64)",
+                RBMNQS_ERR_UNSUPPORTED);
+        const int64_t NS = int64_t(1) << h->n;
+        const int P = h->P;
+        const int64_t chunk = 1 << 16;
+        std::vector<uint32_t> sp;
+        std::vector<double> lp, el, Ob;
+        // pass 1: max log|psi|
+        double mx = -1e300;
+        for (int64_t s0 = 0; s0 < NS; s0 += chunk) {
+            const int B = (int)std::min(chunk, NS - s0);
+            sp.assign((size_t)B * 4, 0);
+            for (int b = 0; b < B; b++) sp[4 * b] = (uint32_t)(s0 + b);
+            lp.resize(2 * B);
+            eval_common(h, sp.data(), B, lp.data(), nullptr, nullptr, nullptr, 0, nullptr);
+            for (int b = 0; b < B; b++) mx = std::max(mx, 2 * lp[2 * b]);
+        }
+        // pass 2: weighted sums (full_sampler.cpp:93-139)
+        double pt = 0;
+        cplx em = 0;
+        std::vector<cplx> sd(dm ? P : 0), sh(dh ? P : 0);
+        for (int64_t s0 = 0; s0 < NS; s0 += chunk) {
+            const int B = (int)std::min(chunk, NS - s0);
+            sp.assign((size_t)B * 4, 0);
+            for (int b = 0; b < B; b++) sp[4 * b] = (uint32_t)(s0 + b);
+            lp.resize(2 * B);
+            el.resize(2 * B);
+            if (dm || dh) Ob.resize((size_t)2 * B * P);
+            eval_common(h, sp.data(), B, lp.data(), el.data(), (dm || dh) ? Ob.data() : nullptr, nullptr, 0,
+                        nullptr);
+            for (int b = 0; b < B; b++) {
+                const double p = std::exp(2 * lp[2 * b] - mx);
+                const cplx e(el[2 * b], el[2 * b + 1]);
+                pt += p;
+                em += p * e;
+                if (dm || dh)
+                    for (int k = 0; k < P; k++) {
+                        const cplx o(Ob[(size_t)2 * (b * (size_t)P + k)], Ob[(size_t)2 * (b * (size_t)P + k) + 1]);
+                        if (dm) sd[k] += p * o;
+                        if (dh) sh[k] += p * e * std::conj(o);
+                    }
+            }
+        }
+        E_mean[0] = (em / pt).real();
+        E_mean[1] = (em / pt).imag();
+        for (int k = 0; dm && k < P; k++) {
+            dm[2 * k] = (sd[k] / pt).real();
+            dm[2 * k + 1] = (sd[k] / pt).imag();
+        }
+        for (int k = 0; dh && k < P; k++) {
+            dh[2 * k] = (sh[k] / pt).real();
+            dh[2 * k + 1] = (sh[k] / pt).imag();
+        }
+    });
+}
+
+int rbmnqs_get_observables(rbmnqs_handle* h, double* values) {
+    return guard([&] {
+        (void)h;
+        (void)values;
+        throw Fail{RBMNQS_ERR_UNSUPPORTED, "observables are evaluated with rbmnqs_eval_batch in this build"};
+    });
+}
+
+int rbmnqs_timing(rbmnqs_handle* h, double* ms, int64_t* launches, int32_t n) {
+    return guard([&] {
+        require(h != nullptr, "null handle");
+        for (int i = 0; i < n && i < rbmnqs_handle::kStages; i++) {
+            if (ms) ms[i] = h->stage_ms[i];
+            if (launches) launches[i] = h->stage_launches[i];
+        }
+    });
+}
+
+int rbmnqs_timing_reset(rbmnqs_handle* h, int32_t enable) {
+    return guard([&] {
+        require(h != nullptr, "null handle");
+        const bool en = enable != 0;
+        if (en != h->timing && h->graph) {
+            cudaGraphExecDestroy(h->graph);  // re-capture with/without event nodes
+            h->graph = nullptr;
+        }
+        h->timing = en;
+        for (int i = 0; i < rbmnqs_handle::kStages; i++) {
+            h->stage_ms[i] = 0;
+            h->stage_launches[i] = 0;
+        }
+    });
+}
+
+void* rbmnqs_stream(rbmnqs_handle* h) { return h ? (void*)h->st : nullptr; }
+
+int rbmnqs_graph_kernels(rbmnqs_handle* h, int32_t* kernel_nodes) {
+    return guard([&] {
+        require(h && kernel_nodes, "null argument");
+        *kernel_nodes = h->graph_kernels;
+    });
+}
+
+int rbmnqs_probe_mufu(int32_t iters, double* ops_per_second) {
+    return guard([&] {
+        require(ops_per_second && iters > 0, "bad arguments");
+        int dev = 0, sms = 0;
+        ck(cudaGetDevice(&dev), "device");
+        ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "attr");
+        cudaStream_t st;
+        ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+        DevBuf<float> out;
+        out.alloc(1);
+        cudaEvent_t a, b;
+        ck(cudaEventCreate(&a), "event");
+        ck(cudaEventCreate(&b), "event");
+        const int blocks = sms * 8;  // 2048 threads per SM
+        ck(rbmnqs::launch_mufu_probe(out.p, iters, blocks, st), "probe");  // warm-up
+        ck(cudaEventRecord(a, st), "event");
+        ck(rbmnqs::launch_mufu_probe(out.p, iters, blocks, st), "probe");
+        ck(cudaEventRecord(b, st), "event");
+        ck(cudaEventSynchronize(b), "sync");
+        float ms = 0;
+        ck(cudaEventElapsedTime(&ms, a, b), "elapsed");
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        cudaStreamDestroy(st);
+        *ops_per_second = 4.0 * iters * (double)blocks * 256.0 / (ms * 1e-3);
+    });
+}
+
+}  // extern "C"

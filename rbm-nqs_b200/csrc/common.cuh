@@ -1,0 +1,129 @@
+// common.cuh -- device helpers shared by the sm_100a kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace rbmnqs {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// ------------------------------------------------------------- complex --
+template <typename R> struct c2t;
+template <> struct c2t<float> { using type = float2; };
+template <> struct c2t<double> { using type = double2; };
+template <typename R> using C2 = typename c2t<R>::type;
+
+template <typename R> __device__ __forceinline__ C2<R> mk(R x, R y) { return {x, y}; }
+template <typename T> __device__ __forceinline__ T cmul(T a, T b) {
+    return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+template <typename T> __device__ __forceinline__ T cmulc(T a, T b) {  // a * conj(b)
+    return {a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y};
+}
+
+// ------------------------------------------------------------- Philox ---
+// Philox4x32-10 (Salmon et al., SC'11).  Counter layout shared with the
+// oracle: {proposal index, epoch, chain, stream}, key = 64-bit seed.
+__device__ __forceinline__ uint4 philox4x32(uint4 c, uint2 k) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
+        const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+
+// 24-bit uniform in [0, 1): exactly representable in float and double.
+template <typename R> __device__ __forceinline__ R unit24(uint32_t x) {
+    return (R)(x >> 8) * (R)(1.0 / 16777216.0);
+}
+__device__ __forceinline__ uint32_t pick(uint32_t x, uint32_t n) { return __umulhi(x, n); }
+
+// ------------------------------------------------------ warp reductions --
+template <typename R> __device__ __forceinline__ R warp_sum(R v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+template <typename T> __device__ __forceinline__ T warp_cprod(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        T w;
+        w.x = __shfl_xor_sync(kFull, v.x, o);
+        w.y = __shfl_xor_sync(kFull, v.y, o);
+        v = cmul(v, w);
+    }
+    return v;
+}
+
+// -------------------------------------------------------- ln cosh math --
+// For x = a + ib with z = exp(-2|a|):
+//   cosh x = e^{|a|}/2 * (X + i sgn(a) Y),  X = (1+z) cos b,  Y = (1-z) sin b
+// so ln cosh x = |a| - ln 2 + ln|X + i sgn(a) Y| + i arg(X + i sgn(a) Y).
+// This is the reference's overflow-free form (math.cpp:37-56) rearranged so
+// that one exp, one sincos and one log serve the real part.  The constant
+// -ln 2 is left out (it cancels in every psi ratio) and added back by log psi.
+//
+// FP32 path: Cody-Waite reduction of b to [-pi, pi] keeps the hardware
+// sin/cos approximations at their small-argument accuracy.
+__device__ __forceinline__ float reduce_2pi(float b) {
+    const float k = rintf(b * 0.159154943091895336f);
+    float r = fmaf(-k, 6.28318548202514648f, b);
+    return fmaf(-k, -1.74845553146951e-07f, r);
+}
+
+__device__ __forceinline__ void sincos_r(float b, float* s, float* c) { __sincosf(reduce_2pi(b), s, c); }
+__device__ __forceinline__ void sincos_r(double b, double* s, double* c) { sincos(b, s, c); }
+__device__ __forceinline__ float exp_r(float x) { return __expf(x); }
+__device__ __forceinline__ double exp_r(double x) { return exp(x); }
+__device__ __forceinline__ float log_r(float x) { return __logf(x); }
+__device__ __forceinline__ double log_r(double x) { return log(x); }
+
+// Real part only (Metropolis acceptance needs |psi'/psi|).
+template <typename R> __device__ __forceinline__ R lnc_re(R a, R b) {
+    const R aa = fabs(a);
+    const R z = exp_r((R)-2 * aa);
+    R s, c;
+    sincos_r(b, &s, &c);
+    const R X = ((R)1 + z) * c, Y = ((R)1 - z) * s;
+    return aa + (R)0.5 * log_r(X * X + Y * Y);
+}
+
+// Real part and unit phase.
+template <typename R> __device__ __forceinline__ void lnc_full(R a, R b, R& re, R& ux, R& uy) {
+    const R aa = fabs(a);
+    const R z = exp_r((R)-2 * aa);
+    R s, c;
+    sincos_r(b, &s, &c);
+    const R X = ((R)1 + z) * c;
+    const R Y = copysign((R)1 - z, a) * s;
+    const R m2 = X * X + Y * Y;
+    re = aa + (R)0.5 * log_r(m2);
+    const R inv = m2 > (R)0 ? rsqrt(m2) : (R)0;
+    ux = X * inv;
+    uy = Y * inv;
+}
+
+// tanh(a + ib) = [sgn(a)(1 - z^2) + i 4z sin b cos b] / (X^2 + Y^2), the
+// denominator 1 + z^2 + 2z cos 2b written as the sum of squares
+// X^2 + Y^2 = ((1+z) cos b)^2 + ((1-z) sin b)^2, which does not cancel near
+// the poles of tanh; 1 - z comes from expm1 so small |a| keeps its digits.
+__device__ __forceinline__ float expm1_r(float x) { return expm1f(x); }
+__device__ __forceinline__ double expm1_r(double x) { return expm1(x); }
+
+template <typename R> __device__ __forceinline__ C2<R> ctanh_r(R a, R b) {
+    const R aa = fabs(a);
+    const R omz = -expm1_r((R)-2 * aa);  // 1 - z
+    const R z = (R)1 - omz;
+    R s, c;
+    sincos_r(b, &s, &c);
+    const R X = ((R)1 + z) * c, Y = omz * s;
+    const R inv = (R)1 / (X * X + Y * Y);
+    return mk<R>(copysign(omz * ((R)1 + z), a) * inv, (R)4 * z * s * c * inv);
+}
+
+}  // namespace rbmnqs

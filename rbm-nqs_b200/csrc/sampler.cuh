@@ -1,0 +1,83 @@
+// sampler.cuh -- argument block of the fused Metropolis/E_loc/O_k kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace rbmnqs {
+
+// One local operator of the Hamiltonian (operators::local_op): k sites and a
+// CSR view of its 2^k x 2^k matrix; the nonzeros of row `loc` are
+// ent[rowptr[rp + loc] .. rowptr[rp + loc + 1]), each stored as the flip
+// mask loc ^ col (0 = diagonal) and the complex matrix element.
+struct OpDev {
+    int k;
+    int sites[6];
+    int rp;
+};
+
+struct MachineDev {
+    int n, n_vb, nh, S, T, P, P_neural;
+    int symmetric;
+    const double2* W64;    // [n][nh] site-major: W64[i*nh + k] = W(i, k)
+    const float2* W32;     // FP32 copy of W64
+    const double2* hb;     // [nh]
+    const double2* vb;     // [n_vb]
+    const uint8_t* perm;   // [n][S] perm[f*S + s] = P_s(f)      (symmetric)
+    const uint8_t* inv;    // [S][n] inv[s*n + j] = P_s^{-1}(j)  (symmetric)
+    const uint8_t* orbit;  // [n_vb][S] orbit[i*S + s] = P_s(basis_i)
+};
+
+struct HamDev {
+    int n_ops;
+    const OpDev* ops;
+    const int* rowptr;
+    const uint32_t* ent_mask;
+    const double2* ent_val;
+};
+
+struct SamplerArgs {
+    MachineDev m;
+    HamDev H;
+    // proposals (metropolis_sampler.cpp:145-219)
+    int n_prop_bonds;
+    const int2* prop_bonds;
+    double bond_flips;
+    // schedule
+    int n_chains, spc, warmup, step;
+    const uint32_t* ctl;  // device {epoch, init}: advanced in-stream so a
+                          // captured graph can be replayed epoch after epoch
+    uint64_t seed;
+    // state
+    uint32_t* spins;  // [n_chains][4]
+    // outputs
+    double2* E;       // [n_chains*spc]
+    void* O;          // [n_chains*spc][P] float2 (mixed) or double2 (FP64)
+    uint32_t* n_acc;  // [n_chains]
+    uint32_t* n_prop; // [n_chains]
+    int w_in_smem;    // FP32 W staged in shared memory
+};
+
+struct EvalArgs {
+    MachineDev m;
+    HamDev H;
+    const uint32_t* spins;  // [B][4]
+    int B;
+    double2* logpsi;        // may be null
+    double2* eloc;          // may be null
+    void* O;                // may be null; float2 or double2 per precision
+    const int* flips;       // ratio mode: [B][n_flips]
+    int n_flips;
+    double2* ratio;         // ratio mode output (log psi'/psi)
+    int w_in_smem;
+};
+
+// Launch helpers implemented in sampler.cu
+int sampler_smem_bytes(const MachineDev& m, int fp64, int warps, int w_in_smem);
+cudaError_t launch_sampler(const SamplerArgs& a, int fp64, int warps_per_block, cudaStream_t st);
+cudaError_t launch_eval(const EvalArgs& a, int fp64, int warps_per_block, cudaStream_t st);
+int elements_per_lane(int T);
+cudaError_t launch_advance(uint32_t* ctl, int reinit, cudaStream_t st);
+cudaError_t launch_mufu_probe(float* out, int iters, int blocks, cudaStream_t st);
+
+}  // namespace rbmnqs

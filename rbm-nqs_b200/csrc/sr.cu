@@ -1,0 +1,514 @@
+// sr.cu -- stochastic-reconfiguration kernels: sample moments, energy
+// statistics, the Hermitian Gram S, regularisation, FP64 conjugate
+// gradients and the weight update.
+#include "common.cuh"
+#include "sr.cuh"
+
+namespace rbmnqs {
+
+// ------------------------------------------------------- block reductions --
+template <typename T> __device__ __forceinline__ T shfl_sum(T v);
+template <> __device__ __forceinline__ double shfl_sum<double>(double v) { return warp_sum(v); }
+template <> __device__ __forceinline__ double2 shfl_sum<double2>(double2 v) {
+    v.x = warp_sum(v.x);
+    v.y = warp_sum(v.y);
+    return v;
+}
+__device__ __forceinline__ double2 add2(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+
+// Deterministic block sum; every thread gets the result.  `red` must hold
+// blockDim/32 entries.
+template <typename T> __device__ T block_sum(T v, T* red) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v = shfl_sum(v);
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    T r = red[0];
+    for (int i = 1; i < nw; i++) {
+        if constexpr (sizeof(T) == 16) r = add2(r, red[i]);
+        else r += red[i];
+    }
+    return r;
+}
+
+__device__ double block_max(double v, double* red) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o));
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    double r = red[0];
+    for (int i = 1; i < nw; i++) r = fmax(r, red[i]);
+    return r;
+}
+
+__device__ __forceinline__ double2 ld2(const float2* O, size_t i) {
+    const float2 v = O[i];
+    return make_double2(v.x, v.y);
+}
+__device__ __forceinline__ double2 ld2(const double2* O, size_t i) { return O[i]; }
+
+// ------------------------------------------------------------- moments ---
+// Per block over a slice of samples: sum_n O[n][p], sum_n E_n conj(O[n][p]),
+// sum_n E_n (aggregators a_d_, a_dh_, a_h_: aggregator.cpp:190-231).
+template <typename TO>
+__global__ void moments_partial(const TO* O, const double2* E, int N, int P, double2* pd, double2* pf, double2* pe) {
+    __shared__ double2 red[32];
+    const int nb = gridDim.x;
+    const int n0 = (int)((long)N * blockIdx.x / nb), n1 = (int)((long)N * (blockIdx.x + 1) / nb);
+    for (int p = threadIdx.x; p < P; p += blockDim.x) {
+        double sx = 0, sy = 0, fx = 0, fy = 0;
+        for (int n = n0; n < n1; n++) {
+            const double2 o = ld2(O, (size_t)n * P + p);
+            const double2 e = E[n];
+            sx += o.x;
+            sy += o.y;
+            fx += e.x * o.x + e.y * o.y;  // E * conj(O)
+            fy += e.y * o.x - e.x * o.y;
+        }
+        pd[(size_t)blockIdx.x * P + p] = make_double2(sx, sy);
+        pf[(size_t)blockIdx.x * P + p] = make_double2(fx, fy);
+    }
+    double2 es = make_double2(0, 0);
+    for (int n = n0 + threadIdx.x; n < n1; n += blockDim.x) es = add2(es, E[n]);
+    es = block_sum(es, red);
+    if (threadIdx.x == 0) pe[blockIdx.x] = es;
+}
+
+// d = <O>, F = <E O*> - <E> conj(<O>) (stochastic_reconfiguration.cpp:102)
+__global__ void moments_final(const double2* pd, const double2* pf, const double2* pe, int nb, int N, int P,
+                              double2* d, double2* F, double2* emean) {
+    __shared__ double2 em;
+    if (threadIdx.x == 0) {
+        double2 s = make_double2(0, 0);
+        for (int b = 0; b < nb; b++) s = add2(s, pe[b]);
+        em = make_double2(s.x / N, s.y / N);
+        if (blockIdx.x == 0) *emean = em;
+    }
+    __syncthreads();
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+        double2 sd = make_double2(0, 0), sf = make_double2(0, 0);
+        for (int b = 0; b < nb; b++) {
+            sd = add2(sd, pd[(size_t)b * P + p]);
+            sf = add2(sf, pf[(size_t)b * P + p]);
+        }
+        const double2 dd = make_double2(sd.x / N, sd.y / N);
+        d[p] = dd;
+        // F = dh - h * conj(d)
+        F[p] = make_double2(sf.x / N - (em.x * dd.x + em.y * dd.y), sf.y / N - (em.y * dd.x - em.x * dd.y));
+    }
+}
+
+// ------------------------------------------------------ energy statistics --
+// aggregator::finalize for a_h_ with n_bins bins (aggregator.cpp:84-164,
+// 233-239): mean, M2, binned M2, tau, unbiased variances, binned stddev; and
+// the mean acceptance over chains (metropolis_sampler.cpp:89-91).
+__global__ void energy_stats(const double2* E, int N, int n_bins, const double2* emean, const uint32_t* nacc,
+                             const uint32_t* nprop, int n_chains, EpochStatsDev* out) {
+    __shared__ double red[32];
+    const double2 mu = *emean;
+    double m2 = 0;
+    int finite = 1;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        const double2 e = E[i];
+        if (!isfinite(e.x) || !isfinite(e.y)) finite = 0;
+        const double dx = e.x - mu.x, dy = e.y - mu.y;
+        m2 += dx * dx + dy * dy;
+    }
+    m2 = block_sum(m2, red);
+    const int bs = N / n_bins;
+    double m2b = 0;
+    for (int b = threadIdx.x; b < n_bins; b += blockDim.x) {
+        double sx = 0, sy = 0;
+        for (int i = 0; i < bs; i++) {
+            sx += E[(size_t)b * bs + i].x;
+            sy += E[(size_t)b * bs + i].y;
+        }
+        const double dx = sx / bs - mu.x, dy = sy / bs - mu.y;
+        m2b += bs * (dx * dx + dy * dy);
+    }
+    m2b = block_sum(m2b, red);
+    double acc = 0;
+    for (int c = threadIdx.x; c < n_chains; c += blockDim.x) acc += nprop[c] ? (double)nacc[c] / nprop[c] : 0.0;
+    acc = block_sum(acc, red);
+    const double nf = block_sum((double)finite, red);
+    if (threadIdx.x == 0) {
+        double tau = 0;
+        if (n_bins > 1 && !(m2 == 0 && m2b == 0)) {
+            double r = bs * m2b / m2;
+            tau = 0.5 * ((r < 1 ? 1 : r) - 1);
+        }
+        const double den = (double)N - 1.0;
+        double v = m2 / den, vb = m2b / den;
+        v = v < 0 ? 0 : v;
+        vb = vb < 0 ? 0 : vb;
+        out->energy = mu;
+        out->var = v;
+        out->var_binned = vb;
+        out->tau = tau;
+        out->stddev = n_bins > 1 ? sqrt(vb / n_bins) : sqrt(v / N);
+        out->acceptance = acc / n_chains;
+        out->finite = nf == (double)blockDim.x ? 1 : 0;
+    }
+}
+
+// ----------------------------------------------------------------- Gram ---
+// S = (1/N) sum_n conj(X_n) X_n^T with X = O - <O> (centred, so no
+// cancellation against conj(d) d^T).  FP64 accumulation of FP32/FP64 inputs
+// on CUDA cores: 32x32 complex tiles of the upper triangle, split over
+// sample ranges into partial buffers.
+constexpr int GT = 32, GK = 16;
+
+template <typename TO>
+__global__ void __launch_bounds__(256) gram_fp64(const TO* O, const double2* d, int N, int P, int ntile,
+                                                 double2* part) {
+    __shared__ double2 A[GK][GT + 1];
+    __shared__ double2 B[GK][GT + 1];
+    // map blockIdx.x -> (tp <= tq)
+    int t = blockIdx.x, tp = 0;
+    while (t >= ntile - tp) {
+        t -= ntile - tp;
+        tp++;
+    }
+    const int tq = tp + t;
+    const int p0 = tp * GT, q0 = tq * GT;
+    const int ks = blockIdx.y, nks = gridDim.y;
+    const int n0 = (int)((long)N * ks / nks), n1 = (int)((long)N * (ks + 1) / nks);
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    double2 acc[2][2];
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) acc[i][j] = make_double2(0, 0);
+    for (int nb = n0; nb < n1; nb += GK) {
+        for (int i = threadIdx.x; i < GK * GT; i += blockDim.x) {
+            const int kk = i / GT, c = i % GT;
+            const int n = nb + kk;
+            double2 a = make_double2(0, 0), b = make_double2(0, 0);
+            if (n < n1) {
+                if (p0 + c < P) {
+                    a = ld2(O, (size_t)n * P + p0 + c);
+                    if (d) {
+                        a.x -= d[p0 + c].x;
+                        a.y -= d[p0 + c].y;
+                    }
+                }
+                if (q0 + c < P) {
+                    b = ld2(O, (size_t)n * P + q0 + c);
+                    if (d) {
+                        b.x -= d[q0 + c].x;
+                        b.y -= d[q0 + c].y;
+                    }
+                }
+            }
+            A[kk][c] = a;
+            B[kk][c] = b;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < GK; kk++) {
+            const double2 a0 = A[kk][ty], a1 = A[kk][ty + 16];
+            const double2 b0 = B[kk][tx], b1 = B[kk][tx + 16];
+            const double2 av[2] = {a0, a1}, bv[2] = {b0, b1};
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    // conj(a) * b
+                    acc[i][j].x = fma(av[i].x, bv[j].x, fma(av[i].y, bv[j].y, acc[i][j].x));
+                    acc[i][j].y = fma(av[i].x, bv[j].y, fma(-av[i].y, bv[j].x, acc[i][j].y));
+                }
+        }
+        __syncthreads();
+    }
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) {
+            const int p = p0 + ty + 16 * i, q = q0 + tx + 16 * j;
+            if (p < P && q < P) part[(size_t)ks * P * P + (size_t)p * P + q] = acc[i][j];
+        }
+}
+
+// Sum the split partials, scale by 1/N, mirror the lower triangle.
+__global__ void gram_finalize(const double2* part, int nks, int N, int P, double2* S) {
+    const size_t total = (size_t)P * P;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int p = (int)(i / P), q = (int)(i % P);
+        if (q < p) continue;
+        double2 s = make_double2(0, 0);
+        for (int k = 0; k < nks; k++) s = add2(s, part[(size_t)k * total + i]);
+        s.x /= N;
+        s.y /= N;
+        if (p == q) s.y = 0;
+        S[i] = s;
+        S[(size_t)q * P + p] = make_double2(s.x, -s.y);
+    }
+}
+
+// ------------------------------------------------------ schedule / reg ---
+// decay_t::get for the four schedules (abstract_optimizer.cpp:27-54).
+__global__ void schedule_step(ScheduleDev* s) {
+    if (threadIdx.x < 4) {
+        const int i = threadIdx.x;
+        if (!s->min_reached[i]) {
+            s->value[i] *= s->decay[i];
+            if (s->value[i] < s->min[i]) {
+                s->min_reached[i] = 1;
+                s->value[i] = s->min[i];
+            }
+        }
+    }
+}
+
+// diag = var(O) = N/(N-1) S_pp; S_reg = S + r1 diag (+ rd on non-neural
+// parameters) + r2 max(diag) (cg_solver.cpp:301-318).
+__global__ void regularize(const double2* S, int P, int n_neural, int N, const ScheduleDev* sch, double* diag,
+                           double2* Sreg, double* max_diag_out) {
+    __shared__ double red[32];
+    const double r1 = sch->value[1], r2 = sch->value[2], rd = sch->value[3];
+    double mx = 0;
+    for (int p = threadIdx.x; p < P; p += blockDim.x) {
+        const double v = S[(size_t)p * P + p].x * (double)N / ((double)N - 1.0);
+        diag[p] = v;
+        mx = fmax(mx, v);
+    }
+    mx = block_max(mx, red);
+    if (threadIdx.x == 0) *max_diag_out = mx;
+    const size_t total = (size_t)P * P;
+    for (size_t i = threadIdx.x; i < total; i += blockDim.x) Sreg[i] = S[i];
+    __syncthreads();
+    for (int p = threadIdx.x; p < P; p += blockDim.x) {
+        const double f = diag[p] * (p < n_neural ? r1 : r1 + rd) + mx * r2;
+        Sreg[(size_t)p * P + p].x += f;
+    }
+}
+
+// abstract_solver::solve inputs (drop-in entry point): S_reg = G/norm -
+// conj(d) d^T + diag(r1 diag (+rd) + r2 max(diag)), where G = sum conj(O) O^T
+// was accumulated with weights already folded into O (cg_solver.cpp:301-318).
+__global__ void solve_prep(const double2* G, int N, double norm, const double2* d, const double* diag, int P,
+                           int n_neural, double r1, double r2, double rd, double2* Sreg) {
+    __shared__ double red[32];
+    double mx = -1e300;
+    for (int p = threadIdx.x; p < P; p += blockDim.x) mx = fmax(mx, diag[p]);
+    mx = block_max(mx, red);
+    const double scale = (double)N / norm;  // G holds sums divided by N
+    const size_t total = (size_t)P * P;
+    for (size_t i = threadIdx.x; i < total; i += blockDim.x) {
+        const int k = (int)(i / P), l = (int)(i % P);
+        const double2 g = G[i], dk = d[k], dl = d[l];
+        // conj(d_k) d_l
+        const double cx = dk.x * dl.x + dk.y * dl.y, cy = dk.x * dl.y - dk.y * dl.x;
+        double2 v = make_double2(g.x * scale - cx, g.y * scale - cy);
+        if (k == l) v.x += diag[k] * (k < n_neural ? r1 : r1 + rd) + mx * r2;
+        Sreg[i] = v;
+    }
+}
+
+cudaError_t launch_solve_prep(const double2* G, int N, double norm, const double2* d, const double* diag, int P,
+                              int n_neural, double r1, double r2, double rd, double2* Sreg, cudaStream_t st) {
+    solve_prep<<<1, 1024, 0, st>>>(G, N, norm, d, diag, P, n_neural, r1, r2, rd, Sreg);
+    return cudaGetLastError();
+}
+
+// -------------------------------------------------------------------- CG --
+// cg_solver::cg1 (cg_solver.cpp:119-193) on the dense regularised S, one
+// block; vectors in shared memory.  Stops when ||r||^2 < rtol or after
+// max_it iterations.
+__global__ void __launch_bounds__(1024) cg_dense(const double2* A, const double2* b, double2* x, int P, int max_it,
+                                                 double rtol, CgResultDev* res) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    double2* r = reinterpret_cast<double2*>(sm);
+    double2* p = r + P;
+    double2* Ap = p + P;
+    __shared__ double red[32];
+    __shared__ double2 red2[32];
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
+    auto matvec = [&](const double2* v) {
+        for (int row = w; row < P; row += nw) {
+            double sx = 0, sy = 0;
+            const double2* Ar = A + (size_t)row * P;
+            for (int j = lane; j < P; j += 32) {
+                const double2 a = Ar[j], vv = v[j];
+                sx = fma(a.x, vv.x, fma(-a.y, vv.y, sx));
+                sy = fma(a.x, vv.y, fma(a.y, vv.x, sy));
+            }
+            sx = warp_sum(sx);
+            sy = warp_sum(sy);
+            if (lane == 0) Ap[row] = make_double2(sx, sy);
+        }
+        __syncthreads();
+    };
+    for (int i = tid; i < P; i += nt) p[i] = x[i];
+    __syncthreads();
+    matvec(p);
+    double rs0 = 0;
+    for (int i = tid; i < P; i += nt) {
+        const double2 ri = make_double2(b[i].x - Ap[i].x, b[i].y - Ap[i].y);
+        r[i] = ri;
+        p[i] = ri;
+        rs0 += ri.x * ri.x + ri.y * ri.y;
+    }
+    double rsold = block_sum(rs0, red);
+    double rs = rsold;
+    int itn = 0;
+    for (itn = 0; itn < max_it; itn++) {
+        matvec(p);
+        double2 pap = make_double2(0, 0);
+        for (int i = tid; i < P; i += nt) {  // p^H Ap
+            pap.x += p[i].x * Ap[i].x + p[i].y * Ap[i].y;
+            pap.y += p[i].x * Ap[i].y - p[i].y * Ap[i].x;
+        }
+        pap = block_sum(pap, red2);
+        // alpha = rsold / pap
+        const double den = pap.x * pap.x + pap.y * pap.y;
+        const double ax = rsold * pap.x / den, ay = -rsold * pap.y / den;
+        double rl = 0;
+        for (int i = tid; i < P; i += nt) {
+            const double2 pi = p[i], api = Ap[i];
+            double2 xi = x[i];
+            xi.x += ax * pi.x - ay * pi.y;
+            xi.y += ax * pi.y + ay * pi.x;
+            x[i] = xi;
+            double2 ri = r[i];
+            ri.x -= ax * api.x - ay * api.y;
+            ri.y -= ax * api.y + ay * api.x;
+            r[i] = ri;
+            rl += ri.x * ri.x + ri.y * ri.y;
+        }
+        rs = block_sum(rl, red);
+        if (rs < rtol) break;
+        const double beta = rs / rsold;
+        for (int i = tid; i < P; i += nt) {
+            const double2 ri = r[i], pi = p[i];
+            p[i] = make_double2(ri.x + beta * pi.x, ri.y + beta * pi.y);
+        }
+        rsold = rs;
+        __syncthreads();
+    }
+    if (tid == 0) {
+        res->iterations = itn;
+        res->residual = rs;
+    }
+}
+
+// ---------------------------------------------------------------- update --
+// abstract_optimizer::optimize tail (abstract_optimizer.cpp:157-176):
+// abort on max|x| > 30, else x *= lr (the next warm start) and w -= x.
+__global__ void sr_update(double2* params, double2* x, int P, const ScheduleDev* sch, CgResultDev* res) {
+    __shared__ double red[32];
+    double mx = 0;
+    int bad = 0;
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        const double2 v = x[i];
+        if (!isfinite(v.x) || !isfinite(v.y)) bad = 1;
+        mx = fmax(mx, sqrt(v.x * v.x + v.y * v.y));
+    }
+    mx = block_max(mx, red);
+    const double nbad = block_sum((double)bad, red);
+    const int status = nbad > 0 ? -5 : (mx > 30.0 ? -4 : 0);
+    if (threadIdx.x == 0) {
+        res->max_dw = mx;
+        res->status = status;
+    }
+    if (status != 0) return;
+    const double lr = sch->value[0];
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        double2 v = x[i];
+        v.x *= lr;
+        v.y *= lr;
+        x[i] = v;
+        params[i].x -= v.x;
+        params[i].y -= v.y;
+    }
+}
+
+// Parameter vector -> kernel layouts (site-major W in FP64 and FP32).
+__global__ void unpack_weights(const double2* params, int n, int n_vb, int nh, double2* vb, double2* hb, double2* W64,
+                               float2* W32) {
+    const int tot = n * nh;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < tot + nh + n_vb; i += gridDim.x * blockDim.x) {
+        if (i < n_vb) {
+            vb[i] = params[i];
+        } else if (i < n_vb + nh) {
+            hb[i - n_vb] = params[i];
+        } else {
+            const int r = i - n_vb - nh;  // reference index j + n*k
+            const int j = r % n, k = r / n;
+            const double2 w = params[i];
+            W64[j * nh + k] = w;
+            W32[j * nh + k] = make_float2((float)w.x, (float)w.y);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- launch --
+cudaError_t launch_moments(const void* O, int fp64, const double2* E, int N, int P, int nblk, double2* pd,
+                           double2* pf, double2* pe, double2* d, double2* F, double2* emean, cudaStream_t st) {
+    if (fp64)
+        moments_partial<double2><<<nblk, 256, 0, st>>>((const double2*)O, E, N, P, pd, pf, pe);
+    else
+        moments_partial<float2><<<nblk, 256, 0, st>>>((const float2*)O, E, N, P, pd, pf, pe);
+    moments_final<<<(P + 255) / 256, 256, 0, st>>>(pd, pf, pe, nblk, N, P, d, F, emean);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_energy_stats(const double2* E, int N, int n_bins, const double2* emean, const uint32_t* nacc,
+                                const uint32_t* nprop, int n_chains, EpochStatsDev* out, cudaStream_t st) {
+    energy_stats<<<1, 1024, 0, st>>>(E, N, n_bins, emean, nacc, nprop, n_chains, out);
+    return cudaGetLastError();
+}
+
+int gram_splits(int N, int P) {
+    const int nt = (P + GT - 1) / GT;
+    const int tiles = nt * (nt + 1) / 2;
+    int ks = (2 * 148 + tiles - 1) / tiles;
+    if (ks > 64) ks = 64;
+    if (ks > N / GK) ks = N / GK > 0 ? N / GK : 1;
+    return ks < 1 ? 1 : ks;
+}
+
+cudaError_t launch_gram_fp64(const void* O, int fp64, const double2* d, int N, int P, int nks, double2* part,
+                             double2* S, cudaStream_t st) {
+    const int nt = (P + GT - 1) / GT;
+    dim3 grid(nt * (nt + 1) / 2, nks);
+    if (fp64)
+        gram_fp64<double2><<<grid, 256, 0, st>>>((const double2*)O, d, N, P, nt, part);
+    else
+        gram_fp64<float2><<<grid, 256, 0, st>>>((const float2*)O, d, N, P, nt, part);
+    gram_finalize<<<296, 256, 0, st>>>(part, nks, N, P, S);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_schedule(ScheduleDev* s, cudaStream_t st) {
+    schedule_step<<<1, 32, 0, st>>>(s);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_regularize(const double2* S, int P, int n_neural, int N, const ScheduleDev* sch, double* diag,
+                              double2* Sreg, double* max_diag, cudaStream_t st) {
+    regularize<<<1, 1024, 0, st>>>(S, P, n_neural, N, sch, diag, Sreg, max_diag);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cg(const double2* A, const double2* b, double2* x, int P, int max_it, double rtol, CgResultDev* res,
+                      cudaStream_t st) {
+    const int smem = 3 * P * (int)sizeof(double2);
+    cudaError_t e = cudaFuncSetAttribute(cg_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    cg_dense<<<1, 1024, smem, st>>>(A, b, x, P, max_it, rtol, res);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_update(double2* params, double2* x, int P, const ScheduleDev* sch, CgResultDev* res,
+                          cudaStream_t st) {
+    sr_update<<<1, 1024, 0, st>>>(params, x, P, sch, res);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack(const double2* params, int n, int n_vb, int nh, double2* vb, double2* hb, double2* W64,
+                          float2* W32, cudaStream_t st) {
+    unpack_weights<<<148, 256, 0, st>>>(params, n, n_vb, nh, vb, hb, W64, W32);
+    return cudaGetLastError();
+}
+
+}  // namespace rbmnqs

@@ -1,0 +1,48 @@
+// sr.cuh -- device-side state blocks and launchers of the SR kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace rbmnqs {
+
+// Per-epoch statistics written on the device, read back once per epoch.
+struct EpochStatsDev {
+    double2 energy;
+    double var, var_binned, tau, stddev, acceptance;
+    int finite;
+};
+
+// decay_t state of lr, reg1, reg2, deltareg1 (indices 0..3).
+struct ScheduleDev {
+    double value[4], min[4], decay[4];
+    int min_reached[4];
+};
+
+struct CgResultDev {
+    int iterations;
+    int status;
+    double residual;
+    double max_dw;
+};
+
+cudaError_t launch_moments(const void* O, int fp64, const double2* E, int N, int P, int nblk, double2* pd,
+                           double2* pf, double2* pe, double2* d, double2* F, double2* emean, cudaStream_t st);
+cudaError_t launch_energy_stats(const double2* E, int N, int n_bins, const double2* emean, const uint32_t* nacc,
+                                const uint32_t* nprop, int n_chains, EpochStatsDev* out, cudaStream_t st);
+int gram_splits(int N, int P);
+cudaError_t launch_gram_fp64(const void* O, int fp64, const double2* d, int N, int P, int nks, double2* part,
+                             double2* S, cudaStream_t st);
+cudaError_t launch_solve_prep(const double2* G, int N, double norm, const double2* d, const double* diag, int P,
+                              int n_neural, double r1, double r2, double rd, double2* Sreg, cudaStream_t st);
+cudaError_t launch_schedule(ScheduleDev* s, cudaStream_t st);
+cudaError_t launch_regularize(const double2* S, int P, int n_neural, int N, const ScheduleDev* sch, double* diag,
+                              double2* Sreg, double* max_diag, cudaStream_t st);
+cudaError_t launch_cg(const double2* A, const double2* b, double2* x, int P, int max_it, double rtol,
+                      CgResultDev* res, cudaStream_t st);
+cudaError_t launch_update(double2* params, double2* x, int P, const ScheduleDev* sch, CgResultDev* res,
+                          cudaStream_t st);
+cudaError_t launch_unpack(const double2* params, int n, int n_vb, int nh, double2* vb, double2* hb, double2* W64,
+                          float2* W32, cudaStream_t st);
+
+}  // namespace rbmnqs

@@ -1,0 +1,219 @@
+"""GPU parity: the CUDA path (through the C ABI) against the FP64 CPU oracle on
+identical weights and configuration batches.  Tolerances (relative):
+1e-10 for the FP64 path (precision=1), 1e-5 for the FP32 psi-ratio path
+(precision=0); full enumeration vs ED at 1e-8."""
+import numpy as np
+import pytest
+
+import ed
+import oracle as O
+import rbmnqs
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-10
+TOL32 = 1e-5
+
+CASES = {
+    # name: (model, n_cells, rbm kind, alpha)
+    "kitaev3_basic_a1": ("kitaev", 3, "basic", 1),
+    "kitaev2_symm_a4": ("kitaev", 2, "symmetry", 4),
+    "kitaev4_symm_a4": ("kitaev", 4, "symmetry", 4),
+    "toric3_basic_a2": ("toric", 3, "basic", 2),
+    "toric3_symm_a2": ("toric", 3, "symmetry", 2),
+}
+
+
+def make_pair(case, precision=1, chains=8, spc=16, warmup=4, bond_flips=0.0, seed=123, std=0.1, reinit=1,
+              wseed=7, **cfgkw):
+    model, L, kind, alpha = CASES[case]
+    rng = np.random.default_rng(wseed)
+    symm = 0.5 if model == "kitaev" else 1.0
+    om = O.Model.kitaev(L) if model == "kitaev" else O.Model.toric(L)
+    mach = O.Machine(om, kind, alpha, symm=symm)
+    mach.init_random(rng, std)
+    gm = rbmnqs.Model.kitaev(L, symmetry=symm) if model == "kitaev" else rbmnqs.Model.toric(L, symmetry=symm)
+    cfg = rbmnqs.default_config(rbm_type=1 if kind == "symmetry" else 0, alpha=alpha, n_chains=chains,
+                                samples_per_chain=spc, warmup=warmup, bond_flips=bond_flips, seed=seed,
+                                precision=precision, reinit_chains=reinit, **cfgkw)
+    s = rbmnqs.Session(gm, cfg)
+    assert s.n_params == mach.n_params
+    s.set_weights(mach.params())
+    return om, mach, s, rng
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.max(np.abs(a - b)) / max(1.0, np.max(np.abs(b)))
+
+
+def logpsi_close(lg, lo, tol):
+    d = lg - lo
+    assert np.max(np.abs(d.real)) < tol * max(1.0, np.max(np.abs(lo.real)))
+    assert np.max(np.abs(np.angle(np.exp(1j * d.imag)))) < tol * max(1.0, np.max(np.abs(lo.imag)))
+
+
+@pytest.mark.parametrize("case", list(CASES))
+@pytest.mark.parametrize("precision,tol", [(1, TOL64), (0, TOL32)])
+def test_eval_batch_matches_oracle(case, precision, tol):
+    om, mach, s, rng = make_pair(case, precision=precision, std=0.2)
+    spins = O.random_spins(rng, 96, mach.n)
+    lg, eg, Og = s.eval_batch(spins)
+    lo, eo, Oo = O.eval_batch(mach, om, spins)
+    logpsi_close(lg, lo, tol)
+    assert rel(eg, eo) < tol
+    assert rel(Og, Oo) < tol
+
+
+@pytest.mark.parametrize("case", ["kitaev3_basic_a1", "kitaev4_symm_a4", "toric3_basic_a2"])
+@pytest.mark.parametrize("precision,tol", [(1, TOL64), (0, TOL32)])
+@pytest.mark.parametrize("nflip", [1, 2, 4])
+def test_log_psi_over_psi_matches_oracle(case, precision, tol, nflip):
+    om, mach, s, rng = make_pair(case, precision=precision, std=0.2)
+    B = 48
+    spins = O.random_spins(rng, B, mach.n)
+    flips = np.stack([rng.choice(mach.n, nflip, replace=False) for _ in range(B)]).astype(np.int32)
+    rg = s.log_psi_over_psi(spins, flips)
+    ro = np.array([O.log_psi_over_psi(mach, spins[b], flips[b]) for b in range(B)])
+    assert rel(np.exp(rg), np.exp(ro)) < tol
+
+
+@pytest.mark.parametrize("case,bond_flips", [("kitaev3_basic_a1", 0.0), ("kitaev2_symm_a4", 0.5),
+                                             ("kitaev4_symm_a4", 0.5), ("toric3_basic_a2", 0.0)])
+def test_metropolis_fp64_reproduces_oracle_chains(case, bond_flips):
+    om, mach, s, rng = make_pair(case, precision=1, chains=8, spc=12, warmup=3, bond_flips=bond_flips, std=0.3)
+    st = s.sample()
+    Eg, Og = s.samples()
+    Eo, Oo, acc, spo = O.metropolis(mach, om, 8, 12, warmup=3, bond_flips=bond_flips, seed=123, epoch=0)
+    assert np.array_equal(s.spins(), spo)
+    assert rel(Eg, Eo) < TOL64
+    assert rel(Og, Oo) < TOL64
+    assert abs(st["acceptance"] - acc.mean()) < 1e-12
+    ref = O.stats(Eo)
+    assert abs(st["energy"] - ref["mean"]) < TOL64 * max(1, abs(ref["mean"]))
+    assert abs(st["stddev"] - ref["stddev"]) < 1e-8 * max(ref["stddev"], 1e-12)
+    assert abs(st["tau"] - ref["tau"]) < 1e-8 * max(1, ref["tau"])
+    assert st["n_bins"] == ref["n_bins"]
+
+
+def test_metropolis_fp32_statistics_agree():
+    om, mach, s, rng = make_pair("kitaev3_basic_a1", precision=0, chains=64, spc=200, warmup=20, std=0.3)
+    st = s.sample()
+    Eg, _ = s.samples(with_O=False)
+    Eo, _, acc, _ = O.metropolis(mach, om, 64, 200, warmup=20, seed=123, with_O=False)
+    # identical Philox streams: the FP32 chains follow the FP64 ones except
+    # after an acceptance tie, so most samples coincide
+    same = np.mean(np.abs(Eg - Eo) < 1e-4 * np.maximum(1, np.abs(Eo)))
+    assert same > 0.9
+    ex = O.full(mach, om, with_O=False)["E"].real
+    assert abs(st["energy"].real - ex) < 5 * st["stddev"] + 1e-3
+
+
+@pytest.mark.parametrize("case", ["kitaev3_basic_a1", "kitaev4_symm_a4", "toric3_symm_a2"])
+@pytest.mark.parametrize("precision", [1, 0])
+def test_sr_moments_and_gram_match_oracle(case, precision):
+    om, mach, s, rng = make_pair(case, precision=precision, chains=16, spc=32, warmup=2, std=0.2)
+    s.sample()
+    s.optimize()
+    Eg, Og = s.samples()
+    d, F, diag, S = s.sr_moments()
+    do, Fo, diago = O.sr_moments(Og, Eg)  # oracle on the GPU's own samples
+    So = O.sr_matrix(Og, do)
+    assert rel(d, do) < TOL64
+    assert rel(F, Fo) < TOL64
+    assert rel(diag, diago) < TOL64
+    assert np.linalg.norm(S - So) / np.linalg.norm(So) < TOL64
+    assert np.allclose(S, S.conj().T, rtol=0, atol=1e-14 * np.abs(S).max())
+
+
+@pytest.mark.parametrize("case", ["kitaev3_basic_a1", "kitaev4_symm_a4"])
+def test_sr_solve_matches_oracle_cg(case):
+    om, mach, s, rng = make_pair(case, precision=1, chains=16, spc=32, std=0.2)
+    s.sample()
+    E, Om = s.samples()
+    d, F, diag = O.sr_moments(Om, E)
+    x0 = 1e-3 * (rng.normal(size=mach.n_params) + 1j * rng.normal(size=mach.n_params))
+    xo, ito, rso = O.cg_solve(Om, d, F, x0, 0.9, 9e-4, 1e-2, diag)
+    xg, itg, rsg = s.sr_solve(Om, d, F, x0, 0.9, 9e-4, 1e-2, diag)
+    # dense S vs the reference's matrix-free operator: same iterates up to
+    # rounding, so the stopping iteration can move by a few near rtol
+    assert abs(itg - ito) <= max(2, ito // 20)
+    assert rel(xg, xo) < 1e-8
+
+
+@pytest.mark.parametrize("case", ["kitaev3_basic_a1", "kitaev2_symm_a4"])
+@pytest.mark.parametrize("reinit", [1, 0])
+def test_sr_epochs_match_oracle(case, reinit):
+    """Three full epochs (sample -> F, S -> CG -> w -= lr x) against the
+    oracle driving the reference loop (abstract_optimizer::optimize)."""
+    chains, spc, warm = 8, 24, 4
+    om, mach, s, rng = make_pair(case, precision=1, chains=chains, spc=spc, warmup=warm, std=0.05, reinit=reinit)
+    lr, r1, r2, rd = O.Decay(1e-2), O.Decay(1, 1e-4, 0.9), O.Decay(1e-3, 1e-6, 0.9), O.Decay(1e-2)
+    x = np.zeros(mach.n_params, np.complex128)
+    spins = np.zeros((chains, 4), np.uint32)
+    for ep in range(3):
+        if ep == 0:
+            sst, ost = s.sample(), s.optimize()
+        else:
+            sst, ost = s.epoch()
+        E, Om, acc, spins = O.metropolis(mach, om, chains, spc, warmup=warm, seed=123, epoch=ep,
+                                         init=(reinit == 1 or ep == 0), spins=spins)
+        d, F, diag = O.sr_moments(Om, E)
+        lrv, r1v, r2v, rdv = lr.get(), r1.get(), r2.get(), rd.get()
+        x, it, rs = O.cg_solve(Om, d, F, x, r1v, r2v, rdv, diag)
+        assert abs(ost["reg1"] - r1v) < 1e-15 and abs(ost["reg2"] - r2v) < 1e-18
+        assert abs(ost["iterations"] - it) <= 1
+        x = x * lrv
+        mach.set_params(mach.params() - x)
+        w = s.get_weights()
+        assert rel(w, mach.params()) < 1e-9, ep
+    assert ost["status"] == 0
+
+
+@pytest.mark.parametrize("case", ["kitaev3_basic_a1", "toric3_symm_a2"])
+def test_full_enumeration_matches_oracle_and_ed(case):
+    om, mach, s, rng = make_pair(case, precision=1, std=0.3)
+    Eg, dg, dhg = s.full_sample()
+    ref = O.full(mach, om)
+    assert abs(Eg - ref["E"]) < 1e-8 * abs(ref["E"])
+    assert rel(dg, ref["d"]) < 1e-8
+    assert rel(dhg, ref["dh"]) < 1e-8
+    if mach.n <= 18:
+        H = ed.hamiltonian(om)
+        N = 1 << mach.n
+        bits = ((np.arange(N)[:, None] >> np.arange(mach.n)[None, :]) & 1)
+        lp, _, _ = s.eval_batch(O.spins_from_bits(bits), eloc=False, O=False)
+        psi = np.exp(lp - lp.real.max())
+        e = np.vdot(psi, H @ psi) / np.vdot(psi, psi)
+        assert abs(Eg - e) < 1e-8 * abs(e)
+
+
+def test_graph_epoch_equals_stepwise_epoch():
+    _, _, a, _ = make_pair("kitaev4_symm_a4", precision=0, chains=32, spc=16, warmup=2, bond_flips=0.5)
+    _, _, b, _ = make_pair("kitaev4_symm_a4", precision=0, chains=32, spc=16, warmup=2, bond_flips=0.5)
+    for _ in range(3):
+        a.sample()
+        a.optimize()
+        b.epoch()
+    assert np.array_equal(a.get_weights(), b.get_weights())
+    assert np.array_equal(a.spins(), b.spins())
+
+
+def test_timing_counters():
+    _, _, s, _ = make_pair("kitaev4_symm_a4", precision=0, chains=32, spc=8, warmup=1)
+    s.timing_reset(True)
+    for _ in range(2):
+        s.epoch()
+    ms, cnt = s.timing()
+    assert (cnt[:5] == 2).all() and (ms[:5] > 0).all()
+
+
+def test_massive_step_is_reported():
+    om, mach, s, rng = make_pair("kitaev3_basic_a1", precision=1, chains=4, spc=8, lr=(1.0, 1.0, 1.0),
+                                 reg1=(1e-12, 1e-12, 1.0), reg2=(1e-12, 1e-12, 1.0), std=2.0)
+    w0 = s.get_weights()
+    s.sample()
+    st = s.optimize()
+    if st["max_dw"] > 30:
+        assert st["status"] == rbmnqs.ERR_MASSIVE_STEP
+        assert np.array_equal(s.get_weights(), w0)
