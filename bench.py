@@ -237,7 +237,8 @@ def run_ours(args, rank, world, local):
             "tau": tau, "energy_per_site": float(np.mean(energies)) / model.n, "acceptance": acc,
             "cg_iterations": float(np.mean(its)),
             "stage_ms_per_epoch": {nm: stage_ms[i] / max(1, stage_cnt[i]) for i, nm in
-                                   enumerate(["sampler", "moments+stats", "gram+regularise", "cg", "update"])},
+                                   enumerate(["sampler", "eval", "moments+stats", "gram+regularise", "cg",
+                                              "update"])},
             "roofline": {"bound": "mufu", "kernel": "sampler_kernel", "achieved": achieved / 1e9,
                          "peak": mufu / 1e9, "unit": "Gop/s (MUFU)", "frac": achieved / mufu,
                          "peak_source": "measured in this run by rbmnqs_probe_mufu (no MUFU figure in "

@@ -187,8 +187,9 @@ int rbmnqs_get_observables(rbmnqs_handle* h, double* values);
 
 /* ----------------------------------------------------------- timing ---- */
 /* Device time (ms, CUDA events on the handle's stream) accumulated per stage
- * since the last reset: 0 sample kernel, 1 moments, 2 Gram, 3 CG, 4 update,
- * 5 stats.  `launches` counts kernel launches per stage. */
+ * since the last reset: 0 Metropolis sweeps, 1 E_loc + O_k evaluation,
+ * 2 moments + energy statistics, 3 Gram + regularisation, 4 CG, 5 update.
+ * `launches` counts how often each stage ran. */
 int rbmnqs_timing(rbmnqs_handle* h, double* ms, int64_t* launches, int32_t n);
 int rbmnqs_timing_reset(rbmnqs_handle* h, int32_t enable);
 /* Number of kernel launches one rbmnqs_epoch performs (kernel nodes of the

@@ -107,6 +107,8 @@ struct rbmnqs_handle {
     rbmnqs::model model;
     int n = 0, n_vb = 0, nh = 0, S = 0, T = 0, P = 0, P_neural = 0, N = 0, n_bins = 1;
     int fp64 = 0, wpb = 8, w_in_smem = 1;
+    rbmnqs::SamplerShape shape{};
+    uint32_t bond_thr24 = 0;
     int gram_ks = 1, mom_blocks = 1;
     cudaStream_t st = nullptr;
 
@@ -118,12 +120,14 @@ struct rbmnqs_handle {
     DevBuf<uint32_t> emask;
     DevBuf<double2> eval;
     DevBuf<int2> bonds;
-    DevBuf<uint32_t> spins, nacc, nprop, ctl;
+    DevBuf<uint32_t> spins, nacc, nprop, ctl, samples;
     DevBuf<double2> E;
     DevBuf<unsigned char> O;
     DevBuf<double2> pd, pf, pe, d, F, emean, part, Sm, Sreg;
     DevBuf<double> diag, maxdiag;
     DevBuf<rbmnqs::ScheduleDev> sched;
+    DevBuf<rbmnqs::MachineDev> mdev;
+    DevBuf<rbmnqs::HamDev> hdev;
     DevBuf<rbmnqs::CgResultDev> cgres;
     DevBuf<rbmnqs::EpochStatsDev> stats;
     int n_ops = 0, n_prop_bonds = 0;
@@ -132,7 +136,7 @@ struct rbmnqs_handle {
 
     cudaGraphExec_t graph = nullptr;
     int graph_kernels = 0;
-    static constexpr int kStages = 6;
+    static constexpr int kStages = 6;  // sampler, eval, moments+stats, gram+reg, cg, update
     cudaEvent_t ev[kStages + 1] = {};
     bool timing = false;
     double stage_ms[kStages] = {};
@@ -184,9 +188,11 @@ struct rbmnqs_handle {
         rbmnqs::SamplerArgs a{};
         a.m = machine();
         a.H = ham();
+        a.md = mdev.p;
+        a.hd = hdev.p;
         a.n_prop_bonds = n_prop_bonds;
         a.prop_bonds = bonds.p;
-        a.bond_flips = cfg.bond_flips;
+        a.bond_thr24 = bond_thr24;
         a.n_chains = cfg.n_chains;
         a.spc = cfg.samples_per_chain;
         a.warmup = cfg.warmup;
@@ -194,34 +200,45 @@ struct rbmnqs_handle {
         a.ctl = ctl.p;
         a.seed = cfg.seed;
         a.spins = spins.p;
-        a.E = E.p;
-        a.O = O.p;
+        a.samples = samples.p;
         a.n_acc = nacc.p;
         a.n_prop = nprop.p;
-        a.w_in_smem = w_in_smem;
         mark(0);
-        ck(rbmnqs::launch_sampler(a, fp64, wpb, st), "sampler kernel");
+        ck(rbmnqs::launch_sampler(a, fp64, shape, st), "sampler kernel");
         mark(1);
+        // E_loc and O_k of every sample (local_op::evaluate, derivative)
+        rbmnqs::EvalArgs ea{};
+        ea.m = machine();
+        ea.H = ham();
+        ea.md = mdev.p;
+        ea.hd = hdev.p;
+        ea.spins = samples.p;
+        ea.B = N;
+        ea.eloc = E.p;
+        ea.O = O.p;
+        ea.plan = rbmnqs::SmemPlan{0, w_in_smem, 0};
+        ck(rbmnqs::launch_eval(ea, fp64, wpb, st), "eval kernel");
+        mark(2);
         ck(rbmnqs::launch_moments(O.p, fp64, E.p, N, P, mom_blocks, pd.p, pf.p, pe.p, d.p, F.p, emean.p, st),
            "moments");
         ck(rbmnqs::launch_energy_stats(E.p, N, n_bins, emean.p, nacc.p, nprop.p, cfg.n_chains, stats.p, st),
            "energy stats");
         ck(rbmnqs::launch_advance(ctl.p, cfg.reinit_chains, st), "advance");
-        mark(2);
+        mark(3);
     }
     void enqueue_optimize() {
         ck(rbmnqs::launch_schedule(sched.p, st), "schedule");
         ck(rbmnqs::launch_gram_fp64(O.p, fp64, d.p, N, P, gram_ks, part.p, Sm.p, st), "gram");
         ck(rbmnqs::launch_regularize(Sm.p, P, P_neural, N, sched.p, diag.p, Sreg.p, maxdiag.p, st), "regularize");
-        mark(3);
+        mark(4);
         int max_it = std::min(2 * P, cfg.max_iterations);
         if (max_it == 0) max_it = 2 * P;
         const double rtol = cfg.rtol == 0 ? 1e-16 : cfg.rtol;
         ck(rbmnqs::launch_cg(Sreg.p, F.p, x.p, P, max_it, rtol, cgres.p, st), "cg");
-        mark(4);
+        mark(5);
         ck(rbmnqs::launch_update(params.p, x.p, P, sched.p, cgres.p, st), "update");
         ck(rbmnqs::launch_unpack(params.p, n, n_vb, nh, vb.p, hb.p, W64.p, W32.p, st), "unpack");
-        mark(5);
+        mark(6);
     }
     void collect_timing(int first, int last) {
         if (!timing) return;
@@ -451,6 +468,7 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         const uint32_t ctl0[2] = {0, 1};
         ck(cudaMemcpy(h->ctl.p, ctl0, sizeof(ctl0), cudaMemcpyHostToDevice), "c");
         h->E.alloc(h->N);
+        h->samples.alloc((size_t)h->N * 4);
         h->O.alloc((size_t)h->N * h->P * h->osize());
         h->mom_blocks = std::max(1, std::min(296, h->N / 64));
         h->pd.alloc((size_t)h->mom_blocks * h->P);
@@ -478,11 +496,29 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
             sd.min_reached[i] = src[i][2] == 1.0;
         }
         ck(cudaMemcpy(h->sched.p, &sd, sizeof(sd), cudaMemcpyHostToDevice), "c");
-        // launch shape: FP32 W in shared memory when it fits comfortably
-        h->w_in_smem = (size_t)n * nh * 8 <= 96 * 1024 ? 1 : 0;
+        // device copies of the machine / Hamiltonian descriptors
+        h->mdev.alloc(1);
+        h->hdev.alloc(1);
+        {
+            const rbmnqs::MachineDev md = h->machine();
+            const rbmnqs::HamDev hd = h->ham();
+            ck(cudaMemcpy(h->mdev.p, &md, sizeof(md), cudaMemcpyHostToDevice), "c");
+            ck(cudaMemcpy(h->hdev.p, &hd, sizeof(hd), cudaMemcpyHostToDevice), "c");
+        }
+        // launch shapes: persistent sampler blocks; evaluation kernels with
+        // FP32 W in shared memory when it fits
+        ck(rbmnqs::plan_sampler(h->machine(), h->fp64, cfg->n_chains, &h->shape), "sampler plan");
+        if (h->n_prop_bonds > 0 && cfg->bond_flips > 0) {
+            const double thr = std::ceil(cfg->bond_flips * 16777216.0);
+            h->bond_thr24 = (uint32_t)std::min(thr, 16777216.0);
+        }
+        h->w_in_smem = (size_t)n * nh * 8 <= 64 * 1024 ? 1 : 0;
         h->wpb = 8;
-        while (h->wpb > 1 && rbmnqs::sampler_smem_bytes(h->machine(), h->fp64, h->wpb, h->w_in_smem) > 200 * 1024)
-            h->wpb >>= 1;
+        {
+            rbmnqs::SmemPlan pl{0, h->w_in_smem, 0};
+            while (h->wpb > 1 && rbmnqs::sampler_smem_bytes(h->machine(), h->fp64, h->wpb, pl) > 200 * 1024)
+                h->wpb >>= 1;
+        }
         ck(cudaStreamSynchronize(h->st), "sync");
         *out = h.release();
     });
@@ -559,7 +595,7 @@ int rbmnqs_sample(rbmnqs_handle* h, rbmnqs_sample_stats* out) {
     return guard([&] {
         require(h != nullptr, "null handle");
         h->enqueue_sample();
-        h->collect_timing(0, 2);
+        h->collect_timing(0, 3);
         read_sample_stats(h, out);
         h->sampled = true;
     });
@@ -569,9 +605,9 @@ int rbmnqs_optimize(rbmnqs_handle* h, rbmnqs_sr_stats* out) {
     return guard([&] {
         require(h != nullptr, "null handle");
         require(h->sampled, "rbmnqs_optimize needs a preceding rbmnqs_sample");
-        if (h->timing) ck(cudaEventRecordWithFlags(h->ev[2], h->st, cudaEventRecordExternal), "event");
+        if (h->timing) ck(cudaEventRecordWithFlags(h->ev[3], h->st, cudaEventRecordExternal), "event");
         h->enqueue_optimize();
-        h->collect_timing(2, 5);
+        h->collect_timing(3, 6);
         read_sr_stats(h, out);
     });
 }
@@ -604,7 +640,7 @@ int rbmnqs_epoch(rbmnqs_handle* h, rbmnqs_sample_stats* s, rbmnqs_sr_stats* o) {
             cudaGraphDestroy(g);
         }
         ck(cudaGraphLaunch(h->graph, h->st), "graph launch");
-        h->collect_timing(0, 5);
+        h->collect_timing(0, 6);
         read_sample_stats(h, s);
         read_sr_stats(h, o);
         h->sampled = true;
@@ -676,9 +712,11 @@ static void eval_common(rbmnqs_handle* h, const uint32_t* spins, int B, double* 
     rbmnqs::EvalArgs a{};
     a.m = h->machine();
     a.H = h->ham();
+    a.md = h->mdev.p;
+    a.hd = h->hdev.p;
     a.spins = ds.p;
     a.B = B;
-    a.w_in_smem = h->w_in_smem;
+    a.plan = rbmnqs::SmemPlan{0, h->w_in_smem, 0};
     if (logpsi) {
         dl.alloc(B);
         a.logpsi = dl.p;

@@ -37,40 +37,35 @@ __device__ __forceinline__ void flip_bit(uint32_t sp[4], int i) {
     else sp[3] ^= b;
 }
 
-// Per-lane view of the theta entries it owns.
-template <int E> struct Slots {
-    int k[E], s[E];
-    bool v[E];
-    __device__ __forceinline__ void init(int lane, int T, int nh) {
-#pragma unroll
-        for (int e = 0; e < E; e++) {
-            const int t = lane + 32 * e;
-            v[e] = t < T;
-            const int tt = v[e] ? t : 0;
-            k[e] = tt % nh;
-            s[e] = tt / nh;
-        }
-    }
-};
+// Lane `lane` owns theta entries t = lane + 32 e (e < E), t = k + nh*s.
+__device__ __forceinline__ bool slot_valid(int lane, int e, int T) { return lane + 32 * e < T; }
 
 template <typename R>
 __device__ __forceinline__ int urow(const MachineDev& m, const uint8_t* sPerm, int f, int s) {
     return m.symmetric ? (int)sPerm[f * m.S + s] : f;
 }
 
+__device__ __forceinline__ int smem_bit(const uint32_t* wsp, int i) { return (wsp[i >> 5] >> (i & 31)) & 1; }
+
 // theta = b + W^T(P_s sigma) in FP64, rounded to R (rbm_base.cpp:161-172).
 template <int E, typename R>
-__device__ void theta_fp64(const MachineDev& m, const uint8_t* sPerm, const Slots<E>& sl,
+__device__ __forceinline__ void theta_fp64(const MachineDev& m, const double2* W64, const uint8_t* sPerm, int lane,
                            const uint32_t sp[4], C2<R> th[E]) {
     double2 acc[E];
+    int kk[E], ss[E];
 #pragma unroll
-    for (int e = 0; e < E; e++) acc[e] = sl.v[e] ? m.hb[sl.k[e]] : make_double2(0, 0);
+    for (int e = 0; e < E; e++) {
+        const int t = slot_valid(lane, e, m.T) ? lane + 32 * e : 0;
+        kk[e] = t % m.nh;
+        ss[e] = t / m.nh;
+        acc[e] = slot_valid(lane, e, m.T) ? m.hb[kk[e]] : make_double2(0, 0);
+    }
     for (int i = 0; i < m.n; i++) {
         const double sg = spin_bit(sp, i) ? -1.0 : 1.0;
 #pragma unroll
         for (int e = 0; e < E; e++) {
-            if (!sl.v[e]) continue;
-            const double2 w = m.W64[urow<R>(m, sPerm, i, sl.s[e]) * m.nh + sl.k[e]];
+            if (!slot_valid(lane, e, m.T)) continue;
+            const double2 w = W64[urow<R>(m, sPerm, i, ss[e]) * m.nh + kk[e]];
             acc[e].x = fma(sg, w.x, acc[e].x);
             acc[e].y = fma(sg, w.y, acc[e].y);
         }
@@ -80,7 +75,8 @@ __device__ void theta_fp64(const MachineDev& m, const uint8_t* sPerm, const Slot
 }
 
 // Bias part of log(psi'/psi): sum_f -2 sigma_f v[f mod n_vb]
-// (rbm_base.cpp:306-318).
+// (rbm_base.cpp:306-318), for configuration bits in registers or in the
+// warp's scratch.
 __device__ __forceinline__ double2 bias_delta(const MachineDev& m, const uint32_t sp[4], const int* fl, int nf) {
     double2 b = make_double2(0, 0);
     for (int q = 0; q < nf; q++) {
@@ -92,60 +88,75 @@ __device__ __forceinline__ double2 bias_delta(const MachineDev& m, const uint32_
     return b;
 }
 
-// psi(sigma with flips)/psi(sigma) for the RBM part, given the lane's theta
-// entries and the per-entry ln cosh cache (cre, cu) of the current theta.
-// Returns the real log-magnitude sum (without bias) and the phase product.
+__device__ __forceinline__ double2 bias_delta_smem(const MachineDev& m, const uint32_t* wsp, const int* fl, int nf) {
+    double2 b = make_double2(0, 0);
+    for (int q = 0; q < nf; q++) {
+        const double sg = smem_bit(wsp, fl[q]) ? -1.0 : 1.0;
+        const double2 v = m.vb[fl[q] % m.n_vb];
+        b.x -= 2.0 * sg * v.x;
+        b.y -= 2.0 * sg * v.y;
+    }
+    return b;
+}
+
+// psi(sigma with flips)/psi(sigma) for the RBM part from the warp's theta
+// (wth) and the per-entry ln cosh cache (cre, cu) of the current theta, all
+// in the warp's shared scratch.  Returns the real log-magnitude sum (without
+// bias) and the phase product.
 template <int E, typename R>
 __device__ __forceinline__ void ratio_terms(const MachineDev& m, const uint8_t* sPerm, const C2<R>* W,
-                                            const Slots<E>& sl, const C2<R> th[E], const uint32_t sp[4],
-                                            const int* fl, int nf, const R* cre, const C2<R>* cu, int lane,
-                                            R& dre, C2<R>& ph) {
+                                            const C2<R>* wth, const uint32_t* wsp, const int* fl, int nf,
+                                            const R* cre, const C2<R>* cu, int lane, R& dre, C2<R>& ph) {
     R sgn2[6];
-    for (int q = 0; q < nf; q++) sgn2[q] = spin_bit(sp, fl[q]) ? (R)2 : (R)-2;  // -2 sigma_f
+    for (int q = 0; q < nf; q++) sgn2[q] = smem_bit(wsp, fl[q]) ? (R)2 : (R)-2;  // -2 sigma_f
     dre = 0;
     ph = mk<R>(1, 0);
 #pragma unroll
     for (int e = 0; e < E; e++) {
-        if (!sl.v[e]) continue;
-        C2<R> t = th[e];
+        if (!slot_valid(lane, e, m.T)) continue;
+        const int t = lane + 32 * e, k = t % m.nh, s = t / m.nh;
+        C2<R> x = wth[t];
         for (int q = 0; q < nf; q++) {
-            const C2<R> u = W[urow<R>(m, sPerm, fl[q], sl.s[e]) * m.nh + sl.k[e]];
-            t.x = fma(sgn2[q], u.x, t.x);
-            t.y = fma(sgn2[q], u.y, t.y);
+            const C2<R> u = W[urow<R>(m, sPerm, fl[q], s) * m.nh + k];
+            x.x = fma(sgn2[q], u.x, x.x);
+            x.y = fma(sgn2[q], u.y, x.y);
         }
         R re, ux, uy;
-        lnc_full<R>(t.x, t.y, re, ux, uy);
-        const int tt = lane + 32 * e;
-        dre += re - cre[tt];
-        ph = cmul(ph, cmulc(mk<R>(ux, uy), cu[tt]));
+        lnc_full<R>(x.x, x.y, re, ux, uy);
+        dre += re - cre[t];
+        ph = cmul(ph, cmulc(mk<R>(ux, uy), cu[t]));
     }
     dre = warp_sum(dre);
     ph = warp_cprod(ph);
 }
 
-// E_loc and O_k of the warp's current configuration (local_op.cpp:31-60,
-// rbm_base.cpp:194-217, rbm_symmetry.cpp:97-130).
+// E_loc and O_k of the configuration in the warp's scratch (wsp bits, wth
+// theta): local_op.cpp:31-60, rbm_base.cpp:194-217, rbm_symmetry.cpp:97-130.
+// Kept out of line: it runs once per sample, the sweep loop keeps its
+// registers.
 template <int E, typename R>
-__device__ void evaluate(const MachineDev& m, const HamDev& H, const uint8_t* sPerm, const uint8_t* sInv,
-                         const C2<R>* W, const Slots<E>& sl, const C2<R> th[E], const uint32_t sp[4],
-                         uint32_t* wsp, R* cre, C2<R>* cu, int lane, double2* Eout, C2<R>* Orow) {
+__device__ __noinline__ void evaluate(const MachineDev* __restrict__ mp, const HamDev* __restrict__ hp,
+                                      const uint8_t* sPerm, const uint8_t* sInv, const C2<R>* W, const C2<R>* wth,
+                                      const uint32_t* wsp, R* cre, C2<R>* cu, int lane, double2* Eout, C2<R>* Orow) {
+    const MachineDev m = *mp;
+    const HamDev H = *hp;
     // ln cosh cache of the current theta
 #pragma unroll
     for (int e = 0; e < E; e++) {
-        if (!sl.v[e]) continue;
+        if (!slot_valid(lane, e, m.T)) continue;
+        const int t = lane + 32 * e;
         R re, ux, uy;
-        lnc_full<R>(th[e].x, th[e].y, re, ux, uy);
-        cre[lane + 32 * e] = re;
-        cu[lane + 32 * e] = mk<R>(ux, uy);
+        lnc_full<R>(wth[t].x, wth[t].y, re, ux, uy);
+        cre[t] = re;
+        cu[t] = mk<R>(ux, uy);
     }
-    if (lane < 4) wsp[lane] = sp[lane];
     __syncwarp();
     if (Eout) {
         double ex = 0, ey = 0;
         for (int o = 0; o < H.n_ops; o++) {
             const OpDev op = H.ops[o];
             int loc = 0;
-            for (int i = 0; i < op.k; i++) loc |= spin_bit(sp, op.sites[i]) << i;
+            for (int i = 0; i < op.k; i++) loc |= smem_bit(wsp, op.sites[i]) << i;
             const int q0 = H.rowptr[op.rp + loc], q1 = H.rowptr[op.rp + loc + 1];
             for (int q = q0; q < q1; q++) {
                 const uint32_t mask = H.ent_mask[q];
@@ -160,8 +171,8 @@ __device__ void evaluate(const MachineDev& m, const HamDev& H, const uint8_t* sP
                     if ((mask >> i) & 1) fl[nf++] = op.sites[i];
                 R dre;
                 C2<R> ph;
-                ratio_terms<E, R>(m, sPerm, W, sl, th, sp, fl, nf, cre, cu, lane, dre, ph);
-                const double2 b = bias_delta(m, sp, fl, nf);
+                ratio_terms<E, R>(m, sPerm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph);
+                const double2 b = bias_delta_smem(m, wsp, fl, nf);
                 const double mag = exp((double)dre + b.x);
                 double sb, cb;
                 sincos(b.y, &sb, &cb);
@@ -178,10 +189,13 @@ __device__ void evaluate(const MachineDev& m, const HamDev& H, const uint8_t* sP
         __syncwarp();
 #pragma unroll
         for (int e = 0; e < E; e++)
-            if (sl.v[e]) cu[lane + 32 * e] = ctanh_r<R>(th[e].x, th[e].y);
+            if (slot_valid(lane, e, m.T)) {
+                const int t = lane + 32 * e;
+                cu[t] = ctanh_r<R>(wth[t].x, wth[t].y);
+            }
         __syncwarp();
         const int n = m.n, nh = m.nh, S = m.S, nvb = m.n_vb;
-        auto sg = [&](int i) -> R { return ((wsp[i >> 5] >> (i & 31)) & 1) ? (R)-1 : (R)1; };
+        auto sg = [&](int i) -> R { return smem_bit(wsp, i) ? (R)-1 : (R)1; };
         if (!m.symmetric) {
             for (int q = lane; q < nvb; q += 32) Orow[q] = mk<R>(sg(q), 0);
             for (int q = lane; q < nh; q += 32) Orow[nvb + q] = cu[q];
@@ -223,86 +237,116 @@ __device__ void evaluate(const MachineDev& m, const HamDev& H, const uint8_t* sP
     __syncwarp();
 }
 
+// Publish the warp's configuration and theta to its scratch for evaluate().
+template <int E, typename R>
+__device__ __forceinline__ void stage(const MachineDev& m, const uint32_t sp[4], const C2<R> th[E], uint32_t* wsp,
+                                      C2<R>* wth, int lane) {
+    if (lane < 4) wsp[lane] = sp[lane];
+#pragma unroll
+    for (int e = 0; e < E; e++)
+        if (slot_valid(lane, e, m.T)) wth[lane + 32 * e] = th[e];
+    __syncwarp();
+}
+
 // ---------------------------------------------------------------------------
-// Shared-memory carve-up.
+// Shared-memory carve-up.  Block-wide tables (shared by every chain of the
+// block) followed by one scratch area per warp.  The same byte arithmetic
+// runs on host (launch sizing) and device (carving).
 struct Smem {
-    float2* W32;
-    uint8_t* perm;
-    uint8_t* inv;
+    float2* U;      // expanded FP32 flip table U[f*T + t] = W[P_s(f), k]
+    float2* W32;    // FP32 W, site-major
+    double2* W64;   // FP64 W, site-major (theta recompute)
+    uint8_t* perm;  // [n][S]
+    uint8_t* inv;   // [S][n]
+    float* bre;     // [n] Re v[f mod n_vb] (Metropolis bias term)
     unsigned char* warp0;
     int warp_bytes;
 };
 
 __host__ __device__ inline int align16(int x) { return (x + 15) & ~15; }
 
-__host__ __device__ inline int warp_bytes_for(int T, int rsize) { return align16(16 + T * rsize + T * 2 * rsize); }
+// per-warp scratch: spins (16 B) | theta [T] | ln cosh re [T] | phase / tanh [T]
+// | proposal ln|cosh| [T]
+__host__ __device__ inline int warp_bytes_for(int T, int rsize) { return align16(16 + T * 6 * rsize); }
 
-__host__ __device__ inline int table_bytes(const MachineDev& m, int fp64, int w_in_smem) {
+__host__ __device__ inline int table_bytes(const MachineDev& m, int fp64, const SmemPlan& pl) {
     int b = 0;
-    if (!fp64 && w_in_smem) b += align16(m.n * m.nh * 8);
+    if (pl.use_u) b += align16(m.n * m.T * 8);
+    if (!fp64 && pl.w32) b += align16(m.n * m.nh * 8);
+    if (pl.w64) b += align16(m.n * m.nh * 16);
     if (m.symmetric) b += align16(m.n * m.S) * 2;
+    b += align16(m.n * 4);
     return b;
 }
 
-__device__ inline Smem carve(unsigned char* base, const MachineDev& m, int fp64, int w_in_smem, int rsize) {
-    Smem s;
+__device__ inline Smem carve(unsigned char* base, const MachineDev& m, int fp64, const SmemPlan& pl, int rsize) {
+    Smem s{};
     int off = 0;
-    s.W32 = nullptr;
-    if (!fp64 && w_in_smem) {
+    if (pl.use_u) {
+        s.U = reinterpret_cast<float2*>(base + off);
+        off += align16(m.n * m.T * 8);
+    }
+    if (!fp64 && pl.w32) {
         s.W32 = reinterpret_cast<float2*>(base + off);
         off += align16(m.n * m.nh * 8);
     }
-    s.perm = s.inv = nullptr;
+    if (pl.w64) {
+        s.W64 = reinterpret_cast<double2*>(base + off);
+        off += align16(m.n * m.nh * 16);
+    }
     if (m.symmetric) {
         s.perm = base + off;
         off += align16(m.n * m.S);
         s.inv = base + off;
         off += align16(m.n * m.S);
     }
+    s.bre = reinterpret_cast<float*>(base + off);
+    off += align16(m.n * 4);
     s.warp0 = base + off;
     s.warp_bytes = warp_bytes_for(m.T, rsize);
     return s;
 }
 
-__device__ inline void load_tables(const MachineDev& m, const Smem& s, int fp64, int w_in_smem) {
+__device__ inline void load_tables(const MachineDev& m, const Smem& s, int fp64, const SmemPlan& pl) {
     const int tid = threadIdx.x, nt = blockDim.x;
-    if (!fp64 && w_in_smem)
+    if (!fp64 && pl.w32)
         for (int i = tid; i < m.n * m.nh; i += nt) s.W32[i] = m.W32[i];
+    if (pl.w64)
+        for (int i = tid; i < m.n * m.nh; i += nt) s.W64[i] = m.W64[i];
     if (m.symmetric)
         for (int i = tid; i < m.n * m.S; i += nt) {
             s.perm[i] = m.perm[i];
             s.inv[i] = m.inv[i];
         }
+    for (int i = tid; i < m.n; i += nt) s.bre[i] = (float)m.vb[i % m.n_vb].x;
+    if (pl.use_u)
+        for (int i = tid; i < m.n * m.T; i += nt) {
+            const int f = i / m.T, t = i % m.T;
+            const int k = t % m.nh, sy = t / m.nh;
+            const int row = m.symmetric ? (int)m.perm[f * m.S + sy] : f;
+            s.U[i] = m.W32[row * m.nh + k];
+        }
     __syncthreads();
 }
 
-// ---------------------------------------------------------------------------
-// metropolis_sampler::sample_chain for every chain at once
-// (metropolis_sampler.cpp:118-273).  Randomness: Philox4x32-10 with counter
-// {proposal, epoch, chain, 0}; lane j draws proposal (base + j) so one
+// One chain: metropolis_sampler::sample_chain (metropolis_sampler.cpp:118-273)
+// for the warp's chain.  Sampled configurations (16 bytes each) are recorded
+// and evaluated afterwards by eval_kernel, one warp per sample: calling the
+// evaluation from inside the sweep loop would make the call's register saves
+// push the loop's live state (theta, ln cosh, bits) to local memory.  Randomness: Philox4x32-10 with counter
+// {proposal, epoch, chain, 0}; lane j draws proposal (base + j), so one
 // Philox call per lane serves 32 proposals.
-template <int E, typename R>
-__global__ void __launch_bounds__(256) sampler_kernel(const SamplerArgs a) {
-    extern __shared__ __align__(16) unsigned char smem[];
+template <int E, typename R, bool EXP>
+__device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, int chain, int lane, uint32_t* wsp,
+                                          C2<R>* wth, R* cre, C2<R>* cu, R* wlp) {
     const MachineDev& m = a.m;
-    const int fp64 = sizeof(R) == 8;
-    Smem sm = carve(smem, m, fp64, a.w_in_smem, sizeof(R));
-    load_tables(m, sm, fp64, a.w_in_smem);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int chain = blockIdx.x * (blockDim.x >> 5) + warp;
-    if (chain >= a.n_chains) return;
-
-    unsigned char* wbase = sm.warp0 + warp * sm.warp_bytes;
-    uint32_t* wsp = reinterpret_cast<uint32_t*>(wbase);
-    R* cre = reinterpret_cast<R*>(wbase + 16);
-    C2<R>* cu = reinterpret_cast<C2<R>*>(wbase + 16 + m.T * sizeof(R));
-    const C2<R>* W = Wsel<R>::get(m, a.w_in_smem ? sm.W32 : m.W32);
-
+    const C2<R>* W = Wsel<R>::get(m, sm.W32 ? sm.W32 : m.W32);
+    const double2* W64 = sm.W64 ? sm.W64 : m.W64;
     const uint2 key = make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32));
     const uint32_t epoch = a.ctl[0];
     uint32_t sp[4];
     if (a.ctl[1]) {
-        const uint4 r = philox4x32(make_uint4(0, epoch, (uint32_t)chain, 1), key);
+        const uint4 r = philox4x32(make_uint4(0, epoch, (uint32_t)chain, 1), key);  // stream 1: initial bits
         const uint32_t rw[4] = {r.x, r.y, r.z, r.w};
 #pragma unroll
         for (int w = 0; w < 4; w++) {
@@ -315,23 +359,32 @@ __global__ void __launch_bounds__(256) sampler_kernel(const SamplerArgs a) {
         for (int w = 0; w < 4; w++) sp[w] = a.spins[4 * chain + w];
     }
 
-    Slots<E> sl;
-    sl.init(lane, m.T, m.nh);
     C2<R> th[E];
-    R L[E], Lp[E];
-    theta_fp64<E, R>(m, sm.perm, sl, sp, th);
+    R L[E];
+    theta_fp64<E, R>(m, W64, sm.perm, lane, sp, th);
 #pragma unroll
-    for (int e = 0; e < E; e++) L[e] = sl.v[e] ? lnc_re<R>(th[e].x, th[e].y) : (R)0;
+    for (int e = 0; e < E; e++) L[e] = slot_valid(lane, e, m.T) ? lnc_re<R>(th[e].x, th[e].y) : (R)0;
+
+    // U(f, e): the flip row of site f for this lane's entry e
+    auto U = [&](int f, int e) -> C2<R> {
+        if constexpr (EXP) {
+            const float2 u = sm.U[f * m.T + lane + 32 * e];
+            return mk<R>(u.x, u.y);
+        } else {
+            const int t = lane + 32 * e;
+            return W[urow<R>(m, sm.perm, f, t / m.nh) * m.nh + t % m.nh];
+        }
+    };
 
     const int n = m.n;
     // warm-up sweeps run every epoch, as in the reference; persistent chains
     // only differ in starting from the previous epoch's configuration
     const int warmup = a.warmup;
-    const long total = (long)a.spc * a.step + warmup;
+    const int total = a.spc * a.step + warmup;
     uint32_t prop = 0, nacc = 0;
     uint32_t rr0 = 0, rr1 = 0, rr2 = 0;
-    const bool bonds = a.n_prop_bonds > 0 && a.bond_flips > 0;
-    for (long st = 0; st < total; st++) {
+    const uint32_t thr = a.bond_thr24;  // bond proposal iff (r0 >> 8) < thr
+    for (int st = 0; st < total; st++) {
         int slot = 0;
         while (slot < n) {
             if ((prop & 31u) == 0) {
@@ -346,7 +399,7 @@ __global__ void __launch_bounds__(256) sampler_kernel(const SamplerArgs a) {
             const uint32_t r2 = __shfl_sync(kFull, rr2, src);
             prop++;
             int f0, f1 = -1;
-            if (bonds && unit24<double>(r0) < a.bond_flips) {
+            if ((r0 >> 8) < thr) {
                 const int2 b = a.prop_bonds[pick(r1, (uint32_t)a.n_prop_bonds)];
                 f0 = b.x;
                 f1 = b.y;
@@ -355,43 +408,49 @@ __global__ void __launch_bounds__(256) sampler_kernel(const SamplerArgs a) {
                 f0 = (int)pick(r1, (uint32_t)n);
                 slot += 1;
             }
-            const R g0 = spin_bit(sp, f0) ? (R)2 : (R)-2;
-            const R g1 = (f1 >= 0 && spin_bit(sp, f1)) ? (R)2 : (R)-2;
+            const bool s0 = spin_bit(sp, f0), s1 = f1 >= 0 && spin_bit(sp, f1);
+            const R g0 = s0 ? (R)2 : (R)-2;  // -2 sigma_f
+            const R g1 = s1 ? (R)2 : (R)-2;
             R d = 0;
 #pragma unroll
             for (int e = 0; e < E; e++) {
-                if (!sl.v[e]) continue;
+                if (!slot_valid(lane, e, m.T)) continue;
                 C2<R> t = th[e];
-                const C2<R> u0 = W[urow<R>(m, sm.perm, f0, sl.s[e]) * m.nh + sl.k[e]];
+                const C2<R> u0 = U(f0, e);
                 t.x = fma(g0, u0.x, t.x);
                 t.y = fma(g0, u0.y, t.y);
                 if (f1 >= 0) {
-                    const C2<R> u1 = W[urow<R>(m, sm.perm, f1, sl.s[e]) * m.nh + sl.k[e]];
+                    const C2<R> u1 = U(f1, e);
                     t.x = fma(g1, u1.x, t.x);
                     t.y = fma(g1, u1.y, t.y);
                 }
-                Lp[e] = lnc_re<R>(t.x, t.y);
-                d += Lp[e] - L[e];
+                const R lp = lnc_re<R>(t.x, t.y);
+                wlp[lane + 32 * e] = lp;  // read back only if accepted
+                d += lp - L[e];
             }
             d = warp_sum(d);
-            {
+            // bias: -2 sigma_f Re v[f mod n_vb] (rbm_base.cpp:306-318)
+            if constexpr (sizeof(R) == 4) {
+                d += g0 * sm.bre[f0];
+                if (f1 >= 0) d += g1 * sm.bre[f1];
+            } else {
                 const int fl[2] = {f0, f1};
-                d += (R)bias_delta(m, sp, fl, f1 >= 0 ? 2 : 1).x;
+                d += bias_delta(m, sp, fl, f1 >= 0 ? 2 : 1).x;
             }
             // accept with min(1, |psi'/psi|^2) (metropolis_sampler.cpp:223-243)
-            if (unit24<R>(r2) < exp((R)2 * d)) {
+            if (unit24<R>(r2) < exp_r((R)2 * d)) {
 #pragma unroll
                 for (int e = 0; e < E; e++) {
-                    if (!sl.v[e]) continue;
-                    const C2<R> u0 = W[urow<R>(m, sm.perm, f0, sl.s[e]) * m.nh + sl.k[e]];
+                    if (!slot_valid(lane, e, m.T)) continue;
+                    const C2<R> u0 = U(f0, e);
                     th[e].x = fma(g0, u0.x, th[e].x);
                     th[e].y = fma(g0, u0.y, th[e].y);
                     if (f1 >= 0) {
-                        const C2<R> u1 = W[urow<R>(m, sm.perm, f1, sl.s[e]) * m.nh + sl.k[e]];
+                        const C2<R> u1 = U(f1, e);
                         th[e].x = fma(g1, u1.x, th[e].x);
                         th[e].y = fma(g1, u1.y, th[e].y);
                     }
-                    L[e] = Lp[e];
+                    L[e] = wlp[lane + 32 * e];
                 }
                 flip_bit(sp, f0);
                 if (f1 >= 0) flip_bit(sp, f1);
@@ -399,15 +458,13 @@ __global__ void __launch_bounds__(256) sampler_kernel(const SamplerArgs a) {
             }
         }
         // FP64 recompute of theta once per sweep
-        theta_fp64<E, R>(m, sm.perm, sl, sp, th);
+        theta_fp64<E, R>(m, W64, sm.perm, lane, sp, th);
 #pragma unroll
-        for (int e = 0; e < E; e++) L[e] = sl.v[e] ? lnc_re<R>(th[e].x, th[e].y) : (R)0;
+        for (int e = 0; e < E; e++) L[e] = slot_valid(lane, e, m.T) ? lnc_re<R>(th[e].x, th[e].y) : (R)0;
         if (st >= warmup && (st - warmup) % a.step == 0) {
-            const long j = (st - warmup) / a.step;
+            const int j = (st - warmup) / a.step;
             const size_t idx = (size_t)chain * a.spc + j;
-            C2<R>* Orow = a.O ? reinterpret_cast<C2<R>*>(a.O) + idx * m.P : nullptr;
-            evaluate<E, R>(m, a.H, sm.perm, sm.inv, W, sl, th, sp, wsp, cre, cu, lane, a.E ? a.E + idx : nullptr,
-                           Orow);
+            if (lane < 4) a.samples[4 * idx + lane] = sp[lane];
         }
     }
     if (lane < 4) a.spins[4 * chain + lane] = sp[lane];
@@ -415,6 +472,33 @@ __global__ void __launch_bounds__(256) sampler_kernel(const SamplerArgs a) {
         a.n_acc[chain] = nacc;
         a.n_prop[chain] = prop;
     }
+}
+
+// Thread bound per entries-per-lane: 28 warps (896 threads, 72 registers)
+// keep 4096 chains resident on 148 SMs for E <= 4.
+template <int E> struct MaxThreads {
+    static constexpr int v = E <= 2 ? 1024 : (E <= 4 ? 896 : (E <= 8 ? 512 : 256));
+};
+
+// All chains at once, persistent warps: global warp g = warp * gridDim.x +
+// blockIdx.x takes chains g, g + total_warps, ... so consecutive chains land
+// on different SMs and every block holds the tables once.
+template <int E, typename R, bool EXP>
+__global__ void __launch_bounds__(MaxThreads<E>::v, 1) sampler_kernel(const SamplerArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int fp64 = sizeof(R) == 8;
+    Smem sm = carve(smem, a.m, fp64, a.plan, sizeof(R));
+    load_tables(a.m, sm, fp64, a.plan);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* wbase = sm.warp0 + warp * sm.warp_bytes;
+    uint32_t* wsp = reinterpret_cast<uint32_t*>(wbase);
+    C2<R>* wth = reinterpret_cast<C2<R>*>(wbase + 16);
+    R* cre = reinterpret_cast<R*>(wbase + 16 + a.m.T * 2 * sizeof(R));
+    C2<R>* cu = reinterpret_cast<C2<R>*>(wbase + 16 + a.m.T * 3 * sizeof(R));
+    R* wlp = reinterpret_cast<R*>(wbase + 16 + a.m.T * 5 * sizeof(R));
+    const int total_warps = (blockDim.x >> 5) * gridDim.x;
+    for (int chain = warp * gridDim.x + blockIdx.x; chain < a.n_chains; chain += total_warps)
+        run_chain<E, R, EXP>(a, sm, chain, lane, wsp, wth, cre, cu, wlp);
 }
 
 // ---------------------------------------------------------------------------
@@ -425,23 +509,23 @@ __global__ void __launch_bounds__(256) eval_kernel(const EvalArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const MachineDev& m = a.m;
     const int fp64 = sizeof(R) == 8;
-    Smem sm = carve(smem, m, fp64, a.w_in_smem, sizeof(R));
-    load_tables(m, sm, fp64, a.w_in_smem);
+    Smem sm = carve(smem, m, fp64, a.plan, sizeof(R));
+    load_tables(m, sm, fp64, a.plan);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b = blockIdx.x * (blockDim.x >> 5) + warp;
     if (b >= a.B) return;
     unsigned char* wbase = sm.warp0 + warp * sm.warp_bytes;
     uint32_t* wsp = reinterpret_cast<uint32_t*>(wbase);
-    R* cre = reinterpret_cast<R*>(wbase + 16);
-    C2<R>* cu = reinterpret_cast<C2<R>*>(wbase + 16 + m.T * sizeof(R));
-    const C2<R>* W = Wsel<R>::get(m, a.w_in_smem ? sm.W32 : m.W32);
+    C2<R>* wth = reinterpret_cast<C2<R>*>(wbase + 16);
+    R* cre = reinterpret_cast<R*>(wbase + 16 + m.T * 2 * sizeof(R));
+    C2<R>* cu = reinterpret_cast<C2<R>*>(wbase + 16 + m.T * 3 * sizeof(R));
+    const C2<R>* W = Wsel<R>::get(m, sm.W32 ? sm.W32 : m.W32);
     uint32_t sp[4];
 #pragma unroll
     for (int w = 0; w < 4; w++) sp[w] = a.spins[4 * b + w];
-    Slots<E> sl;
-    sl.init(lane, m.T, m.nh);
     C2<R> th[E];
-    theta_fp64<E, R>(m, sm.perm, sl, sp, th);
+    theta_fp64<E, R>(m, m.W64, sm.perm, lane, sp, th);
+    stage<E, R>(m, sp, th, wsp, wth, lane);
 
     if (a.logpsi) {
         // log psi = bias + sum ln cosh theta (rbm_base.cpp:294-304,
@@ -449,7 +533,7 @@ __global__ void __launch_bounds__(256) eval_kernel(const EvalArgs a) {
         R re = 0, im = 0;
 #pragma unroll
         for (int e = 0; e < E; e++) {
-            if (!sl.v[e]) continue;
+            if (!slot_valid(lane, e, m.T)) continue;
             R r, ux, uy;
             lnc_full<R>(th[e].x, th[e].y, r, ux, uy);
             re += r;
@@ -475,7 +559,7 @@ __global__ void __launch_bounds__(256) eval_kernel(const EvalArgs a) {
     if (a.ratio) {
 #pragma unroll
         for (int e = 0; e < E; e++) {
-            if (!sl.v[e]) continue;
+            if (!slot_valid(lane, e, m.T)) continue;
             R r, ux, uy;
             lnc_full<R>(th[e].x, th[e].y, r, ux, uy);
             cre[lane + 32 * e] = r;
@@ -487,20 +571,20 @@ __global__ void __launch_bounds__(256) eval_kernel(const EvalArgs a) {
         for (int q = 0; q < nf; q++) fl[q] = a.flips[b * nf + q];
         R dre;
         C2<R> ph;
-        ratio_terms<E, R>(m, sm.perm, W, sl, th, sp, fl, nf, cre, cu, lane, dre, ph);
+        ratio_terms<E, R>(m, sm.perm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph);
         if (lane == 0) {
-            const double2 bd = bias_delta(m, sp, fl, nf);
+            const double2 bd = bias_delta_smem(m, wsp, fl, nf);
             a.ratio[b] = make_double2((double)dre + bd.x, atan2((double)ph.y, (double)ph.x) + bd.y);
         }
         __syncwarp();
     }
     if (a.eloc || a.O) {
         C2<R>* Orow = a.O ? reinterpret_cast<C2<R>*>(a.O) + (size_t)b * m.P : nullptr;
-        evaluate<E, R>(m, a.H, sm.perm, sm.inv, W, sl, th, sp, wsp, cre, cu, lane, a.eloc ? a.eloc + b : nullptr,
-                       Orow);
+        evaluate<E, R>(a.md, a.hd, sm.perm, sm.inv, W, wth, wsp, cre, cu, lane, a.eloc ? a.eloc + b : nullptr, Orow);
     }
 }
 
+// ---------------------------------------------------------------------------
 // Special-function-unit throughput probe: each thread runs `iters` rounds of
 // four independent ex2/lg2/sin/cos chains.  Used as the measured peak for
 // the sampler's roofline (its ln cosh work is MUFU-bound, not HBM/tensor).
@@ -542,23 +626,82 @@ int elements_per_lane(int T) {
     return -1;
 }
 
-int sampler_smem_bytes(const MachineDev& m, int fp64, int warps, int w_in_smem) {
-    return table_bytes(m, fp64, w_in_smem) + warps * warp_bytes_for(m.T, fp64 ? 8 : 4);
+int sampler_smem_bytes(const MachineDev& m, int fp64, int warps, const SmemPlan& plan) {
+    return table_bytes(m, fp64, plan) + warps * warp_bytes_for(m.T, fp64 ? 8 : 4);
 }
 
-template <int E, typename R>
-static cudaError_t launch_s(const SamplerArgs& a, int wpb, cudaStream_t st) {
-    const int smem = sampler_smem_bytes(a.m, sizeof(R) == 8, wpb, a.w_in_smem);
-    cudaError_t err = cudaFuncSetAttribute(sampler_kernel<E, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+template <int E, typename R, bool EXP> static const void* sampler_fn() {
+    return reinterpret_cast<const void*>(sampler_kernel<E, R, EXP>);
+}
+
+static const void* pick_sampler(int E, int fp64, int exp_table) {
+#define RBMNQS_PICK(EE)                                                   \
+    if (E == EE) {                                                        \
+        if (fp64) return sampler_fn<EE, double, false>();                 \
+        return exp_table ? sampler_fn<EE, float, true>() : sampler_fn<EE, float, false>(); \
+    }
+    RBMNQS_PICK(1) RBMNQS_PICK(2) RBMNQS_PICK(4) RBMNQS_PICK(8) RBMNQS_PICK(16)
+#undef RBMNQS_PICK
+    return nullptr;
+}
+
+cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, SamplerShape* out) {
+    const int E = elements_per_lane(m.T);
+    if (E < 0) return cudaErrorInvalidValue;
+    int dev = 0, sms = 0, smem_max = 0;
+    cudaError_t err = cudaGetDevice(&dev);
     if (err != cudaSuccess) return err;
-    const int blocks = (a.n_chains + wpb - 1) / wpb;
-    sampler_kernel<E, R><<<blocks, 32 * wpb, smem, st>>>(a);
-    return cudaGetLastError();
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    SmemPlan pl{};
+    const int budget = smem_max - 16 * 1024;
+    pl.w32 = !fp64 && m.n * m.nh * 8 <= 64 * 1024;
+    pl.w64 = m.n * m.nh * 16 <= 32 * 1024;
+    pl.use_u = !fp64 && pl.w32 && m.n * m.T * 8 <= 64 * 1024;
+    const void* fn = pick_sampler(E, fp64, pl.use_u);
+    cudaFuncAttributes fa;
+    err = cudaFuncGetAttributes(&fa, fn);
+    if (err != cudaSuccess) return err;
+    // warps per block: enough for one block per SM to hold every chain,
+    // limited by the kernel's thread bound, registers and shared memory
+    int want = (n_chains + sms - 1) / sms;
+    int wpb = fa.maxThreadsPerBlock / 32;
+    const int regs = fa.numRegs > 0 ? fa.numRegs : 64;
+    const int reg_warps = 65536 / (regs * 32);
+    if (wpb > reg_warps) wpb = reg_warps;
+    if (wpb > want) wpb = want;
+    if (wpb < 1) wpb = 1;
+    while (wpb > 1 && sampler_smem_bytes(m, fp64, wpb, pl) > budget) wpb--;
+    const int smem = sampler_smem_bytes(m, fp64, wpb, pl);
+    if (smem > budget) return cudaErrorInvalidValue;
+    err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (err != cudaSuccess) return err;
+    int per_sm = 0;
+    err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, smem);
+    if (err != cudaSuccess) return err;
+    if (per_sm < 1) per_sm = 1;
+    long blocks = ((long)n_chains + wpb - 1) / wpb;
+    if (blocks > (long)sms * per_sm) blocks = (long)sms * per_sm;
+    out->plan = pl;
+    out->warps_per_block = wpb;
+    out->blocks = (int)blocks;
+    out->smem = smem;
+    return cudaSuccess;
+}
+
+cudaError_t launch_sampler(const SamplerArgs& a0, int fp64, const SamplerShape& sh, cudaStream_t st) {
+    SamplerArgs a = a0;
+    a.plan = sh.plan;
+    const int E = elements_per_lane(a.m.T);
+    const void* fn = pick_sampler(E, fp64, sh.plan.use_u);
+    if (!fn) return cudaErrorInvalidValue;
+    void* args[] = {&a};
+    return cudaLaunchKernel(fn, dim3(sh.blocks), dim3(32 * sh.warps_per_block), args, sh.smem, st);
 }
 
 template <int E, typename R>
 static cudaError_t launch_e(const EvalArgs& a, int wpb, cudaStream_t st) {
-    const int smem = sampler_smem_bytes(a.m, sizeof(R) == 8, wpb, a.w_in_smem);
+    const int smem = sampler_smem_bytes(a.m, sizeof(R) == 8, wpb, a.plan);
     cudaError_t err = cudaFuncSetAttribute(eval_kernel<E, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (err != cudaSuccess) return err;
     const int blocks = (a.B + wpb - 1) / wpb;
@@ -575,10 +718,6 @@ static cudaError_t launch_e(const EvalArgs& a, int wpb, cudaStream_t st) {
         case 16: return fp64 ? FN<16, double>(ARGS, wpb, st) : FN<16, float>(ARGS, wpb, st); \
         default: return cudaErrorInvalidValue;                               \
     }
-
-cudaError_t launch_sampler(const SamplerArgs& a, int fp64, int wpb, cudaStream_t st) {
-    RBMNQS_DISPATCH(launch_s, a)
-}
 
 cudaError_t launch_eval(const EvalArgs& a, int fp64, int wpb, cudaStream_t st) {
     RBMNQS_DISPATCH(launch_e, a)

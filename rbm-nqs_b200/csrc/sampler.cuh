@@ -36,13 +36,23 @@ struct HamDev {
     const double2* ent_val;
 };
 
+// Which tables live in shared memory (decided on the host from their sizes).
+struct SmemPlan {
+    int use_u;  // expanded FP32 flip table U[n][T]
+    int w32;    // FP32 W
+    int w64;    // FP64 W
+};
+
 struct SamplerArgs {
     MachineDev m;
     HamDev H;
+    const MachineDev* md;  // device copies of m and H for the out-of-line
+    const HamDev* hd;      // per-sample evaluation
     // proposals (metropolis_sampler.cpp:145-219)
     int n_prop_bonds;
     const int2* prop_bonds;
-    double bond_flips;
+    uint32_t bond_thr24;  // bond proposal iff (r >> 8) < bond_thr24, i.e.
+                          // unit24(r) < bond_flips (0 disables bonds)
     // schedule
     int n_chains, spc, warmup, step;
     const uint32_t* ctl;  // device {epoch, init}: advanced in-stream so a
@@ -51,16 +61,18 @@ struct SamplerArgs {
     // state
     uint32_t* spins;  // [n_chains][4]
     // outputs
-    double2* E;       // [n_chains*spc]
-    void* O;          // [n_chains*spc][P] float2 (mixed) or double2 (FP64)
+    uint32_t* samples;  // [n_chains*spc][4] sampled configurations, evaluated
+                        // afterwards by the batched E_loc / O_k kernel
     uint32_t* n_acc;  // [n_chains]
     uint32_t* n_prop; // [n_chains]
-    int w_in_smem;    // FP32 W staged in shared memory
+    SmemPlan plan;
 };
 
 struct EvalArgs {
     MachineDev m;
     HamDev H;
+    const MachineDev* md;
+    const HamDev* hd;
     const uint32_t* spins;  // [B][4]
     int B;
     double2* logpsi;        // may be null
@@ -69,12 +81,22 @@ struct EvalArgs {
     const int* flips;       // ratio mode: [B][n_flips]
     int n_flips;
     double2* ratio;         // ratio mode output (log psi'/psi)
-    int w_in_smem;
+    SmemPlan plan;
 };
 
 // Launch helpers implemented in sampler.cu
-int sampler_smem_bytes(const MachineDev& m, int fp64, int warps, int w_in_smem);
-cudaError_t launch_sampler(const SamplerArgs& a, int fp64, int warps_per_block, cudaStream_t st);
+int sampler_smem_bytes(const MachineDev& m, int fp64, int warps, const SmemPlan& plan);
+// Plan + launch shape of the sampler for this machine and chain count:
+// one persistent block per SM with enough warps to hold every chain when
+// registers allow.
+struct SamplerShape {
+    SmemPlan plan;
+    int warps_per_block;
+    int blocks;
+    int smem;
+};
+cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, SamplerShape* out);
+cudaError_t launch_sampler(const SamplerArgs& a, int fp64, const SamplerShape& shape, cudaStream_t st);
 cudaError_t launch_eval(const EvalArgs& a, int fp64, int warps_per_block, cudaStream_t st);
 int elements_per_lane(int T);
 cudaError_t launch_advance(uint32_t* ctl, int reinit, cudaStream_t st);

@@ -391,6 +391,165 @@ __global__ void __launch_bounds__(1024) cg_dense(const double2* A, const double2
     }
 }
 
+// Same iteration with S_reg resident in shared memory as its packed upper
+// triangle (row i holds S_ij, j >= i, at off(i) + j - i with
+// off(i) = i P - i(i-1)/2; S_ji = conj(S_ij)).  Fits for P <= 157.
+// Work split: 8 lanes per matrix row (each lane ~P/8 complex MACs, a 3-level
+// shuffle finishes the row); p^H Ap is accumulated in the matvec epilogue;
+// block sums go through one partial per warp reduced with shuffles, so one
+// iteration costs three barriers.
+__host__ __device__ inline size_t packed_size(int P) { return (size_t)P * (P + 1) / 2; }
+
+__device__ __forceinline__ double2 shfl_xor2(double2 v, int o) {
+    return make_double2(__shfl_xor_sync(kFull, v.x, o), __shfl_xor_sync(kFull, v.y, o));
+}
+
+// Sum of the per-warp partials part[0..nw) seen by every thread.
+__device__ __forceinline__ double2 sum_partials2(const double2* part, int nw) {
+    const int lane = threadIdx.x & 31;
+    double2 v = lane < nw ? part[lane] : make_double2(0, 0);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double2 w = shfl_xor2(v, o);
+        v.x += w.x;
+        v.y += w.y;
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(1024) cg_packed(const double2* A, const double2* b, double2* xg, int P, int max_it,
+                                                  double rtol, CgResultDev* res) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    double2* U = reinterpret_cast<double2*>(sm);
+    double2* r = U + packed_size(P);
+    double2* p = r + P;
+    double2* Ap = p + P;
+    double2* x = Ap + P;
+    __shared__ double2 partA[32], partB[32];
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
+    const int sub = lane & 7;  // lane within the 8-lane row group
+    for (int i = w; i < P; i += nw) {
+        const size_t o = (size_t)i * P - (size_t)i * (i - 1) / 2;
+        for (int j = i + lane; j < P; j += 32) U[o + j - i] = A[(size_t)i * P + j];
+    }
+    for (int i = tid; i < P; i += nt) {
+        x[i] = xg[i];
+        p[i] = xg[i];
+    }
+    __syncthreads();
+    // Ap = A p; returns this thread's share of p^H Ap (summed over rows it
+    // finished), caller reduces
+    auto matvec = [&]() -> double2 {
+        double2 pap = make_double2(0, 0);
+        // warp-uniform trip count: warp w covers rows r0 .. r0+3 of each
+        // block of 4 * nw rows; lanes of rows >= P compute nothing but still
+        // join every shuffle
+        for (int r0 = 4 * w; r0 < P; r0 += 4 * nw) {
+            const int row = r0 + (lane >> 3);
+            const bool ok = row < P;
+            double sx = 0, sy = 0;
+            if (ok) {
+                const size_t orow = (size_t)row * P - (size_t)row * (row - 1) / 2;
+                for (int j = sub; j < P; j += 8) {
+                    double2 a;
+                    if (j >= row) {
+                        a = U[orow + j - row];
+                    } else {
+                        const double2 t = U[(size_t)j * P - (size_t)j * (j - 1) / 2 + row - j];
+                        a = make_double2(t.x, -t.y);
+                    }
+                    const double2 vv = p[j];
+                    sx = fma(a.x, vv.x, fma(-a.y, vv.y, sx));
+                    sy = fma(a.x, vv.y, fma(a.y, vv.x, sy));
+                }
+            }
+#pragma unroll
+            for (int o = 4; o > 0; o >>= 1) {
+                sx += __shfl_xor_sync(kFull, sx, o);
+                sy += __shfl_xor_sync(kFull, sy, o);
+            }
+            if (ok && sub == 0) {
+                Ap[row] = make_double2(sx, sy);
+                const double2 pr = p[row];
+                pap.x += pr.x * sx + pr.y * sy;  // conj(p) * Ap
+                pap.y += pr.x * sy - pr.y * sx;
+            }
+        }
+        return pap;
+    };
+    auto warp_total2 = [&](double2 v) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double2 t = shfl_xor2(v, o);
+            v.x += t.x;
+            v.y += t.y;
+        }
+        return v;
+    };
+    (void)matvec();
+    __syncthreads();
+    double rs0 = 0;
+    for (int i = tid; i < P; i += nt) {
+        const double2 ri = make_double2(b[i].x - Ap[i].x, b[i].y - Ap[i].y);
+        r[i] = ri;
+        p[i] = ri;
+        rs0 += ri.x * ri.x + ri.y * ri.y;
+    }
+    {
+        const double2 t = warp_total2(make_double2(rs0, 0));
+        if (lane == 0) partB[w] = t;
+    }
+    __syncthreads();
+    double rsold = sum_partials2(partB, nw).x;
+    double rs = rsold;
+    int itn = 0;
+    for (itn = 0; itn < max_it; itn++) {
+        // (1) Ap = A p and p^H Ap
+        {
+            const double2 t = warp_total2(matvec());
+            if (lane == 0) partA[w] = t;
+        }
+        __syncthreads();
+        // (2) alpha, x += alpha p, r -= alpha Ap, ||r||^2
+        const double2 pap = sum_partials2(partA, nw);
+        const double den = pap.x * pap.x + pap.y * pap.y;
+        const double ax = rsold * pap.x / den, ay = -rsold * pap.y / den;
+        double rl = 0;
+        for (int i = tid; i < P; i += nt) {
+            const double2 pi = p[i], api = Ap[i];
+            double2 xi = x[i];
+            xi.x += ax * pi.x - ay * pi.y;
+            xi.y += ax * pi.y + ay * pi.x;
+            x[i] = xi;
+            double2 ri = r[i];
+            ri.x -= ax * api.x - ay * api.y;
+            ri.y -= ax * api.y + ay * api.x;
+            r[i] = ri;
+            rl += ri.x * ri.x + ri.y * ri.y;
+        }
+        {
+            const double2 t = warp_total2(make_double2(rl, 0));
+            if (lane == 0) partB[w] = t;
+        }
+        __syncthreads();
+        // (3) convergence test and p = r + beta p
+        rs = sum_partials2(partB, nw).x;
+        if (rs < rtol) break;
+        const double beta = rs / rsold;
+        for (int i = tid; i < P; i += nt) {
+            const double2 ri = r[i], pi = p[i];
+            p[i] = make_double2(ri.x + beta * pi.x, ri.y + beta * pi.y);
+        }
+        rsold = rs;
+        __syncthreads();
+    }
+    for (int i = tid; i < P; i += nt) xg[i] = x[i];
+    if (tid == 0) {
+        res->iterations = itn;
+        res->residual = rs;
+    }
+}
+
 // ---------------------------------------------------------------- update --
 // abstract_optimizer::optimize tail (abstract_optimizer.cpp:157-176):
 // abort on max|x| > 30, else x *= lr (the next warm start) and w -= x.
@@ -492,6 +651,13 @@ cudaError_t launch_regularize(const double2* S, int P, int n_neural, int N, cons
 
 cudaError_t launch_cg(const double2* A, const double2* b, double2* x, int P, int max_it, double rtol, CgResultDev* res,
                       cudaStream_t st) {
+    const size_t packed = (packed_size(P) + 4 * (size_t)P) * sizeof(double2);
+    if (packed <= 200 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(cg_packed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)packed);
+        if (e != cudaSuccess) return e;
+        cg_packed<<<1, 1024, packed, st>>>(A, b, x, P, max_it, rtol, res);
+        return cudaGetLastError();
+    }
     const int smem = 3 * P * (int)sizeof(double2);
     cudaError_t e = cudaFuncSetAttribute(cg_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;

@@ -205,7 +205,7 @@ def test_timing_counters():
     for _ in range(2):
         s.epoch()
     ms, cnt = s.timing()
-    assert (cnt[:5] == 2).all() and (ms[:5] > 0).all()
+    assert (cnt[:6] == 2).all() and (ms[:6] > 0).all()
 
 
 def test_massive_step_is_reported():
