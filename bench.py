@@ -209,18 +209,15 @@ def run_ours(args, rank, world, local):
         ms_step = t_ms / args.steps
         mufu = rbmnqs.probe_mufu()
         sampler_ms = stage_ms[0] / max(1, stage_cnt[0])
-        # algorithmic MUFU work of one sampler launch: every proposal
-        # evaluates T ln|cosh| terms (ex2, sin, cos, lg2), the FP64 theta
-        # recompute re-evaluates T terms per sweep, each sample adds the
-        # complex ln cosh cache (5 MUFU per entry), one ratio per
-        # off-diagonal Hamiltonian term (5 per entry) and tanh (4 per entry)
+        # algorithmic special-function work of one sweep-kernel launch: every
+        # proposal evaluates ln|cosh| of all T theta entries (one exp, one cos,
+        # one log each) and the FP64 theta recompute after every sweep
+        # re-evaluates the T entries; proposals per sweep = n / (1 + p_bond)
         T = sess.n_hidden * sess.n_symm
         acc = float(np.mean(accs))
         sweeps = wl["warmup"] + wl["samples_per_chain"] * wl["step"]
         props_per_sweep = model.n / (1 + wl["bond_flips"])
-        n_offdiag = model.n  # Kitaev: one off-diagonal term per x and y bond
-        per_chain = sweeps * (props_per_sweep * T * 4 + T * 4) + \
-            wl["samples_per_chain"] * (T * 5 + n_offdiag * T * 5 + T * 4)
+        per_chain = sweeps * (props_per_sweep * T * 3 + T * 3)
         mufu_ops = per_chain * wl["n_chains"]
         achieved = mufu_ops / (sampler_ms * 1e-3)
         result = {

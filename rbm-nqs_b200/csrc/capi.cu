@@ -216,7 +216,7 @@ struct rbmnqs_handle {
         ea.B = N;
         ea.eloc = E.p;
         ea.O = O.p;
-        ea.plan = rbmnqs::SmemPlan{0, w_in_smem, 0};
+        ea.plan = rbmnqs::SmemPlan{0, w_in_smem, 0, 0, 0};
         ck(rbmnqs::launch_eval(ea, fp64, wpb, st), "eval kernel");
         mark(2);
         ck(rbmnqs::launch_moments(O.p, fp64, E.p, N, P, mom_blocks, pd.p, pf.p, pe.p, d.p, F.p, emean.p, st),
@@ -507,7 +507,7 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         }
         // launch shapes: persistent sampler blocks; evaluation kernels with
         // FP32 W in shared memory when it fits
-        ck(rbmnqs::plan_sampler(h->machine(), h->fp64, cfg->n_chains, &h->shape), "sampler plan");
+        ck(rbmnqs::plan_sampler(h->machine(), h->fp64, cfg->n_chains, h->n_prop_bonds, &h->shape), "sampler plan");
         if (h->n_prop_bonds > 0 && cfg->bond_flips > 0) {
             const double thr = std::ceil(cfg->bond_flips * 16777216.0);
             h->bond_thr24 = (uint32_t)std::min(thr, 16777216.0);
@@ -515,8 +515,8 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         h->w_in_smem = (size_t)n * nh * 8 <= 64 * 1024 ? 1 : 0;
         h->wpb = 8;
         {
-            rbmnqs::SmemPlan pl{0, h->w_in_smem, 0};
-            while (h->wpb > 1 && rbmnqs::sampler_smem_bytes(h->machine(), h->fp64, h->wpb, pl) > 200 * 1024)
+            rbmnqs::SmemPlan pl{0, h->w_in_smem, 0, 0, 0};
+            while (h->wpb > 1 && rbmnqs::eval_smem_bytes(h->machine(), h->fp64, h->wpb, pl) > 200 * 1024)
                 h->wpb >>= 1;
         }
         ck(cudaStreamSynchronize(h->st), "sync");
@@ -716,7 +716,7 @@ static void eval_common(rbmnqs_handle* h, const uint32_t* spins, int B, double* 
     a.hd = h->hdev.p;
     a.spins = ds.p;
     a.B = B;
-    a.plan = rbmnqs::SmemPlan{0, h->w_in_smem, 0};
+    a.plan = rbmnqs::SmemPlan{0, h->w_in_smem, 0, 0, 0};
     if (logpsi) {
         dl.alloc(B);
         a.logpsi = dl.p;

@@ -251,40 +251,56 @@ __device__ __forceinline__ void stage(const MachineDev& m, const uint32_t sp[4],
 // ---------------------------------------------------------------------------
 // Shared-memory carve-up.  Block-wide tables (shared by every chain of the
 // block) followed by one scratch area per warp.  The same byte arithmetic
-// runs on host (launch sizing) and device (carving).
+// runs on host (launch sizing) and device (carving).  Expanded tables are
+// padded to TP = 32 E columns (zero beyond T) so the FP32 sweep needs no
+// per-entry bounds test: a zero column leaves its theta entry, and so its
+// ln cosh, unchanged.
 struct Smem {
-    float2* U;      // expanded FP32 flip table U[f*T + t] = W[P_s(f), k]
+    float2* U;      // [n+1][TP] U[f*TP + t] = W[P_s(f), k], row n = 0
+    double2* U64;   // [n][TP] FP64 copy for the theta recompute
     float2* W32;    // FP32 W, site-major
-    double2* W64;   // FP64 W, site-major (theta recompute)
+    double2* W64;   // FP64 W, site-major (theta recompute, gather path)
     uint8_t* perm;  // [n][S]
     uint8_t* inv;   // [S][n]
-    float* bre;     // [n] Re v[f mod n_vb] (Metropolis bias term)
+    float* bre;     // [n+1] Re v[f mod n_vb] (Metropolis bias term), [n] = 0
+    int2* bonds;    // proposal bonds
     unsigned char* warp0;
     int warp_bytes;
 };
 
 __host__ __device__ inline int align16(int x) { return (x + 15) & ~15; }
+__host__ __device__ inline int padded_T(int T) { return 32 * ((T + 31) / 32); }
 
-// per-warp scratch: spins (16 B) | theta [T] | ln cosh re [T] | phase / tanh [T]
-// | proposal ln|cosh| [T]
-__host__ __device__ inline int warp_bytes_for(int T, int rsize) { return align16(16 + T * 6 * rsize); }
+// per-warp scratch.  Evaluation: spins (16 B) | theta [T] | ln cosh re [T] |
+// phase / tanh [T].  Sweeps: proposal ln|cosh| [TP].
+__host__ __device__ inline int eval_warp_bytes(int T, int rsize) { return align16(16 + T * 5 * rsize); }
+__host__ __device__ inline int sweep_warp_bytes(int T, int rsize) { return align16(padded_T(T) * rsize); }
 
-__host__ __device__ inline int table_bytes(const MachineDev& m, int fp64, const SmemPlan& pl) {
+__host__ __device__ inline int table_bytes(const MachineDev& m, int fp64, const SmemPlan& pl, int n_bonds) {
+    const int TP = padded_T(m.T);
     int b = 0;
-    if (pl.use_u) b += align16(m.n * m.T * 8);
+    if (pl.use_u) b += align16((m.n + 1) * TP * 8);
+    if (pl.u64) b += align16(m.n * TP * 16);
     if (!fp64 && pl.w32) b += align16(m.n * m.nh * 8);
     if (pl.w64) b += align16(m.n * m.nh * 16);
     if (m.symmetric) b += align16(m.n * m.S) * 2;
-    b += align16(m.n * 4);
+    b += align16((m.n + 1) * 4);
+    if (pl.bonds) b += align16(n_bonds * 8);
     return b;
 }
 
-__device__ inline Smem carve(unsigned char* base, const MachineDev& m, int fp64, const SmemPlan& pl, int rsize) {
+__device__ inline Smem carve(unsigned char* base, const MachineDev& m, int fp64, const SmemPlan& pl, int n_bonds,
+                             int warp_bytes) {
+    const int TP = padded_T(m.T);
     Smem s{};
     int off = 0;
     if (pl.use_u) {
         s.U = reinterpret_cast<float2*>(base + off);
-        off += align16(m.n * m.T * 8);
+        off += align16((m.n + 1) * TP * 8);
+    }
+    if (pl.u64) {
+        s.U64 = reinterpret_cast<double2*>(base + off);
+        off += align16(m.n * TP * 16);
     }
     if (!fp64 && pl.w32) {
         s.W32 = reinterpret_cast<float2*>(base + off);
@@ -301,14 +317,20 @@ __device__ inline Smem carve(unsigned char* base, const MachineDev& m, int fp64,
         off += align16(m.n * m.S);
     }
     s.bre = reinterpret_cast<float*>(base + off);
-    off += align16(m.n * 4);
+    off += align16((m.n + 1) * 4);
+    if (pl.bonds) {
+        s.bonds = reinterpret_cast<int2*>(base + off);
+        off += align16(n_bonds * 8);
+    }
     s.warp0 = base + off;
-    s.warp_bytes = warp_bytes_for(m.T, rsize);
+    s.warp_bytes = warp_bytes;
     return s;
 }
 
-__device__ inline void load_tables(const MachineDev& m, const Smem& s, int fp64, const SmemPlan& pl) {
+__device__ inline void load_tables(const MachineDev& m, const Smem& s, int fp64, const SmemPlan& pl,
+                                   const int2* bonds, int n_bonds) {
     const int tid = threadIdx.x, nt = blockDim.x;
+    const int TP = padded_T(m.T);
     if (!fp64 && pl.w32)
         for (int i = tid; i < m.n * m.nh; i += nt) s.W32[i] = m.W32[i];
     if (pl.w64)
@@ -318,46 +340,71 @@ __device__ inline void load_tables(const MachineDev& m, const Smem& s, int fp64,
             s.perm[i] = m.perm[i];
             s.inv[i] = m.inv[i];
         }
-    for (int i = tid; i < m.n; i += nt) s.bre[i] = (float)m.vb[i % m.n_vb].x;
-    if (pl.use_u)
-        for (int i = tid; i < m.n * m.T; i += nt) {
-            const int f = i / m.T, t = i % m.T;
-            const int k = t % m.nh, sy = t / m.nh;
-            const int row = m.symmetric ? (int)m.perm[f * m.S + sy] : f;
-            s.U[i] = m.W32[row * m.nh + k];
+    for (int i = tid; i <= m.n; i += nt) s.bre[i] = i < m.n ? (float)m.vb[i % m.n_vb].x : 0.f;
+    if (pl.bonds)
+        for (int i = tid; i < n_bonds; i += nt) s.bonds[i] = bonds[i];
+    if (pl.use_u || pl.u64)
+        for (int i = tid; i < (m.n + 1) * TP; i += nt) {
+            const int f = i / TP, t = i % TP;
+            double2 w = make_double2(0, 0);
+            if (f < m.n && t < m.T) {
+                const int k = t % m.nh, sy = t / m.nh;
+                const int row = m.symmetric ? (int)m.perm[f * m.S + sy] : f;
+                w = m.W64[row * m.nh + k];
+            }
+            if (pl.use_u) s.U[i] = make_float2((float)w.x, (float)w.y);
+            if (pl.u64 && f < m.n) s.U64[i] = w;
         }
     __syncthreads();
 }
 
-// One chain: metropolis_sampler::sample_chain (metropolis_sampler.cpp:118-273)
-// for the warp's chain.  Sampled configurations (16 bytes each) are recorded
-// and evaluated afterwards by eval_kernel, one warp per sample: calling the
-// evaluation from inside the sweep loop would make the call's register saves
-// push the loop's live state (theta, ln cosh, bits) to local memory.  Randomness: Philox4x32-10 with counter
-// {proposal, epoch, chain, 0}; lane j draws proposal (base + j), so one
-// Philox call per lane serves 32 proposals.
-template <int E, typename R, bool EXP>
-__device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, int chain, int lane, uint32_t* wsp,
-                                          C2<R>* wth, R* cre, C2<R>* cu, R* wlp) {
-    const MachineDev& m = a.m;
-    const C2<R>* W = Wsel<R>::get(m, sm.W32 ? sm.W32 : m.W32);
-    const double2* W64 = sm.W64 ? sm.W64 : m.W64;
-    const uint2 key = make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32));
-    const uint32_t epoch = a.ctl[0];
-    uint32_t sp[4];
+// Initial configuration of a chain: Philox stream 1 bits for a fresh chain,
+// else the persisted configuration.
+__device__ __forceinline__ void chain_start(const SamplerArgs& a, int chain, uint2 key, uint32_t epoch, uint32_t sp[4]) {
+    const int n = a.m.n;
     if (a.ctl[1]) {
-        const uint4 r = philox4x32(make_uint4(0, epoch, (uint32_t)chain, 1), key);  // stream 1: initial bits
+        const uint4 r = philox4x32(make_uint4(0, epoch, (uint32_t)chain, 1), key);
         const uint32_t rw[4] = {r.x, r.y, r.z, r.w};
 #pragma unroll
         for (int w = 0; w < 4; w++) {
             const int lo = 32 * w;
-            const uint32_t mask = m.n >= lo + 32 ? 0xffffffffu : (m.n > lo ? ((1u << (m.n - lo)) - 1) : 0u);
+            const uint32_t mask = n >= lo + 32 ? 0xffffffffu : (n > lo ? ((1u << (n - lo)) - 1) : 0u);
             sp[w] = rw[w] & mask;
         }
     } else {
 #pragma unroll
         for (int w = 0; w < 4; w++) sp[w] = a.spins[4 * chain + w];
     }
+}
+
+__device__ __forceinline__ void chain_finish(const SamplerArgs& a, int chain, int lane, const uint32_t sp[4],
+                                             uint32_t nacc, uint32_t prop) {
+    if (lane < 4) a.spins[4 * chain + lane] = sp[lane];
+    if (lane == 0) {
+        a.n_acc[chain] = nacc;
+        a.n_prop[chain] = prop;
+    }
+}
+
+// One chain: metropolis_sampler::sample_chain (metropolis_sampler.cpp:118-273)
+// for the warp's chain, general path (FP64 parity mode, and FP32 when the
+// expanded flip table does not fit in shared memory).  Sampled
+// configurations (16 bytes each) are recorded and evaluated afterwards by
+// eval_kernel, one warp per sample: calling the evaluation from inside the
+// sweep loop would make the call's register saves push the loop's live state
+// (theta, ln cosh, bits) to local memory.  Randomness: Philox4x32-10 with
+// counter {proposal, epoch, chain, 0}; lane j draws proposal (base + j), so
+// one Philox call per lane serves 32 proposals.
+template <int E, typename R>
+__device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, int chain, int lane, R* wlp) {
+    const MachineDev& m = a.m;
+    const C2<R>* W = Wsel<R>::get(m, sm.W32 ? sm.W32 : m.W32);
+    const double2* W64 = sm.W64 ? sm.W64 : m.W64;
+    const int2* bonds = sm.bonds ? sm.bonds : a.prop_bonds;
+    const uint2 key = make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32));
+    const uint32_t epoch = a.ctl[0];
+    uint32_t sp[4];
+    chain_start(a, chain, key, epoch, sp);
 
     C2<R> th[E];
     R L[E];
@@ -367,13 +414,8 @@ __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, 
 
     // U(f, e): the flip row of site f for this lane's entry e
     auto U = [&](int f, int e) -> C2<R> {
-        if constexpr (EXP) {
-            const float2 u = sm.U[f * m.T + lane + 32 * e];
-            return mk<R>(u.x, u.y);
-        } else {
-            const int t = lane + 32 * e;
-            return W[urow<R>(m, sm.perm, f, t / m.nh) * m.nh + t % m.nh];
-        }
+        const int t = lane + 32 * e;
+        return W[urow<R>(m, sm.perm, f, t / m.nh) * m.nh + t % m.nh];
     };
 
     const int n = m.n;
@@ -400,7 +442,7 @@ __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, 
             prop++;
             int f0, f1 = -1;
             if ((r0 >> 8) < thr) {
-                const int2 b = a.prop_bonds[pick(r1, (uint32_t)a.n_prop_bonds)];
+                const int2 b = bonds[pick(r1, (uint32_t)a.n_prop_bonds)];
                 f0 = b.x;
                 f1 = b.y;
                 slot += 2;
@@ -430,12 +472,9 @@ __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, 
             }
             d = warp_sum(d);
             // bias: -2 sigma_f Re v[f mod n_vb] (rbm_base.cpp:306-318)
-            if constexpr (sizeof(R) == 4) {
-                d += g0 * sm.bre[f0];
-                if (f1 >= 0) d += g1 * sm.bre[f1];
-            } else {
+            {
                 const int fl[2] = {f0, f1};
-                d += bias_delta(m, sp, fl, f1 >= 0 ? 2 : 1).x;
+                d += (R)bias_delta(m, sp, fl, f1 >= 0 ? 2 : 1).x;
             }
             // accept with min(1, |psi'/psi|^2) (metropolis_sampler.cpp:223-243)
             if (unit24<R>(r2) < exp_r((R)2 * d)) {
@@ -467,11 +506,135 @@ __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, 
             if (lane < 4) a.samples[4 * idx + lane] = sp[lane];
         }
     }
-    if (lane < 4) a.spins[4 * chain + lane] = sp[lane];
-    if (lane == 0) {
-        a.n_acc[chain] = nacc;
-        a.n_prop[chain] = prop;
+    chain_finish(a, chain, lane, sp, nacc, prop);
+}
+
+// ln|cosh(a + ib)| without the constant -ln 2, FP32 sweep form.  With
+// z = exp(-2|a|):  4 e^{-2|a|} |cosh x|^2 = 1 + z^2 + 2 z cos 2b, so
+//   ln|cosh x| = |a| - ln 2 + 0.5 ln(1 + z^2 + 2 z cos 2b):
+// one ex2, one cos, one lg2.  The sum of squares form used by lnc_re avoids
+// the cancellation at the zeros of cosh (a = 0, b = pi/2 + k pi); this form
+// only loses digits there, which leaves the Metropolis decision unchanged
+// except for transitions at configurations of vanishing amplitude.  The
+// hardware cosine takes the argument in revolutions, so 2b needs no
+// separate range reduction for the accuracy the acceptance test needs.
+__device__ __forceinline__ float lnc_sweep(float2 t) {
+    const float aa = fabsf(t.x);
+    const float z = __expf(-2.f * aa);
+    const float c2 = __cosf(2.f * t.y);
+    const float m2 = fmaf(2.f * z, c2, fmaf(z, z, 1.f));
+    return fmaf(0.346573590279972655f, __log2f(m2), aa);  // aa + 0.5 ln(m2)
+}
+
+// FP32 sweep path with the expanded flip table in shared memory.  Proposals
+// are decoded lane-parallel: with each Philox batch, lane j turns its draw
+// into a packed (f0, f1, bond) code and 0.5 ln u, so a proposal costs two
+// shuffles; a single-site proposal uses the all-zero pad row n as its second
+// flip, which keeps the update branch-free; acceptance compares
+// 0.5 ln u < log|psi'/psi| (the same test as u < |psi'/psi|^2).
+template <int E>
+__device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem& sm, int chain, int lane) {
+    const MachineDev& m = a.m;
+    const int n = m.n, TP = 32 * E;
+    const uint2 key = make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32));
+    const uint32_t epoch = a.ctl[0];
+    uint32_t sp[4];
+    chain_start(a, chain, key, epoch, sp);
+
+    float2 th[E];
+    float SL = 0.f;  // this lane's sum of ln|cosh theta_e| (current state)
+    auto recompute = [&]() {
+        if (sm.U64) {
+            double2 acc[E];
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                const int t = lane + 32 * e;
+                acc[e] = t < m.T ? m.hb[t % m.nh] : make_double2(0, 0);
+            }
+            const double2* col = sm.U64 + lane;
+            for (int f = 0; f < n; f++, col += TP) {
+                const double sg = spin_bit(sp, f) ? -1.0 : 1.0;
+#pragma unroll
+                for (int e = 0; e < E; e++) {
+                    const double2 w = col[32 * e];
+                    acc[e].x = fma(sg, w.x, acc[e].x);
+                    acc[e].y = fma(sg, w.y, acc[e].y);
+                }
+            }
+#pragma unroll
+            for (int e = 0; e < E; e++) th[e] = make_float2((float)acc[e].x, (float)acc[e].y);
+        } else {
+            theta_fp64<E, float>(m, sm.W64 ? sm.W64 : m.W64, sm.perm, lane, sp, th);
+        }
+        SL = 0.f;
+#pragma unroll
+        for (int e = 0; e < E; e++) SL += lnc_sweep(th[e]);
+    };
+    recompute();
+
+    const int2* bonds = sm.bonds ? sm.bonds : a.prop_bonds;
+    const int warmup = a.warmup;
+    const int total = a.spc * a.step + warmup;
+    const uint32_t thr = a.bond_thr24;
+    uint32_t prop = 0, nacc = 0, pcode = 0;
+    float plu = 0.f;
+    for (int st = 0; st < total; st++) {
+        int slot = 0;
+        while (slot < n) {
+            if ((prop & 31u) == 0) {
+                const uint4 r = philox4x32(make_uint4(prop + lane, epoch, (uint32_t)chain, 0), key);
+                uint32_t f0, f1, bond;
+                if ((r.x >> 8) < thr) {
+                    const int2 b = bonds[pick(r.y, (uint32_t)a.n_prop_bonds)];
+                    f0 = (uint32_t)b.x;
+                    f1 = (uint32_t)b.y;
+                    bond = 1;
+                } else {
+                    f0 = pick(r.y, (uint32_t)n);
+                    f1 = (uint32_t)n;
+                    bond = 0;
+                }
+                pcode = f0 | (f1 << 8) | (bond << 16);
+                plu = 0.5f * __logf(unit24<float>(r.z));
+            }
+            const int src = prop & 31u;
+            const uint32_t code = __shfl_sync(kFull, pcode, src);
+            const float lu = __shfl_sync(kFull, plu, src);
+            prop++;
+            const int f0 = code & 255u, f1 = (code >> 8) & 255u;
+            const bool bond = (code >> 16) != 0;
+            slot += bond ? 2 : 1;
+            const float g0 = spin_bit(sp, f0) ? 2.f : -2.f;  // -2 sigma_f
+            const float g1 = (bond && spin_bit(sp, f1)) ? 2.f : -2.f;
+            const float2 G0 = make_float2(g0, g0), G1 = make_float2(g1, g1);
+            const float2* u0 = sm.U + f0 * TP + lane;
+            const float2* u1 = sm.U + f1 * TP + lane;
+            float sp_new = 0.f;
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                const float2 t = __ffma2_rn(G1, u1[32 * e], __ffma2_rn(G0, u0[32 * e], th[e]));
+                sp_new += lnc_sweep(t);
+            }
+            float d = warp_sum(sp_new - SL);
+            d = fmaf(g0, sm.bre[f0], d);
+            d = fmaf(g1, sm.bre[f1], d);
+            if (lu < d) {
+#pragma unroll
+                for (int e = 0; e < E; e++) th[e] = __ffma2_rn(G1, u1[32 * e], __ffma2_rn(G0, u0[32 * e], th[e]));
+                SL = sp_new;
+                flip_bit(sp, f0);
+                if (bond) flip_bit(sp, f1);
+                nacc++;
+            }
+        }
+        recompute();  // FP64 recompute of theta once per sweep
+        if (st >= warmup && (st - warmup) % a.step == 0) {
+            const int j = (st - warmup) / a.step;
+            const size_t idx = (size_t)chain * a.spc + j;
+            if (lane < 4) a.samples[4 * idx + lane] = sp[lane];
+        }
     }
+    chain_finish(a, chain, lane, sp, nacc, prop);
 }
 
 // Thread bound per entries-per-lane: 28 warps (896 threads, 72 registers)
@@ -482,23 +645,23 @@ template <int E> struct MaxThreads {
 
 // All chains at once, persistent warps: global warp g = warp * gridDim.x +
 // blockIdx.x takes chains g, g + total_warps, ... so consecutive chains land
-// on different SMs and every block holds the tables once.
-template <int E, typename R, bool EXP>
+// on different SMs and every block holds the tables once.  FAST selects the
+// FP32 expanded-table path.
+template <int E, typename R, bool FAST>
 __global__ void __launch_bounds__(MaxThreads<E>::v, 1) sampler_kernel(const SamplerArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int fp64 = sizeof(R) == 8;
-    Smem sm = carve(smem, a.m, fp64, a.plan, sizeof(R));
-    load_tables(a.m, sm, fp64, a.plan);
+    Smem sm = carve(smem, a.m, fp64, a.plan, a.n_prop_bonds, sweep_warp_bytes(a.m.T, sizeof(R)));
+    load_tables(a.m, sm, fp64, a.plan, a.prop_bonds, a.n_prop_bonds);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char* wbase = sm.warp0 + warp * sm.warp_bytes;
-    uint32_t* wsp = reinterpret_cast<uint32_t*>(wbase);
-    C2<R>* wth = reinterpret_cast<C2<R>*>(wbase + 16);
-    R* cre = reinterpret_cast<R*>(wbase + 16 + a.m.T * 2 * sizeof(R));
-    C2<R>* cu = reinterpret_cast<C2<R>*>(wbase + 16 + a.m.T * 3 * sizeof(R));
-    R* wlp = reinterpret_cast<R*>(wbase + 16 + a.m.T * 5 * sizeof(R));
+    R* wlp = reinterpret_cast<R*>(sm.warp0 + warp * sm.warp_bytes);
     const int total_warps = (blockDim.x >> 5) * gridDim.x;
-    for (int chain = warp * gridDim.x + blockIdx.x; chain < a.n_chains; chain += total_warps)
-        run_chain<E, R, EXP>(a, sm, chain, lane, wsp, wth, cre, cu, wlp);
+    for (int chain = warp * gridDim.x + blockIdx.x; chain < a.n_chains; chain += total_warps) {
+        if constexpr (FAST)
+            run_chain_fast<E>(a, sm, chain, lane);
+        else
+            run_chain<E, R>(a, sm, chain, lane, wlp);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -509,8 +672,8 @@ __global__ void __launch_bounds__(256) eval_kernel(const EvalArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const MachineDev& m = a.m;
     const int fp64 = sizeof(R) == 8;
-    Smem sm = carve(smem, m, fp64, a.plan, sizeof(R));
-    load_tables(m, sm, fp64, a.plan);
+    Smem sm = carve(smem, m, fp64, a.plan, 0, eval_warp_bytes(m.T, sizeof(R)));
+    load_tables(m, sm, fp64, a.plan, nullptr, 0);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b = blockIdx.x * (blockDim.x >> 5) + warp;
     if (b >= a.B) return;
@@ -626,12 +789,16 @@ int elements_per_lane(int T) {
     return -1;
 }
 
-int sampler_smem_bytes(const MachineDev& m, int fp64, int warps, const SmemPlan& plan) {
-    return table_bytes(m, fp64, plan) + warps * warp_bytes_for(m.T, fp64 ? 8 : 4);
+int sampler_smem_bytes(const MachineDev& m, int fp64, int warps, const SmemPlan& plan, int n_bonds) {
+    return table_bytes(m, fp64, plan, n_bonds) + warps * sweep_warp_bytes(m.T, fp64 ? 8 : 4);
 }
 
-template <int E, typename R, bool EXP> static const void* sampler_fn() {
-    return reinterpret_cast<const void*>(sampler_kernel<E, R, EXP>);
+int eval_smem_bytes(const MachineDev& m, int fp64, int warps, const SmemPlan& plan) {
+    return table_bytes(m, fp64, plan, 0) + warps * eval_warp_bytes(m.T, fp64 ? 8 : 4);
+}
+
+template <int E, typename R, bool FAST> static const void* sampler_fn() {
+    return reinterpret_cast<const void*>(sampler_kernel<E, R, FAST>);
 }
 
 static const void* pick_sampler(int E, int fp64, int exp_table) {
@@ -645,7 +812,7 @@ static const void* pick_sampler(int E, int fp64, int exp_table) {
     return nullptr;
 }
 
-cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, SamplerShape* out) {
+cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bonds, SamplerShape* out) {
     const int E = elements_per_lane(m.T);
     if (E < 0) return cudaErrorInvalidValue;
     int dev = 0, sms = 0, smem_max = 0;
@@ -653,26 +820,32 @@ cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, SamplerSha
     if (err != cudaSuccess) return err;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const int budget = smem_max - 8 * 1024;
+    const int TP = 32 * E;
     SmemPlan pl{};
-    const int budget = smem_max - 16 * 1024;
-    pl.w32 = !fp64 && m.n * m.nh * 8 <= 64 * 1024;
+    // FP32 expanded-table path when the table fits; its theta recompute uses
+    // the FP64 expanded table when that fits too, else FP64 W
+    pl.use_u = !fp64 && (m.n + 1) * TP * 8 <= 64 * 1024;
+    pl.u64 = pl.use_u && m.n * TP * 16 <= 96 * 1024;
+    pl.w32 = !fp64 && !pl.use_u && m.n * m.nh * 8 <= 64 * 1024;
     pl.w64 = m.n * m.nh * 16 <= 32 * 1024;
-    pl.use_u = !fp64 && pl.w32 && m.n * m.T * 8 <= 64 * 1024;
+    pl.bonds = n_bonds > 0 && n_bonds * 8 <= 8 * 1024;
     const void* fn = pick_sampler(E, fp64, pl.use_u);
     cudaFuncAttributes fa;
     err = cudaFuncGetAttributes(&fa, fn);
     if (err != cudaSuccess) return err;
     // warps per block: enough for one block per SM to hold every chain,
     // limited by the kernel's thread bound, registers and shared memory
-    int want = (n_chains + sms - 1) / sms;
+    const int want = (n_chains + sms - 1) / sms;
     int wpb = fa.maxThreadsPerBlock / 32;
     const int regs = fa.numRegs > 0 ? fa.numRegs : 64;
     const int reg_warps = 65536 / (regs * 32);
     if (wpb > reg_warps) wpb = reg_warps;
     if (wpb > want) wpb = want;
     if (wpb < 1) wpb = 1;
-    while (wpb > 1 && sampler_smem_bytes(m, fp64, wpb, pl) > budget) wpb--;
-    const int smem = sampler_smem_bytes(m, fp64, wpb, pl);
+    if (pl.u64 && sampler_smem_bytes(m, fp64, wpb, pl, n_bonds) > budget) pl.u64 = 0;
+    while (wpb > 1 && sampler_smem_bytes(m, fp64, wpb, pl, n_bonds) > budget) wpb--;
+    const int smem = sampler_smem_bytes(m, fp64, wpb, pl, n_bonds);
     if (smem > budget) return cudaErrorInvalidValue;
     err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (err != cudaSuccess) return err;
@@ -701,7 +874,7 @@ cudaError_t launch_sampler(const SamplerArgs& a0, int fp64, const SamplerShape& 
 
 template <int E, typename R>
 static cudaError_t launch_e(const EvalArgs& a, int wpb, cudaStream_t st) {
-    const int smem = sampler_smem_bytes(a.m, sizeof(R) == 8, wpb, a.plan);
+    const int smem = eval_smem_bytes(a.m, sizeof(R) == 8, wpb, a.plan);
     cudaError_t err = cudaFuncSetAttribute(eval_kernel<E, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (err != cudaSuccess) return err;
     const int blocks = (a.B + wpb - 1) / wpb;

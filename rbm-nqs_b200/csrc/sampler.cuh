@@ -38,9 +38,11 @@ struct HamDev {
 
 // Which tables live in shared memory (decided on the host from their sizes).
 struct SmemPlan {
-    int use_u;  // expanded FP32 flip table U[n][T]
+    int use_u;  // expanded FP32 flip table U[n+1][TP] (row n all zero)
     int w32;    // FP32 W
     int w64;    // FP64 W
+    int u64;    // expanded FP64 table U64[n][TP] for the theta recompute
+    int bonds;  // proposal bond list
 };
 
 struct SamplerArgs {
@@ -85,7 +87,8 @@ struct EvalArgs {
 };
 
 // Launch helpers implemented in sampler.cu
-int sampler_smem_bytes(const MachineDev& m, int fp64, int warps, const SmemPlan& plan);
+int sampler_smem_bytes(const MachineDev& m, int fp64, int warps, const SmemPlan& plan, int n_bonds);
+int eval_smem_bytes(const MachineDev& m, int fp64, int warps, const SmemPlan& plan);
 // Plan + launch shape of the sampler for this machine and chain count:
 // one persistent block per SM with enough warps to hold every chain when
 // registers allow.
@@ -95,7 +98,7 @@ struct SamplerShape {
     int blocks;
     int smem;
 };
-cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, SamplerShape* out);
+cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bonds, SamplerShape* out);
 cudaError_t launch_sampler(const SamplerArgs& a, int fp64, const SamplerShape& shape, cudaStream_t st);
 cudaError_t launch_eval(const EvalArgs& a, int fp64, int warps_per_block, cudaStream_t st);
 int elements_per_lane(int T);

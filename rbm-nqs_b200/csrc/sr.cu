@@ -1,8 +1,12 @@
 // sr.cu -- stochastic-reconfiguration kernels: sample moments, energy
 // statistics, the Hermitian Gram S, regularisation, FP64 conjugate
 // gradients and the weight update.
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 #include "sr.cuh"
+
+namespace cgx = cooperative_groups;
 
 namespace rbmnqs {
 
@@ -550,6 +554,159 @@ __global__ void __launch_bounds__(1024) cg_packed(const double2* A, const double
     }
 }
 
+// The same iteration spread over one thread-block cluster of kClusterCta
+// CTAs on as many SMs.  CTA c owns rows [c*rp, (c+1)*rp) of S_reg (full rows
+// in its shared memory) and the matching slices of x, r, Ap; every CTA keeps
+// a full copy of p.  Per iteration: local mat-vec and p^H Ap partial, partial
+// pushed into every CTA's shared memory (DSMEM store), cluster barrier;
+// alpha, x/r update and ||r||^2 partial, pushed, barrier; beta, new p rows
+// pushed to every CTA's copy, barrier.  The operator, the arithmetic order
+// within a row and the stopping rule are those of cg_packed.
+constexpr int kClusterCta = 8;
+
+__global__ void __cluster_dims__(kClusterCta, 1, 1) __launch_bounds__(256)
+    cg_cluster(const double2* A, const double2* b, double2* xg, int P, int max_it, double rtol, CgResultDev* res) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    cgx::cluster_group cl = cgx::this_cluster();
+    const int rank = (int)cl.block_rank();
+    const int rp = (P + kClusterCta - 1) / kClusterCta;
+    const int r0 = rank * rp, r1 = min(P, r0 + rp), nr = max(0, r1 - r0);
+    double2* Srow = reinterpret_cast<double2*>(sm);  // [rp][P]
+    double2* p = Srow + (size_t)rp * P;              // [P] full copy
+    double2* x = p + P;                              // [rp]
+    double2* r = x + rp;                             // [rp]
+    double2* Ap = r + rp;                            // [rp]
+    __shared__ double2 partA[kClusterCta], partB[kClusterCta];
+    __shared__ double2 wred[8];
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
+    const int sub = lane & 7;
+    for (int i = tid; i < nr * P; i += nt) Srow[i] = A[(size_t)r0 * P + i];
+    for (int i = tid; i < P; i += nt) p[i] = xg[i];
+    for (int i = tid; i < nr; i += nt) x[i] = xg[r0 + i];
+    __syncthreads();
+
+    auto cta_sum = [&](double2 v) -> double2 {  // every thread gets the CTA total
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            v.x += __shfl_xor_sync(kFull, v.x, o);
+            v.y += __shfl_xor_sync(kFull, v.y, o);
+        }
+        __syncthreads();
+        if (lane == 0) wred[w] = v;
+        __syncthreads();
+        double2 t = make_double2(0, 0);
+        for (int i = 0; i < nw; i++) {
+            t.x += wred[i].x;
+            t.y += wred[i].y;
+        }
+        return t;
+    };
+    // push this CTA's partial into slot `rank` of every CTA's array
+    auto push = [&](double2* arr, double2 v) {
+        if (tid < kClusterCta) {
+            double2* dst = cl.map_shared_rank(arr, tid);
+            dst[rank] = v;
+        }
+    };
+    auto total = [&](const double2* arr) {
+        double2 t = make_double2(0, 0);
+        for (int i = 0; i < kClusterCta; i++) {
+            t.x += arr[i].x;
+            t.y += arr[i].y;
+        }
+        return t;
+    };
+    // local rows of A p; returns this thread's share of p^H Ap
+    auto matvec = [&]() -> double2 {
+        double2 pap = make_double2(0, 0);
+        for (int q0 = 4 * w; q0 < nr; q0 += 4 * nw) {
+            const int q = q0 + (lane >> 3);
+            const bool ok = q < nr;
+            double sx = 0, sy = 0;
+            if (ok) {
+                const double2* Ar = Srow + (size_t)q * P;
+                for (int j = sub; j < P; j += 8) {
+                    const double2 a = Ar[j], vv = p[j];
+                    sx = fma(a.x, vv.x, fma(-a.y, vv.y, sx));
+                    sy = fma(a.x, vv.y, fma(a.y, vv.x, sy));
+                }
+            }
+#pragma unroll
+            for (int o = 4; o > 0; o >>= 1) {
+                sx += __shfl_xor_sync(kFull, sx, o);
+                sy += __shfl_xor_sync(kFull, sy, o);
+            }
+            if (ok && sub == 0) {
+                Ap[q] = make_double2(sx, sy);
+                const double2 pr = p[r0 + q];
+                pap.x += pr.x * sx + pr.y * sy;
+                pap.y += pr.x * sy - pr.y * sx;
+            }
+        }
+        return pap;
+    };
+
+    (void)matvec();
+    __syncthreads();
+    double rl0 = 0;
+    for (int i = tid; i < nr; i += nt) {
+        const double2 ri = make_double2(b[r0 + i].x - Ap[i].x, b[r0 + i].y - Ap[i].y);
+        r[i] = ri;
+        rl0 += ri.x * ri.x + ri.y * ri.y;
+    }
+    push(partB, cta_sum(make_double2(rl0, 0)));
+    cl.sync();  // every CTA has finished reading p = x0
+    // p = r: one thread per own row publishes it to every CTA's copy
+    for (int q = tid; q < nr; q += nt) {
+        const double2 v = r[q];
+        for (int c = 0; c < kClusterCta; c++) cl.map_shared_rank(p, c)[r0 + q] = v;
+    }
+    cl.sync();
+    double rsold = total(partB).x;
+    double rs = rsold;
+    int itn = 0;
+    for (itn = 0; itn < max_it; itn++) {
+        push(partA, cta_sum(matvec()));
+        cl.sync();
+        const double2 pap = total(partA);
+        const double den = pap.x * pap.x + pap.y * pap.y;
+        const double ax = rsold * pap.x / den, ay = -rsold * pap.y / den;
+        double rl = 0;
+        for (int i = tid; i < nr; i += nt) {
+            const double2 pi = p[r0 + i], api = Ap[i];
+            double2 xi = x[i];
+            xi.x += ax * pi.x - ay * pi.y;
+            xi.y += ax * pi.y + ay * pi.x;
+            x[i] = xi;
+            double2 ri = r[i];
+            ri.x -= ax * api.x - ay * api.y;
+            ri.y -= ax * api.y + ay * api.x;
+            r[i] = ri;
+            rl += ri.x * ri.x + ri.y * ri.y;
+        }
+        push(partB, cta_sum(make_double2(rl, 0)));
+        cl.sync();
+        rs = total(partB).x;
+        if (rs < rtol) break;
+        const double beta = rs / rsold;
+        // new p rows: one thread per own row reads the old value once and
+        // writes the new one to every CTA's copy (its own included)
+        for (int q = tid; q < nr; q += nt) {
+            const double2 ri = r[q], pi = p[r0 + q];
+            const double2 v = make_double2(ri.x + beta * pi.x, ri.y + beta * pi.y);
+            for (int c = 0; c < kClusterCta; c++) cl.map_shared_rank(p, c)[r0 + q] = v;
+        }
+        rsold = rs;
+        cl.sync();
+    }
+    for (int i = tid; i < nr; i += nt) xg[r0 + i] = x[i];
+    if (rank == 0 && tid == 0) {
+        res->iterations = itn;
+        res->residual = rs;
+    }
+    cl.sync();  // no CTA leaves while others may still write its memory
+}
+
 // ---------------------------------------------------------------- update --
 // abstract_optimizer::optimize tail (abstract_optimizer.cpp:157-176):
 // abort on max|x| > 30, else x *= lr (the next warm start) and w -= x.
@@ -651,6 +808,14 @@ cudaError_t launch_regularize(const double2* S, int P, int n_neural, int N, cons
 
 cudaError_t launch_cg(const double2* A, const double2* b, double2* x, int P, int max_it, double rtol, CgResultDev* res,
                       cudaStream_t st) {
+    const int rp = (P + kClusterCta - 1) / kClusterCta;
+    const size_t csm = ((size_t)rp * P + P + 3 * (size_t)rp) * sizeof(double2);
+    if (csm <= 200 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(cg_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm);
+        if (e != cudaSuccess) return e;
+        cg_cluster<<<kClusterCta, 256, csm, st>>>(A, b, x, P, max_it, rtol, res);
+        return cudaGetLastError();
+    }
     const size_t packed = (packed_size(P) + 4 * (size_t)P) * sizeof(double2);
     if (packed <= 200 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(cg_packed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)packed);
