@@ -203,6 +203,34 @@ void* rbmnqs_stream(rbmnqs_handle* h);
  * counterpart in the reference (measurement helper). */
 int rbmnqs_probe_mufu(int32_t iters, double* ops_per_second);
 
+/* ------------------------------------------ allocation-free SR solve ---- */
+/* No counterpart in the reference.  The same solve as rbmnqs_sr_solve for
+ * callers that cannot allocate device memory: code inside a runtime that
+ * owns all device memory through its own pool and forbids raw
+ * cudaMalloc/cudaFree, and latency-critical loops that cannot take the
+ * implicit device-wide synchronisation of cudaMalloc/cudaFree.
+ * All buffers are the caller's DEVICE pointers (interleaved complex):
+ * O (N x n_params, sample-major), d, F, x (warm start in, solution out,
+ * n_params each) and diag (n_params doubles); the work is queued on
+ * `stream` (a cudaStream_t, NULL = default stream).  Working memory is one
+ * fixed array of (2 + 2) * 256^2 * 16 + 256 bytes (4 MiB + 256 B) that every
+ * GPU loading this library holds until the process exits; n_params above
+ * RBMNQS_NOALLOC_MAX_PARAMS is rejected with RBMNQS_ERR_ARG.  The first call
+ * on a device resolves the array's device address (cudaGetSymbolAddress with
+ * that device current), so make that first call before any stream capture.
+ * Every call shares the array: calls that overlap on the GPU (other streams,
+ * other threads) race and must be serialised by the caller.  When
+ * `iterations` or `residual` is non-NULL the call waits for `stream` to read
+ * them back.  Allocates nothing: no cudaMalloc, cudaFree or allocating
+ * library routine. */
+#define RBMNQS_NOALLOC_MAX_PARAMS 256
+int rbmnqs_sr_solve_noalloc(const double* O, int32_t N, int32_t n_params,
+                            int32_t n_neural, const double* d, double norm,
+                            const double* F, double* x, double r1, double r2,
+                            double rd, const double* diag,
+                            int32_t max_iterations, double rtol, void* stream,
+                            int32_t* iterations, double* residual);
+
 #ifdef __cplusplus
 }
 #endif

@@ -102,6 +102,8 @@ HamHost build_ham(const std::vector<rbmnqs::local_op>& ops) {
 
 }  // namespace
 
+void rbmnqs::set_last_error(const std::string& msg) { g_err = msg; }
+
 struct rbmnqs_handle {
     rbmnqs_config cfg{};
     rbmnqs::model model;

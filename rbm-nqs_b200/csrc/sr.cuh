@@ -3,8 +3,12 @@
 
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <string>
 
 namespace rbmnqs {
+
+// Message returned by rbmnqs_last_error() on the calling thread.
+void set_last_error(const std::string& msg);
 
 // Per-epoch statistics written on the device, read back once per epoch.
 struct EpochStatsDev {

@@ -106,6 +106,9 @@ def _declare(L):
         f = getattr(L, name)
         f.argtypes = args
         f.restype = None if name in ("rbmnqs_model_destroy", "rbmnqs_destroy") else C.c_int
+    L.rbmnqs_sr_solve_noalloc.argtypes = [VP, C.c_int32, C.c_int32, C.c_int32, VP, C.c_double, VP, VP, C.c_double,
+                                          C.c_double, C.c_double, VP, C.c_int32, C.c_double, VP, P_I, P_D]
+    L.rbmnqs_sr_solve_noalloc.restype = C.c_int
     L.rbmnqs_probe_mufu.argtypes = [C.c_int32, P_D]
     L.rbmnqs_probe_mufu.restype = C.c_int
     L.rbmnqs_last_error.restype = C.c_char_p
@@ -129,6 +132,17 @@ def probe_mufu(iters=4096):
     v = C.c_double()
     _ck(lib().rbmnqs_probe_mufu(iters, C.byref(v)))
     return v.value
+
+
+def sr_solve_noalloc(O_ptr, N, n_params, n_neural, d_ptr, norm, F_ptr, x_ptr, r1, r2, rd, diag_ptr,
+                     max_iterations=0, rtol=0.0, stream=0):
+    """rbmnqs_sr_solve_noalloc on caller-owned device buffers (raw device
+    addresses).  The solve allocates no device memory; x is updated in
+    place.  Returns (iterations, residual)."""
+    it, rs = C.c_int32(), C.c_double()
+    _ck(lib().rbmnqs_sr_solve_noalloc(O_ptr, N, n_params, n_neural, d_ptr, norm, F_ptr, x_ptr, r1, r2, rd, diag_ptr,
+                                      max_iterations, rtol, stream, C.byref(it), C.byref(rs)))
+    return it.value, rs.value
 
 
 def header_symbols():
