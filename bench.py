@@ -42,6 +42,9 @@ WORKLOADS = {
                              reg2=(1e-4, 1e-4, 1.0)),
 }
 METRIC = "uncorrelated samples/s (SR epoch, E_loc binning tau)"
+# DRAM bytes per sampler launch from an ncu capture of the same workload: the
+# theta tables, flip tables and chains live in shared memory and registers
+SAMPLER_DRAM_BYTES = {"kitaev32_symm_a4": 138752.0}
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -240,7 +243,10 @@ def run_ours(args, rank, world, local):
                          "peak": mufu / 1e9, "unit": "Gop/s (MUFU)", "frac": achieved / mufu,
                          "peak_source": "measured in this run by rbmnqs_probe_mufu (no MUFU figure in "
                                         "MEASURED_PEAKS.json)",
-                         "algorithmic_ops_per_launch": mufu_ops, "traffic": None},
+                         "algorithmic_ops_per_launch": mufu_ops,
+                         "traffic": SAMPLER_DRAM_BYTES.get(args.workload),
+                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture "
+                                           "(profiles/sampler_kernel_kitaev32_symm_a4.md)"},
             "e2e": {"value": e2e, "unit": "samples/s", "h2d_bytes_per_step": P * 16,
                     "d2h_bytes_per_step": P * 16 + 96},
             "gpu_launches": kern_per_epoch * args.steps,

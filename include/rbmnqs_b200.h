@@ -99,6 +99,9 @@ typedef struct {
                                      recompute, TF32x3 tensor-core Gram;
                                   1: FP64 throughout */
     int32_t n_updates;         /* rbm n_updates_ (decay_t offset on resume) */
+    int32_t gram;              /* S build: 0 = by precision (TF32x3 tensor
+                                  cores when precision is 0, FP64 when 1);
+                                  1 = FP64 CUDA cores in either precision */
 } rbmnqs_config;
 
 /* Fills the reference defaults (src/tools/ini.cpp:38-120). */

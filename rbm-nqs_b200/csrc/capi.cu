@@ -14,6 +14,7 @@
 
 #include "../host/model.hpp"
 #include "rbmnqs_b200.h"
+#include "gram_tc.cuh"
 #include "sampler.cuh"
 #include "sr.cuh"
 
@@ -132,6 +133,12 @@ struct rbmnqs_handle {
     DevBuf<rbmnqs::HamDev> hdev;
     DevBuf<rbmnqs::CgResultDev> cgres;
     DevBuf<rbmnqs::EpochStatsDev> stats;
+    // tensor-core Gram (mixed precision): TF32 hi / lo planes, FP32 split-K
+    // partial tiles, pipeline error flag
+    bool gram_tc = false;
+    rbmnqs::GramTC gtc;
+    DevBuf<float> gplanes, gpart;
+    DevBuf<int> gerr;
     int n_ops = 0, n_prop_bonds = 0;
     uint32_t epoch = 0;
     bool sampled = false;
@@ -230,7 +237,10 @@ struct rbmnqs_handle {
     }
     void enqueue_optimize() {
         ck(rbmnqs::launch_schedule(sched.p, st), "schedule");
-        ck(rbmnqs::launch_gram_fp64(O.p, fp64, d.p, N, P, gram_ks, part.p, Sm.p, st), "gram");
+        if (gram_tc)
+            ck(rbmnqs::launch_gram_tc(gtc, O.p, fp64, d.p, gpart.p, gerr.p, Sm.p, st), "tensor-core gram");
+        else
+            ck(rbmnqs::launch_gram_fp64(O.p, fp64, d.p, N, P, gram_ks, part.p, Sm.p, st), "gram");
         ck(rbmnqs::launch_regularize(Sm.p, P, P_neural, N, sched.p, diag.p, Sreg.p, maxdiag.p, st), "regularize");
         mark(4);
         int max_it = std::min(2 * P, cfg.max_iterations);
@@ -370,6 +380,7 @@ int rbmnqs_config_default(rbmnqs_config* c) {
         c->rtol = 0;
         c->precision = 0;
         c->n_updates = 0;
+        c->gram = 0;
     });
 }
 
@@ -479,8 +490,20 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         h->d.alloc(h->P);
         h->F.alloc(h->P);
         h->emean.alloc(1);
-        h->gram_ks = rbmnqs::gram_splits(h->N, h->P);
-        h->part.alloc((size_t)h->gram_ks * h->P * h->P);
+        h->gram_tc = !h->fp64 && cfg->gram == 0;
+        if (h->gram_tc) {
+            ck(rbmnqs::gram_tc_plan(h->N, h->P, &h->gtc), "gram plan");
+            const size_t pf = h->gtc.plane_floats();
+            h->gplanes.alloc(2 * pf);
+            ck(cudaMemsetAsync(h->gplanes.p, 0, 2 * pf * sizeof(float), h->st), "memset");  // padding stays 0
+            h->gpart.alloc(h->gtc.partial_bytes() / sizeof(float));
+            h->gerr.alloc(1);
+            ck(cudaMemsetAsync(h->gerr.p, 0, sizeof(int), h->st), "memset");
+            ck(rbmnqs::gram_tc_maps(&h->gtc, h->gplanes.p, h->gplanes.p + pf), "tensor map");
+        } else {
+            h->gram_ks = rbmnqs::gram_splits(h->N, h->P);
+            h->part.alloc((size_t)h->gram_ks * h->P * h->P);
+        }
         h->Sm.alloc((size_t)h->P * h->P);
         h->Sreg.alloc((size_t)h->P * h->P);
         h->diag.alloc(h->P);
@@ -580,7 +603,10 @@ static void read_sr_stats(rbmnqs_handle* h, rbmnqs_sr_stats* out) {
     rbmnqs::ScheduleDev sd{};
     ck(cudaMemcpyAsync(&r, h->cgres.p, sizeof(r), cudaMemcpyDeviceToHost, h->st), "copy");
     ck(cudaMemcpyAsync(&sd, h->sched.p, sizeof(sd), cudaMemcpyDeviceToHost, h->st), "copy");
+    int gerr = 0;
+    if (h->gram_tc) ck(cudaMemcpyAsync(&gerr, h->gerr.p, sizeof(int), cudaMemcpyDeviceToHost, h->st), "copy");
     ck(cudaStreamSynchronize(h->st), "sync");
+    if (gerr) throw Fail{RBMNQS_ERR_CUDA, "tensor-core Gram: pipeline wait timed out (code " + std::to_string(gerr) + ")"};
     if (out) {
         out->iterations = r.iterations;
         out->status = r.status;

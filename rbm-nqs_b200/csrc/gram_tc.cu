@@ -1,0 +1,381 @@
+// gram_tc.cu -- the SR Gram S = <conj(O - d) (O - d)^T> on the 5th-generation
+// tensor cores (tcgen05, kind::tf32, accumulator in TMEM).
+//
+// Real embedding: with X[n][2p] = Re(O - d)[n][p], X[n][2p+1] = Im(...), the
+// real Gram G = X^T X gives S_pq = (G[2p][2q] + G[2p+1][2q+1]
+//                                   + i (G[2p][2q+1] - G[2p+1][2q])) / N.
+// Split precision: X = Xh + Xl with Xh, Xl rounded to TF32;
+// G ~= Xh Xh^T + Xh Xl^T + Xl Xh^T accumulated in FP32 inside TMEM (the
+// dropped Xl Xl^T term is ~2^-22 relative), split-K partial tiles are
+// summed in FP64.
+//
+// Layout: Xh, Xl are K-major [R][K] fp32 (row r = real parameter 2p or
+// 2p+1, K = samples, both zero-padded to tile multiples).  One CTA owns one
+// 128x128 tile (tp <= tq) of G and one range of K: TMA (128-byte swizzle,
+// box 32 x 128) fills a two-stage ring of {Ah, Al, Bh, Bl} tiles; one thread
+// issues three tcgen05.mma (M = N = 128, K = 8) per k-step and commits each
+// stage back to its "empty" barrier; four warps read the accumulator with
+// tcgen05.ld and store the FP32 partial tile.  Every wait is bounded: on
+// timeout the kernel records an error code, stops issuing, drains and frees
+// its TMEM.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cstdint>
+
+#include "common.cuh"
+#include "gram_tc.cuh"
+
+namespace rbmnqs {
+namespace {
+
+constexpr int TILE = 128;                     // M = N tile (rows of G)
+constexpr int BK = 32;                        // K per stage (128 B of fp32)
+constexpr int STAGE_TILE_BYTES = TILE * BK * 4;  // 16 KB
+constexpr int STAGE_BYTES = 4 * STAGE_TILE_BYTES;  // Ah, Al, Bh, Bl
+constexpr int STAGES = 3;
+constexpr uint32_t kSpin = 1u << 22;          // bounded mbarrier waits
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false after kSpin unsuccessful polls.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+    for (uint32_t i = 0; i < kSpin; i++)
+        if (mbar_try(bar, phase)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
+        : "memory");
+}
+
+// K-major operand tile, 128-byte swizzle: start >> 4, LBO field 1, SBO =
+// 1024 B (8 rows of 128 B), descriptor version 1, layout type 2.
+__device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)(1024 >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+
+// kind::tf32 instruction descriptor: FP32 accumulate, TF32 A and B, both
+// K-major, N = 128, M = 128.
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TILE >> 3) << 17) |
+                            ((uint32_t)(TILE >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t a, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem),
+        "l"(a), "l"(b), "r"(kIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__global__ void __launch_bounds__(128, 1)
+    gram_tc_kernel(const __grid_constant__ CUtensorMap mh, const __grid_constant__ CUtensorMap ml, int ntile,
+                   int nkb_total, float* __restrict__ part, int* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full_bar[STAGES], empty_bar[STAGES], done_bar;
+    __shared__ uint32_t tmem_base;
+    __shared__ int failed, mma_count;
+
+    // tile (tp <= tq) of the upper triangle and this CTA's k-block range
+    int t = blockIdx.x, tp = 0;
+    while (t >= ntile - tp) {
+        t -= ntile - tp;
+        tp++;
+    }
+    const int tq = tp + t;
+    const int split = blockIdx.y, nsplit = gridDim.y;
+    const int kb0 = (int)((long)nkb_total * split / nsplit), kb1 = (int)((long)nkb_total * (split + 1) / nsplit);
+    const int nkb = kb1 - kb0;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;  // 1024-B aligned ring
+
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(smem_u32(&full_bar[s]), 1);
+            mbar_init(smem_u32(&empty_bar[s]), 1);
+        }
+        mbar_init(smem_u32(&done_bar), 1);
+        failed = 0;
+        mma_count = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                     "r"(TILE));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base;
+
+    if (tid == 0 && nkb > 0) {
+        auto stage_addr = [&](int s, int which) { return base + s * STAGE_BYTES + which * STAGE_TILE_BYTES; };
+        auto load = [&](int i) {  // k-block i of this CTA into stage i % STAGES
+            const int s = i % STAGES;
+            const uint32_t fb = smem_u32(&full_bar[s]);
+            const int x = (kb0 + i) * BK;
+            mbar_expect_tx(fb, STAGE_BYTES);
+            tma_load_2d(stage_addr(s, 0), &mh, fb, x, tp * TILE);
+            tma_load_2d(stage_addr(s, 1), &ml, fb, x, tp * TILE);
+            tma_load_2d(stage_addr(s, 2), &mh, fb, x, tq * TILE);
+            tma_load_2d(stage_addr(s, 3), &ml, fb, x, tq * TILE);
+        };
+        bool ok = true;
+        int issued = 0, consumed = 0;  // loads issued, k-blocks whose MMAs were issued
+        for (; issued < nkb && issued < STAGES; issued++) load(issued);
+        for (int i = 0; i < nkb; i++) {
+            const int s = i % STAGES;
+            if (!(ok = mbar_wait(smem_u32(&full_bar[s]), (i / STAGES) & 1))) break;
+            asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll
+            for (int k = 0; k < BK / 8; k++) {
+                const uint32_t off = k * 32;  // 8 tf32 = 32 B along K inside the swizzled row
+                const uint64_t ah = desc_sw128(stage_addr(s, 0) + off), al = desc_sw128(stage_addr(s, 1) + off);
+                const uint64_t bh = desc_sw128(stage_addr(s, 2) + off), bl = desc_sw128(stage_addr(s, 3) + off);
+                mma_tf32(tmem, ah, bh, (i > 0 || k > 0) ? 1u : 0u);
+                mma_tf32(tmem, ah, bl, 1u);
+                mma_tf32(tmem, al, bh, 1u);
+            }
+            mma_commit(smem_u32(&empty_bar[s]));
+            consumed = i + 1;
+            // refill the stage of k-block i-1 once its MMAs are done (those
+            // of k-block i stay queued meanwhile)
+            if (i >= 1 && issued < nkb) {
+                const int j = i - 1;
+                if (!(ok = mbar_wait(smem_u32(&empty_bar[j % STAGES]), (j / STAGES) & 1))) break;
+                load(issued++);
+            }
+        }
+        if (consumed > 0) mma_commit(smem_u32(&done_bar));
+        if (!ok) {
+            failed = 1;
+            atomicExch(err, 1);
+            // drain (bounded): loads in flight that no MMA consumed
+            for (int i = consumed; i < issued; i++) (void)mbar_wait(smem_u32(&full_bar[i % STAGES]), (i / STAGES) & 1);
+        }
+        mma_count = consumed;
+    }
+    __syncthreads();
+    // all MMAs retired (also after a failure); 'have' is block-uniform so the
+    // warp-collective TMEM loads below run converged
+    const int done = mma_count > 0 ? (int)mbar_wait(smem_u32(&done_bar), 0) : 1;
+    const bool have = __syncthreads_and(done) && nkb > 0 && !failed;
+    if (!have && tid == 0 && !failed && nkb > 0) atomicExch(err, 2);
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    // epilogue: warp w reads TMEM lanes (rows) 32w..32w+31, 16 columns at a time
+    const int row = 32 * warp + lane;
+    float* dst = part + (((size_t)split * gridDim.x + blockIdx.x) * TILE + row) * TILE;
+    __syncwarp();
+    for (int c = 0; c < TILE; c += 16) {
+        uint32_t r[16];
+        if (have) {
+            tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c, r);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; j++) r[j] = 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < 16; j += 4)
+            *reinterpret_cast<float4*>(dst + c + j) =
+                make_float4(__uint_as_float(r[j]), __uint_as_float(r[j + 1]), __uint_as_float(r[j + 2]),
+                            __uint_as_float(r[j + 3]));
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TILE));
+    }
+}
+
+// O (N x P complex, fp32 or fp64), d -> K-major TF32 hi / lo planes
+// Xh[r][n], Xl[r][n] with r = 2p (real) / 2p+1 (imag); 32 x 32 transpose
+// tiles through shared memory.
+template <typename TO>
+__global__ void gram_prep(const TO* __restrict__ O, const double2* __restrict__ d, int N, int P, int ld,
+                          float* __restrict__ Xh, float* __restrict__ Xl) {
+    __shared__ float2 tile[32][33];
+    const int n0 = blockIdx.x * 32, p0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+    for (int r = ty; r < 32; r += 8) {
+        const int n = n0 + r, p = p0 + tx;
+        float2 v = make_float2(0.f, 0.f);
+        if (n < N && p < P) {
+            const double2 dd = d[p];
+            if constexpr (sizeof(TO) == 8) {
+                const float2 o = reinterpret_cast<const float2*>(O)[(size_t)n * P + p];
+                v = make_float2((float)((double)o.x - dd.x), (float)((double)o.y - dd.y));
+            } else {
+                const double2 o = reinterpret_cast<const double2*>(O)[(size_t)n * P + p];
+                v = make_float2((float)(o.x - dd.x), (float)(o.y - dd.y));
+            }
+        }
+        tile[r][tx] = v;
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const int p = p0 + r, n = n0 + tx;
+        if (p >= P || n >= N) continue;
+        const float2 v = tile[tx][r];
+        const float c[2] = {v.x, v.y};
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            uint32_t hi;
+            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(c[q]));
+            const float h = __uint_as_float(hi);
+            uint32_t lo;
+            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(c[q] - h));
+            Xh[(size_t)(2 * p + q) * ld + n] = h;
+            Xl[(size_t)(2 * p + q) * ld + n] = __uint_as_float(lo);
+        }
+    }
+}
+
+// S[p][q] (p <= q) from the split partial tiles of G; Hermitian mirror.
+__global__ void gram_tc_finalize(const float* __restrict__ part, int ntile, int nsplit, int N, int P,
+                                 double2* __restrict__ S) {
+    const int nup = ntile * (ntile + 1) / 2;
+    const size_t total = (size_t)P * P;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int p = (int)(i / P), q = (int)(i % P);
+        if (q < p) continue;
+        const int rr = 2 * p, cc = 2 * q;
+        const int tp = rr / TILE, tq = cc / TILE;
+        const int tile = tp * ntile - tp * (tp - 1) / 2 + (tq - tp);
+        const int lr = rr % TILE, lc = cc % TILE;
+        double g00 = 0, g11 = 0, g01 = 0, g10 = 0;
+        for (int s = 0; s < nsplit; s++) {
+            const float* T = part + ((size_t)s * nup + tile) * TILE * TILE;
+            g00 += T[lr * TILE + lc];
+            g11 += T[(lr + 1) * TILE + lc + 1];
+            g01 += T[lr * TILE + lc + 1];
+            g10 += T[(lr + 1) * TILE + lc];
+        }
+        double2 v = make_double2((g00 + g11) / N, (g01 - g10) / N);
+        if (p == q) v.y = 0;
+        S[i] = v;
+        S[(size_t)q * P + p] = make_double2(v.x, -v.y);
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+}  // namespace
+
+size_t GramTC::partial_bytes() const { return (size_t)nsplit * (ntile * (ntile + 1) / 2) * TILE * TILE * 4; }
+
+cudaError_t gram_tc_plan(int N, int P, GramTC* g) {
+    g->N = N;
+    g->P = P;
+    g->R = ((2 * P + TILE - 1) / TILE) * TILE;
+    g->K = ((N + BK - 1) / BK) * BK;
+    g->ntile = g->R / TILE;
+    const int nup = g->ntile * (g->ntile + 1) / 2;
+    const int nkb = g->K / BK;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int ns = sms / nup;
+    if (ns < 1) ns = 1;
+    if (ns > nkb) ns = nkb;
+    g->nsplit = ns;
+    return cudaSuccess;
+}
+
+cudaError_t gram_tc_maps(GramTC* g, float* Xh, float* Xl) {
+    auto fn = encode_fn();
+    if (!fn) return cudaErrorNotSupported;
+    g->Xh = Xh;
+    g->Xl = Xl;
+    for (int which = 0; which < 2; which++) {
+        CUtensorMap* m = reinterpret_cast<CUtensorMap*>(which == 0 ? g->map_h : g->map_l);
+        const cuuint64_t dims[2] = {(cuuint64_t)g->K, (cuuint64_t)g->R};
+        const cuuint64_t strides[1] = {(cuuint64_t)g->K * 4};
+        const cuuint32_t box[2] = {BK, TILE};
+        const cuuint32_t estr[2] = {1, 1};
+        CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, which == 0 ? (void*)Xh : (void*)Xl, dims, strides, box,
+                        estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_gram_tc(const GramTC& g, const void* O, int fp64, const double2* d, float* part, int* err,
+                           double2* S, cudaStream_t st) {
+    dim3 pg((g.N + 31) / 32, (g.P + 31) / 32);
+    if (fp64)
+        gram_prep<double2><<<pg, 256, 0, st>>>((const double2*)O, d, g.N, g.P, g.K, g.Xh, g.Xl);
+    else
+        gram_prep<float2><<<pg, 256, 0, st>>>((const float2*)O, d, g.N, g.P, g.K, g.Xh, g.Xl);
+    const int smem = STAGES * STAGE_BYTES + 1024;
+    cudaError_t e = cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const int nup = g.ntile * (g.ntile + 1) / 2;
+    const CUtensorMap* mh = reinterpret_cast<const CUtensorMap*>(g.map_h);
+    const CUtensorMap* ml = reinterpret_cast<const CUtensorMap*>(g.map_l);
+    gram_tc_kernel<<<dim3(nup, g.nsplit), 128, smem, st>>>(*mh, *ml, g.ntile, g.K / BK, part, err);
+    gram_tc_finalize<<<296, 256, 0, st>>>(part, g.ntile, g.nsplit, g.N, g.P, S);
+    return cudaGetLastError();
+}
+
+}  // namespace rbmnqs

@@ -38,7 +38,7 @@ class Config(C.Structure):
         ("pfaffian_refresh", C.c_int32), ("reinit_chains", C.c_int32), ("seed", C.c_uint64),
         ("lr", C.c_double * 3), ("reg1", C.c_double * 3), ("reg2", C.c_double * 3),
         ("deltareg1", C.c_double * 3), ("max_iterations", C.c_int32), ("rtol", C.c_double),
-        ("precision", C.c_int32), ("n_updates", C.c_int32),
+        ("precision", C.c_int32), ("n_updates", C.c_int32), ("gram", C.c_int32),
     ]
 
 

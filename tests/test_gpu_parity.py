@@ -110,9 +110,11 @@ def test_metropolis_fp32_statistics_agree():
 
 
 @pytest.mark.parametrize("case", ["kitaev3_basic_a1", "kitaev4_symm_a4", "toric3_symm_a2"])
-@pytest.mark.parametrize("precision", [1, 0])
-def test_sr_moments_and_gram_match_oracle(case, precision):
-    om, mach, s, rng = make_pair(case, precision=precision, chains=16, spc=32, warmup=2, std=0.2)
+@pytest.mark.parametrize("precision,gram", [(1, 0), (0, 1), (0, 0)])
+def test_sr_moments_and_gram_match_oracle(case, precision, gram):
+    """precision 1 and gram 1: FP64 Gram (1e-10); precision 0 with gram 0:
+    TF32x3 tensor-core Gram with FP32 accumulation (1e-5)."""
+    om, mach, s, rng = make_pair(case, precision=precision, chains=16, spc=32, warmup=2, std=0.2, gram=gram)
     s.sample()
     s.optimize()
     Eg, Og = s.samples()
@@ -121,9 +123,33 @@ def test_sr_moments_and_gram_match_oracle(case, precision):
     So = O.sr_matrix(Og, do)
     assert rel(d, do) < TOL64
     assert rel(F, Fo) < TOL64
-    assert rel(diag, diago) < TOL64
-    assert np.linalg.norm(S - So) / np.linalg.norm(So) < TOL64
+    # diag = N/(N-1) S_pp comes from the Gram
+    tol = TOL32 if (precision == 0 and gram == 0) else TOL64
+    assert rel(diag, diago) < tol
+    assert np.linalg.norm(S - So) / np.linalg.norm(So) < tol
     assert np.allclose(S, S.conj().T, rtol=0, atol=1e-14 * np.abs(S).max())
+
+
+@pytest.mark.parametrize("case,chains,spc", [
+    ("kitaev3_basic_a1", 9, 7),      # N = 63: ragged sample count, 6 x 6 tiles of G
+    ("kitaev3_basic_a1", 256, 16),   # N = 4096, P = 360
+    ("toric3_basic_a2", 128, 16),    # P = 702: 11 x 11 tiles, 66 upper-triangle CTAs
+    ("kitaev4_symm_a4", 256, 16),    # the 32-spin symmetric alpha=4 shape, P = 133
+])
+def test_tensor_core_gram_matches_oracle(case, chains, spc):
+    """S from the tcgen05 TF32x3 Gram against the FP64 oracle on the GPU's own
+    O samples: Frobenius-relative error below 1e-5, element-wise error
+    below 1e-5 of max|S|, exactly Hermitian with a real diagonal."""
+    om, mach, s, rng = make_pair(case, precision=0, chains=chains, spc=spc, warmup=2, std=0.2)
+    s.sample()
+    s.optimize()
+    Eg, Og = s.samples()
+    d, F, diag, S = s.sr_moments()
+    So = O.sr_matrix(Og, O.sr_moments(Og, Eg)[0])
+    assert np.linalg.norm(S - So) / np.linalg.norm(So) < TOL32
+    assert np.max(np.abs(S - So)) < TOL32 * np.abs(So).max()
+    assert np.array_equal(S, S.conj().T)
+    assert np.all(np.diag(S).imag == 0)
 
 
 @pytest.mark.parametrize("case", ["kitaev3_basic_a1", "kitaev4_symm_a4"])
