@@ -70,6 +70,11 @@ int rbmnqs_model_op(const rbmnqs_model* m, int32_t o, int32_t* k,
  * by rbm.type=symmetry (bravais.cpp:160-247, honeycomb.cpp:69-134). */
 int rbmnqs_model_symmetry(const rbmnqs_model* m, int32_t* S, int32_t* n_vb,
                           int32_t* perm, int32_t* basis);
+/* Pfaffian pair-class matrix bs_ (pfaffian.cpp:31-85) of the model's lattice
+ * for a symmetry value: bs[i*n + j] = signed 1-based class of pair (i, j)
+ * (bs may be NULL) and the number of classes n_indep.  Host only. */
+int rbmnqs_model_pfaffian_classes(const rbmnqs_model* m, double symmetry,
+                                  int32_t* bs, int32_t* n_indep);
 void rbmnqs_model_destroy(rbmnqs_model* m);
 
 /* ----------------------------------------------------------- config ---- */

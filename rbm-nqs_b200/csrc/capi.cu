@@ -133,6 +133,12 @@ struct rbmnqs_handle {
     DevBuf<rbmnqs::HamDev> hdev;
     DevBuf<rbmnqs::CgResultDev> cgres;
     DevBuf<rbmnqs::EpochStatsDev> stats;
+    // Pfaffian factor: class matrix, derivative pairs, unscramble buffers
+    int pf_n = 0, pf_indep = 0;
+    DevBuf<int16_t> pf_bs;
+    DevBuf<int> pf_ptr;
+    DevBuf<uint32_t> pf_pairs;
+    DevBuf<double2> pf_scratch;
     // tensor-core Gram (mixed precision): TF32 hi / lo planes, FP32 split-K
     // partial tiles, pipeline error flag
     bool gram_tc = false;
@@ -175,6 +181,16 @@ struct rbmnqs_handle {
         m.perm = perm.p;
         m.inv = inv.p;
         m.orbit = orbit.p;
+        if (pf_n) {
+            m.pf.n = pf_n;
+            m.pf.n_indep = pf_indep;
+            m.pf.refresh = cfg.pfaffian_refresh;
+            m.pf.bs = pf_bs.p;
+            m.pf.fs = params.p + P_neural;
+            m.pf.pair_ptr = pf_ptr.p;
+            m.pf.pairs = pf_pairs.p;
+            m.pf.scratch = pf_scratch.p;
+        }
         return m;
     }
     rbmnqs::HamDev ham() const {
@@ -351,6 +367,18 @@ int rbmnqs_model_symmetry(const rbmnqs_model* m, int32_t* S, int32_t* n_vb, int3
     });
 }
 
+int rbmnqs_model_pfaffian_classes(const rbmnqs_model* m, double symmetry, int32_t* bs, int32_t* n_indep) {
+    return guard([&] {
+        require(m != nullptr && m->m.lat() != nullptr, "null model");
+        const auto* lat = m->m.lat();
+        int ni = 0;
+        auto v = rbmnqs::pfaffian_index_matrix(m->m.n, lat->symmetry(symmetry), lat->symmetry_basis(symmetry), &ni);
+        if (bs)
+            for (size_t i = 0; i < v.size(); i++) bs[i] = v[i];
+        if (n_indep) *n_indep = ni;
+    });
+}
+
 void rbmnqs_model_destroy(rbmnqs_model* m) { delete m; }
 
 int rbmnqs_config_default(rbmnqs_config* c) {
@@ -391,7 +419,9 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
             throw Fail{RBMNQS_ERR_NO_DEVICE, "no CUDA device available"};
         require(cfg->rbm_type == 0 || cfg->rbm_type == 1, "rbm.type must be basic (0) or symmetry (1)");
-        require(!cfg->pfaffian, "the Pfaffian factor is not available in this build", RBMNQS_ERR_UNSUPPORTED);
+        require(!cfg->pfaffian || mdl->m.n <= rbmnqs::kPfMaxSites,
+                "the Pfaffian factor supports at most 32 sites", RBMNQS_ERR_UNSUPPORTED);
+        require(cfg->pfaffian_refresh >= 0, "sampler.pfaffian_refresh must be >= 0");
         require(cfg->alpha >= 1 && cfg->n_chains >= 1 && cfg->samples_per_chain >= 1 && cfg->step >= 1 &&
                     cfg->warmup >= 0,
                 "bad sampler/machine sizes");
@@ -412,6 +442,18 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         h->T = h->nh * h->S;
         h->P_neural = h->n_vb + h->nh + h->n * h->nh;
         h->P = h->P_neural;
+        std::vector<int> pf_bs_host;
+        if (cfg->pfaffian) {
+            // pfaffian::pfaffian (pfaffian.cpp:31-85) with its own symmetry
+            const auto* lat = m.lat();
+            require(lat != nullptr, "model has no lattice");
+            const double ps = cfg->pfaffian_symmetry;
+            auto pperm = lat->symmetry(ps);
+            auto pbasis = lat->symmetry_basis(ps);
+            pf_bs_host = rbmnqs::pfaffian_index_matrix(h->n, pperm, pbasis, &h->pf_indep);
+            h->pf_n = h->n;
+            h->P += 4 * h->pf_indep;
+        }
         require(rbmnqs::elements_per_lane(h->T) > 0, "theta table larger than 512 entries per chain",
                 RBMNQS_ERR_UNSUPPORTED);
         require(h->P <= 2048, "dense SR path supports at most 2048 parameters", RBMNQS_ERR_UNSUPPORTED);
@@ -450,6 +492,30 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
             ck(cudaMemcpy(h->perm.p, perm.data(), perm.size(), cudaMemcpyHostToDevice), "copy");
             ck(cudaMemcpy(h->inv.p, inv.data(), inv.size(), cudaMemcpyHostToDevice), "copy");
             ck(cudaMemcpy(h->orbit.p, orbit.data(), orbit.size(), cudaMemcpyHostToDevice), "copy");
+        }
+        if (h->pf_n) {
+            const int pn = h->pf_n;
+            std::vector<int16_t> b16(pf_bs_host.begin(), pf_bs_host.end());
+            // derivative gather lists: pairs (i > j) of each class
+            std::vector<std::vector<uint32_t>> cls(h->pf_indep);
+            for (int i = 0; i < pn; i++)
+                for (int j = 0; j < i; j++) {
+                    const int b = pf_bs_host[(size_t)i * pn + j];
+                    require(b != 0, "Pfaffian class matrix has a zero off-diagonal entry");
+                    cls[std::abs(b) - 1].push_back(((uint32_t)i << 16) | ((uint32_t)j << 8) | (b > 0 ? 1u : 0u));
+                }
+            std::vector<int> ptr(1, 0);
+            std::vector<uint32_t> pairs;
+            for (auto& c : cls) {
+                pairs.insert(pairs.end(), c.begin(), c.end());
+                ptr.push_back((int)pairs.size());
+            }
+            h->pf_bs.alloc(b16.size());
+            h->pf_ptr.alloc(ptr.size());
+            h->pf_pairs.alloc(pairs.size());
+            ck(cudaMemcpy(h->pf_bs.p, b16.data(), b16.size() * sizeof(int16_t), cudaMemcpyHostToDevice), "c");
+            ck(cudaMemcpy(h->pf_ptr.p, ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice), "c");
+            ck(cudaMemcpy(h->pf_pairs.p, pairs.data(), pairs.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "c");
         }
         // Hamiltonian
         HamHost hh = build_ham(m.hamiltonian);
@@ -533,6 +599,9 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         // launch shapes: persistent sampler blocks; evaluation kernels with
         // FP32 W in shared memory when it fits
         ck(rbmnqs::plan_sampler(h->machine(), h->fp64, cfg->n_chains, h->n_prop_bonds, &h->shape), "sampler plan");
+        if (h->pf_n)  // one X^{-1} unscramble buffer per sampler warp
+            h->pf_scratch.alloc((size_t)h->shape.blocks * h->shape.warps_per_block * rbmnqs::kPfMaxSites *
+                                rbmnqs::kPfMaxSites);
         if (h->n_prop_bonds > 0 && cfg->bond_flips > 0) {
             const double thr = std::ceil(cfg->bond_flips * 16777216.0);
             h->bond_thr24 = (uint32_t)std::min(thr, 16777216.0);

@@ -10,8 +10,9 @@
 // memory through the per-site permutation table.  psi ratios reduce over the
 // lanes with warp shuffles; every lane holds the same configuration bits and
 // takes the same accept/reject branch.  theta is recomputed in FP64 from the
-// configuration after every sweep (north-star precision scheme), so FP32
-// drift never outlives one sweep.
+// configuration after every sweep (mixed-precision scheme), so FP32
+// drift never outlives one sweep.  With the Pfaffian factor (sites <= 32) each
+// lane also holds its row of X^{-1} in FP64 registers (pfaffian.cuh).
 #include "common.cuh"
 #include "sampler.cuh"
 
@@ -134,10 +135,34 @@ __device__ __forceinline__ void ratio_terms(const MachineDev& m, const uint8_t* 
 // theta): local_op.cpp:31-60, rbm_base.cpp:194-217, rbm_symmetry.cpp:97-130.
 // Kept out of line: it runs once per sample, the sweep loop keeps its
 // registers.
-template <int E, typename R>
+// Pfaffian factor (PF): term ratios multiply by the rank-2m ratio from the
+// warp's X^{-1} in shared memory (pA, leading dimension kPfLd), the O_k of
+// the pair parameters are gathered from it.
+template <int NF>
+__device__ __forceinline__ double2 pf_ratio_smem(const PfDev& p, uint32_t bits, const int* fl, int lane, PfStage& st,
+                                                 const double2* pA) {
+    double2 ib[2 * kPfMaxFlips];
+    auto xi = [&](int t) { return pA[lane * kPfLd + t]; };
+    auto xcol = [&](int f) { return pA[lane * kPfLd + f]; };
+    return pf_ratio<NF>(p, bits, fl, lane, st, xi, xcol, ib);
+}
+
+__device__ __noinline__ double2 pf_ratio_any(const PfDev& p, uint32_t bits, const int* fl, int nf, int lane,
+                                             PfStage& st, const double2* pA) {
+    switch (nf) {
+        case 1: return pf_ratio_smem<1>(p, bits, fl, lane, st, pA);
+        case 2: return pf_ratio_smem<2>(p, bits, fl, lane, st, pA);
+        case 3: return pf_ratio_smem<3>(p, bits, fl, lane, st, pA);
+        case 4: return pf_ratio_smem<4>(p, bits, fl, lane, st, pA);
+        default: return make_double2(nan(""), nan(""));  // more flips than the staging holds
+    }
+}
+
+template <int E, typename R, bool PF>
 __device__ __noinline__ void evaluate(const MachineDev* __restrict__ mp, const HamDev* __restrict__ hp,
                                       const uint8_t* sPerm, const uint8_t* sInv, const C2<R>* W, const C2<R>* wth,
-                                      const uint32_t* wsp, R* cre, C2<R>* cu, int lane, double2* Eout, C2<R>* Orow) {
+                                      const uint32_t* wsp, R* cre, C2<R>* cu, int lane, double2* Eout, C2<R>* Orow,
+                                      PfStage* pst, const double2* pA) {
     const MachineDev m = *mp;
     const HamDev H = *hp;
     // ln cosh cache of the current theta
@@ -176,8 +201,14 @@ __device__ __noinline__ void evaluate(const MachineDev* __restrict__ mp, const H
                 const double mag = exp((double)dre + b.x);
                 double sb, cb;
                 sincos(b.y, &sb, &cb);
-                const double rx = mag * ((double)ph.x * cb - (double)ph.y * sb);
-                const double ry = mag * ((double)ph.x * sb + (double)ph.y * cb);
+                double rx = mag * ((double)ph.x * cb - (double)ph.y * sb);
+                double ry = mag * ((double)ph.x * sb + (double)ph.y * cb);
+                if constexpr (PF) {
+                    const double2 c2 = pf_ratio_any(m.pf, wsp[0], fl, nf, lane, *pst, pA);
+                    const double2 r = zmul(make_double2(rx, ry), c2);
+                    rx = r.x;
+                    ry = r.y;
+                }
                 ex += val.x * rx - val.y * ry;
                 ey += val.x * ry + val.y * rx;
             }
@@ -273,8 +304,16 @@ __host__ __device__ inline int padded_T(int T) { return 32 * ((T + 31) / 32); }
 
 // per-warp scratch.  Evaluation: spins (16 B) | theta [T] | ln cosh re [T] |
 // phase / tanh [T].  Sweeps: proposal ln|cosh| [TP].
-__host__ __device__ inline int eval_warp_bytes(int T, int rsize) { return align16(16 + T * 5 * rsize); }
-__host__ __device__ inline int sweep_warp_bytes(int T, int rsize) { return align16(padded_T(T) * rsize); }
+// With the Pfaffian factor: + the PfStage staging and the n x n FP64 matrix
+// X^{-1} (both), + the evaluation's unscramble buffer.
+__host__ __device__ inline int eval_rbm_bytes(int T, int rsize) { return align16(16 + T * 5 * rsize); }
+__host__ __device__ inline int sweep_rbm_bytes(int T, int rsize) { return align16(padded_T(T) * rsize); }
+__host__ __device__ inline int eval_warp_bytes(int T, int rsize, int pf) {
+    return eval_rbm_bytes(T, rsize) + (pf ? (int)sizeof(PfStage) + 2 * kPfMatBytes : 0);
+}
+__host__ __device__ inline int sweep_warp_bytes(int T, int rsize, int pf) {
+    return sweep_rbm_bytes(T, rsize) + (pf ? (int)sizeof(PfStage) + kPfMatBytes : 0);
+}
 
 __host__ __device__ inline int table_bytes(const MachineDev& m, int fp64, const SmemPlan& pl, int n_bonds) {
     const int TP = padded_T(m.T);
@@ -395,8 +434,15 @@ __device__ __forceinline__ void chain_finish(const SamplerArgs& a, int chain, in
 // (theta, ln cosh, bits) to local memory.  Randomness: Philox4x32-10 with
 // counter {proposal, epoch, chain, 0}; lane j draws proposal (base + j), so
 // one Philox call per lane serves 32 proposals.
-template <int E, typename R>
-__device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, int chain, int lane, R* wlp) {
+//
+// PF: the Pfaffian factor rides along (pfaffian.cuh): fresh X^{-1} at chain
+// start, ratio of every proposal by the rank-2m formula, X^{-1} updated on
+// acceptance and rebuilt every pf.refresh accepted moves
+// (abstract_sampler.cpp:103-113).  pst / pA: the warp's staging and X^{-1}
+// in shared memory; pscr: its unscramble buffer in global memory.
+template <int E, typename R, bool PF>
+__device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, int chain, int lane, R* wlp,
+                                          PfStage* pst, double2* pA, double2* pscr) {
     const MachineDev& m = a.m;
     const C2<R>* W = Wsel<R>::get(m, sm.W32 ? sm.W32 : m.W32);
     const double2* W64 = sm.W64 ? sm.W64 : m.W64;
@@ -411,6 +457,13 @@ __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, 
     theta_fp64<E, R>(m, W64, sm.perm, lane, sp, th);
 #pragma unroll
     for (int e = 0; e < E; e++) L[e] = slot_valid(lane, e, m.T) ? lnc_re<R>(th[e].x, th[e].y) : (R)0;
+
+    // Pfaffian context (pfaffian.cpp:284-297)
+    double2 ib[2 * kPfMaxFlips];
+    int ar = 0;  // accepted moves since the chain start (refresh counter)
+    if constexpr (PF) pf_fresh(m.pf, sp[0], lane, pA, *pst, pscr, kPfMaxSites);
+    auto xi = [&](int t) { return pA[lane * kPfLd + t]; };
+    auto xcol = [&](int f) { return pA[lane * kPfLd + f]; };
 
     // U(f, e): the flip row of site f for this lane's entry e
     auto U = [&](int f, int e) -> C2<R> {
@@ -476,8 +529,18 @@ __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, 
                 const int fl[2] = {f0, f1};
                 d += (R)bias_delta(m, sp, fl, f1 >= 0 ? 2 : 1).x;
             }
-            // accept with min(1, |psi'/psi|^2) (metropolis_sampler.cpp:223-243)
-            if (unit24<R>(r2) < exp_r((R)2 * d)) {
+            // accept with min(1, |psi'/psi|^2) (metropolis_sampler.cpp:223-243);
+            // with the Pfaffian factor |psi'/psi|^2 = e^{2d} |Pf ratio|^2
+            bool accept;
+            if constexpr (PF) {
+                const int fl[2] = {f0, f1};
+                const double2 c2 = f1 >= 0 ? pf_ratio<2>(m.pf, sp[0], fl, lane, *pst, xi, xcol, ib)
+                                           : pf_ratio<1>(m.pf, sp[0], fl, lane, *pst, xi, xcol, ib);
+                accept = (double)unit24<R>(r2) < exp(2.0 * (double)d) * zabs2(c2);
+            } else {
+                accept = unit24<R>(r2) < exp_r((R)2 * d);
+            }
+            if (accept) {
 #pragma unroll
                 for (int e = 0; e < E; e++) {
                     if (!slot_valid(lane, e, m.T)) continue;
@@ -494,6 +557,13 @@ __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, 
                 flip_bit(sp, f0);
                 if (f1 >= 0) flip_bit(sp, f1);
                 nacc++;
+                if constexpr (PF) {
+                    ar++;
+                    if (m.pf.refresh && ar % m.pf.refresh == 0)
+                        pf_fresh(m.pf, sp[0], lane, pA, *pst, pscr, kPfMaxSites);
+                    else
+                        pf_accept(f1 >= 0 ? 2 : 1, lane, *pst, ib, pA, m.pf.n);
+                }
             }
         }
         // FP64 recompute of theta once per sweep
@@ -639,40 +709,44 @@ __device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem&
 
 // Thread bound per entries-per-lane: 28 warps (896 threads, 72 registers)
 // keep 4096 chains resident on 148 SMs for E <= 4.
-template <int E> struct MaxThreads {
-    static constexpr int v = E <= 2 ? 1024 : (E <= 4 ? 896 : (E <= 8 ? 512 : 256));
+template <int E, bool PF = false> struct MaxThreads {
+    static constexpr int v = PF ? 256 : (E <= 2 ? 1024 : (E <= 4 ? 896 : (E <= 8 ? 512 : 256)));
 };
 
 // All chains at once, persistent warps: global warp g = warp * gridDim.x +
 // blockIdx.x takes chains g, g + total_warps, ... so consecutive chains land
 // on different SMs and every block holds the tables once.  FAST selects the
 // FP32 expanded-table path.
-template <int E, typename R, bool FAST>
-__global__ void __launch_bounds__(MaxThreads<E>::v, 1) sampler_kernel(const SamplerArgs a) {
+template <int E, typename R, bool FAST, bool PF>
+__global__ void __launch_bounds__(MaxThreads<E, PF>::v, 1) sampler_kernel(const SamplerArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int fp64 = sizeof(R) == 8;
-    Smem sm = carve(smem, a.m, fp64, a.plan, a.n_prop_bonds, sweep_warp_bytes(a.m.T, sizeof(R)));
+    Smem sm = carve(smem, a.m, fp64, a.plan, a.n_prop_bonds, sweep_warp_bytes(a.m.T, sizeof(R), PF));
     load_tables(a.m, sm, fp64, a.plan, a.prop_bonds, a.n_prop_bonds);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     R* wlp = reinterpret_cast<R*>(sm.warp0 + warp * sm.warp_bytes);
+    PfStage* pst = reinterpret_cast<PfStage*>(sm.warp0 + warp * sm.warp_bytes + sweep_rbm_bytes(a.m.T, sizeof(R)));
+    double2* pA = reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(pst) + sizeof(PfStage));
+    double2* pscr = PF ? a.m.pf.scratch + (size_t)(blockIdx.x * (blockDim.x >> 5) + warp) * kPfMaxSites * kPfMaxSites
+                       : nullptr;
     const int total_warps = (blockDim.x >> 5) * gridDim.x;
     for (int chain = warp * gridDim.x + blockIdx.x; chain < a.n_chains; chain += total_warps) {
         if constexpr (FAST)
             run_chain_fast<E>(a, sm, chain, lane);
         else
-            run_chain<E, R>(a, sm, chain, lane, wlp);
+            run_chain<E, R, PF>(a, sm, chain, lane, wlp, pst, pA, pscr);
     }
 }
 
 // ---------------------------------------------------------------------------
 // Batched evaluation at given configurations: log psi, E_loc, O_k, or the
 // log psi ratio for given flips (parity entry points).
-template <int E, typename R>
+template <int E, typename R, bool PF>
 __global__ void __launch_bounds__(256) eval_kernel(const EvalArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const MachineDev& m = a.m;
     const int fp64 = sizeof(R) == 8;
-    Smem sm = carve(smem, m, fp64, a.plan, 0, eval_warp_bytes(m.T, sizeof(R)));
+    Smem sm = carve(smem, m, fp64, a.plan, 0, eval_warp_bytes(m.T, sizeof(R), PF));
     load_tables(m, sm, fp64, a.plan, nullptr, 0);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b = blockIdx.x * (blockDim.x >> 5) + warp;
@@ -682,6 +756,8 @@ __global__ void __launch_bounds__(256) eval_kernel(const EvalArgs a) {
     C2<R>* wth = reinterpret_cast<C2<R>*>(wbase + 16);
     R* cre = reinterpret_cast<R*>(wbase + 16 + m.T * 2 * sizeof(R));
     C2<R>* cu = reinterpret_cast<C2<R>*>(wbase + 16 + m.T * 3 * sizeof(R));
+    PfStage* pst = reinterpret_cast<PfStage*>(wbase + eval_rbm_bytes(m.T, sizeof(R)));
+    double2* pA = reinterpret_cast<double2*>(wbase + eval_rbm_bytes(m.T, sizeof(R)) + sizeof(PfStage));
     const C2<R>* W = Wsel<R>::get(m, sm.W32 ? sm.W32 : m.W32);
     uint32_t sp[4];
 #pragma unroll
@@ -704,6 +780,8 @@ __global__ void __launch_bounds__(256) eval_kernel(const EvalArgs a) {
         }
         re = warp_sum(re);
         im = warp_sum(im);
+        double2 lpf = make_double2(0.0, 0.0);
+        if constexpr (PF) lpf = pf_log_pfaffian(m.pf, sp[0], lane, pA);  // pfaffian.hpp:73-75
         if (lane == 0) {
             double bx = 0, by = 0;
             for (int i = 0; i < m.n_vb; i++) {
@@ -716,8 +794,12 @@ __global__ void __launch_bounds__(256) eval_kernel(const EvalArgs a) {
                 bx += m.vb[i].x * ssum;
                 by += m.vb[i].y * ssum;
             }
-            a.logpsi[b] = make_double2(bx + (double)re - 0.69314718055994531 * m.T, by + (double)im);
+            a.logpsi[b] = make_double2(bx + (double)re - 0.69314718055994531 * m.T + lpf.x, by + (double)im + lpf.y);
         }
+    }
+    if constexpr (PF) {
+        // X^{-1} of this configuration into the warp's matrix
+        if (a.ratio || a.eloc || a.O) pf_fresh(m.pf, sp[0], lane, pA, *pst, pA + kPfMaxSites * kPfLd, kPfLd);
     }
     if (a.ratio) {
 #pragma unroll
@@ -735,15 +817,23 @@ __global__ void __launch_bounds__(256) eval_kernel(const EvalArgs a) {
         R dre;
         C2<R> ph;
         ratio_terms<E, R>(m, sm.perm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph);
+        double2 lr = make_double2(0.0, 0.0);
+        if constexpr (PF) {
+            const double2 c2 = pf_ratio_any(m.pf, sp[0], fl, nf, lane, *pst, pA);
+            lr = make_double2(0.5 * log(zabs2(c2)), atan2(c2.y, c2.x));
+        }
         if (lane == 0) {
             const double2 bd = bias_delta_smem(m, wsp, fl, nf);
-            a.ratio[b] = make_double2((double)dre + bd.x, atan2((double)ph.y, (double)ph.x) + bd.y);
+            a.ratio[b] = make_double2((double)dre + bd.x + lr.x, atan2((double)ph.y, (double)ph.x) + bd.y + lr.y);
         }
         __syncwarp();
     }
     if (a.eloc || a.O) {
         C2<R>* Orow = a.O ? reinterpret_cast<C2<R>*>(a.O) + (size_t)b * m.P : nullptr;
-        evaluate<E, R>(a.md, a.hd, sm.perm, sm.inv, W, wth, wsp, cre, cu, lane, a.eloc ? a.eloc + b : nullptr, Orow);
+        evaluate<E, R, PF>(a.md, a.hd, sm.perm, sm.inv, W, wth, wsp, cre, cu, lane, a.eloc ? a.eloc + b : nullptr,
+                           Orow, pst, pA);
+        if constexpr (PF)
+            if (Orow) pf_derivative(m.pf, sp[0], lane, pA, Orow + m.P_neural);
     }
 }
 
@@ -790,22 +880,31 @@ int elements_per_lane(int T) {
 }
 
 int sampler_smem_bytes(const MachineDev& m, int fp64, int warps, const SmemPlan& plan, int n_bonds) {
-    return table_bytes(m, fp64, plan, n_bonds) + warps * sweep_warp_bytes(m.T, fp64 ? 8 : 4);
+    return table_bytes(m, fp64, plan, n_bonds) + warps * sweep_warp_bytes(m.T, fp64 ? 8 : 4, m.pf.n > 0);
 }
 
 int eval_smem_bytes(const MachineDev& m, int fp64, int warps, const SmemPlan& plan) {
-    return table_bytes(m, fp64, plan, 0) + warps * eval_warp_bytes(m.T, fp64 ? 8 : 4);
+    return table_bytes(m, fp64, plan, 0) + warps * eval_warp_bytes(m.T, fp64 ? 8 : 4, m.pf.n > 0);
 }
 
-template <int E, typename R, bool FAST> static const void* sampler_fn() {
-    return reinterpret_cast<const void*>(sampler_kernel<E, R, FAST>);
+template <int E, typename R, bool FAST, bool PF> static const void* sampler_fn() {
+    return reinterpret_cast<const void*>(sampler_kernel<E, R, FAST, PF>);
 }
 
-static const void* pick_sampler(int E, int fp64, int exp_table) {
+// The Pfaffian variants exist for theta tables up to 128 entries (32 sites,
+// alpha <= 4); they take the general (non-table) sweep.
+static const void* pick_sampler(int E, int fp64, int exp_table, int pf) {
+    if (pf) {
+#define RBMNQS_PICK_PF(EE) \
+    if (E == EE) return fp64 ? sampler_fn<EE, double, false, true>() : sampler_fn<EE, float, false, true>();
+        RBMNQS_PICK_PF(1) RBMNQS_PICK_PF(2) RBMNQS_PICK_PF(4)
+#undef RBMNQS_PICK_PF
+        return nullptr;
+    }
 #define RBMNQS_PICK(EE)                                                   \
     if (E == EE) {                                                        \
-        if (fp64) return sampler_fn<EE, double, false>();                 \
-        return exp_table ? sampler_fn<EE, float, true>() : sampler_fn<EE, float, false>(); \
+        if (fp64) return sampler_fn<EE, double, false, false>();          \
+        return exp_table ? sampler_fn<EE, float, true, false>() : sampler_fn<EE, float, false, false>(); \
     }
     RBMNQS_PICK(1) RBMNQS_PICK(2) RBMNQS_PICK(4) RBMNQS_PICK(8) RBMNQS_PICK(16)
 #undef RBMNQS_PICK
@@ -825,12 +924,14 @@ cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bond
     SmemPlan pl{};
     // FP32 expanded-table path when the table fits; its theta recompute uses
     // the FP64 expanded table when that fits too, else FP64 W
-    pl.use_u = !fp64 && (m.n + 1) * TP * 8 <= 64 * 1024;
+    const int pf = m.pf.n > 0;
+    pl.use_u = !fp64 && !pf && (m.n + 1) * TP * 8 <= 64 * 1024;
     pl.u64 = pl.use_u && m.n * TP * 16 <= 96 * 1024;
     pl.w32 = !fp64 && !pl.use_u && m.n * m.nh * 8 <= 64 * 1024;
     pl.w64 = m.n * m.nh * 16 <= 32 * 1024;
     pl.bonds = n_bonds > 0 && n_bonds * 8 <= 8 * 1024;
-    const void* fn = pick_sampler(E, fp64, pl.use_u);
+    const void* fn = pick_sampler(E, fp64, pl.use_u, pf);
+    if (!fn) return cudaErrorInvalidValue;
     cudaFuncAttributes fa;
     err = cudaFuncGetAttributes(&fa, fn);
     if (err != cudaSuccess) return err;
@@ -866,20 +967,30 @@ cudaError_t launch_sampler(const SamplerArgs& a0, int fp64, const SamplerShape& 
     SamplerArgs a = a0;
     a.plan = sh.plan;
     const int E = elements_per_lane(a.m.T);
-    const void* fn = pick_sampler(E, fp64, sh.plan.use_u);
+    const void* fn = pick_sampler(E, fp64, sh.plan.use_u, a.m.pf.n > 0);
     if (!fn) return cudaErrorInvalidValue;
     void* args[] = {&a};
     return cudaLaunchKernel(fn, dim3(sh.blocks), dim3(32 * sh.warps_per_block), args, sh.smem, st);
 }
 
-template <int E, typename R>
-static cudaError_t launch_e(const EvalArgs& a, int wpb, cudaStream_t st) {
+template <int E, typename R, bool PF>
+static cudaError_t launch_e2(const EvalArgs& a, int wpb, cudaStream_t st) {
     const int smem = eval_smem_bytes(a.m, sizeof(R) == 8, wpb, a.plan);
-    cudaError_t err = cudaFuncSetAttribute(eval_kernel<E, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t err =
+        cudaFuncSetAttribute(eval_kernel<E, R, PF>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (err != cudaSuccess) return err;
     const int blocks = (a.B + wpb - 1) / wpb;
-    eval_kernel<E, R><<<blocks, 32 * wpb, smem, st>>>(a);
+    eval_kernel<E, R, PF><<<blocks, 32 * wpb, smem, st>>>(a);
     return cudaGetLastError();
+}
+
+template <int E, typename R>
+static cudaError_t launch_e(const EvalArgs& a, int wpb, cudaStream_t st) {
+    if (a.m.pf.n > 0) {
+        if constexpr (E <= 4) return launch_e2<E, R, true>(a, wpb, st);
+        return cudaErrorInvalidValue;
+    }
+    return launch_e2<E, R, false>(a, wpb, st);
 }
 
 #define RBMNQS_DISPATCH(FN, ARGS)                                            \

@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "pfaffian.cuh"
+
 namespace rbmnqs {
 
 // One local operator of the Hamiltonian (operators::local_op): k sites and a
@@ -26,6 +28,7 @@ struct MachineDev {
     const uint8_t* perm;   // [n][S] perm[f*S + s] = P_s(f)      (symmetric)
     const uint8_t* inv;    // [S][n] inv[s*n + j] = P_s^{-1}(j)  (symmetric)
     const uint8_t* orbit;  // [n_vb][S] orbit[i*S + s] = P_s(basis_i)
+    PfDev pf;              // Pfaffian factor (pf.n == 0: none)
 };
 
 struct HamDev {

@@ -78,6 +78,7 @@ def _declare(L):
         "rbmnqs_model_bonds": [VP, P_I],
         "rbmnqs_model_op": [VP, C.c_int32, P_I, P_I, P_D],
         "rbmnqs_model_symmetry": [VP, P_I, P_I, P_I, P_I],
+        "rbmnqs_model_pfaffian_classes": [VP, C.c_double, P_I, P_I],
         "rbmnqs_model_destroy": [VP],
         "rbmnqs_config_default": [C.POINTER(Config)],
         "rbmnqs_create": [VP, C.POINTER(Config), C.POINTER(VP)],
@@ -209,6 +210,14 @@ class Model:
         basis = np.zeros(nvb.value, np.int32)
         _ck(lib().rbmnqs_model_symmetry(self._h, None, None, _p(perm, P_I), _p(basis, P_I)))
         return perm.reshape(S.value, self.n), basis
+
+    def pfaffian_classes(self, symmetry=0.5):
+        """(bs [n, n] signed 1-based pair classes, n_indep) of pfaffian.cpp:31-85."""
+        ni = C.c_int32()
+        _ck(lib().rbmnqs_model_pfaffian_classes(self._h, symmetry, None, C.byref(ni)))
+        bs = np.zeros(self.n * self.n, np.int32)
+        _ck(lib().rbmnqs_model_pfaffian_classes(self._h, symmetry, _p(bs, P_I), C.byref(ni)))
+        return bs.reshape(self.n, self.n), ni.value
 
     def add_hexagons(self):
         _ck(lib().rbmnqs_model_add_hexagons(self._h))

@@ -68,6 +68,18 @@ def test_toric_tables_match_oracle(L):
     assert np.array_equal(perm, rp) and np.array_equal(basis, rb)
 
 
+@pytest.mark.parametrize("kind,L", [("kitaev", 2), ("kitaev", 3), ("kitaev", 4), ("toric", 3), ("toric", 4)])
+@pytest.mark.parametrize("psym", [0.0, 0.5, 1.0])
+def test_pfaffian_classes_match_oracle(kind, L, psym):
+    """Pair-class matrix bs_ and n_indep of pfaffian.cpp:31-85, bit for bit."""
+    m = rbmnqs.Model.kitaev(L) if kind == "kitaev" else rbmnqs.Model.toric(L)
+    om = O.Model.kitaev(L) if kind == "kitaev" else O.Model.toric(L)
+    ref = O.Machine(om, "basic", 1, pfaffian=True, pf_symm=psym)
+    bs, ni = m.pfaffian_classes(psym)
+    assert ni == ref.n_indep
+    assert np.array_equal(bs, ref.bs)
+
+
 def test_hexagon_observables_match_oracle():
     m = rbmnqs.Model.kitaev(3)
     m.add_hexagons()
