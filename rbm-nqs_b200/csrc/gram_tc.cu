@@ -36,6 +36,8 @@ constexpr int STAGE_TILE_BYTES = TILE * BK * 4;  // 16 KB
 constexpr int STAGE_BYTES = 4 * STAGE_TILE_BYTES;  // Ah, Al, Bh, Bl
 constexpr int STAGES = 3;
 constexpr uint32_t kSpin = 1u << 22;          // bounded mbarrier waits
+constexpr int kMaxKbPerSplit = 8;             // FP32 accumulation length per CTA
+constexpr long kMaxPartialBytes = 64L << 20;  // split-K partial tiles
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -334,7 +336,14 @@ cudaError_t gram_tc_plan(int N, int P, GramTC* g) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // enough CTAs for the SMs, and FP32 accumulation runs of at most
+    // kMaxKbPerSplit k-blocks (256 samples) while the partial tiles stay
+    // within kMaxPartialBytes; splits are summed in FP64
     int ns = sms / nup;
+    int acc_splits = (nkb + kMaxKbPerSplit - 1) / kMaxKbPerSplit;
+    const long cap = kMaxPartialBytes / ((long)nup * TILE * TILE * 4);
+    if (acc_splits > cap) acc_splits = (int)(cap < 1 ? 1 : cap);
+    if (ns < acc_splits) ns = acc_splits;
     if (ns < 1) ns = 1;
     if (ns > nkb) ns = nkb;
     g->nsplit = ns;

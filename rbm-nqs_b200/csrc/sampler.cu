@@ -161,8 +161,8 @@ __device__ __noinline__ double2 pf_ratio_any(const PfDev& p, uint32_t bits, cons
 template <int E, typename R, bool PF>
 __device__ __noinline__ void evaluate(const MachineDev* __restrict__ mp, const HamDev* __restrict__ hp,
                                       const uint8_t* sPerm, const uint8_t* sInv, const C2<R>* W, const C2<R>* wth,
-                                      const uint32_t* wsp, R* cre, C2<R>* cu, int lane, double2* Eout, C2<R>* Orow,
-                                      PfStage* pst, const double2* pA) {
+                                      const uint32_t* wsp, R* cre, C2<R>* cu, const C2<R>* tn, int lane,
+                                      double2* Eout, C2<R>* Orow, PfStage* pst, const double2* pA) {
     const MachineDev m = *mp;
     const HamDev H = *hp;
     // ln cosh cache of the current theta
@@ -216,22 +216,15 @@ __device__ __noinline__ void evaluate(const MachineDev* __restrict__ mp, const H
         if (lane == 0) *Eout = make_double2(ex, ey);
     }
     if (Orow) {
-        // tanh(theta) into the (now free) phase cache
-        __syncwarp();
-#pragma unroll
-        for (int e = 0; e < E; e++)
-            if (slot_valid(lane, e, m.T)) {
-                const int t = lane + 32 * e;
-                cu[t] = ctanh_r<R>(wth[t].x, wth[t].y);
-            }
+        // tanh(theta) from the warp's scratch (tn)
         __syncwarp();
         const int n = m.n, nh = m.nh, S = m.S, nvb = m.n_vb;
         auto sg = [&](int i) -> R { return smem_bit(wsp, i) ? (R)-1 : (R)1; };
         if (!m.symmetric) {
             for (int q = lane; q < nvb; q += 32) Orow[q] = mk<R>(sg(q), 0);
-            for (int q = lane; q < nh; q += 32) Orow[nvb + q] = cu[q];
+            for (int q = lane; q < nh; q += 32) Orow[nvb + q] = tn[q];
             for (int k = 0; k < nh; k++) {
-                const C2<R> t = cu[k];
+                const C2<R> t = tn[k];
                 for (int j = lane; j < n; j += 32) {
                     const R s = sg(j);
                     Orow[nvb + nh + j + n * k] = mk<R>(s * t.x, s * t.y);
@@ -246,8 +239,8 @@ __device__ __noinline__ void evaluate(const MachineDev* __restrict__ mp, const H
             for (int q = lane; q < nh; q += 32) {
                 C2<R> acc = mk<R>(0, 0);
                 for (int s = 0; s < S; s++) {
-                    acc.x += cu[q + nh * s].x;
-                    acc.y += cu[q + nh * s].y;
+                    acc.x += tn[q + nh * s].x;
+                    acc.y += tn[q + nh * s].y;
                 }
                 Orow[nvb + q] = acc;
             }
@@ -256,7 +249,7 @@ __device__ __noinline__ void evaluate(const MachineDev* __restrict__ mp, const H
                     C2<R> acc = mk<R>(0, 0);
                     for (int s = 0; s < S; s++) {
                         const R sv = sg(sInv[s * n + j]);
-                        const C2<R> t = cu[k + nh * s];
+                        const C2<R> t = tn[k + nh * s];
                         acc.x = fma(sv, t.x, acc.x);
                         acc.y = fma(sv, t.y, acc.y);
                     }
@@ -303,10 +296,11 @@ __host__ __device__ inline int align16(int x) { return (x + 15) & ~15; }
 __host__ __device__ inline int padded_T(int T) { return 32 * ((T + 31) / 32); }
 
 // per-warp scratch.  Evaluation: spins (16 B) | theta [T] | ln cosh re [T] |
-// phase / tanh [T].  Sweeps: proposal ln|cosh| [TP].
+// phase [T] | tanh theta [T] (evaluated in FP64 from the FP64 theta, so
+// O_k keep FP32 accuracy next to the poles of tanh).  Sweeps: proposal ln|cosh| [TP].
 // With the Pfaffian factor: + the PfStage staging and the n x n FP64 matrix
 // X^{-1} (both), + the evaluation's unscramble buffer.
-__host__ __device__ inline int eval_rbm_bytes(int T, int rsize) { return align16(16 + T * 5 * rsize); }
+__host__ __device__ inline int eval_rbm_bytes(int T, int rsize) { return align16(16 + T * 7 * rsize); }
 __host__ __device__ inline int sweep_rbm_bytes(int T, int rsize) { return align16(padded_T(T) * rsize); }
 __host__ __device__ inline int eval_warp_bytes(int T, int rsize, int pf) {
     return eval_rbm_bytes(T, rsize) + (pf ? (int)sizeof(PfStage) + 2 * kPfMatBytes : 0);
@@ -756,14 +750,26 @@ __global__ void __launch_bounds__(256) eval_kernel(const EvalArgs a) {
     C2<R>* wth = reinterpret_cast<C2<R>*>(wbase + 16);
     R* cre = reinterpret_cast<R*>(wbase + 16 + m.T * 2 * sizeof(R));
     C2<R>* cu = reinterpret_cast<C2<R>*>(wbase + 16 + m.T * 3 * sizeof(R));
+    C2<R>* tn = reinterpret_cast<C2<R>*>(wbase + 16 + m.T * 5 * sizeof(R));
     PfStage* pst = reinterpret_cast<PfStage*>(wbase + eval_rbm_bytes(m.T, sizeof(R)));
     double2* pA = reinterpret_cast<double2*>(wbase + eval_rbm_bytes(m.T, sizeof(R)) + sizeof(PfStage));
     const C2<R>* W = Wsel<R>::get(m, sm.W32 ? sm.W32 : m.W32);
     uint32_t sp[4];
 #pragma unroll
     for (int w = 0; w < 4; w++) sp[w] = a.spins[4 * b + w];
+    C2<double> th64[E];
+    theta_fp64<E, double>(m, m.W64, sm.perm, lane, sp, th64);
     C2<R> th[E];
-    theta_fp64<E, R>(m, m.W64, sm.perm, lane, sp, th);
+#pragma unroll
+    for (int e = 0; e < E; e++) th[e] = mk<R>((R)th64[e].x, (R)th64[e].y);
+    if (a.O) {
+#pragma unroll
+        for (int e = 0; e < E; e++)
+            if (slot_valid(lane, e, m.T)) {
+                const C2<double> t = ctanh_r<double>(th64[e].x, th64[e].y);
+                tn[lane + 32 * e] = mk<R>((R)t.x, (R)t.y);
+            }
+    }
     stage<E, R>(m, sp, th, wsp, wth, lane);
 
     if (a.logpsi) {
@@ -830,8 +836,8 @@ __global__ void __launch_bounds__(256) eval_kernel(const EvalArgs a) {
     }
     if (a.eloc || a.O) {
         C2<R>* Orow = a.O ? reinterpret_cast<C2<R>*>(a.O) + (size_t)b * m.P : nullptr;
-        evaluate<E, R, PF>(a.md, a.hd, sm.perm, sm.inv, W, wth, wsp, cre, cu, lane, a.eloc ? a.eloc + b : nullptr,
-                           Orow, pst, pA);
+        evaluate<E, R, PF>(a.md, a.hd, sm.perm, sm.inv, W, wth, wsp, cre, cu, tn, lane,
+                           a.eloc ? a.eloc + b : nullptr, Orow, pst, pA);
         if constexpr (PF)
             if (Orow) pf_derivative(m.pf, sp[0], lane, pA, Orow + m.P_neural);
     }

@@ -66,7 +66,8 @@ def test_pf_eval_batch_matches_oracle(case, precision, tol):
     logpsi_close(lg, lo, tol)
     assert rel(eg, eo) < tol
     assert rel(Og, Oo) < tol
-    # the pair-parameter block is FP64 arithmetic in both precisions
+    # the pair-parameter block is FP64 arithmetic in both precisions (stored
+    # as FP32 in precision 0)
     P0 = mach.n_neural
     assert rel(Og[:, P0:], Oo[:, P0:]) < (TOL64 if precision == 1 else 1e-6)
 
