@@ -36,10 +36,26 @@ sys.path.insert(0, os.path.join(ROOT, "rbm-nqs_b200"))
 
 import numpy as np  # noqa: E402
 
+# Workloads (seeded synthetic inputs of the benchmark shapes).  The metric
+# line is quoted on kitaev32_symm_a4; the others measure the Pfaffian path and
+# the 128-spin lattice with the same harness.
 WORKLOADS = {
+    # Kitaev 32 spins, symmetric RBM alpha=4, 4096 chains x 64 sweeps,
+    # FP32 sweep / FP64 theta recompute, TF32x3 tensor-core Gram, FP64 CG
     "kitaev32_symm_a4": dict(model="kitaev", n_cells=4, rbm_type=1, alpha=4, symmetry=0.5, n_chains=4096,
                              samples_per_chain=1, warmup=63, step=1, bond_flips=0.5, std=1e-4,
-                             reg2=(1e-4, 1e-4, 1.0)),
+                             reg2=(1e-4, 1e-4, 1.0), precision=0, gram=0),
+    # RBM alpha=2 + Pfaffian (pair classes of symmetry 0.5, std 1e-2), 2048
+    # chains, X^{-1} rebuilt every 32 accepted moves, FP64 Gram and CG
+    "kitaev32_pf_symm_a2": dict(model="kitaev", n_cells=4, rbm_type=1, alpha=2, symmetry=0.5, n_chains=2048,
+                                samples_per_chain=1, warmup=63, step=1, bond_flips=0.5, std=1e-4,
+                                reg2=(1e-4, 1e-4, 1.0), precision=0, gram=1, pfaffian=1, pf_symmetry=0.5,
+                                pf_std=1e-2, pf_refresh=32),
+    # Kitaev 128 spins, symmetric RBM alpha=4, 16384 chains, plain
+    # single-spin/bond Metropolis
+    "kitaev128_symm_a4": dict(model="kitaev", n_cells=8, rbm_type=1, alpha=4, symmetry=0.5, n_chains=16384,
+                              samples_per_chain=1, warmup=63, step=1, bond_flips=0.5, std=1e-4,
+                              reg2=(1e-4, 1e-4, 1.0), precision=0, gram=0),
 }
 METRIC = "uncorrelated samples/s (SR epoch, E_loc binning tau)"
 # DRAM bytes per sampler launch from an ncu capture of the same workload: the
@@ -56,7 +72,18 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="kitaev32_symm_a4", choices=list(WORKLOADS))
     ap.add_argument("--cpu-baseline", type=int, default=1, help="time the CPU restatement beside our arm")
+    ap.add_argument("--chains", type=int, default=0, help="override the workload's chain count (profiling)")
+    ap.add_argument("--sweeps", type=int, default=0, help="override the sweeps per epoch (profiling)")
     return ap.parse_args()
+
+
+def workload(args):
+    wl = dict(WORKLOADS[args.workload])
+    if args.chains:
+        wl["n_chains"] = args.chains
+    if args.sweeps:
+        wl["warmup"] = args.sweeps - wl["samples_per_chain"] * wl["step"]
+    return wl
 
 
 def dist_env():
@@ -74,9 +101,28 @@ def init_dist(world, backend):
     return dist
 
 
-def make_weights(P, std, seed):
+def make_weights(P, std, seed, n_neural=None, pf_std=None):
+    """complex Gaussian weights; pair parameters (index >= n_neural) with pf_std"""
     rng = np.random.default_rng(seed)
-    return rng.normal(0, std, P) + 1j * rng.normal(0, std, P)
+    w = rng.normal(0, std, P) + 1j * rng.normal(0, std, P)
+    if n_neural is not None and pf_std is not None and n_neural < P:
+        m = P - n_neural
+        w[n_neural:] = rng.normal(0, pf_std, m) + 1j * rng.normal(0, pf_std, m)
+    return w
+
+
+def describe(wl, P):
+    kind = "symmetric RBM" if wl["rbm_type"] == 1 else "RBM"
+    d = {"model": f"kitaev honeycomb n_cells={wl['n_cells']} ({2 * wl['n_cells'] ** 2} spins) J=-1",
+         "machine": f"{kind} alpha={wl['alpha']}" + (" + Pfaffian (pair symmetry %g)" % wl["pf_symmetry"]
+                                                      if wl.get("pfaffian") else "") + f", {P} params",
+         "n_chains": wl["n_chains"], "sweeps_per_epoch": wl["warmup"] + wl["samples_per_chain"] * wl["step"],
+         "samples_per_epoch": wl["n_chains"] * wl["samples_per_chain"], "bond_flips": wl["bond_flips"],
+         "gram": "TF32x3 tcgen05" if wl["gram"] == 0 and wl["precision"] == 0 else "FP64",
+         "sr": "CG reg2=1e-4 reg1=(1,1e-4,0.9) lr=1e-2"}
+    if wl.get("pfaffian"):
+        d["pfaffian_refresh"] = wl["pf_refresh"]
+    return d
 
 
 class ClockSampler:
@@ -136,15 +182,17 @@ def run_ours(args, rank, world, local):
 
     dist = init_dist(world, "nccl")
     torch.cuda.set_device(local)
-    wl = WORKLOADS[args.workload]
+    wl = workload(args)
     model = rbmnqs.Model.kitaev(wl["n_cells"], symmetry=wl["symmetry"])
     cfg = rbmnqs.default_config(rbm_type=wl["rbm_type"], alpha=wl["alpha"], n_chains=wl["n_chains"],
                                 samples_per_chain=wl["samples_per_chain"], warmup=wl["warmup"], step=wl["step"],
-                                bond_flips=wl["bond_flips"], seed=1234 + rank, precision=0, reinit_chains=0,
-                                reg2=wl["reg2"])
+                                bond_flips=wl["bond_flips"], seed=1234 + rank, precision=wl["precision"],
+                                gram=wl["gram"], reinit_chains=0, reg2=wl["reg2"],
+                                pfaffian=wl.get("pfaffian", 0), pfaffian_symmetry=wl.get("pf_symmetry", 0.5),
+                                pfaffian_refresh=wl.get("pf_refresh", 0))
     sess = rbmnqs.Session(model, cfg)
     P, N = sess.n_params, sess.N
-    w0 = make_weights(P, wl["std"], 99 + rank)
+    w0 = make_weights(P, wl["std"], 99 + rank, sess.n_neural, wl.get("pf_std"))
     sess.set_weights(w0)
     stream = torch.cuda.ExternalStream(sess.stream())
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
@@ -228,11 +276,8 @@ def run_ours(args, rank, world, local):
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32 ratios / fp64 theta+CG",
             "data": "synthetic (seeded complex Gaussian weights std 1e-4, Philox chains)",
-            "config": {"workload": args.workload, "model": "kitaev honeycomb n_cells=4 (32 spins) J=-1",
-                       "machine": "symmetric RBM alpha=4 (S=32, 133 params)", "n_chains": wl["n_chains"],
-                       "sweeps_per_epoch": sweeps, "samples_per_epoch": N, "bond_flips": wl["bond_flips"],
-                       "sr": "CG reg2=1e-4 reg1=(1,1e-4,0.9) lr=1e-2", "parallelism": f"replicas x{world}",
-                       "l2": "256 MiB L2 flush between timed epochs (outside the event pairs)"},
+            "config": dict(workload=args.workload, **describe(wl, P), parallelism=f"replicas x{world}",
+                           l2="256 MiB L2 flush between timed epochs (outside the event pairs)"),
             "sr_epochs_per_s": world * args.steps / (t_ms * 1e-3),
             "tau": tau, "energy_per_site": float(np.mean(energies)) / model.n, "acceptance": acc,
             "cg_iterations": float(np.mean(its)),
@@ -265,13 +310,15 @@ def cpu_epoch(wl, chains, seed, threads):
     import oracle as O
 
     om = O.Model.kitaev(wl["n_cells"])
-    mach = O.Machine(om, "symmetry", wl["alpha"], symm=wl["symmetry"])
-    mach.set_params(make_weights(mach.n_params, wl["std"], 99))
+    mach = O.Machine(om, "symmetry" if wl["rbm_type"] == 1 else "basic", wl["alpha"], symm=wl["symmetry"],
+                     pfaffian=bool(wl.get("pfaffian")), pf_symm=wl.get("pf_symmetry", 0.5))
+    mach.set_params(make_weights(mach.n_params, wl["std"], 99, mach.n_neural, wl.get("pf_std")))
     t0 = time.perf_counter()
     E, Om, acc, _ = O.metropolis(mach, om, chains, wl["samples_per_chain"], warmup=wl["warmup"],
-                                 step=wl["step"], bond_flips=wl["bond_flips"], seed=seed, threads=threads)
+                                 step=wl["step"], bond_flips=wl["bond_flips"], seed=seed, threads=threads,
+                                 pf_refresh=wl.get("pf_refresh", 0))
     d, F, diag = O.sr_moments(Om, E)
-    O.cg_solve(Om, d, F, np.zeros(mach.n_params), 0.9, wl["reg2"][0], 1e-2, diag)
+    O.cg_solve(Om, d, F, np.zeros(mach.n_params), 0.9, wl["reg2"][0], 1e-2, diag, n_neural=mach.n_neural)
     dt = time.perf_counter() - t0
     return dt, O.stats(E)["tau"], len(E)
 
@@ -293,7 +340,7 @@ def cpu_arm(wl, steps, warmup, chains=256):
 def main():
     args = parse()
     rank, world, local = dist_env()
-    wl = WORKLOADS[args.workload]
+    wl = workload(args)
     if args.impl == "reference":
         if rank != 0:
             return

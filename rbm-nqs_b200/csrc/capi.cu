@@ -473,7 +473,8 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         h->vb.alloc(h->n_vb);
         h->hb.alloc(nh);
         h->W64.alloc((size_t)n * nh);
-        h->W32.alloc((size_t)n * nh);
+        h->W32.alloc((size_t)(n + 1) * nh);  // row n: zero pad row of the gather sweep
+        ck(cudaMemsetAsync(h->W32.p, 0, (size_t)(n + 1) * nh * sizeof(float2), h->st), "memset");
         h->x.alloc(h->P);
         ck(cudaMemsetAsync(h->params.p, 0, h->P * sizeof(double2), h->st), "memset");
         ck(cudaMemsetAsync(h->x.p, 0, h->P * sizeof(double2), h->st), "memset");

@@ -288,6 +288,8 @@ struct Smem {
     uint8_t* inv;   // [S][n]
     float* bre;     // [n+1] Re v[f mod n_vb] (Metropolis bias term), [n] = 0
     int2* bonds;    // proposal bonds
+    float2* Wg;     // gather path: [n+1][nh] FP32 W, row n = 0 (shared or global)
+    uint8_t* Pg;    // gather path, symmetric: [n+1][S] P_s(f), row n = n
     unsigned char* warp0;
     int warp_bytes;
 };
@@ -319,6 +321,8 @@ __host__ __device__ inline int table_bytes(const MachineDev& m, int fp64, const 
     if (m.symmetric) b += align16(m.n * m.S) * 2;
     b += align16((m.n + 1) * 4);
     if (pl.bonds) b += align16(n_bonds * 8);
+    if (pl.gather && pl.wg) b += align16((m.n + 1) * m.nh * 8);
+    if (pl.gather && m.symmetric) b += align16((m.n + 1) * m.S);
     return b;
 }
 
@@ -355,6 +359,18 @@ __device__ inline Smem carve(unsigned char* base, const MachineDev& m, int fp64,
         s.bonds = reinterpret_cast<int2*>(base + off);
         off += align16(n_bonds * 8);
     }
+    if (pl.gather) {
+        if (pl.wg) {
+            s.Wg = reinterpret_cast<float2*>(base + off);
+            off += align16((m.n + 1) * m.nh * 8);
+        } else {
+            s.Wg = const_cast<float2*>(m.W32);  // [n+1][nh] in global memory
+        }
+        if (m.symmetric) {
+            s.Pg = base + off;
+            off += align16((m.n + 1) * m.S);
+        }
+    }
     s.warp0 = base + off;
     s.warp_bytes = warp_bytes;
     return s;
@@ -376,6 +392,10 @@ __device__ inline void load_tables(const MachineDev& m, const Smem& s, int fp64,
     for (int i = tid; i <= m.n; i += nt) s.bre[i] = i < m.n ? (float)m.vb[i % m.n_vb].x : 0.f;
     if (pl.bonds)
         for (int i = tid; i < n_bonds; i += nt) s.bonds[i] = bonds[i];
+    if (pl.gather && pl.wg)
+        for (int i = tid; i < (m.n + 1) * m.nh; i += nt) s.Wg[i] = i < m.n * m.nh ? m.W32[i] : make_float2(0.f, 0.f);
+    if (pl.gather && m.symmetric)
+        for (int i = tid; i < (m.n + 1) * m.S; i += nt) s.Pg[i] = i < m.n * m.S ? m.perm[i] : (uint8_t)m.n;
     if (pl.use_u || pl.u64)
         for (int i = tid; i < (m.n + 1) * TP; i += nt) {
             const int f = i / TP, t = i % TP;
@@ -701,18 +721,153 @@ __device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem&
     chain_finish(a, chain, lane, sp, nacc, prop);
 }
 
+// FP32 sweep path with gathered flip rows, for theta tables whose expanded
+// flip table does not fit in shared memory (e.g. 128 sites x 512 entries):
+// entry e of this lane is (k_e, s_e) = ((lane + 32 e) mod nh, (lane + 32 e) /
+// nh), computed once per chain; the flip row of site f is
+// W[P_{s_e}(f), k_e], two dependent shared-memory loads (the symmetry table
+// byte, then the FP32 W element).  Site n is the all-zero pad row (single-
+// site proposals use it as their second flip).  The proposal's theta' is
+// kept in registers and becomes theta on acceptance.  Otherwise the same
+// proposal decoding, running ln|cosh| sum and FP64 recompute per sweep as
+// run_chain_fast.
+template <int E, bool SYM>
+__device__ __forceinline__ void run_chain_gather(const SamplerArgs& a, const Smem& sm, int chain, int lane) {
+    const MachineDev& m = a.m;
+    const int n = m.n, nh = m.nh, S = m.S;
+    const uint2 key = make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32));
+    const uint32_t epoch = a.ctl[0];
+    uint32_t sp[4];
+    chain_start(a, chain, key, epoch, sp);
+
+    uint32_t ent[E];   // (s_e << 16) | k_e
+    uint32_t vmask = 0;
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+        const int t = lane + 32 * e;
+        const bool ok = t < m.T;
+        const int k = ok ? t % nh : 0, s = ok ? t / nh : 0;
+        ent[e] = ((uint32_t)s << 16) | (uint32_t)k;
+        vmask |= ok ? 1u << e : 0u;
+    }
+    const float2* Wg = sm.Wg;
+    const uint8_t* Pg = sm.Pg;
+    auto row = [&](int f, uint32_t en) -> int { return SYM ? (int)Pg[f * S + (en >> 16)] : f; };
+    auto urd = [&](int f, int e) -> float2 {
+        const float2 u = Wg[row(f, ent[e]) * nh + (ent[e] & 0xffffu)];
+        return ((vmask >> e) & 1u) ? u : make_float2(0.f, 0.f);
+    };
+
+    float2 th[E];
+    float SL = 0.f;
+    const double2* W64 = sm.W64 ? sm.W64 : m.W64;
+    auto recompute = [&]() {
+        // FP64 theta = b + sum_f sigma_f W[P_s(f), k], four entries at a time
+#pragma unroll
+        for (int c = 0; c < E; c += 4) {
+            double2 acc[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                acc[q] = (c + q < E && ((vmask >> (c + q)) & 1u)) ? m.hb[ent[c + q] & 0xffffu] : make_double2(0, 0);
+            for (int f = 0; f < n; f++) {
+                const double sg = spin_bit(sp, f) ? -1.0 : 1.0;
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    if (c + q >= E || !((vmask >> (c + q)) & 1u)) continue;
+                    const uint32_t en = ent[c + q];
+                    const double2 w = W64[row(f, en) * nh + (en & 0xffffu)];
+                    acc[q].x = fma(sg, w.x, acc[q].x);
+                    acc[q].y = fma(sg, w.y, acc[q].y);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (c + q < E) th[c + q] = make_float2((float)acc[q].x, (float)acc[q].y);
+        }
+        SL = 0.f;
+#pragma unroll
+        for (int e = 0; e < E; e++) SL += lnc_sweep(th[e]);
+    };
+    recompute();
+
+    const int2* bonds = sm.bonds ? sm.bonds : a.prop_bonds;
+    const int warmup = a.warmup;
+    const int total = a.spc * a.step + warmup;
+    const uint32_t thr = a.bond_thr24;
+    uint32_t prop = 0, nacc = 0, pcode = 0;
+    float plu = 0.f;
+    for (int st = 0; st < total; st++) {
+        int slot = 0;
+        while (slot < n) {
+            if ((prop & 31u) == 0) {
+                const uint4 r = philox4x32(make_uint4(prop + lane, epoch, (uint32_t)chain, 0), key);
+                uint32_t f0, f1, bond;
+                if ((r.x >> 8) < thr) {
+                    const int2 b = bonds[pick(r.y, (uint32_t)a.n_prop_bonds)];
+                    f0 = (uint32_t)b.x;
+                    f1 = (uint32_t)b.y;
+                    bond = 1;
+                } else {
+                    f0 = pick(r.y, (uint32_t)n);
+                    f1 = (uint32_t)n;
+                    bond = 0;
+                }
+                pcode = f0 | (f1 << 8) | (bond << 16);
+                plu = 0.5f * __logf(unit24<float>(r.z));
+            }
+            const int src = prop & 31u;
+            const uint32_t code = __shfl_sync(kFull, pcode, src);
+            const float lu = __shfl_sync(kFull, plu, src);
+            prop++;
+            const int f0 = code & 255u, f1 = (code >> 8) & 255u;
+            const bool bond = (code >> 16) != 0;
+            slot += bond ? 2 : 1;
+            const float g0 = spin_bit(sp, f0) ? 2.f : -2.f;  // -2 sigma_f
+            const float g1 = (bond && spin_bit(sp, f1)) ? 2.f : -2.f;
+            const float2 G0 = make_float2(g0, g0), G1 = make_float2(g1, g1);
+            float2 tn[E];
+            float sp_new = 0.f;
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                tn[e] = __ffma2_rn(G1, urd(f1, e), __ffma2_rn(G0, urd(f0, e), th[e]));
+                sp_new += lnc_sweep(tn[e]);
+            }
+            float d = warp_sum(sp_new - SL);
+            d = fmaf(g0, sm.bre[f0], d);
+            d = fmaf(g1, sm.bre[f1], d);
+            if (lu < d) {
+#pragma unroll
+                for (int e = 0; e < E; e++) th[e] = tn[e];
+                SL = sp_new;
+                flip_bit(sp, f0);
+                if (bond) flip_bit(sp, f1);
+                nacc++;
+            }
+        }
+        recompute();  // FP64 recompute of theta once per sweep
+        if (st >= warmup && (st - warmup) % a.step == 0) {
+            const int j = (st - warmup) / a.step;
+            const size_t idx = (size_t)chain * a.spc + j;
+            if (lane < 4) a.samples[4 * idx + lane] = sp[lane];
+        }
+    }
+    chain_finish(a, chain, lane, sp, nacc, prop);
+}
+
 // Thread bound per entries-per-lane: 28 warps (896 threads, 72 registers)
 // keep 4096 chains resident on 148 SMs for E <= 4.
 template <int E, bool PF = false> struct MaxThreads {
     static constexpr int v = PF ? 256 : (E <= 2 ? 1024 : (E <= 4 ? 896 : (E <= 8 ? 512 : 256)));
+    static constexpr int gather = E <= 4 ? 896 : (E <= 8 ? 640 : 384);
 };
 
 // All chains at once, persistent warps: global warp g = warp * gridDim.x +
 // blockIdx.x takes chains g, g + total_warps, ... so consecutive chains land
 // on different SMs and every block holds the tables once.  FAST selects the
 // FP32 expanded-table path.
-template <int E, typename R, bool FAST, bool PF>
-__global__ void __launch_bounds__(MaxThreads<E, PF>::v, 1) sampler_kernel(const SamplerArgs a) {
+template <int E, typename R, int FAST, bool PF>
+__global__ void __launch_bounds__(FAST == 2 ? MaxThreads<E, PF>::gather : MaxThreads<E, PF>::v, 1)
+    sampler_kernel(const SamplerArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int fp64 = sizeof(R) == 8;
     Smem sm = carve(smem, a.m, fp64, a.plan, a.n_prop_bonds, sweep_warp_bytes(a.m.T, sizeof(R), PF));
@@ -725,9 +880,14 @@ __global__ void __launch_bounds__(MaxThreads<E, PF>::v, 1) sampler_kernel(const 
                        : nullptr;
     const int total_warps = (blockDim.x >> 5) * gridDim.x;
     for (int chain = warp * gridDim.x + blockIdx.x; chain < a.n_chains; chain += total_warps) {
-        if constexpr (FAST)
+        if constexpr (FAST == 1)
             run_chain_fast<E>(a, sm, chain, lane);
-        else
+        else if constexpr (FAST == 2) {
+            if (a.m.symmetric)
+                run_chain_gather<E, true>(a, sm, chain, lane);
+            else
+                run_chain_gather<E, false>(a, sm, chain, lane);
+        } else
             run_chain<E, R, PF>(a, sm, chain, lane, wlp, pst, pA, pscr);
     }
 }
@@ -893,24 +1053,25 @@ int eval_smem_bytes(const MachineDev& m, int fp64, int warps, const SmemPlan& pl
     return table_bytes(m, fp64, plan, 0) + warps * eval_warp_bytes(m.T, fp64 ? 8 : 4, m.pf.n > 0);
 }
 
-template <int E, typename R, bool FAST, bool PF> static const void* sampler_fn() {
+template <int E, typename R, int FAST, bool PF> static const void* sampler_fn() {
     return reinterpret_cast<const void*>(sampler_kernel<E, R, FAST, PF>);
 }
 
 // The Pfaffian variants exist for theta tables up to 128 entries (32 sites,
 // alpha <= 4); they take the general (non-table) sweep.
-static const void* pick_sampler(int E, int fp64, int exp_table, int pf) {
+static const void* pick_sampler(int E, int fp64, int exp_table, int pf, int gather) {
     if (pf) {
 #define RBMNQS_PICK_PF(EE) \
-    if (E == EE) return fp64 ? sampler_fn<EE, double, false, true>() : sampler_fn<EE, float, false, true>();
+    if (E == EE) return fp64 ? sampler_fn<EE, double, 0, true>() : sampler_fn<EE, float, 0, true>();
         RBMNQS_PICK_PF(1) RBMNQS_PICK_PF(2) RBMNQS_PICK_PF(4)
 #undef RBMNQS_PICK_PF
         return nullptr;
     }
 #define RBMNQS_PICK(EE)                                                   \
     if (E == EE) {                                                        \
-        if (fp64) return sampler_fn<EE, double, false, false>();          \
-        return exp_table ? sampler_fn<EE, float, true, false>() : sampler_fn<EE, float, false, false>(); \
+        if (fp64) return sampler_fn<EE, double, 0, false>();              \
+        if (exp_table) return sampler_fn<EE, float, 1, false>();          \
+        return gather ? sampler_fn<EE, float, 2, false>() : sampler_fn<EE, float, 0, false>(); \
     }
     RBMNQS_PICK(1) RBMNQS_PICK(2) RBMNQS_PICK(4) RBMNQS_PICK(8) RBMNQS_PICK(16)
 #undef RBMNQS_PICK
@@ -932,11 +1093,15 @@ cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bond
     // the FP64 expanded table when that fits too, else FP64 W
     const int pf = m.pf.n > 0;
     pl.use_u = !fp64 && !pf && (m.n + 1) * TP * 8 <= 64 * 1024;
+    // FP32 without the expanded table: gathered flip rows (W32 with its pad
+    // row in shared memory when it fits, else from L2)
+    pl.gather = !fp64 && !pf && !pl.use_u;
+    pl.wg = pl.gather && (m.n + 1) * m.nh * 8 <= 64 * 1024;
     pl.u64 = pl.use_u && m.n * TP * 16 <= 96 * 1024;
-    pl.w32 = !fp64 && !pl.use_u && m.n * m.nh * 8 <= 64 * 1024;
+    pl.w32 = !fp64 && !pl.use_u && !pl.gather && m.n * m.nh * 8 <= 64 * 1024;
     pl.w64 = m.n * m.nh * 16 <= 32 * 1024;
     pl.bonds = n_bonds > 0 && n_bonds * 8 <= 8 * 1024;
-    const void* fn = pick_sampler(E, fp64, pl.use_u, pf);
+    const void* fn = pick_sampler(E, fp64, pl.use_u, pf, pl.gather);
     if (!fn) return cudaErrorInvalidValue;
     cudaFuncAttributes fa;
     err = cudaFuncGetAttributes(&fa, fn);
@@ -973,7 +1138,7 @@ cudaError_t launch_sampler(const SamplerArgs& a0, int fp64, const SamplerShape& 
     SamplerArgs a = a0;
     a.plan = sh.plan;
     const int E = elements_per_lane(a.m.T);
-    const void* fn = pick_sampler(E, fp64, sh.plan.use_u, a.m.pf.n > 0);
+    const void* fn = pick_sampler(E, fp64, sh.plan.use_u, a.m.pf.n > 0, sh.plan.gather);
     if (!fn) return cudaErrorInvalidValue;
     void* args[] = {&a};
     return cudaLaunchKernel(fn, dim3(sh.blocks), dim3(32 * sh.warps_per_block), args, sh.smem, st);

@@ -46,6 +46,8 @@ struct SmemPlan {
     int w64;    // FP64 W
     int u64;    // expanded FP64 table U64[n][TP] for the theta recompute
     int bonds;  // proposal bond list
+    int gather; // FP32 sweep with gathered flip rows (the expanded table does not fit)
+    int wg;     // gather path: W32 with its zero pad row in shared memory
 };
 
 struct SamplerArgs {

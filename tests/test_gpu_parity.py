@@ -109,6 +109,34 @@ def test_metropolis_fp32_statistics_agree():
     assert abs(st["energy"].real - ex) < 5 * st["stddev"] + 1e-3
 
 
+@pytest.mark.parametrize("L,kind,alpha,model", [
+    (8, "symmetry", 4, "kitaev"),   # 128 sites, 512 theta entries (16 per lane), W in shared memory
+    (5, "symmetry", 4, "kitaev"),   # 50 sites, 200 entries (8 per lane)
+    (8, "symmetry", 2, "toric"),    # 128 sites, 4 hidden rows x 64 translations
+])
+def test_gather_sweep_fp32_follows_fp64_chains(L, kind, alpha, model):
+    """The FP32 sweep with gathered flip rows (expanded table too large for
+    shared memory) against the FP64 oracle chains on the same Philox
+    streams: samples coincide except after acceptance ties."""
+    rng = np.random.default_rng(5)
+    symm = 0.5 if model == "kitaev" else 1.0
+    om = O.Model.kitaev(L) if model == "kitaev" else O.Model.toric(L)
+    mach = O.Machine(om, kind, alpha, symm=symm).init_random(rng, 0.05)
+    gm = rbmnqs.Model.kitaev(L, symmetry=symm) if model == "kitaev" else rbmnqs.Model.toric(L, symmetry=symm)
+    bf = 0.5 if model == "kitaev" else 0.0
+    cfg = rbmnqs.default_config(rbm_type=1 if kind == "symmetry" else 0, alpha=alpha, n_chains=16,
+                                samples_per_chain=6, warmup=4, bond_flips=bf, seed=77, precision=0)
+    s = rbmnqs.Session(gm, cfg)
+    s.set_weights(mach.params())
+    st = s.sample()
+    Eg, Og = s.samples()
+    Eo, Oo, acc, _ = O.metropolis(mach, om, 16, 6, warmup=4, bond_flips=bf, seed=77)
+    same = np.abs(Eg - Eo) < 1e-4 * np.maximum(1, np.abs(Eo))
+    assert np.mean(same) > 0.9
+    assert rel(Og[same], Oo[same]) < TOL32
+    assert abs(st["acceptance"] - acc.mean()) < 0.02
+
+
 @pytest.mark.parametrize("case", ["kitaev3_basic_a1", "kitaev4_symm_a4", "toric3_symm_a2"])
 @pytest.mark.parametrize("precision,gram", [(1, 0), (0, 1), (0, 0)])
 def test_sr_moments_and_gram_match_oracle(case, precision, gram):
