@@ -24,6 +24,10 @@ struct rbmnqs_model {
     rbmnqs::model m;
 };
 
+// Largest parameter count with a formed P x P matrix S (dense Gram + CG in
+// shared memory); above it the matrix-free operator is used.
+constexpr int kDenseMax = 2048;
+
 namespace {
 
 thread_local std::string g_err;
@@ -133,6 +137,11 @@ struct rbmnqs_handle {
     DevBuf<rbmnqs::HamDev> hdev;
     DevBuf<rbmnqs::CgResultDev> cgres;
     DevBuf<rbmnqs::EpochStatsDev> stats;
+    // matrix-free SR (n_params above the dense limit): no S is formed
+    bool mfree = false;
+    rbmnqs::MfreePlan mfp{};
+    rbmnqs::MfreeWork mfw{};
+    DevBuf<unsigned char> mfbuf;
     // Pfaffian factor: class matrix, derivative pairs, unscramble buffers
     int pf_n = 0, pf_indep = 0;
     DevBuf<int16_t> pf_bs;
@@ -253,17 +262,28 @@ struct rbmnqs_handle {
     }
     void enqueue_optimize() {
         ck(rbmnqs::launch_schedule(sched.p, st), "schedule");
-        if (gram_tc)
-            ck(rbmnqs::launch_gram_tc(gtc, O.p, fp64, d.p, gpart.p, gerr.p, Sm.p, st), "tensor-core gram");
-        else
-            ck(rbmnqs::launch_gram_fp64(O.p, fp64, d.p, N, P, gram_ks, part.p, Sm.p, st), "gram");
-        ck(rbmnqs::launch_regularize(Sm.p, P, P_neural, N, sched.p, diag.p, Sreg.p, maxdiag.p, st), "regularize");
-        mark(4);
         int max_it = std::min(2 * P, cfg.max_iterations);
         if (max_it == 0) max_it = 2 * P;
         const double rtol = cfg.rtol == 0 ? 1e-16 : cfg.rtol;
-        ck(rbmnqs::launch_cg(Sreg.p, F.p, x.p, P, max_it, rtol, cgres.p, st), "cg");
-        mark(5);
+        if (mfree) {
+            // diag = var(O) straight from O; CG on the operator (cg_solver.cpp aprod)
+            ck(rbmnqs::launch_var_diag(O.p, fp64, d.p, N, P, mfp, mfw, diag.p, maxdiag.p, st), "var diag");
+            mark(4);
+            ck(rbmnqs::launch_cg_mfree(O.p, fp64, d.p, (double)N, N, P, P_neural, F.p, x.p, diag.p, maxdiag.p,
+                                       sched.p, 0, 0, 0, max_it, rtol, mfp, mfw, cgres.p, st),
+               "matrix-free cg");
+            mark(5);
+        } else {
+            if (gram_tc)
+                ck(rbmnqs::launch_gram_tc(gtc, O.p, fp64, d.p, gpart.p, gerr.p, Sm.p, st), "tensor-core gram");
+            else
+                ck(rbmnqs::launch_gram_fp64(O.p, fp64, d.p, N, P, gram_ks, part.p, Sm.p, st), "gram");
+            ck(rbmnqs::launch_regularize(Sm.p, P, P_neural, N, sched.p, diag.p, Sreg.p, maxdiag.p, st),
+               "regularize");
+            mark(4);
+            ck(rbmnqs::launch_cg(Sreg.p, F.p, x.p, P, max_it, rtol, cgres.p, st), "cg");
+            mark(5);
+        }
         ck(rbmnqs::launch_update(params.p, x.p, P, sched.p, cgres.p, st), "update");
         ck(rbmnqs::launch_unpack(params.p, n, n_vb, nh, vb.p, hb.p, W64.p, W32.p, st), "unpack");
         mark(6);
@@ -456,7 +476,8 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         }
         require(rbmnqs::elements_per_lane(h->T) > 0, "theta table larger than 512 entries per chain",
                 RBMNQS_ERR_UNSUPPORTED);
-        require(h->P <= 2048, "dense SR path supports at most 2048 parameters", RBMNQS_ERR_UNSUPPORTED);
+        // dense S up to kDenseMax parameters, the matrix-free operator above
+        h->mfree = h->P > kDenseMax;
         h->N = cfg->n_chains * cfg->samples_per_chain;
         require(h->N >= 2, "need at least two samples");
         int k = 50;
@@ -557,8 +578,12 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         h->d.alloc(h->P);
         h->F.alloc(h->P);
         h->emean.alloc(1);
-        h->gram_tc = !h->fp64 && cfg->gram == 0;
-        if (h->gram_tc) {
+        h->gram_tc = !h->fp64 && cfg->gram == 0 && !h->mfree;
+        if (h->mfree) {
+            ck(rbmnqs::mfree_plan(h->N, h->P, &h->mfp), "matrix-free plan");
+            h->mfbuf.alloc(rbmnqs::mfree_work_bytes(h->N, h->P, h->mfp));
+            h->mfw = rbmnqs::mfree_carve(h->mfbuf.p, h->N, h->P, h->mfp);
+        } else if (h->gram_tc) {
             ck(rbmnqs::gram_tc_plan(h->N, h->P, &h->gtc), "gram plan");
             const size_t pf = h->gtc.plane_floats();
             h->gplanes.alloc(2 * pf);
@@ -571,8 +596,10 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
             h->gram_ks = rbmnqs::gram_splits(h->N, h->P);
             h->part.alloc((size_t)h->gram_ks * h->P * h->P);
         }
-        h->Sm.alloc((size_t)h->P * h->P);
-        h->Sreg.alloc((size_t)h->P * h->P);
+        if (!h->mfree) {
+            h->Sm.alloc((size_t)h->P * h->P);
+            h->Sreg.alloc((size_t)h->P * h->P);
+        }
         h->diag.alloc(h->P);
         h->maxdiag.alloc(1);
         h->sched.alloc(1);
@@ -774,7 +801,11 @@ int rbmnqs_get_sr(rbmnqs_handle* h, double* d, double* F, double* diag, double* 
         if (d) ck(cudaMemcpyAsync(d, h->d.p, P * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "c");
         if (F) ck(cudaMemcpyAsync(F, h->F.p, P * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "c");
         if (diag) ck(cudaMemcpyAsync(diag, h->diag.p, P * sizeof(double), cudaMemcpyDeviceToHost, h->st), "c");
-        if (S) ck(cudaMemcpyAsync(S, h->Sm.p, P * P * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "c");
+        if (S) {
+            require(!h->mfree, "S is not formed above " + std::to_string(kDenseMax) +
+                                   " parameters (matrix-free CG)", RBMNQS_ERR_UNSUPPORTED);
+            ck(cudaMemcpyAsync(S, h->Sm.p, P * P * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "c");
+        }
         ck(cudaStreamSynchronize(h->st), "sync");
     });
 }
@@ -876,7 +907,7 @@ int rbmnqs_sr_solve(rbmnqs_handle* h, const double* O, int32_t N, const double* 
         require(h && O && d && F && x_io && diag && N >= 1 && norm > 0, "bad arguments");
         const int P = h->P;
         DevBuf<double2> dO, dd, dF, dx, part, G, Sreg;
-        DevBuf<double> ddiag;
+        DevBuf<double> ddiag, dmax;
         DevBuf<rbmnqs::CgResultDev> res;
         dO.alloc((size_t)N * P);
         dd.alloc(P);
@@ -884,22 +915,37 @@ int rbmnqs_sr_solve(rbmnqs_handle* h, const double* O, int32_t N, const double* 
         dx.alloc(P);
         ddiag.alloc(P);
         res.alloc(1);
-        G.alloc((size_t)P * P);
-        Sreg.alloc((size_t)P * P);
-        const int ks = rbmnqs::gram_splits(N, P);
-        part.alloc((size_t)ks * P * P);
         ck(cudaMemcpyAsync(dO.p, O, (size_t)N * P * sizeof(double2), cudaMemcpyHostToDevice, h->st), "c");
         ck(cudaMemcpyAsync(dd.p, d, P * sizeof(double2), cudaMemcpyHostToDevice, h->st), "c");
         ck(cudaMemcpyAsync(dF.p, F, P * sizeof(double2), cudaMemcpyHostToDevice, h->st), "c");
         ck(cudaMemcpyAsync(dx.p, x_io, P * sizeof(double2), cudaMemcpyHostToDevice, h->st), "c");
         ck(cudaMemcpyAsync(ddiag.p, diag, P * sizeof(double), cudaMemcpyHostToDevice, h->st), "c");
-        ck(rbmnqs::launch_gram_fp64(dO.p, 1, nullptr, N, P, ks, part.p, G.p, h->st), "gram");
-        ck(rbmnqs::launch_solve_prep(G.p, N, norm, dd.p, ddiag.p, P, h->P_neural, r1, r2, rd, Sreg.p, h->st),
-           "prep");
         int max_it = std::min(2 * P, h->cfg.max_iterations);
         if (max_it == 0) max_it = 2 * P;
         const double rtol = h->cfg.rtol == 0 ? 1e-16 : h->cfg.rtol;
-        ck(rbmnqs::launch_cg(Sreg.p, dF.p, dx.p, P, max_it, rtol, res.p, h->st), "cg");
+        if (P > kDenseMax) {
+            // the operator form (cg_solver.cpp aprod) on the given O, d, norm
+            rbmnqs::MfreePlan pl{};
+            ck(rbmnqs::mfree_plan(N, P, &pl), "matrix-free plan");
+            DevBuf<unsigned char> wb;
+            wb.alloc(rbmnqs::mfree_work_bytes(N, P, pl));
+            const rbmnqs::MfreeWork wk = rbmnqs::mfree_carve(wb.p, N, P, pl);
+            dmax.alloc(1);
+            ck(rbmnqs::launch_max_diag(ddiag.p, P, dmax.p, h->st), "max diag");
+            ck(rbmnqs::launch_cg_mfree(dO.p, 1, dd.p, norm, N, P, h->P_neural, dF.p, dx.p, ddiag.p, dmax.p, nullptr,
+                                       r1, r2, rd, max_it, rtol, pl, wk, res.p, h->st),
+               "matrix-free cg");
+            ck(cudaStreamSynchronize(h->st), "sync");  // before wb goes out of scope
+        } else {
+            G.alloc((size_t)P * P);
+            Sreg.alloc((size_t)P * P);
+            const int ks = rbmnqs::gram_splits(N, P);
+            part.alloc((size_t)ks * P * P);
+            ck(rbmnqs::launch_gram_fp64(dO.p, 1, nullptr, N, P, ks, part.p, G.p, h->st), "gram");
+            ck(rbmnqs::launch_solve_prep(G.p, N, norm, dd.p, ddiag.p, P, h->P_neural, r1, r2, rd, Sreg.p, h->st),
+               "prep");
+            ck(rbmnqs::launch_cg(Sreg.p, dF.p, dx.p, P, max_it, rtol, res.p, h->st), "cg");
+        }
         rbmnqs::CgResultDev r{};
         ck(cudaMemcpyAsync(x_io, dx.p, P * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "c");
         ck(cudaMemcpyAsync(&r, res.p, sizeof(r), cudaMemcpyDeviceToHost, h->st), "c");

@@ -1,0 +1,407 @@
+// cg_mfree.cu -- matrix-free SR conjugate gradients for parameter counts
+// whose P x P matrix S is not formed (cg_solver.cpp:260-334 with the
+// operator of minresqlp_adapter.cpp / cg_solver.cpp aprod):
+//
+//   A b = (1/N) O^H (O b) - conj(d) (d . b) + f o b,
+//   f_p = diag_p (r1 (+ rd for non-neural p)) + r2 max(diag),
+//
+// cg1 semantics (warm start x0, stop at ||r||^2 < rtol or max_it).  One
+// cooperative persistent kernel runs the whole solve; per iteration it
+// streams O twice (rows for O b, columns for O^H v) and meets at five grid
+// barriers.  The barriers are a counter + generation pair with bounded
+// spins: a block that waits too long records an error and the solve returns
+// (status RBMNQS_ERR_CUDA) instead of hanging.  Reductions are summed in a
+// fixed order, so results are deterministic.
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+#include "sr.cuh"
+
+namespace rbmnqs {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kColTile = 64;  // columns per block in the O^H v pass (4 row groups)
+constexpr uint32_t kBarrierSpin = 1u << 24;
+
+__device__ __forceinline__ double2 zld(const float2* O, size_t i) {
+    const float2 v = __ldg(O + i);
+    return make_double2(v.x, v.y);
+}
+__device__ __forceinline__ double2 zld(const double2* O, size_t i) { return __ldg(O + i); }
+
+// Data written by other blocks of the same launch is read through L2
+// (ld.global.cg): the SMs' L1 caches are not coherent with each other.
+template <typename T> __device__ __forceinline__ T cg_ld(const T* p) { return __ldcg(p); }
+
+// Grid barrier with a bounded wait.  Returns false (on every thread of the
+// block) if this block gave up or another block already did.
+__device__ bool grid_barrier(MfreeSync* sync, uint32_t nblocks) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ok = 1;
+        volatile uint32_t* gen = &sync->gen;
+        volatile int* bad = &sync->bad;
+        const uint32_t g = *gen;
+        __threadfence();
+        if (atomicAdd(&sync->count, 1u) == nblocks - 1) {
+            sync->count = 0;
+            __threadfence();
+            atomicAdd(&sync->gen, 1u);
+        } else {
+            uint32_t spins = 0;
+            while (*gen == g) {
+                if (++spins > kBarrierSpin || *bad) {
+                    ok = 0;
+                    atomicExch(&sync->bad, 1);
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        if (*bad) ok = 0;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+template <typename T> __device__ T bsum(T v, T* red);
+template <> __device__ double bsum<double>(double v, double* red) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    double r = red[0];
+    for (int i = 1; i < nw; i++) r += red[i];
+    return r;
+}
+template <> __device__ double2 bsum<double2>(double2 v, double2* red) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v.x = warp_sum(v.x);
+    v.y = warp_sum(v.y);
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    double2 r = red[0];
+    for (int i = 1; i < nw; i++) r = make_double2(r.x + red[i].x, r.y + red[i].y);
+    return r;
+}
+
+// sum of the per-block partials in block order (every block gets the same value)
+__device__ __forceinline__ double sum_parts(const double* p, int G) {
+    double s = 0;
+    for (int i = 0; i < G; i++) s += cg_ld(p + i);
+    return s;
+}
+__device__ __forceinline__ double2 sum_parts(const double2* p, int G) {
+    double2 s = make_double2(0, 0);
+    for (int i = 0; i < G; i++) {
+        const double2 v = cg_ld(p + i);
+        s = make_double2(s.x + v.x, s.y + v.y);
+    }
+    return s;
+}
+
+template <typename TO>
+__global__ void __launch_bounds__(kThreads) cg_mfree_kernel(const TO* __restrict__ O, const double2* __restrict__ d,
+                                                            double norm, int N, int P, int n_neural,
+                                                            const double2* __restrict__ F, double2* x,
+                                                            const double* __restrict__ diag, const double* max_diag,
+                                                            const ScheduleDev* sch, double r1_, double r2_,
+                                                            double rd_, int max_it, double rtol, MfreeWork w,
+                                                            CgResultDev* res) {
+    __shared__ double redd[kThreads / 32];
+    __shared__ double2 redz[kThreads / 32];
+    __shared__ double2 colred[kThreads];
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int G = gridDim.x, blk = blockIdx.x;
+    const int gw = blk * (kThreads / 32) + (tid >> 5), nwarps = G * (kThreads / 32);
+    const int gt = blk * kThreads + tid, nthreads = G * kThreads;
+    const double r1 = sch ? sch->value[1] : r1_, r2 = sch ? sch->value[2] : r2_, rd = sch ? sch->value[3] : rd_;
+    const double mxd = *max_diag;
+    if (blk == 0 && tid == 0) res->status = 0;
+
+    // A b into Ap (b = x at the start, p afterwards); returns false on a
+    // barrier timeout.  With want_pap, also leaves sum_q conj(b_q) Ap_q.
+    auto aprod = [&](const double2* b, bool want_pap, double2* pap) -> bool {
+        // phase A: partial row dots (n, segment j) and d . b
+        const int nseg = w.nseg, lseg = w.lseg;
+        const long items = (long)nseg * N;
+        for (long it = gw; it < items; it += nwarps) {
+            const int j = (int)(it / N), n = (int)(it % N);
+            const int q0 = j * lseg, q1 = min(P, q0 + lseg);
+            double ax = 0, ay = 0;
+            const size_t row = (size_t)n * P;
+            for (int q = q0 + lane; q < q1; q += 32) {
+                const double2 o = zld(O, row + q), v = cg_ld(b + q);
+                ax = fma(o.x, v.x, fma(-o.y, v.y, ax));
+                ay = fma(o.x, v.y, fma(o.y, v.x, ay));
+            }
+            ax = warp_sum(ax);
+            ay = warp_sum(ay);
+            if (lane == 0) w.partA[(size_t)j * N + n] = make_double2(ax, ay);
+        }
+        double2 db = make_double2(0, 0);
+        for (int q = gt; q < P; q += nthreads) {
+            const double2 dq = d[q], v = cg_ld(b + q);
+            db.x += dq.x * v.x - dq.y * v.y;
+            db.y += dq.x * v.y + dq.y * v.x;
+        }
+        db = bsum(db, redz);
+        if (tid == 0) w.zpart[blk] = db;
+        if (!grid_barrier(w.sync, G)) return false;
+        // phase A2: O b per sample
+        for (int n = gt; n < N; n += nthreads) {
+            double2 s = make_double2(0, 0);
+            for (int j = 0; j < nseg; j++) {
+                const double2 v = cg_ld(w.partA + (size_t)j * N + n);
+                s = make_double2(s.x + v.x, s.y + v.y);
+            }
+            w.tmpN[n] = s;
+        }
+        db = sum_parts(w.zpart, G);
+        if (!grid_barrier(w.sync, G)) return false;
+        // phase B: columns, 4 row groups x 64 columns per block
+        const int c = tid % kColTile, rg = tid / kColTile, ngr = kThreads / kColTile;
+        const int ntiles = (P + kColTile - 1) / kColTile;
+        double2 pp = make_double2(0, 0);
+        for (int tile = blk; tile < ntiles; tile += G) {
+            const int q = tile * kColTile + c;
+            double ax = 0, ay = 0;
+            if (q < P) {
+                for (int n = rg; n < N; n += ngr) {
+                    const double2 o = zld(O, (size_t)n * P + q), v = cg_ld(w.tmpN + n);
+                    ax = fma(o.x, v.x, fma(o.y, v.y, ax));   // conj(o) v
+                    ay = fma(o.x, v.y, fma(-o.y, v.x, ay));
+                }
+            }
+            colred[tid] = make_double2(ax, ay);
+            __syncthreads();
+            if (rg == 0 && q < P) {
+                double sx = 0, sy = 0;
+                for (int g = 0; g < ngr; g++) {
+                    sx += colred[g * kColTile + c].x;
+                    sy += colred[g * kColTile + c].y;
+                }
+                const double2 dq = d[q], bq = cg_ld(b + q);
+                const double f = diag[q] * (q < n_neural ? r1 : r1 + rd) + mxd * r2;
+                // acc / norm - conj(d_q) (d . b), plus the shift
+                double2 a;
+                a.x = f * bq.x + sx / norm - (dq.x * db.x + dq.y * db.y);
+                a.y = f * bq.y + sy / norm - (dq.x * db.y - dq.y * db.x);
+                w.Ap[q] = a;
+                if (want_pap) {
+                    pp.x += bq.x * a.x + bq.y * a.y;
+                    pp.y += bq.x * a.y - bq.y * a.x;
+                }
+            }
+            __syncthreads();
+        }
+        if (want_pap) {
+            pp = bsum(pp, redz);
+            if (tid == 0) w.zpart[blk] = pp;
+        }
+        if (!grid_barrier(w.sync, G)) return false;
+        if (want_pap) *pap = sum_parts(w.zpart, G);
+        return true;
+    };
+
+    bool ok = aprod(x, false, nullptr);
+    // r = F - A x0, p = r
+    double rl = 0;
+    if (ok) {
+        for (int q = gt; q < P; q += nthreads) {
+            const double2 aq = cg_ld(w.Ap + q);
+            const double2 rq = make_double2(F[q].x - aq.x, F[q].y - aq.y);
+            w.r[q] = rq;
+            w.p[q] = rq;
+            rl += rq.x * rq.x + rq.y * rq.y;
+        }
+        rl = bsum(rl, redd);
+        if (tid == 0) w.dpart[blk] = rl;
+        ok = grid_barrier(w.sync, G);
+    }
+    double rsold = ok ? sum_parts(w.dpart, G) : 0.0, rs = rsold;
+    int itn = 0;
+    if (ok) {
+        for (itn = 0; itn < max_it; itn++) {
+            double2 pap;
+            if (!(ok = aprod(w.p, true, &pap))) break;
+            // alpha = rsold / (p^H A p)
+            const double den = pap.x * pap.x + pap.y * pap.y;
+            const double ax = rsold * pap.x / den, ay = -rsold * pap.y / den;
+            rl = 0;
+            for (int q = gt; q < P; q += nthreads) {
+                const double2 pq = cg_ld(w.p + q), aq = cg_ld(w.Ap + q);
+                double2 xq = cg_ld(x + q), rq = cg_ld(w.r + q);
+                xq.x += ax * pq.x - ay * pq.y;
+                xq.y += ax * pq.y + ay * pq.x;
+                rq.x -= ax * aq.x - ay * aq.y;
+                rq.y -= ax * aq.y + ay * aq.x;
+                x[q] = xq;
+                w.r[q] = rq;
+                rl += rq.x * rq.x + rq.y * rq.y;
+            }
+            rl = bsum(rl, redd);
+            if (tid == 0) w.dpart[blk] = rl;
+            if (!(ok = grid_barrier(w.sync, G))) break;
+            rs = sum_parts(w.dpart, G);
+            if (rs < rtol) break;
+            const double beta = rs / rsold;
+            for (int q = gt; q < P; q += nthreads) {
+                const double2 rq = cg_ld(w.r + q), pq = cg_ld(w.p + q);
+                w.p[q] = make_double2(rq.x + beta * pq.x, rq.y + beta * pq.y);
+            }
+            rsold = rs;
+            if (!(ok = grid_barrier(w.sync, G))) break;
+        }
+    }
+    if (blk == 0 && tid == 0) {
+        res->iterations = itn;
+        res->residual = rs;
+        if (!ok) res->status = -2;
+    }
+}
+
+// diag_p = (1/(N-1)) sum_n |O_np - d_p|^2 (the unbiased var(O) of the
+// aggregator, aggregator.cpp:84-164) and per-block maxima.
+template <typename TO>
+__global__ void __launch_bounds__(kThreads) var_diag_kernel(const TO* __restrict__ O, const double2* __restrict__ d,
+                                                            int N, int P, double* diag, double* maxpart) {
+    __shared__ double colred[kThreads];
+    __shared__ double red[kThreads / 32];
+    const int tid = threadIdx.x, c = tid % kColTile, rg = tid / kColTile, ngr = kThreads / kColTile;
+    const int ntiles = (P + kColTile - 1) / kColTile;
+    double mx = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int q = tile * kColTile + c;
+        double s = 0;
+        if (q < P) {
+            const double2 dq = d[q];
+            for (int n = rg; n < N; n += ngr) {
+                const double2 o = zld(O, (size_t)n * P + q);
+                const double ex = o.x - dq.x, ey = o.y - dq.y;
+                s = fma(ex, ex, fma(ey, ey, s));
+            }
+        }
+        colred[tid] = s;
+        __syncthreads();
+        if (rg == 0 && q < P) {
+            double t = 0;
+            for (int g = 0; g < ngr; g++) t += colred[g * kColTile + c];
+            t /= (double)N - 1.0;
+            diag[q] = t;
+            mx = fmax(mx, t);
+        }
+        __syncthreads();
+    }
+    const int lane = tid & 31, w = tid >> 5;
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) red[w] = mx;
+    __syncthreads();
+    if (tid == 0) {
+        double m = red[0];
+        for (int i = 1; i < kThreads / 32; i++) m = fmax(m, red[i]);
+        maxpart[blockIdx.x] = m;
+    }
+}
+
+__global__ void max_parts_kernel(const double* maxpart, int n, double* out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double m = maxpart[0];
+        for (int i = 1; i < n; i++) m = fmax(m, maxpart[i]);
+        *out = m;
+    }
+}
+
+template <typename TO> const void* cg_fn() { return reinterpret_cast<const void*>(cg_mfree_kernel<TO>); }
+
+}  // namespace
+
+cudaError_t mfree_plan(int N, int P, MfreePlan* pl) {
+    int dev = 0, sms = 148, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    if (!coop) return cudaErrorNotSupported;
+    // the smaller of the two instantiations' residency bounds
+    int b32 = 0, b64 = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b32, cg_mfree_kernel<float2>, kThreads, 0);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b64, cg_mfree_kernel<double2>, kThreads, 0);
+    if (e != cudaSuccess) return e;
+    per_sm = b32 < b64 ? b32 : b64;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    if (per_sm > 2) per_sm = 2;
+    pl->blocks = sms * per_sm;
+    const int nwarps = pl->blocks * (kThreads / 32);
+    int nseg = (2 * nwarps + N - 1) / N;
+    if (nseg < 1) nseg = 1;
+    int lseg = (P + nseg - 1) / nseg;
+    lseg = (lseg + 31) / 32 * 32;
+    nseg = (P + lseg - 1) / lseg;
+    pl->nseg = nseg;
+    pl->lseg = lseg;
+    pl->diag_blocks = pl->blocks;
+    return cudaSuccess;
+}
+
+size_t mfree_work_bytes(int N, int P, const MfreePlan& pl) {
+    return ((size_t)3 * P + N + (size_t)pl.nseg * N + 2 * (size_t)pl.blocks) * sizeof(double2) +
+           (size_t)pl.blocks * sizeof(double) * 2 + sizeof(MfreeSync) + 256;
+}
+
+MfreeWork mfree_carve(void* base, int N, int P, const MfreePlan& pl) {
+    MfreeWork w{};
+    auto* z = reinterpret_cast<double2*>(base);
+    w.r = z;
+    w.p = w.r + P;
+    w.Ap = w.p + P;
+    w.tmpN = w.Ap + P;
+    w.partA = w.tmpN + N;
+    w.zpart = w.partA + (size_t)pl.nseg * N;
+    auto* dd = reinterpret_cast<double*>(w.zpart + 2 * (size_t)pl.blocks);
+    w.dpart = dd;
+    w.maxpart = dd + pl.blocks;
+    w.sync = reinterpret_cast<MfreeSync*>(reinterpret_cast<uintptr_t>(w.maxpart + pl.blocks) + 255 & ~uintptr_t(255));
+    w.nseg = pl.nseg;
+    w.lseg = pl.lseg;
+    return w;
+}
+
+cudaError_t launch_max_diag(const double* diag, int P, double* max_diag, cudaStream_t st) {
+    max_parts_kernel<<<1, 32, 0, st>>>(diag, P, max_diag);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_var_diag(const void* O, int fp64, const double2* d, int N, int P, const MfreePlan& pl,
+                            const MfreeWork& w, double* diag, double* max_diag, cudaStream_t st) {
+    if (fp64)
+        var_diag_kernel<double2><<<pl.diag_blocks, kThreads, 0, st>>>((const double2*)O, d, N, P, diag, w.maxpart);
+    else
+        var_diag_kernel<float2><<<pl.diag_blocks, kThreads, 0, st>>>((const float2*)O, d, N, P, diag, w.maxpart);
+    max_parts_kernel<<<1, 32, 0, st>>>(w.maxpart, pl.diag_blocks, max_diag);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cg_mfree(const void* O, int fp64, const double2* d, double norm, int N, int P, int n_neural,
+                            const double2* F, double2* x, const double* diag, const double* max_diag,
+                            const ScheduleDev* sch, double r1, double r2, double rd, int max_it, double rtol,
+                            const MfreePlan& pl, const MfreeWork& w, CgResultDev* res, cudaStream_t st) {
+    // barrier state: count 0, no failure
+    cudaError_t e = cudaMemsetAsync(w.sync, 0, sizeof(MfreeSync), st);
+    if (e != cudaSuccess) return e;
+    MfreeWork wk = w;
+    CgResultDev* r = res;
+    const void* args[] = {&O, &d, &norm, &N, &P, &n_neural, &F, &x, &diag, &max_diag, &sch, &r1, &r2, &rd,
+                          &max_it, &rtol, &wk, &r};
+    return cudaLaunchCooperativeKernel(fp64 ? cg_fn<double2>() : cg_fn<float2>(), dim3(pl.blocks), dim3(kThreads),
+                                       const_cast<void**>(args), 0, st);
+}
+
+}  // namespace rbmnqs

@@ -712,6 +712,7 @@ __global__ void __cluster_dims__(kClusterCta, 1, 1) __launch_bounds__(256)
 // abort on max|x| > 30, else x *= lr (the next warm start) and w -= x.
 __global__ void sr_update(double2* params, double2* x, int P, const ScheduleDev* sch, CgResultDev* res) {
     __shared__ double red[32];
+    if (res->status == -2) return;  // the solve itself failed (matrix-free CG barrier timeout)
     double mx = 0;
     int bad = 0;
     for (int i = threadIdx.x; i < P; i += blockDim.x) {

@@ -46,6 +46,33 @@ cudaError_t launch_cg(const double2* A, const double2* b, double2* x, int P, int
                       CgResultDev* res, cudaStream_t st);
 cudaError_t launch_update(double2* params, double2* x, int P, const ScheduleDev* sch, CgResultDev* res,
                           cudaStream_t st);
+// Matrix-free CG (cg_mfree.cu) for parameter counts without a formed S.
+struct MfreeSync {
+    uint32_t count, gen;
+    int bad;
+};
+struct MfreePlan {
+    int blocks, nseg, lseg, diag_blocks;
+};
+struct MfreeWork {
+    double2 *r, *p, *Ap, *tmpN, *partA, *zpart;
+    double *dpart, *maxpart;
+    MfreeSync* sync;
+    int nseg, lseg;
+};
+cudaError_t mfree_plan(int N, int P, MfreePlan* pl);
+size_t mfree_work_bytes(int N, int P, const MfreePlan& pl);
+MfreeWork mfree_carve(void* base, int N, int P, const MfreePlan& pl);
+// diag = unbiased var(O) per parameter and its maximum (device scalar)
+cudaError_t launch_var_diag(const void* O, int fp64, const double2* d, int N, int P, const MfreePlan& pl,
+                            const MfreeWork& w, double* diag, double* max_diag, cudaStream_t st);
+// max of a given diag (explicit-solve entry)
+cudaError_t launch_max_diag(const double* diag, int P, double* max_diag, cudaStream_t st);
+// r1 / r2 / rd from sch when non-null, else the explicit values
+cudaError_t launch_cg_mfree(const void* O, int fp64, const double2* d, double norm, int N, int P, int n_neural,
+                            const double2* F, double2* x, const double* diag, const double* max_diag,
+                            const ScheduleDev* sch, double r1, double r2, double rd, int max_it, double rtol,
+                            const MfreePlan& pl, const MfreeWork& w, CgResultDev* res, cudaStream_t st);
 cudaError_t launch_unpack(const double2* params, int n, int n_vb, int nh, double2* vb, double2* hb, double2* W64,
                           float2* W32, cudaStream_t st);
 

@@ -297,14 +297,17 @@ class Session:
                                      _p(O.view(np.float64), P_D) if with_O else None))
         return E, O
 
-    def sr_moments(self):
+    def sr_moments(self, with_S=None):
+        """d, F, diag and (when formed: n_params <= 2048, or with_S) S."""
         P = self.n_params
+        if with_S is None:
+            with_S = P <= 2048
         d = np.zeros(P, np.complex128)
         F = np.zeros(P, np.complex128)
         diag = np.zeros(P, np.float64)
-        S = np.zeros((P, P), np.complex128)
+        S = np.zeros((P, P), np.complex128) if with_S else None
         _ck(lib().rbmnqs_get_sr(self._h, _p(d.view(np.float64), P_D), _p(F.view(np.float64), P_D),
-                                _p(diag, P_D), _p(S.view(np.float64), P_D)))
+                                _p(diag, P_D), _p(S.view(np.float64), P_D) if with_S else None))
         return d, F, diag, S
 
     def spins(self):

@@ -113,6 +113,8 @@ def test_metropolis_fp32_statistics_agree():
     (8, "symmetry", 4, "kitaev"),   # 128 sites, 512 theta entries (16 per lane), W in shared memory
     (5, "symmetry", 4, "kitaev"),   # 50 sites, 200 entries (8 per lane)
     (8, "symmetry", 2, "toric"),    # 128 sites, 4 hidden rows x 64 translations
+    (6, "basic", 1, "toric"),       # 72 sites, basic RBM (5328 parameters), W in shared memory
+    (8, "basic", 1, "toric"),       # 128 sites, basic RBM (16640 parameters), W read from L2
 ])
 def test_gather_sweep_fp32_follows_fp64_chains(L, kind, alpha, model):
     """The FP32 sweep with gathered flip rows (expanded table too large for
@@ -271,3 +273,60 @@ def test_massive_step_is_reported():
     if st["max_dw"] > 30:
         assert st["status"] == rbmnqs.ERR_MASSIVE_STEP
         assert np.array_equal(s.get_weights(), w0)
+
+
+@pytest.mark.parametrize("precision", [1, 0])
+def test_matrix_free_sr_solve_matches_oracle_cg(precision):
+    """n_params = 2144 > 2048: the solve runs on the operator
+    (1/N) O^H O - conj(d) d^T + shift without forming S (cg_solver.cpp
+    aprod), against the oracle's matrix-free CG on the same O."""
+    rng = np.random.default_rng(3)
+    om = O.Model.toric(4)
+    mach = O.Machine(om, "basic", 2, symm=1.0).init_random(rng, 0.05)
+    gm = rbmnqs.Model.toric(4, symmetry=1.0)
+    cfg = rbmnqs.default_config(rbm_type=0, alpha=2, n_chains=16, samples_per_chain=12, warmup=3, seed=9,
+                                precision=precision, max_iterations=150)
+    s = rbmnqs.Session(gm, cfg)
+    assert s.n_params == mach.n_params == 2144
+    s.set_weights(mach.params())
+    s.sample()
+    E, Om = s.samples()
+    d, F, diag = O.sr_moments(Om, E)
+    x0 = 1e-3 * (rng.normal(size=mach.n_params) + 1j * rng.normal(size=mach.n_params))
+    xo, ito, rso = O.cg_solve(Om, d, F, x0, 0.9, 9e-4, 1e-2, diag, max_iterations=150)
+    xg, itg, rsg = s.sr_solve(Om, d, F, x0, 0.9, 9e-4, 1e-2, diag)
+    assert abs(itg - ito) <= max(2, ito // 20)
+    assert rel(xg, xo) < 1e-8
+
+
+def test_matrix_free_epochs_match_oracle():
+    """Two FP64 epochs with the matrix-free CG inside the captured epoch
+    (diag = var(O) from O, schedules on the device) against the oracle."""
+    chains, spc, warm = 8, 16, 3
+    rng = np.random.default_rng(4)
+    om = O.Model.toric(4)
+    mach = O.Machine(om, "basic", 2, symm=1.0).init_random(rng, 0.05)
+    gm = rbmnqs.Model.toric(4, symmetry=1.0)
+    cfg = rbmnqs.default_config(rbm_type=0, alpha=2, n_chains=chains, samples_per_chain=spc, warmup=warm, seed=21,
+                                precision=1, max_iterations=120)
+    s = rbmnqs.Session(gm, cfg)
+    s.set_weights(mach.params())
+    lr, r1, r2, rd = O.Decay(1e-2), O.Decay(1, 1e-4, 0.9), O.Decay(1e-3, 1e-6, 0.9), O.Decay(1e-2)
+    x = np.zeros(mach.n_params, np.complex128)
+    for ep in range(2):
+        sst, ost = s.epoch()
+        E, Om, acc, _ = O.metropolis(mach, om, chains, spc, warmup=warm, seed=21, epoch=ep)
+        d, F, diag = O.sr_moments(Om, E)
+        lrv, r1v, r2v, rdv = lr.get(), r1.get(), r2.get(), rd.get()
+        x, it, rs = O.cg_solve(Om, d, F, x, r1v, r2v, rdv, diag, max_iterations=120)
+        assert abs(ost["iterations"] - it) <= 1
+        assert ost["status"] == 0
+        x = x * lrv
+        mach.set_params(mach.params() - x)
+        assert rel(s.get_weights(), mach.params()) < 1e-9, ep
+    d, F, diag, S = s.sr_moments()
+    assert S is None
+    E, Om = s.samples()
+    assert rel(diag, O.sr_moments(Om, E)[2]) < TOL64
+    with pytest.raises(rbmnqs.RbmNqsError):
+        s.sr_moments(with_S=True)  # S is not formed above 2048 parameters
