@@ -200,11 +200,36 @@ int rbmnqs_get_observables(rbmnqs_handle* h, double* values);
  * `launches` counts how often each stage ran. */
 int rbmnqs_timing(rbmnqs_handle* h, double* ms, int64_t* launches, int32_t n);
 int rbmnqs_timing_reset(rbmnqs_handle* h, int32_t enable);
+/* Launch-shape autotuner: times the sweep kernel over `sweeps` sweeps (one
+ * recorded sample) for each candidate warps-per-block of the planned shape
+ * and halvings of it, and the evaluation kernel for 1..8 warps per block;
+ * keeps the fastest of each (the session's chains, weights and statistics
+ * are left as they were; the epoch graph is re-captured).  No reference
+ * counterpart (the reference has no launch shapes).  Outputs may be NULL. */
+int rbmnqs_autotune(rbmnqs_handle* h, int32_t sweeps, int32_t* sampler_warps_per_block,
+                    int32_t* eval_warps_per_block, double* sampler_ms);
+
 /* Number of kernel launches one rbmnqs_epoch performs (kernel nodes of the
  * captured epoch graph; 0 before the first rbmnqs_epoch). */
 int rbmnqs_graph_kernels(rbmnqs_handle* h, int32_t* kernel_nodes);
 /* The handle's cudaStream_t, for callers that order work against it. */
 void* rbmnqs_stream(rbmnqs_handle* h);
+
+/* ------------------------------------------- batched independent trainings */
+/* Several sessions (different lattices, machines and sizes allowed) advanced
+ * together: one CUDA-graph launch runs the whole sample + SR epoch of every
+ * session, each on its own branch of the graph so their kernels overlap.
+ * The sessions stay owned by the caller and must outlive the batch; while a
+ * batch exists, do not run their own epochs concurrently with it.  No
+ * reference counterpart (the reference trains one model per process). */
+typedef struct rbmnqs_batch rbmnqs_batch;
+int rbmnqs_batch_create(rbmnqs_handle* const* sessions, int32_t n, rbmnqs_batch** out);
+/* s, o: arrays of n entries (may be NULL). */
+int rbmnqs_batch_epoch(rbmnqs_batch* b, rbmnqs_sample_stats* s, rbmnqs_sr_stats* o);
+/* kernel nodes of the batch graph (0 before the first epoch) */
+int rbmnqs_batch_graph_kernels(rbmnqs_batch* b, int32_t* kernel_nodes);
+void* rbmnqs_batch_stream(rbmnqs_batch* b);
+void rbmnqs_batch_destroy(rbmnqs_batch* b);
 /* Measured special-function (MUFU: ex2/lg2/sin/cos) throughput of the current
  * device in operations per second, from a dependent-chain probe kernel on
  * every SM; the denominator of the sampler kernel's roofline.  No

@@ -218,7 +218,7 @@ struct rbmnqs_handle {
     }
 
     // --- the epoch pieces -------------------------------------------------
-    void enqueue_sample() {
+    rbmnqs::SamplerArgs sampler_args() const {
         rbmnqs::SamplerArgs a{};
         a.m = machine();
         a.H = ham();
@@ -237,10 +237,9 @@ struct rbmnqs_handle {
         a.samples = samples.p;
         a.n_acc = nacc.p;
         a.n_prop = nprop.p;
-        mark(0);
-        ck(rbmnqs::launch_sampler(a, fp64, shape, st), "sampler kernel");
-        mark(1);
-        // E_loc and O_k of every sample (local_op::evaluate, derivative)
+        return a;
+    }
+    rbmnqs::EvalArgs eval_args() const {
         rbmnqs::EvalArgs ea{};
         ea.m = machine();
         ea.H = ham();
@@ -251,7 +250,15 @@ struct rbmnqs_handle {
         ea.eloc = E.p;
         ea.O = O.p;
         ea.plan = rbmnqs::SmemPlan{0, w_in_smem, 0, 0, 0};
-        ck(rbmnqs::launch_eval(ea, fp64, wpb, st), "eval kernel");
+        return ea;
+    }
+    void enqueue_sample() {
+        const rbmnqs::SamplerArgs a = sampler_args();
+        mark(0);
+        ck(rbmnqs::launch_sampler(a, fp64, shape, st), "sampler kernel");
+        mark(1);
+        // E_loc and O_k of every sample (local_op::evaluate, derivative)
+        ck(rbmnqs::launch_eval(eval_args(), fp64, wpb, st), "eval kernel");
         mark(2);
         ck(rbmnqs::launch_moments(O.p, fp64, E.p, N, P, mom_blocks, pd.p, pf.p, pe.p, d.p, F.p, emean.p, st),
            "moments");
@@ -260,7 +267,10 @@ struct rbmnqs_handle {
         ck(rbmnqs::launch_advance(ctl.p, cfg.reinit_chains, st), "advance");
         mark(3);
     }
-    void enqueue_optimize() {
+    // cg_after / cg_done: optional events ordering the matrix-free CG (a
+    // cooperative launch) after another session's, so that two grid-wide
+    // solves never compete for residency inside one batch graph.
+    void enqueue_optimize(cudaEvent_t cg_after = nullptr, cudaEvent_t cg_done = nullptr) {
         ck(rbmnqs::launch_schedule(sched.p, st), "schedule");
         int max_it = std::min(2 * P, cfg.max_iterations);
         if (max_it == 0) max_it = 2 * P;
@@ -269,9 +279,11 @@ struct rbmnqs_handle {
             // diag = var(O) straight from O; CG on the operator (cg_solver.cpp aprod)
             ck(rbmnqs::launch_var_diag(O.p, fp64, d.p, N, P, mfp, mfw, diag.p, maxdiag.p, st), "var diag");
             mark(4);
+            if (cg_after) ck(cudaStreamWaitEvent(st, cg_after, 0), "cg order");
             ck(rbmnqs::launch_cg_mfree(O.p, fp64, d.p, (double)N, N, P, P_neural, F.p, x.p, diag.p, maxdiag.p,
                                        sched.p, 0, 0, 0, max_it, rtol, mfp, mfw, cgres.p, st),
                "matrix-free cg");
+            if (cg_done) ck(cudaEventRecord(cg_done, st), "cg order");
             mark(5);
         } else {
             if (gram_tc)
@@ -678,6 +690,20 @@ int rbmnqs_get_weights(rbmnqs_handle* h, double* w) {
     });
 }
 
+static int count_kernel_nodes(cudaGraph_t g) {
+    size_t nn = 0;
+    ck(cudaGraphGetNodes(g, nullptr, &nn), "graph nodes");
+    std::vector<cudaGraphNode_t> nodes(nn);
+    ck(cudaGraphGetNodes(g, nodes.data(), &nn), "graph nodes");
+    int k = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        ck(cudaGraphNodeGetType(nd, &t), "node type");
+        k += t == cudaGraphNodeTypeKernel;
+    }
+    return k;
+}
+
 static void read_sample_stats(rbmnqs_handle* h, rbmnqs_sample_stats* out) {
     rbmnqs::EpochStatsDev s{};
     ck(cudaMemcpyAsync(&s, h->stats.p, sizeof(s), cudaMemcpyDeviceToHost, h->st), "copy");
@@ -751,16 +777,7 @@ int rbmnqs_epoch(rbmnqs_handle* h, rbmnqs_sample_stats* s, rbmnqs_sr_stats* o) {
                 throw;
             }
             ck(cudaStreamEndCapture(h->st, &g), "end capture");
-            size_t nn = 0;
-            ck(cudaGraphGetNodes(g, nullptr, &nn), "graph nodes");
-            std::vector<cudaGraphNode_t> nodes(nn);
-            ck(cudaGraphGetNodes(g, nodes.data(), &nn), "graph nodes");
-            h->graph_kernels = 0;
-            for (auto nd : nodes) {
-                cudaGraphNodeType t;
-                ck(cudaGraphNodeGetType(nd, &t), "node type");
-                h->graph_kernels += t == cudaGraphNodeTypeKernel;
-            }
+            h->graph_kernels = count_kernel_nodes(g);
             ck(cudaGraphInstantiate(&h->graph, g, 0), "instantiate");
             cudaGraphDestroy(g);
         }
@@ -1084,5 +1101,184 @@ int rbmnqs_probe_mufu(int32_t iters, double* ops_per_second) {
         *ops_per_second = 4.0 * iters * (double)blocks * 256.0 / (ms * 1e-3);
     });
 }
+
+int rbmnqs_autotune(rbmnqs_handle* h, int32_t sweeps, int32_t* sampler_wpb, int32_t* eval_wpb, double* sampler_ms) {
+    return guard([&] {
+        require(h != nullptr && sweeps >= 1, "rbmnqs_autotune: bad arguments");
+        cudaEvent_t a, b;
+        ck(cudaEventCreate(&a), "event");
+        ck(cudaEventCreate(&b), "event");
+        auto timed = [&](auto&& launch) {
+            launch();  // warm-up
+            ck(cudaEventRecord(a, h->st), "event");
+            launch();
+            ck(cudaEventRecord(b, h->st), "event");
+            ck(cudaEventSynchronize(b), "sync");
+            float ms = 0;
+            ck(cudaEventElapsedTime(&ms, a, b), "elapsed");
+            return (double)ms;
+        };
+        // chains restart from the same configurations in every trial and
+        // get them back at the end
+        const size_t sb = (size_t)h->cfg.n_chains * 16;
+        DevBuf<uint32_t> saved;
+        saved.alloc((size_t)h->cfg.n_chains * 4);
+        ck(cudaMemcpyAsync(saved.p, h->spins.p, sb, cudaMemcpyDeviceToDevice, h->st), "save chains");
+        double best_ms = 0;
+        rbmnqs::SamplerArgs args = h->sampler_args();
+        args.spc = 1;
+        args.step = 1;
+        args.warmup = sweeps - 1;
+        if (!h->pf_n) {  // the Pfaffian buffers are sized for the planned shape
+            rbmnqs::SamplerShape best = h->shape;
+            best_ms = -1;
+            std::vector<int> tried;
+            for (int cap = h->shape.warps_per_block; cap >= 1; cap /= 2) {
+                rbmnqs::SamplerShape sh{};
+                ck(rbmnqs::plan_sampler(h->machine(), h->fp64, h->cfg.n_chains, h->n_prop_bonds, &sh, cap),
+                   "sampler plan");
+                if (std::find(tried.begin(), tried.end(), sh.warps_per_block) != tried.end()) continue;
+                tried.push_back(sh.warps_per_block);
+                const double ms = timed([&] {
+                    ck(cudaMemcpyAsync(h->spins.p, saved.p, sb, cudaMemcpyDeviceToDevice, h->st), "restore");
+                    ck(rbmnqs::launch_sampler(args, h->fp64, sh, h->st), "sampler kernel");
+                });
+                if (best_ms < 0 || ms < best_ms) {
+                    best_ms = ms;
+                    best = sh;
+                }
+                if (tried.size() >= 5) break;
+            }
+            // the planner's attribute for the chosen shape must be the last set
+            rbmnqs::SamplerShape chk{};
+            ck(rbmnqs::plan_sampler(h->machine(), h->fp64, h->cfg.n_chains, h->n_prop_bonds, &chk,
+                                    best.warps_per_block),
+               "sampler plan");
+            h->shape = chk;
+        }
+        // evaluation kernel: 1..8 warps per block within the smem budget
+        {
+            rbmnqs::EvalArgs ea = h->eval_args();
+            rbmnqs::SmemPlan pl{0, h->w_in_smem, 0, 0, 0};
+            double best = -1;
+            int bw = h->wpb;
+            for (int w = 1; w <= 8; w *= 2) {
+                if (rbmnqs::eval_smem_bytes(h->machine(), h->fp64, w, pl) > 200 * 1024) break;
+                const double ms = timed([&] { ck(rbmnqs::launch_eval(ea, h->fp64, w, h->st), "eval kernel"); });
+                if (best < 0 || ms < best) {
+                    best = ms;
+                    bw = w;
+                }
+            }
+            h->wpb = bw;
+        }
+        ck(cudaMemcpyAsync(h->spins.p, saved.p, sb, cudaMemcpyDeviceToDevice, h->st), "restore chains");
+        ck(cudaStreamSynchronize(h->st), "sync");
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        if (h->graph) {  // re-capture with the new shapes
+            cudaGraphExecDestroy(h->graph);
+            h->graph = nullptr;
+        }
+        if (sampler_wpb) *sampler_wpb = h->shape.warps_per_block;
+        if (eval_wpb) *eval_wpb = h->wpb;
+        if (sampler_ms) *sampler_ms = best_ms;
+    });
+}
+
+}  // extern "C"
+
+struct rbmnqs_batch {
+    std::vector<rbmnqs_handle*> hs;
+    cudaStream_t st = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> joins, cg_done;
+    cudaGraphExec_t graph = nullptr;
+    int graph_kernels = 0;
+    ~rbmnqs_batch() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (auto e : joins)
+            if (e) cudaEventDestroy(e);
+        for (auto e : cg_done)
+            if (e) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+extern "C" {
+
+int rbmnqs_batch_create(rbmnqs_handle* const* sessions, int32_t n, rbmnqs_batch** out) {
+    return guard([&] {
+        require(sessions && out && n >= 1, "rbmnqs_batch_create: bad arguments");
+        auto b = std::make_unique<rbmnqs_batch>();
+        for (int i = 0; i < n; i++) {
+            require(sessions[i] != nullptr, "rbmnqs_batch_create: null session");
+            require(std::find(b->hs.begin(), b->hs.end(), sessions[i]) == b->hs.end(),
+                    "rbmnqs_batch_create: a session appears twice");
+            b->hs.push_back(sessions[i]);
+        }
+        ck(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking), "stream");
+        ck(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "event");
+        b->joins.resize(n, nullptr);
+        b->cg_done.resize(n, nullptr);
+        for (auto& e : b->joins) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+        for (auto& e : b->cg_done) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+        *out = b.release();
+    });
+}
+
+int rbmnqs_batch_epoch(rbmnqs_batch* b, rbmnqs_sample_stats* s, rbmnqs_sr_stats* o) {
+    return guard([&] {
+        require(b != nullptr, "null batch");
+        if (!b->graph) {
+            // fork: every session's epoch on its own stream, joined back
+            cudaGraph_t g;
+            ck(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal), "capture");
+            try {
+                ck(cudaEventRecord(b->fork, b->st), "fork");
+                cudaEvent_t prev_cg = nullptr;  // matrix-free solves run one after another
+                for (size_t i = 0; i < b->hs.size(); i++) {
+                    rbmnqs_handle* h = b->hs[i];
+                    ck(cudaStreamWaitEvent(h->st, b->fork, 0), "fork wait");
+                    h->enqueue_sample();
+                    if (h->mfree) {
+                        h->enqueue_optimize(prev_cg, b->cg_done[i]);
+                        prev_cg = b->cg_done[i];
+                    } else {
+                        h->enqueue_optimize();
+                    }
+                    ck(cudaEventRecord(b->joins[i], h->st), "join");
+                    ck(cudaStreamWaitEvent(b->st, b->joins[i], 0), "join wait");
+                }
+            } catch (...) {
+                cudaStreamEndCapture(b->st, &g);
+                throw;
+            }
+            ck(cudaStreamEndCapture(b->st, &g), "end capture");
+            b->graph_kernels = count_kernel_nodes(g);
+            ck(cudaGraphInstantiate(&b->graph, g, 0), "instantiate");
+            cudaGraphDestroy(g);
+        }
+        ck(cudaGraphLaunch(b->graph, b->st), "graph launch");
+        ck(cudaStreamSynchronize(b->st), "sync");
+        for (size_t i = 0; i < b->hs.size(); i++) {
+            read_sample_stats(b->hs[i], s ? s + i : nullptr);
+            read_sr_stats(b->hs[i], o ? o + i : nullptr);
+            b->hs[i]->sampled = true;
+        }
+    });
+}
+
+int rbmnqs_batch_graph_kernels(rbmnqs_batch* b, int32_t* kernel_nodes) {
+    return guard([&] {
+        require(b && kernel_nodes, "null argument");
+        *kernel_nodes = b->graph_kernels;
+    });
+}
+
+void* rbmnqs_batch_stream(rbmnqs_batch* b) { return b ? (void*)b->st : nullptr; }
+
+void rbmnqs_batch_destroy(rbmnqs_batch* b) { delete b; }
 
 }  // extern "C"

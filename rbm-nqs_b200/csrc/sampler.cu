@@ -1078,7 +1078,7 @@ static const void* pick_sampler(int E, int fp64, int exp_table, int pf, int gath
     return nullptr;
 }
 
-cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bonds, SamplerShape* out) {
+cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bonds, SamplerShape* out, int max_wpb) {
     const int E = elements_per_lane(m.T);
     if (E < 0) return cudaErrorInvalidValue;
     int dev = 0, sms = 0, smem_max = 0;
@@ -1114,6 +1114,7 @@ cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bond
     const int reg_warps = 65536 / (regs * 32);
     if (wpb > reg_warps) wpb = reg_warps;
     if (wpb > want) wpb = want;
+    if (max_wpb > 0 && wpb > max_wpb) wpb = max_wpb;
     if (wpb < 1) wpb = 1;
     if (pl.u64 && sampler_smem_bytes(m, fp64, wpb, pl, n_bonds) > budget) pl.u64 = 0;
     while (wpb > 1 && sampler_smem_bytes(m, fp64, wpb, pl, n_bonds) > budget) wpb--;

@@ -103,7 +103,9 @@ struct SamplerShape {
     int blocks;
     int smem;
 };
-cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bonds, SamplerShape* out);
+// max_wpb > 0 caps the warps per block (launch-shape autotuning).
+cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bonds, SamplerShape* out,
+                         int max_wpb = 0);
 cudaError_t launch_sampler(const SamplerArgs& a, int fp64, const SamplerShape& shape, cudaStream_t st);
 cudaError_t launch_eval(const EvalArgs& a, int fp64, int warps_per_block, cudaStream_t st);
 int elements_per_lane(int T);

@@ -102,11 +102,16 @@ def _declare(L):
         "rbmnqs_timing": [VP, P_D, P_I64, C.c_int32],
         "rbmnqs_timing_reset": [VP, C.c_int32],
         "rbmnqs_graph_kernels": [VP, P_I],
+        "rbmnqs_autotune": [VP, C.c_int32, P_I, P_I, P_D],
+        "rbmnqs_batch_create": [C.POINTER(VP), C.c_int32, C.POINTER(VP)],
+        "rbmnqs_batch_epoch": [VP, VP, VP],
+        "rbmnqs_batch_graph_kernels": [VP, P_I],
+        "rbmnqs_batch_destroy": [VP],
     }
     for name, args in sig.items():
         f = getattr(L, name)
         f.argtypes = args
-        f.restype = None if name in ("rbmnqs_model_destroy", "rbmnqs_destroy") else C.c_int
+        f.restype = None if name in ("rbmnqs_model_destroy", "rbmnqs_destroy", "rbmnqs_batch_destroy") else C.c_int
     L.rbmnqs_sr_solve_noalloc.argtypes = [VP, C.c_int32, C.c_int32, C.c_int32, VP, C.c_double, VP, VP, C.c_double,
                                           C.c_double, C.c_double, VP, C.c_int32, C.c_double, VP, P_I, P_D]
     L.rbmnqs_sr_solve_noalloc.restype = C.c_int
@@ -115,6 +120,8 @@ def _declare(L):
     L.rbmnqs_last_error.restype = C.c_char_p
     L.rbmnqs_stream.argtypes = [VP]
     L.rbmnqs_stream.restype = VP
+    L.rbmnqs_batch_stream.argtypes = [VP]
+    L.rbmnqs_batch_stream.restype = VP
 
 
 def lib():
@@ -378,3 +385,41 @@ class Session:
 
     def stream(self):
         return lib().rbmnqs_stream(self._h)
+
+    def autotune(self, sweeps=4):
+        """Launch-shape autotuning (rbmnqs_autotune): (sampler warps per
+        block, evaluation warps per block, sampler ms for `sweeps` sweeps)."""
+        sw, ew, ms = C.c_int32(), C.c_int32(), C.c_double()
+        _ck(lib().rbmnqs_autotune(self._h, sweeps, C.byref(sw), C.byref(ew), C.byref(ms)))
+        return sw.value, ew.value, ms.value
+
+
+class Batch:
+    """Independent sessions advanced together: one CUDA-graph launch runs the
+    epoch of every session (rbmnqs_batch_*)."""
+
+    def __init__(self, sessions):
+        self.sessions = list(sessions)
+        arr = (VP * len(self.sessions))(*[x._h for x in self.sessions])
+        h = VP()
+        _ck(lib().rbmnqs_batch_create(arr, len(self.sessions), C.byref(h)))
+        self._h = h
+
+    def epoch(self):
+        n = len(self.sessions)
+        s, o = (SampleStats * n)(), (SrStats * n)()
+        _ck(lib().rbmnqs_batch_epoch(self._h, C.cast(s, VP), C.cast(o, VP)))
+        return [x.as_dict() for x in s], [x.as_dict() for x in o]
+
+    def graph_kernels(self):
+        k = C.c_int32()
+        _ck(lib().rbmnqs_batch_graph_kernels(self._h, C.byref(k)))
+        return k.value
+
+    def stream(self):
+        return lib().rbmnqs_batch_stream(self._h)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.rbmnqs_batch_destroy(self._h)
+            self._h = None

@@ -1,0 +1,59 @@
+"""Batched independent trainings (one CUDA-graph launch for several sessions
+of different lattices and sizes) and the launch-shape autotuner: both must
+leave every session's trajectory bit-for-bit what its own epochs produce."""
+import numpy as np
+import pytest
+
+import oracle as O
+import rbmnqs
+
+pytestmark = pytest.mark.gpu
+
+PROBLEMS = [
+    # (model, L, rbm_type, alpha, precision, chains, spc)
+    ("toric", 3, 0, 2, 0, 32, 8),     # 702 parameters, tensor-core Gram
+    ("toric", 4, 0, 2, 1, 16, 8),     # 2144 parameters: matrix-free CG (cooperative launch)
+    ("toric", 4, 0, 2, 0, 24, 4),     # a second matrix-free solve in the same graph
+    ("kitaev", 3, 0, 1, 1, 16, 8),
+    ("kitaev", 4, 1, 4, 0, 64, 4),
+]
+
+
+def make(spec, seed):
+    model, L, rt, alpha, prec, chains, spc = spec
+    gm = rbmnqs.Model.kitaev(L) if model == "kitaev" else rbmnqs.Model.toric(L, symmetry=1.0)
+    cfg = rbmnqs.default_config(rbm_type=rt, alpha=alpha, n_chains=chains, samples_per_chain=spc, warmup=2,
+                                seed=seed, precision=prec, bond_flips=0.5 if model == "kitaev" else 0.0,
+                                max_iterations=60)
+    s = rbmnqs.Session(gm, cfg)
+    rng = np.random.default_rng(seed)
+    s.set_weights(0.05 * (rng.normal(size=s.n_params) + 1j * rng.normal(size=s.n_params)))
+    return s
+
+
+def test_batch_epochs_equal_individual_epochs():
+    a = [make(p, 100 + i) for i, p in enumerate(PROBLEMS)]
+    b = [make(p, 100 + i) for i, p in enumerate(PROBLEMS)]
+    batch = rbmnqs.Batch(a)
+    for _ in range(3):
+        sa, oa = batch.epoch()
+        for i, s in enumerate(b):
+            sb, ob = s.epoch()
+            assert sa[i]["energy"] == sb["energy"] and oa[i]["iterations"] == ob["iterations"]
+            assert oa[i]["status"] == 0
+    for x, y in zip(a, b):
+        assert np.array_equal(x.get_weights(), y.get_weights())
+        assert np.array_equal(x.spins(), y.spins())
+    assert batch.graph_kernels() == sum(s.graph_kernels() for s in b)
+
+
+def test_autotune_keeps_the_trajectory():
+    spec = ("kitaev", 4, 1, 4, 0, 256, 4)
+    a, b = make(spec, 7), make(spec, 7)
+    sw, ew, ms = a.autotune(sweeps=3)
+    assert sw >= 1 and 1 <= ew <= 8 and ms > 0
+    for _ in range(2):
+        a.epoch()
+        b.epoch()
+    assert np.array_equal(a.get_weights(), b.get_weights())
+    assert np.array_equal(a.spins(), b.spins())
