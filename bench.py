@@ -56,6 +56,12 @@ WORKLOADS = {
     "kitaev128_symm_a4": dict(model="kitaev", n_cells=8, rbm_type=1, alpha=4, symmetry=0.5, n_chains=16384,
                               samples_per_chain=1, warmup=63, step=1, bond_flips=0.5, std=1e-4,
                               reg2=(1e-4, 1e-4, 1.0), precision=0, gram=0),
+    # 48 independent toric-code trainings (L = 3..8, 8 each, basic RBM
+    # alpha=2, 1024 chains each) advanced by one CUDA-graph launch per epoch;
+    # launch shapes autotuned per L; matrix-free CG capped at 100 iterations
+    "toric_batch48": dict(model="toric", batch_L=(3, 4, 5, 6, 7, 8), batch_copies=8, rbm_type=0, alpha=2,
+                          symmetry=1.0, n_chains=1024, samples_per_chain=1, warmup=63, step=1, bond_flips=0.0,
+                          std=1e-4, reg2=(1e-4, 1e-4, 1.0), precision=0, gram=0, max_iterations=100),
 }
 METRIC = "uncorrelated samples/s (SR epoch, E_loc binning tau)"
 # DRAM bytes per sampler launch from an ncu capture of the same workload: the
@@ -300,6 +306,94 @@ def run_ours(args, rank, world, local):
     return result
 
 
+def run_batch(args, rank, world, local):
+    """The batched toric workload: all problems' epochs in one graph launch."""
+    import torch
+    import rbmnqs
+
+    dist = init_dist(world, "nccl")
+    torch.cuda.set_device(local)
+    wl = workload(args)
+    sessions, Ls = [], []
+    for L in wl["batch_L"]:
+        model = rbmnqs.Model.toric(L, symmetry=wl["symmetry"])
+        for c in range(wl["batch_copies"]):
+            cfg = rbmnqs.default_config(rbm_type=wl["rbm_type"], alpha=wl["alpha"], n_chains=wl["n_chains"],
+                                        samples_per_chain=wl["samples_per_chain"], warmup=wl["warmup"],
+                                        step=wl["step"], bond_flips=0.0, seed=1000 * L + c + 77 * rank,
+                                        precision=wl["precision"], gram=wl["gram"], reinit_chains=0,
+                                        reg2=wl["reg2"], max_iterations=wl["max_iterations"])
+            s = rbmnqs.Session(model, cfg)
+            s.set_weights(make_weights(s.n_params, wl["std"], 7 * L + c + rank))
+            sessions.append(s)
+            Ls.append(L)
+    tuned = {}  # launch shapes chosen by the autotuner, per L
+    for s, L in zip(sessions, Ls):
+        shape = s.autotune(sweeps=4)[:2]
+        tuned.setdefault(L, shape)
+    batch = rbmnqs.Batch(sessions)
+    stream = torch.cuda.ExternalStream(batch.stream())
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    for _ in range(max(3, args.warmup)):
+        batch.epoch()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    neff = 0.0
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            ev[k][0].record(stream)
+            st, sr = batch.epoch()
+            ev[k][1].record(stream)
+            neff += sum(s.N / (1.0 + 2.0 * x["tau"]) for s, x in zip(sessions, st))
+        torch.cuda.synchronize()
+    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    # end to end: every session's weights in and out through the C ABI, each step
+    ws = [s.get_weights() for s in sessions]
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        ev2[k][0].record(stream)
+        for s, w in zip(sessions, ws):
+            s.set_weights(w)
+        batch.epoch()
+        ws = [s.get_weights() for s in sessions]
+        ev2[k][1].record(stream)
+    torch.cuda.synchronize()
+    t2_ms = sum(a.elapsed_time(b) for a, b in ev2)
+    if world > 1:
+        t = torch.tensor([t_ms, t2_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms, t2_ms = t.tolist()
+    its = [x["iterations"] for x in sr]
+    Pmax = max(s.n_params for s in sessions)
+    hb = sum(s.n_params for s in sessions) * 16
+    res = {
+        "metric": METRIC, "value": world * neff / (t_ms * 1e-3), "unit": "samples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 ratios / fp64 theta+CG",
+        "data": "synthetic (seeded complex Gaussian weights std 1e-4, Philox chains)",
+        "config": {"workload": args.workload, "problems": len(sessions),
+                   "model": "toric code L x L (2 L^2 spins), L in %s, %d each" % (list(wl["batch_L"]),
+                                                                              wl["batch_copies"]),
+                   "machine": f"RBM alpha={wl['alpha']}, up to {Pmax} params (matrix-free CG above 2048)",
+                   "n_chains_each": wl["n_chains"], "sweeps_per_epoch": wl["warmup"] + 1,
+                   "max_cg_iterations": wl["max_iterations"], "launch_shapes": {str(k): v for k, v in tuned.items()},
+                   "parallelism": f"replicas x{world}", "l2": "256 MiB L2 flush between timed epochs"},
+        "sr_epochs_per_s": world * args.steps / (t_ms * 1e-3), "batch_graph_kernels": batch.graph_kernels(),
+        "cg_iterations_mean": float(np.mean(its)),
+        "e2e": {"value": world * neff / (t2_ms * 1e-3), "unit": "samples/s", "h2d_bytes_per_step": hb,
+                "d2h_bytes_per_step": hb},
+        "gpu_launches": batch.graph_kernels() * args.steps, "clocks": clk.summary(),
+    }
+    if world > 1:
+        dist.destroy_process_group()
+    return res if rank == 0 else None
+
+
 # ------------------------------------------------------------ CPU arm --
 def cpu_epoch(wl, chains, seed, threads):
     """One bounded epoch of the workload on the FP64 CPU restatement:
@@ -356,6 +450,11 @@ def main():
                                            f"on their samples, per step"},
                 "e2e": {"value": v_raw, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
+        return
+    if "batch_L" in wl:
+        res = run_batch(args, rank, world, local)
+        if rank == 0:
+            print(json.dumps(res))
         return
     res = run_ours(args, rank, world, local)
     if rank == 0:

@@ -139,6 +139,7 @@ struct rbmnqs_handle {
     DevBuf<rbmnqs::EpochStatsDev> stats;
     // matrix-free SR (n_params above the dense limit): no S is formed
     bool mfree = false;
+    bool coop_dense = false;  // formed S too large for the cluster CG: cooperative grid CG
     rbmnqs::MfreePlan mfp{};
     rbmnqs::MfreeWork mfw{};
     DevBuf<unsigned char> mfbuf;
@@ -293,7 +294,13 @@ struct rbmnqs_handle {
             ck(rbmnqs::launch_regularize(Sm.p, P, P_neural, N, sched.p, diag.p, Sreg.p, maxdiag.p, st),
                "regularize");
             mark(4);
-            ck(rbmnqs::launch_cg(Sreg.p, F.p, x.p, P, max_it, rtol, cgres.p, st), "cg");
+            if (coop_dense && cg_after) ck(cudaStreamWaitEvent(st, cg_after, 0), "cg order");
+            if (coop_dense)
+                ck(rbmnqs::launch_cg_dense_coop(Sreg.p, F.p, x.p, P, max_it, rtol, mfp, mfw, cgres.p, st),
+                   "cooperative cg");
+            else
+                ck(rbmnqs::launch_cg(Sreg.p, F.p, x.p, P, max_it, rtol, cgres.p, st), "cg");
+            if (coop_dense && cg_done) ck(cudaEventRecord(cg_done, st), "cg order");
             mark(5);
         }
         ck(rbmnqs::launch_update(params.p, x.p, P, sched.p, cgres.p, st), "update");
@@ -591,10 +598,14 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         h->F.alloc(h->P);
         h->emean.alloc(1);
         h->gram_tc = !h->fp64 && cfg->gram == 0 && !h->mfree;
+        h->coop_dense = !h->mfree && !rbmnqs::cg_cluster_fits(h->P);
+        if (h->mfree || h->coop_dense) {
+            const int nn = h->mfree ? h->N : 1;
+            ck(rbmnqs::mfree_plan(nn, h->P, &h->mfp), "cooperative CG plan");
+            h->mfbuf.alloc(rbmnqs::mfree_work_bytes(nn, h->P, h->mfp));
+            h->mfw = rbmnqs::mfree_carve(h->mfbuf.p, nn, h->P, h->mfp);
+        }
         if (h->mfree) {
-            ck(rbmnqs::mfree_plan(h->N, h->P, &h->mfp), "matrix-free plan");
-            h->mfbuf.alloc(rbmnqs::mfree_work_bytes(h->N, h->P, h->mfp));
-            h->mfw = rbmnqs::mfree_carve(h->mfbuf.p, h->N, h->P, h->mfp);
         } else if (h->gram_tc) {
             ck(rbmnqs::gram_tc_plan(h->N, h->P, &h->gtc), "gram plan");
             const size_t pf = h->gtc.plane_floats();
@@ -1149,7 +1160,6 @@ int rbmnqs_autotune(rbmnqs_handle* h, int32_t sweeps, int32_t* sampler_wpb, int3
                 }
                 if (tried.size() >= 5) break;
             }
-            // the planner's attribute for the chosen shape must be the last set
             rbmnqs::SamplerShape chk{};
             ck(rbmnqs::plan_sampler(h->machine(), h->fp64, h->cfg.n_chains, h->n_prop_bonds, &chk,
                                     best.warps_per_block),
@@ -1242,7 +1252,7 @@ int rbmnqs_batch_epoch(rbmnqs_batch* b, rbmnqs_sample_stats* s, rbmnqs_sr_stats*
                     rbmnqs_handle* h = b->hs[i];
                     ck(cudaStreamWaitEvent(h->st, b->fork, 0), "fork wait");
                     h->enqueue_sample();
-                    if (h->mfree) {
+                    if (h->mfree || h->coop_dense) {
                         h->enqueue_optimize(prev_cg, b->cg_done[i]);
                         prev_cg = b->cg_done[i];
                     } else {

@@ -90,19 +90,21 @@ template <> __device__ double2 bsum<double2>(double2 v, double2* red) {
     return r;
 }
 
-// sum of the per-block partials in block order (every block gets the same value)
-__device__ __forceinline__ double sum_parts(const double* p, int G) {
+// Sum of the per-block partials: thread t adds entries t, t + 256, ... and the
+// block reduces in a fixed order, so every block gets the same value (and the
+// loads are issued in parallel rather than as one dependent chain).
+__device__ __forceinline__ double sum_parts(const double* p, int G, double* red) {
     double s = 0;
-    for (int i = 0; i < G; i++) s += cg_ld(p + i);
-    return s;
+    for (int i = threadIdx.x; i < G; i += blockDim.x) s += cg_ld(p + i);
+    return bsum(s, red);
 }
-__device__ __forceinline__ double2 sum_parts(const double2* p, int G) {
+__device__ __forceinline__ double2 sum_parts(const double2* p, int G, double2* red) {
     double2 s = make_double2(0, 0);
-    for (int i = 0; i < G; i++) {
+    for (int i = threadIdx.x; i < G; i += blockDim.x) {
         const double2 v = cg_ld(p + i);
         s = make_double2(s.x + v.x, s.y + v.y);
     }
-    return s;
+    return bsum(s, red);
 }
 
 template <typename TO>
@@ -121,29 +123,89 @@ __global__ void __launch_bounds__(kThreads) cg_mfree_kernel(const TO* __restrict
     const int gw = blk * (kThreads / 32) + (tid >> 5), nwarps = G * (kThreads / 32);
     const int gt = blk * kThreads + tid, nthreads = G * kThreads;
     const double r1 = sch ? sch->value[1] : r1_, r2 = sch ? sch->value[2] : r2_, rd = sch ? sch->value[3] : rd_;
-    const double mxd = *max_diag;
+    const double mxd = max_diag ? *max_diag : 0.0;
     if (blk == 0 && tid == 0) res->status = 0;
 
     // A b into Ap (b = x at the start, p afterwards); returns false on a
     // barrier timeout.  With want_pap, also leaves sum_q conj(b_q) Ap_q.
     auto aprod = [&](const double2* b, bool want_pap, double2* pap) -> bool {
-        // phase A: partial row dots (n, segment j) and d . b
-        const int nseg = w.nseg, lseg = w.lseg;
-        const long items = (long)nseg * N;
-        for (long it = gw; it < items; it += nwarps) {
-            const int j = (int)(it / N), n = (int)(it % N);
-            const int q0 = j * lseg, q1 = min(P, q0 + lseg);
-            double ax = 0, ay = 0;
-            const size_t row = (size_t)n * P;
-            for (int q = q0 + lane; q < q1; q += 32) {
-                const double2 o = zld(O, row + q), v = cg_ld(b + q);
-                ax = fma(o.x, v.x, fma(-o.y, v.y, ax));
-                ay = fma(o.x, v.y, fma(o.y, v.x, ay));
+        if (w.S) {
+            // formed, regularised S: Ap = S b, one warp per row
+            double2 pp = make_double2(0, 0);
+            for (int r = gw; r < P; r += nwarps) {
+                const double2* Sr = w.S + (size_t)r * P;
+                double ax = 0, ay = 0;
+                int q = lane;
+                for (; q + 96 < P; q += 128) {
+                    double2 a[4], v[4];
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        a[u] = __ldg(Sr + q + 32 * u);
+                        v[u] = cg_ld(b + q + 32 * u);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        ax = fma(a[u].x, v[u].x, fma(-a[u].y, v[u].y, ax));
+                        ay = fma(a[u].x, v[u].y, fma(a[u].y, v[u].x, ay));
+                    }
+                }
+                for (; q < P; q += 32) {
+                    const double2 a = __ldg(Sr + q), v = cg_ld(b + q);
+                    ax = fma(a.x, v.x, fma(-a.y, v.y, ax));
+                    ay = fma(a.x, v.y, fma(a.y, v.x, ay));
+                }
+                ax = warp_sum(ax);
+                ay = warp_sum(ay);
+                if (lane == 0) {
+                    w.Ap[r] = make_double2(ax, ay);
+                    if (want_pap) {
+                        const double2 br = cg_ld(b + r);
+                        pp.x += br.x * ax + br.y * ay;
+                        pp.y += br.x * ay - br.y * ax;
+                    }
+                }
             }
-            ax = warp_sum(ax);
-            ay = warp_sum(ay);
-            if (lane == 0) w.partA[(size_t)j * N + n] = make_double2(ax, ay);
+            if (want_pap) {
+                pp = bsum(pp, redz);
+                if (tid == 0) w.zpart[blk] = pp;
+            }
+            if (!grid_barrier(w.sync, G)) return false;
+            if (want_pap) *pap = sum_parts(w.zpart, G, redz);
+            return true;
         }
+        // phase A: O b.  Block blk owns rows blk, blk + G, ...; its 8 warps
+        // split the columns into 8 slices and walk 4 rows at a time, so each
+        // b element read from L2 serves 4 rows.  Partial dots per (slice, row).
+        {
+            const int wib = tid >> 5, nwb = kThreads / 32;
+            const int q0 = (int)((long)P * wib / nwb), q1 = (int)((long)P * (wib + 1) / nwb);
+            for (int n0 = blk; n0 < N; n0 += 4 * G) {
+                int nr[4];
+                bool val[4];
+#pragma unroll
+                for (int r = 0; r < 4; r++) {
+                    nr[r] = n0 + r * G;
+                    val[r] = nr[r] < N;
+                }
+                double ax[4] = {0, 0, 0, 0}, ay[4] = {0, 0, 0, 0};
+                for (int q = q0 + lane; q < q1; q += 32) {
+                    const double2 v = cg_ld(b + q);
+#pragma unroll
+                    for (int r = 0; r < 4; r++) {
+                        if (!val[r]) continue;
+                        const double2 o = zld(O, (size_t)nr[r] * P + q);
+                        ax[r] = fma(o.x, v.x, fma(-o.y, v.y, ax[r]));
+                        ay[r] = fma(o.x, v.y, fma(o.y, v.x, ay[r]));
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < 4; r++) {
+                    const double sx = warp_sum(ax[r]), sy = warp_sum(ay[r]);
+                    if (lane == 0 && val[r]) w.partA[(size_t)wib * N + nr[r]] = make_double2(sx, sy);
+                }
+            }
+        }
+        const int nseg = kThreads / 32;
         double2 db = make_double2(0, 0);
         for (int q = gt; q < P; q += nthreads) {
             const double2 dq = d[q], v = cg_ld(b + q);
@@ -162,7 +224,7 @@ __global__ void __launch_bounds__(kThreads) cg_mfree_kernel(const TO* __restrict
             }
             w.tmpN[n] = s;
         }
-        db = sum_parts(w.zpart, G);
+        db = sum_parts(w.zpart, G, redz);
         if (!grid_barrier(w.sync, G)) return false;
         // phase B: columns, 4 row groups x 64 columns per block
         const int c = tid % kColTile, rg = tid / kColTile, ngr = kThreads / kColTile;
@@ -172,9 +234,24 @@ __global__ void __launch_bounds__(kThreads) cg_mfree_kernel(const TO* __restrict
             const int q = tile * kColTile + c;
             double ax = 0, ay = 0;
             if (q < P) {
-                for (int n = rg; n < N; n += ngr) {
+                // 8 rows in flight per thread: the pass is a stream over O
+                int n = rg;
+                for (; n + 7 * ngr < N; n += 8 * ngr) {
+                    double2 o[8], v[8];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        o[u] = zld(O, (size_t)(n + u * ngr) * P + q);
+                        v[u] = cg_ld(w.tmpN + n + u * ngr);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; u++) {
+                        ax = fma(o[u].x, v[u].x, fma(o[u].y, v[u].y, ax));  // conj(o) v
+                        ay = fma(o[u].x, v[u].y, fma(-o[u].y, v[u].x, ay));
+                    }
+                }
+                for (; n < N; n += ngr) {
                     const double2 o = zld(O, (size_t)n * P + q), v = cg_ld(w.tmpN + n);
-                    ax = fma(o.x, v.x, fma(o.y, v.y, ax));   // conj(o) v
+                    ax = fma(o.x, v.x, fma(o.y, v.y, ax));
                     ay = fma(o.x, v.y, fma(-o.y, v.x, ay));
                 }
             }
@@ -205,7 +282,7 @@ __global__ void __launch_bounds__(kThreads) cg_mfree_kernel(const TO* __restrict
             if (tid == 0) w.zpart[blk] = pp;
         }
         if (!grid_barrier(w.sync, G)) return false;
-        if (want_pap) *pap = sum_parts(w.zpart, G);
+        if (want_pap) *pap = sum_parts(w.zpart, G, redz);
         return true;
     };
 
@@ -224,7 +301,7 @@ __global__ void __launch_bounds__(kThreads) cg_mfree_kernel(const TO* __restrict
         if (tid == 0) w.dpart[blk] = rl;
         ok = grid_barrier(w.sync, G);
     }
-    double rsold = ok ? sum_parts(w.dpart, G) : 0.0, rs = rsold;
+    double rsold = ok ? sum_parts(w.dpart, G, redd) : 0.0, rs = rsold;
     int itn = 0;
     if (ok) {
         for (itn = 0; itn < max_it; itn++) {
@@ -248,7 +325,7 @@ __global__ void __launch_bounds__(kThreads) cg_mfree_kernel(const TO* __restrict
             rl = bsum(rl, redd);
             if (tid == 0) w.dpart[blk] = rl;
             if (!(ok = grid_barrier(w.sync, G))) break;
-            rs = sum_parts(w.dpart, G);
+            rs = sum_parts(w.dpart, G, redd);
             if (rs < rtol) break;
             const double beta = rs / rsold;
             for (int q = gt; q < P; q += nthreads) {
@@ -339,14 +416,8 @@ cudaError_t mfree_plan(int N, int P, MfreePlan* pl) {
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     if (per_sm > 2) per_sm = 2;
     pl->blocks = sms * per_sm;
-    const int nwarps = pl->blocks * (kThreads / 32);
-    int nseg = (2 * nwarps + N - 1) / N;
-    if (nseg < 1) nseg = 1;
-    int lseg = (P + nseg - 1) / nseg;
-    lseg = (lseg + 31) / 32 * 32;
-    nseg = (P + lseg - 1) / lseg;
-    pl->nseg = nseg;
-    pl->lseg = lseg;
+    pl->nseg = kThreads / 32;  // column slices of the O b pass (one per warp of a block)
+    pl->lseg = (P + pl->nseg - 1) / pl->nseg;
     pl->diag_blocks = pl->blocks;
     return cudaSuccess;
 }
@@ -377,6 +448,26 @@ MfreeWork mfree_carve(void* base, int N, int P, const MfreePlan& pl) {
 cudaError_t launch_max_diag(const double* diag, int P, double* max_diag, cudaStream_t st) {
     max_parts_kernel<<<1, 32, 0, st>>>(diag, P, max_diag);
     return cudaGetLastError();
+}
+
+cudaError_t launch_cg_dense_coop(const double2* A, const double2* b, double2* x, int P, int max_it, double rtol,
+                                 const MfreePlan& pl, const MfreeWork& w, CgResultDev* res, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(w.sync, 0, sizeof(MfreeSync), st);
+    if (e != cudaSuccess) return e;
+    MfreeWork wk = w;
+    wk.S = A;
+    const double2* O = nullptr;
+    const double2* d = nullptr;
+    const double* diag = nullptr;
+    const double* mx = nullptr;
+    const ScheduleDev* sch = nullptr;
+    double norm = 1.0, z = 0.0;
+    int N = 1, n_neural = P;
+    CgResultDev* r = res;
+    const void* args[] = {&O, &d, &norm, &N, &P, &n_neural, &b, &x, &diag, &mx, &sch, &z, &z, &z,
+                          &max_it, &rtol, &wk, &r};
+    return cudaLaunchCooperativeKernel(cg_fn<double2>(), dim3(pl.blocks), dim3(kThreads), const_cast<void**>(args), 0,
+                                       st);
 }
 
 cudaError_t launch_var_diag(const void* O, int fp64, const double2* d, int N, int P, const MfreePlan& pl,

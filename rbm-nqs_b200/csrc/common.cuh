@@ -126,4 +126,10 @@ template <typename R> __device__ __forceinline__ C2<R> ctanh_r(R a, R b) {
     return mk<R>(copysign(omz * ((R)1 + z), a) * inv, (R)4 * z * s * c * inv);
 }
 
+// Raise (never lower) a kernel's dynamic shared-memory limit.  The limit is a
+// per-function attribute shared by every session in the process, and launches
+// already captured into CUDA graphs keep the size they were recorded with, so
+// it only ever grows to the largest size any session needs.
+cudaError_t ensure_dynamic_smem(const void* fn, int bytes);
+
 }  // namespace rbmnqs

@@ -377,7 +377,7 @@ cudaError_t launch_gram_tc(const GramTC& g, const void* O, int fp64, const doubl
     else
         gram_prep<float2><<<pg, 256, 0, st>>>((const float2*)O, d, g.N, g.P, g.K, g.Xh, g.Xl);
     const int smem = STAGES * STAGE_BYTES + 1024;
-    cudaError_t e = cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(gram_tc_kernel), smem);
     if (e != cudaSuccess) return e;
     const int nup = g.ntile * (g.ntile + 1) / 2;
     const CUtensorMap* mh = reinterpret_cast<const CUtensorMap*>(g.map_h);

@@ -13,6 +13,9 @@
 // configuration after every sweep (mixed-precision scheme), so FP32
 // drift never outlives one sweep.  With the Pfaffian factor (sites <= 32) each
 // lane also holds its row of X^{-1} in FP64 registers (pfaffian.cuh).
+#include <map>
+#include <mutex>
+
 #include "common.cuh"
 #include "sampler.cuh"
 
@@ -1120,7 +1123,7 @@ cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bond
     while (wpb > 1 && sampler_smem_bytes(m, fp64, wpb, pl, n_bonds) > budget) wpb--;
     const int smem = sampler_smem_bytes(m, fp64, wpb, pl, n_bonds);
     if (smem > budget) return cudaErrorInvalidValue;
-    err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    err = ensure_dynamic_smem(fn, smem);
     if (err != cudaSuccess) return err;
     int per_sm = 0;
     err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, smem);
@@ -1135,12 +1138,25 @@ cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bond
     return cudaSuccess;
 }
 
+cudaError_t ensure_dynamic_smem(const void* fn, int bytes) {
+    static std::mutex mu;
+    static std::map<const void*, int> set;
+    std::lock_guard<std::mutex> lk(mu);
+    int& cur = set[fn];
+    if (bytes <= cur) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
+
 cudaError_t launch_sampler(const SamplerArgs& a0, int fp64, const SamplerShape& sh, cudaStream_t st) {
     SamplerArgs a = a0;
     a.plan = sh.plan;
     const int E = elements_per_lane(a.m.T);
     const void* fn = pick_sampler(E, fp64, sh.plan.use_u, a.m.pf.n > 0, sh.plan.gather);
     if (!fn) return cudaErrorInvalidValue;
+    const cudaError_t e = ensure_dynamic_smem(fn, sh.smem);
+    if (e != cudaSuccess) return e;
     void* args[] = {&a};
     return cudaLaunchKernel(fn, dim3(sh.blocks), dim3(32 * sh.warps_per_block), args, sh.smem, st);
 }
@@ -1148,8 +1164,7 @@ cudaError_t launch_sampler(const SamplerArgs& a0, int fp64, const SamplerShape& 
 template <int E, typename R, bool PF>
 static cudaError_t launch_e2(const EvalArgs& a, int wpb, cudaStream_t st) {
     const int smem = eval_smem_bytes(a.m, sizeof(R) == 8, wpb, a.plan);
-    cudaError_t err =
-        cudaFuncSetAttribute(eval_kernel<E, R, PF>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t err = ensure_dynamic_smem(reinterpret_cast<const void*>(eval_kernel<E, R, PF>), smem);
     if (err != cudaSuccess) return err;
     const int blocks = (a.B + wpb - 1) / wpb;
     eval_kernel<E, R, PF><<<blocks, 32 * wpb, smem, st>>>(a);

@@ -807,25 +807,30 @@ cudaError_t launch_regularize(const double2* S, int P, int n_neural, int N, cons
     return cudaGetLastError();
 }
 
+bool cg_cluster_fits(int P) {
+    const int rp = (P + kClusterCta - 1) / kClusterCta;
+    return ((size_t)rp * P + P + 3 * (size_t)rp) * sizeof(double2) <= 200 * 1024;
+}
+
 cudaError_t launch_cg(const double2* A, const double2* b, double2* x, int P, int max_it, double rtol, CgResultDev* res,
                       cudaStream_t st) {
     const int rp = (P + kClusterCta - 1) / kClusterCta;
     const size_t csm = ((size_t)rp * P + P + 3 * (size_t)rp) * sizeof(double2);
     if (csm <= 200 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(cg_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm);
+        cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(cg_cluster), (int)csm);
         if (e != cudaSuccess) return e;
         cg_cluster<<<kClusterCta, 256, csm, st>>>(A, b, x, P, max_it, rtol, res);
         return cudaGetLastError();
     }
     const size_t packed = (packed_size(P) + 4 * (size_t)P) * sizeof(double2);
     if (packed <= 200 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(cg_packed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)packed);
+        cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(cg_packed), (int)packed);
         if (e != cudaSuccess) return e;
         cg_packed<<<1, 1024, packed, st>>>(A, b, x, P, max_it, rtol, res);
         return cudaGetLastError();
     }
     const int smem = 3 * P * (int)sizeof(double2);
-    cudaError_t e = cudaFuncSetAttribute(cg_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(cg_dense), smem);
     if (e != cudaSuccess) return e;
     cg_dense<<<1, 1024, smem, st>>>(A, b, x, P, max_it, rtol, res);
     return cudaGetLastError();

@@ -55,6 +55,7 @@ struct MfreePlan {
     int blocks, nseg, lseg, diag_blocks;
 };
 struct MfreeWork {
+    const double2* S;  // formed regularised S (dense cooperative mode) or null
     double2 *r, *p, *Ap, *tmpN, *partA, *zpart;
     double *dpart, *maxpart;
     MfreeSync* sync;
@@ -66,6 +67,13 @@ MfreeWork mfree_carve(void* base, int N, int P, const MfreePlan& pl);
 // diag = unbiased var(O) per parameter and its maximum (device scalar)
 cudaError_t launch_var_diag(const void* O, int fp64, const double2* d, int N, int P, const MfreePlan& pl,
                             const MfreeWork& w, double* diag, double* max_diag, cudaStream_t st);
+// CG on a formed regularised S (P x P) with the cooperative kernel: for P
+// whose S does not fit the shared-memory cluster solve.  Work from
+// mfree_plan(1, P) / mfree_carve.
+cudaError_t launch_cg_dense_coop(const double2* A, const double2* b, double2* x, int P, int max_it, double rtol,
+                                 const MfreePlan& pl, const MfreeWork& w, CgResultDev* res, cudaStream_t st);
+// whether the 8-CTA shared-memory CG holds S for this P
+bool cg_cluster_fits(int P);
 // max of a given diag (explicit-solve entry)
 cudaError_t launch_max_diag(const double* diag, int P, double* max_diag, cudaStream_t st);
 // r1 / r2 / rd from sch when non-null, else the explicit values
