@@ -215,6 +215,33 @@ int rbmnqs_graph_kernels(rbmnqs_handle* h, int32_t* kernel_nodes);
 /* The handle's cudaStream_t, for callers that order work against it. */
 void* rbmnqs_stream(rbmnqs_handle* h);
 
+/* ---------------------------------------------- learned proposal network */
+/* The proposal network n_in -> h1 -> h2 -> n_out (GELU, BF16 weights and
+ * activations, FP32 accumulation; forward, backward and Adam on the GPU)
+ * exposed on its own for tests and tools.  No reference counterpart.
+ * Parameters are flat [W1 (h1 x n_in), b1, W2 (h2 x h1), b2, W3 (n_out x h2),
+ * b3], weights row-major [out][in].  h1, h2 multiples of 64 up to 256;
+ * n_in, n_out up to 256. */
+typedef struct rbmnqs_mlp rbmnqs_mlp;
+int rbmnqs_mlp_create(int32_t n_in, int32_t h1, int32_t h2, int32_t n_out, int32_t max_batch,
+                      rbmnqs_mlp** out);
+int rbmnqs_mlp_n_params(const rbmnqs_mlp* m, int64_t* n);
+int rbmnqs_mlp_set_params(rbmnqs_mlp* m, const float* params);
+int rbmnqs_mlp_get_params(rbmnqs_mlp* m, float* params);
+/* weights N(0, std), biases zero (seeded) */
+int rbmnqs_mlp_init(rbmnqs_mlp* m, float std, uint64_t seed);
+/* flip logits [B][n_out] of configurations spins[B][4] (host buffers) */
+int rbmnqs_mlp_forward(rbmnqs_mlp* m, const uint32_t* spins, int32_t B, float* logits);
+/* loss (1/B) sum softplus(l) - t l against flip masks targets[B][4];
+ * gradients in the flat parameter layout (grads may be NULL); apply != 0
+ * takes one Adam step with learning rate lr. */
+int rbmnqs_mlp_train_step(rbmnqs_mlp* m, const uint32_t* spins, const uint32_t* targets, int32_t B, float lr,
+                          int32_t apply, float* loss, float* grads);
+/* tensor of the last pass for tests: 0 a1, 1 a2, 2 z1, 3 z2, 4 g1, 5 g2,
+ * 6 g3 (dL/dlogits); [B][cols] as float (out may be NULL to query cols) */
+int rbmnqs_mlp_intermediate(rbmnqs_mlp* m, int32_t which, int32_t B, float* out, int32_t* cols);
+void rbmnqs_mlp_destroy(rbmnqs_mlp* m);
+
 /* ------------------------------------------- batched independent trainings */
 /* Several sessions (different lattices, machines and sizes allowed) advanced
  * together: one CUDA-graph launch runs the whole sample + SR epoch of every

@@ -15,6 +15,7 @@
 #include "../host/model.hpp"
 #include "rbmnqs_b200.h"
 #include "gram_tc.cuh"
+#include "mlp.cuh"
 #include "sampler.cuh"
 #include "sr.cuh"
 
@@ -1290,5 +1291,154 @@ int rbmnqs_batch_graph_kernels(rbmnqs_batch* b, int32_t* kernel_nodes) {
 void* rbmnqs_batch_stream(rbmnqs_batch* b) { return b ? (void*)b->st : nullptr; }
 
 void rbmnqs_batch_destroy(rbmnqs_batch* b) { delete b; }
+
+}  // extern "C"
+
+struct rbmnqs_mlp {
+    cudaStream_t st = nullptr;
+    std::unique_ptr<rbmnqs::Mlp> net;
+    DevBuf<uint32_t> spins, targets;
+    DevBuf<float> loss;
+    ~rbmnqs_mlp() {
+        net.reset();
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+namespace {
+void mlp_upload(rbmnqs_mlp* m, const uint32_t* spins, const uint32_t* targets, int B) {
+    require(B >= 1 && B <= m->net->max_batch(), "batch larger than max_batch");
+    ck(cudaMemcpyAsync(m->spins.p, spins, (size_t)B * 16, cudaMemcpyHostToDevice, m->st), "copy");
+    if (targets) ck(cudaMemcpyAsync(m->targets.p, targets, (size_t)B * 16, cudaMemcpyHostToDevice, m->st), "copy");
+}
+void mlp_check(rbmnqs_mlp* m) {
+    ck(cudaStreamSynchronize(m->st), "sync");
+    const int e = m->net->error_flag_host();
+    if (e) throw Fail{RBMNQS_ERR_CUDA, "proposal network GEMM: pipeline wait timed out (code " + std::to_string(e) + ")"};
+}
+}  // namespace
+
+extern "C" {
+
+int rbmnqs_mlp_create(int32_t n_in, int32_t h1, int32_t h2, int32_t n_out, int32_t max_batch, rbmnqs_mlp** out) {
+    return guard([&] {
+        require(out && n_in >= 1 && n_in <= 256 && n_out >= 1 && n_out <= 256 && h1 % 64 == 0 && h2 % 64 == 0 &&
+                    h1 >= 64 && h1 <= 256 && h2 >= 64 && h2 <= 256 && max_batch >= 1,
+                "rbmnqs_mlp_create: unsupported sizes");
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+            throw Fail{RBMNQS_ERR_NO_DEVICE, "no CUDA device available"};
+        auto m = std::make_unique<rbmnqs_mlp>();
+        ck(cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking), "stream");
+        rbmnqs::MlpDims d;
+        d.n_in = n_in;
+        d.h1 = h1;
+        d.h2 = h2;
+        d.n_out = n_out;
+        try {
+            m->net = std::make_unique<rbmnqs::Mlp>(d, max_batch, m->st);
+        } catch (cudaError_t e) {
+            ck(e, "proposal network");
+        }
+        const int bm = m->net->max_batch();
+        m->spins.alloc((size_t)bm * 4);
+        m->targets.alloc((size_t)bm * 4);
+        m->loss.alloc(1);
+        ck(cudaStreamSynchronize(m->st), "sync");
+        *out = m.release();
+    });
+}
+
+int rbmnqs_mlp_n_params(const rbmnqs_mlp* m, int64_t* n) {
+    return guard([&] {
+        require(m && n, "null argument");
+        const auto& d = m->net->dims();
+        *n = (int64_t)d.h1 * d.n_in + d.h1 + (int64_t)d.h2 * d.h1 + d.h2 + (int64_t)d.n_out * d.h2 + d.n_out;
+    });
+}
+
+int rbmnqs_mlp_set_params(rbmnqs_mlp* m, const float* params) {
+    return guard([&] {
+        require(m && params, "null argument");
+        ck(m->net->set_params(params), "set params");
+        mlp_check(m);
+    });
+}
+
+int rbmnqs_mlp_get_params(rbmnqs_mlp* m, float* params) {
+    return guard([&] {
+        require(m && params, "null argument");
+        ck(m->net->get_params(params), "get params");
+    });
+}
+
+int rbmnqs_mlp_init(rbmnqs_mlp* m, float std, uint64_t seed) {
+    return guard([&] {
+        require(m != nullptr, "null argument");
+        ck(m->net->init_random(std, seed), "init");
+        mlp_check(m);
+    });
+}
+
+int rbmnqs_mlp_forward(rbmnqs_mlp* m, const uint32_t* spins, int32_t B, float* logits) {
+    return guard([&] {
+        require(m && spins, "null argument");
+        mlp_upload(m, spins, nullptr, B);
+        ck(m->net->forward(m->spins.p, B, m->st), "forward");
+        if (logits) {
+            const auto& d = m->net->dims();
+            std::vector<float> t((size_t)B * d.out_p);
+            ck(cudaMemcpyAsync(t.data(), m->net->logits(), t.size() * 4, cudaMemcpyDeviceToHost, m->st), "copy");
+            mlp_check(m);
+            for (int b = 0; b < B; b++)
+                for (int o = 0; o < d.n_out; o++) logits[(size_t)b * d.n_out + o] = t[(size_t)b * d.out_p + o];
+        } else {
+            mlp_check(m);
+        }
+    });
+}
+
+int rbmnqs_mlp_train_step(rbmnqs_mlp* m, const uint32_t* spins, const uint32_t* targets, int32_t B, float lr,
+                          int32_t apply, float* loss, float* grads) {
+    return guard([&] {
+        require(m && spins && targets, "null argument");
+        mlp_upload(m, spins, targets, B);
+        ck(m->net->train_step(m->spins.p, m->targets.p, B, lr, m->st, m->loss.p, apply != 0), "train step");
+        float l = 0;
+        ck(cudaMemcpyAsync(&l, m->loss.p, 4, cudaMemcpyDeviceToHost, m->st), "copy");
+        std::vector<float> g;
+        if (grads) {
+            g.resize(m->net->n_params());
+            ck(cudaMemcpyAsync(g.data(), m->net->grads(), g.size() * 4, cudaMemcpyDeviceToHost, m->st), "copy");
+        }
+        mlp_check(m);
+        if (loss) *loss = l;
+        if (grads) {
+            // padded -> logical layout
+            const auto& d = m->net->dims();
+            const int rows[3] = {d.h1, d.h2, d.n_out}, cols[3] = {d.n_in, d.h1, d.h2};
+            const int prow[3] = {d.h1, d.h2, d.out_p}, pcol[3] = {d.in_p, d.h1, d.h2};
+            size_t src = 0, dst = 0;
+            for (int l2 = 0; l2 < 3; l2++) {
+                for (int r = 0; r < rows[l2]; r++)
+                    for (int c = 0; c < cols[l2]; c++) grads[dst++] = g[src + (size_t)r * pcol[l2] + c];
+                src += (size_t)prow[l2] * pcol[l2];
+                for (int r = 0; r < rows[l2]; r++) grads[dst++] = g[src + r];
+                src += prow[l2];
+            }
+        }
+    });
+}
+
+int rbmnqs_mlp_intermediate(rbmnqs_mlp* m, int32_t which, int32_t B, float* out, int32_t* cols) {
+    return guard([&] {
+        require(m != nullptr && B >= 1 && B <= m->net->max_batch(), "bad arguments");
+        int c = 0;
+        ck(m->net->intermediate(which, B, out, &c), "intermediate");
+        if (cols) *cols = c;
+    });
+}
+
+void rbmnqs_mlp_destroy(rbmnqs_mlp* m) { delete m; }
 
 }  // extern "C"

@@ -66,6 +66,7 @@ P_D = C.POINTER(C.c_double)
 P_I = C.POINTER(C.c_int32)
 P_U32 = C.POINTER(C.c_uint32)
 P_I64 = C.POINTER(C.c_int64)
+P_F = C.POINTER(C.c_float)
 VP = C.c_void_p
 
 
@@ -107,11 +108,21 @@ def _declare(L):
         "rbmnqs_batch_epoch": [VP, VP, VP],
         "rbmnqs_batch_graph_kernels": [VP, P_I],
         "rbmnqs_batch_destroy": [VP],
+        "rbmnqs_mlp_create": [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(VP)],
+        "rbmnqs_mlp_n_params": [VP, C.POINTER(C.c_int64)],
+        "rbmnqs_mlp_set_params": [VP, P_F],
+        "rbmnqs_mlp_get_params": [VP, P_F],
+        "rbmnqs_mlp_init": [VP, C.c_float, C.c_uint64],
+        "rbmnqs_mlp_forward": [VP, P_U32, C.c_int32, P_F],
+        "rbmnqs_mlp_train_step": [VP, P_U32, P_U32, C.c_int32, C.c_float, C.c_int32, P_F, P_F],
+        "rbmnqs_mlp_intermediate": [VP, C.c_int32, C.c_int32, P_F, P_I],
+        "rbmnqs_mlp_destroy": [VP],
     }
     for name, args in sig.items():
         f = getattr(L, name)
         f.argtypes = args
-        f.restype = None if name in ("rbmnqs_model_destroy", "rbmnqs_destroy", "rbmnqs_batch_destroy") else C.c_int
+        f.restype = None if name in ("rbmnqs_model_destroy", "rbmnqs_destroy", "rbmnqs_batch_destroy",
+                                     "rbmnqs_mlp_destroy") else C.c_int
     L.rbmnqs_sr_solve_noalloc.argtypes = [VP, C.c_int32, C.c_int32, C.c_int32, VP, C.c_double, VP, VP, C.c_double,
                                           C.c_double, C.c_double, VP, C.c_int32, C.c_double, VP, P_I, P_D]
     L.rbmnqs_sr_solve_noalloc.restype = C.c_int
@@ -423,3 +434,73 @@ class Batch:
         if getattr(self, "_h", None) and _LIB is not None:
             _LIB.rbmnqs_batch_destroy(self._h)
             self._h = None
+
+
+class ProposalNet:
+    """The proposal network on the GPU (rbmnqs_mlp_*): BF16 weights and
+    activations, FP32 accumulation, tcgen05 forward and backward, Adam."""
+
+    def __init__(self, n_in=128, h1=256, h2=256, n_out=128, max_batch=16384):
+        h = VP()
+        _ck(lib().rbmnqs_mlp_create(n_in, h1, h2, n_out, max_batch, C.byref(h)))
+        self._h = h
+        self.dims = (n_in, h1, h2, n_out)
+        n = C.c_int64()
+        _ck(lib().rbmnqs_mlp_n_params(self._h, C.byref(n)))
+        self.n_params = n.value
+
+    def init(self, std=0.02, seed=0):
+        _ck(lib().rbmnqs_mlp_init(self._h, std, seed))
+
+    def set_params(self, flat):
+        a = np.ascontiguousarray(flat, dtype=np.float32)
+        assert a.size == self.n_params
+        _ck(lib().rbmnqs_mlp_set_params(self._h, _p(a, P_F)))
+
+    def get_params(self):
+        a = np.zeros(self.n_params, np.float32)
+        _ck(lib().rbmnqs_mlp_get_params(self._h, _p(a, P_F)))
+        return a
+
+    def forward(self, spins):
+        s = np.ascontiguousarray(spins, dtype=np.uint32)
+        out = np.zeros((s.shape[0], self.dims[3]), np.float32)
+        _ck(lib().rbmnqs_mlp_forward(self._h, _p(s, P_U32), s.shape[0], _p(out, P_F)))
+        return out
+
+    def train_step(self, spins, targets, lr=1e-3, apply=True, grads=True):
+        s = np.ascontiguousarray(spins, dtype=np.uint32)
+        t = np.ascontiguousarray(targets, dtype=np.uint32)
+        loss = C.c_float()
+        g = np.zeros(self.n_params, np.float32) if grads else None
+        _ck(lib().rbmnqs_mlp_train_step(self._h, _p(s, P_U32), _p(t, P_U32), s.shape[0], lr, 1 if apply else 0,
+                                        C.byref(loss), _p(g, P_F)))
+        return loss.value, g
+
+    def intermediate(self, which, B):
+        c = C.c_int32()
+        _ck(lib().rbmnqs_mlp_intermediate(self._h, which, B, None, C.byref(c)))
+        out = np.zeros((B, c.value), np.float32)
+        _ck(lib().rbmnqs_mlp_intermediate(self._h, which, B, _p(out, P_F), C.byref(c)))
+        return out
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.rbmnqs_mlp_destroy(self._h)
+            self._h = None
+
+
+def mlp_unflatten(flat, dims):
+    """flat [W1, b1, W2, b2, W3, b3] -> dict of float64 arrays (oracle layout)."""
+    p, o = {}, 0
+    for l in range(3):
+        r, c = dims[l + 1], dims[l]
+        p[f"W{l + 1}"] = np.asarray(flat[o:o + r * c], np.float64).reshape(r, c)
+        o += r * c
+        p[f"b{l + 1}"] = np.asarray(flat[o:o + r], np.float64)
+        o += r
+    return p
+
+
+def mlp_flatten(p):
+    return np.concatenate([np.ravel(p[k]) for k in ("W1", "b1", "W2", "b2", "W3", "b3")]).astype(np.float32)
