@@ -107,6 +107,18 @@ typedef struct {
     int32_t gram;              /* S build: 0 = by precision (TF32x3 tensor
                                   cores when precision is 0, FP64 when 1);
                                   1 = FP64 CUDA cores in either precision */
+    /* Learned proposals (no reference counterpart): 0 = plain Metropolis;
+     * 1 = after every `step` sweeps, learned_steps multi-spin moves drawn
+     * from the proposal network (independent site flips with network
+     * probabilities) and accepted by the exact Metropolis-Hastings ratio
+     * |psi'/psi|^2 q(s|s')/q(s'|s); samples are recorded after them.  The
+     * network is trained every epoch (learned_train Adam steps, learned_lr)
+     * on pairs of the epoch's samples.  Not with the Pfaffian factor. */
+    int32_t proposal;
+    int32_t learned_steps;
+    int32_t learned_train;
+    int32_t learned_hidden;    /* width of both hidden layers (64..256) */
+    double learned_lr;
 } rbmnqs_config;
 
 /* Fills the reference defaults (src/tools/ini.cpp:38-120). */
@@ -136,6 +148,8 @@ typedef struct {
     int64_t n_samples;
     int32_t n_bins;
     int32_t status;       /* RBMNQS_OK or RBMNQS_ERR_NONFINITE */
+    double learned_acceptance; /* acceptance of the learned moves (0 without) */
+    double learned_loss;       /* proposal-network training loss of the epoch */
 } rbmnqs_sample_stats;
 
 /* One Metropolis epoch: sweeps, E_loc, O_k, and the reductions the

@@ -144,6 +144,11 @@ struct rbmnqs_handle {
     rbmnqs::MfreePlan mfp{};
     rbmnqs::MfreeWork mfw{};
     DevBuf<unsigned char> mfbuf;
+    // learned proposals: network, proposed configurations, masks, counters
+    std::unique_ptr<rbmnqs::Mlp> net;
+    DevBuf<uint32_t> lprop, lmask, lacc, ltry, ltgt;
+    DevBuf<float> lqfw, lloss;
+    DevBuf<double> lrate;
     // Pfaffian factor: class matrix, derivative pairs, unscramble buffers
     int pf_n = 0, pf_indep = 0;
     DevBuf<int16_t> pf_bs;
@@ -254,10 +259,64 @@ struct rbmnqs_handle {
         ea.plan = rbmnqs::SmemPlan{0, w_in_smem, 0, 0, 0};
         return ea;
     }
+    rbmnqs::LearnedArgs learned_args() const {
+        rbmnqs::LearnedArgs l{};
+        l.m = machine();
+        l.n_chains = cfg.n_chains;
+        l.spins = spins.p;
+        l.prop = lprop.p;
+        l.mask = lmask.p;
+        l.qfw = lqfw.p;
+        l.logits = net->logits();
+        l.ldl = net->dims().out_p;
+        l.ctl = ctl.p;
+        l.seed = cfg.seed ^ 0x5DEECE66DULL;
+        l.n_acc = lacc.p;
+        l.n_try = ltry.p;
+        l.pmin = 1e-3f;
+        return l;
+    }
+    // sweeps in segments, learned moves between them, samples recorded after them
+    void enqueue_learned_sampling() {
+        rbmnqs::SamplerArgs a = sampler_args();
+        a.record = 0;
+        ck(cudaMemsetAsync(lacc.p, 0, lacc.n * sizeof(uint32_t), st), "memset");
+        ck(cudaMemsetAsync(ltry.p, 0, ltry.n * sizeof(uint32_t), st), "memset");
+        if (cfg.warmup > 0) {
+            a.sweep0 = 0;
+            a.nsweeps = cfg.warmup;
+            ck(rbmnqs::launch_sampler(a, fp64, shape, st), "sampler kernel");
+        }
+        rbmnqs::LearnedArgs l = learned_args();
+        for (int j = 0; j < cfg.samples_per_chain; j++) {
+            a.sweep0 = cfg.warmup + j * cfg.step;
+            a.nsweeps = cfg.step;
+            ck(rbmnqs::launch_sampler(a, fp64, shape, st), "sampler kernel");
+            for (int k = 0; k < cfg.learned_steps; k++) {
+                l.move = (uint32_t)(j * cfg.learned_steps + k);
+                ck(net->forward(spins.p, cfg.n_chains, st), "proposal network");
+                ck(rbmnqs::launch_learned_propose(l, st), "learned propose");
+                ck(net->forward(lprop.p, cfg.n_chains, st), "proposal network");
+                ck(rbmnqs::launch_learned_accept(l, st), "learned accept");
+            }
+            ck(rbmnqs::launch_record(spins.p, cfg.n_chains, cfg.samples_per_chain, j, samples.p, st), "record");
+        }
+        ck(rbmnqs::launch_learned_rate(lacc.p, ltry.p, cfg.n_chains, lrate.p, st), "learned rate");
+    }
+    // the network learns the flip pattern between independent samples of the epoch
+    void enqueue_learned_training() {
+        ck(rbmnqs::launch_pair_targets(samples.p, N, ltgt.p, st), "pair targets");
+        const int B = std::min(N, net->max_batch());
+        for (int t = 0; t < cfg.learned_train; t++)
+            ck(net->train_step(samples.p, ltgt.p, B, (float)cfg.learned_lr, st, lloss.p, true), "proposal training");
+    }
     void enqueue_sample() {
         const rbmnqs::SamplerArgs a = sampler_args();
         mark(0);
-        ck(rbmnqs::launch_sampler(a, fp64, shape, st), "sampler kernel");
+        if (net)
+            enqueue_learned_sampling();
+        else
+            ck(rbmnqs::launch_sampler(a, fp64, shape, st), "sampler kernel");
         mark(1);
         // E_loc and O_k of every sample (local_op::evaluate, derivative)
         ck(rbmnqs::launch_eval(eval_args(), fp64, wpb, st), "eval kernel");
@@ -266,6 +325,7 @@ struct rbmnqs_handle {
            "moments");
         ck(rbmnqs::launch_energy_stats(E.p, N, n_bins, emean.p, nacc.p, nprop.p, cfg.n_chains, stats.p, st),
            "energy stats");
+        if (net) enqueue_learned_training();
         ck(rbmnqs::launch_advance(ctl.p, cfg.reinit_chains, st), "advance");
         mark(3);
     }
@@ -449,6 +509,11 @@ int rbmnqs_config_default(rbmnqs_config* c) {
         c->precision = 0;
         c->n_updates = 0;
         c->gram = 0;
+        c->proposal = 0;
+        c->learned_steps = 1;
+        c->learned_train = 1;
+        c->learned_hidden = 256;
+        c->learned_lr = 1e-3;
     });
 }
 
@@ -462,6 +527,12 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         require(!cfg->pfaffian || mdl->m.n <= rbmnqs::kPfMaxSites,
                 "the Pfaffian factor supports at most 32 sites", RBMNQS_ERR_UNSUPPORTED);
         require(cfg->pfaffian_refresh >= 0, "sampler.pfaffian_refresh must be >= 0");
+        require(cfg->proposal == 0 || cfg->proposal == 1, "proposal must be 0 (plain) or 1 (learned)");
+        require(cfg->proposal == 0 || (!cfg->pfaffian && mdl->m.n <= 256 && cfg->learned_steps >= 0 &&
+                                       cfg->learned_train >= 0 && cfg->learned_hidden % 64 == 0 &&
+                                       cfg->learned_hidden >= 64 && cfg->learned_hidden <= 256),
+                "learned proposals: no Pfaffian factor, <= 256 sites, hidden width 64..256 (multiple of 64)",
+                RBMNQS_ERR_UNSUPPORTED);
         require(cfg->alpha >= 1 && cfg->n_chains >= 1 && cfg->samples_per_chain >= 1 && cfg->step >= 1 &&
                     cfg->warmup >= 0,
                 "bad sampler/machine sizes");
@@ -651,6 +722,27 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         // launch shapes: persistent sampler blocks; evaluation kernels with
         // FP32 W in shared memory when it fits
         ck(rbmnqs::plan_sampler(h->machine(), h->fp64, cfg->n_chains, h->n_prop_bonds, &h->shape), "sampler plan");
+        if (cfg->proposal == 1) {
+            rbmnqs::MlpDims md;
+            md.n_in = md.n_out = n;
+            md.h1 = md.h2 = cfg->learned_hidden;
+            try {
+                h->net = std::make_unique<rbmnqs::Mlp>(md, std::max(cfg->n_chains, h->N), h->st);
+            } catch (cudaError_t e) {
+                ck(e, "proposal network");
+            }
+            ck(h->net->init_random(0.02f, cfg->seed), "proposal network init");
+            h->lprop.alloc((size_t)cfg->n_chains * 4);
+            h->lmask.alloc((size_t)cfg->n_chains * 4);
+            h->lqfw.alloc((size_t)cfg->n_chains * 4);
+            h->lacc.alloc(cfg->n_chains);
+            h->ltry.alloc(cfg->n_chains);
+            h->ltgt.alloc((size_t)h->N * 4);
+            h->lloss.alloc(1);
+            h->lrate.alloc(1);
+            ck(cudaMemsetAsync(h->lloss.p, 0, sizeof(float), h->st), "memset");
+            ck(cudaMemsetAsync(h->lrate.p, 0, sizeof(double), h->st), "memset");
+        }
         if (h->pf_n)  // one X^{-1} unscramble buffer per sampler warp
             h->pf_scratch.alloc((size_t)h->shape.blocks * h->shape.warps_per_block * rbmnqs::kPfMaxSites *
                                 rbmnqs::kPfMaxSites);
@@ -730,6 +822,17 @@ static void read_sample_stats(rbmnqs_handle* h, rbmnqs_sample_stats* out) {
         out->n_samples = h->N;
         out->n_bins = h->n_bins;
         out->status = s.finite ? RBMNQS_OK : RBMNQS_ERR_NONFINITE;
+        out->learned_acceptance = 0;
+        out->learned_loss = 0;
+        if (h->net) {
+            double r = 0;
+            float l = 0;
+            ck(cudaMemcpyAsync(&r, h->lrate.p, sizeof(r), cudaMemcpyDeviceToHost, h->st), "copy");
+            ck(cudaMemcpyAsync(&l, h->lloss.p, sizeof(l), cudaMemcpyDeviceToHost, h->st), "copy");
+            ck(cudaStreamSynchronize(h->st), "sync");
+            out->learned_acceptance = r;
+            out->learned_loss = l;
+        }
     }
 }
 

@@ -13,6 +13,7 @@
 // configuration after every sweep (mixed-precision scheme), so FP32
 // drift never outlives one sweep.  With the Pfaffian factor (sites <= 32) each
 // lane also holds its row of X^{-1} in FP64 registers (pfaffian.cuh).
+#include <algorithm>
 #include <map>
 #include <mutex>
 
@@ -418,7 +419,7 @@ __device__ inline void load_tables(const MachineDev& m, const Smem& s, int fp64,
 // else the persisted configuration.
 __device__ __forceinline__ void chain_start(const SamplerArgs& a, int chain, uint2 key, uint32_t epoch, uint32_t sp[4]) {
     const int n = a.m.n;
-    if (a.ctl[1]) {
+    if (a.ctl[1] && a.sweep0 == 0) {
         const uint4 r = philox4x32(make_uint4(0, epoch, (uint32_t)chain, 1), key);
         const uint32_t rw[4] = {r.x, r.y, r.z, r.w};
 #pragma unroll
@@ -433,12 +434,29 @@ __device__ __forceinline__ void chain_start(const SamplerArgs& a, int chain, uin
     }
 }
 
+// Proposal counter at the start of a segment: 32-aligned (proposals are
+// drawn 32 at a time) and past every proposal of earlier segments (a sweep
+// makes at most n proposals).
+__device__ __forceinline__ uint32_t prop_base(const SamplerArgs& a) {
+    return (uint32_t)a.sweep0 * (uint32_t)(32 * ((a.m.n + 31) / 32));
+}
+__device__ __forceinline__ int segment_sweeps(const SamplerArgs& a) {
+    return a.nsweeps ? a.nsweeps : a.spc * a.step + a.warmup;
+}
+// sample slot of global sweep sg, or -1
+__device__ __forceinline__ int sample_slot(const SamplerArgs& a, int st) {
+    const int sg = a.sweep0 + st;
+    if (!a.record || sg < a.warmup || (sg - a.warmup) % a.step) return -1;
+    return (sg - a.warmup) / a.step;
+}
+
 __device__ __forceinline__ void chain_finish(const SamplerArgs& a, int chain, int lane, const uint32_t sp[4],
                                              uint32_t nacc, uint32_t prop) {
     if (lane < 4) a.spins[4 * chain + lane] = sp[lane];
     if (lane == 0) {
-        a.n_acc[chain] = nacc;
-        a.n_prop[chain] = prop;
+        const uint32_t made = prop - prop_base(a);
+        a.n_acc[chain] = (a.sweep0 ? a.n_acc[chain] : 0u) + nacc;
+        a.n_prop[chain] = (a.sweep0 ? a.n_prop[chain] : 0u) + made;
     }
 }
 
@@ -491,9 +509,8 @@ __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, 
     const int n = m.n;
     // warm-up sweeps run every epoch, as in the reference; persistent chains
     // only differ in starting from the previous epoch's configuration
-    const int warmup = a.warmup;
-    const int total = a.spc * a.step + warmup;
-    uint32_t prop = 0, nacc = 0;
+    const int total = segment_sweeps(a);
+    uint32_t prop = prop_base(a), nacc = 0;
     uint32_t rr0 = 0, rr1 = 0, rr2 = 0;
     const uint32_t thr = a.bond_thr24;  // bond proposal iff (r0 >> 8) < thr
     for (int st = 0; st < total; st++) {
@@ -587,8 +604,7 @@ __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, 
         theta_fp64<E, R>(m, W64, sm.perm, lane, sp, th);
 #pragma unroll
         for (int e = 0; e < E; e++) L[e] = slot_valid(lane, e, m.T) ? lnc_re<R>(th[e].x, th[e].y) : (R)0;
-        if (st >= warmup && (st - warmup) % a.step == 0) {
-            const int j = (st - warmup) / a.step;
+        if (const int j = sample_slot(a, st); j >= 0) {
             const size_t idx = (size_t)chain * a.spc + j;
             if (lane < 4) a.samples[4 * idx + lane] = sp[lane];
         }
@@ -660,10 +676,9 @@ __device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem&
     recompute();
 
     const int2* bonds = sm.bonds ? sm.bonds : a.prop_bonds;
-    const int warmup = a.warmup;
-    const int total = a.spc * a.step + warmup;
+    const int total = segment_sweeps(a);
     const uint32_t thr = a.bond_thr24;
-    uint32_t prop = 0, nacc = 0, pcode = 0;
+    uint32_t prop = prop_base(a), nacc = 0, pcode = 0;
     float plu = 0.f;
     for (int st = 0; st < total; st++) {
         int slot = 0;
@@ -715,8 +730,7 @@ __device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem&
             }
         }
         recompute();  // FP64 recompute of theta once per sweep
-        if (st >= warmup && (st - warmup) % a.step == 0) {
-            const int j = (st - warmup) / a.step;
+        if (const int j = sample_slot(a, st); j >= 0) {
             const size_t idx = (size_t)chain * a.spc + j;
             if (lane < 4) a.samples[4 * idx + lane] = sp[lane];
         }
@@ -794,10 +808,9 @@ __device__ __forceinline__ void run_chain_gather(const SamplerArgs& a, const Sme
     recompute();
 
     const int2* bonds = sm.bonds ? sm.bonds : a.prop_bonds;
-    const int warmup = a.warmup;
-    const int total = a.spc * a.step + warmup;
+    const int total = segment_sweeps(a);
     const uint32_t thr = a.bond_thr24;
-    uint32_t prop = 0, nacc = 0, pcode = 0;
+    uint32_t prop = prop_base(a), nacc = 0, pcode = 0;
     float plu = 0.f;
     for (int st = 0; st < total; st++) {
         int slot = 0;
@@ -848,8 +861,7 @@ __device__ __forceinline__ void run_chain_gather(const SamplerArgs& a, const Sme
             }
         }
         recompute();  // FP64 recompute of theta once per sweep
-        if (st >= warmup && (st - warmup) % a.step == 0) {
-            const int j = (st - warmup) / a.step;
+        if (const int j = sample_slot(a, st); j >= 0) {
             const size_t idx = (size_t)chain * a.spc + j;
             if (lane < 4) a.samples[4 * idx + lane] = sp[lane];
         }
@@ -1004,6 +1016,173 @@ __global__ void __launch_bounds__(256) eval_kernel(const EvalArgs a) {
         if constexpr (PF)
             if (Orow) pf_derivative(m.pf, sp[0], lane, pA, Orow + m.P_neural);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Learned proposals (learned-proposal extension; no reference counterpart).
+// Random streams: Philox counter {(move << 5) | (word << 3) | group, epoch,
+// chain, 3} for the flip draws and {move, epoch, chain, 4} for the
+// acceptance draw, disjoint from the sweep streams 0 and 1.
+__device__ __forceinline__ float clamp_prob(float logit, float pmin) {
+    const float p = 1.f / (1.f + __expf(-logit));
+    return fminf(fmaxf(p, pmin), 1.f - pmin);
+}
+
+__global__ void learned_propose(const LearnedArgs a) {
+    const int total = a.n_chains * 4, n = a.m.n;
+    const uint2 key = make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32));
+    const uint32_t epoch = a.ctl[0];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        const int c = t >> 2, w = t & 3;
+        uint32_t f = 0;
+        float lq = 0.f;
+        for (int g = 0; g < 8; g++) {
+            const int i0 = 32 * w + 4 * g;
+            if (i0 >= n) break;
+            const uint4 r = philox4x32(make_uint4((a.move << 5) | (uint32_t)(w << 3) | (uint32_t)g, epoch,
+                                                  (uint32_t)c, 3),
+                                       key);
+            const uint32_t rr[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int i = i0 + q;
+                if (i >= n) break;
+                const float p = clamp_prob(a.logits[(size_t)c * a.ldl + i], a.pmin);
+                const bool fl = unit24<float>(rr[q]) < p;
+                lq += __logf(fl ? p : 1.f - p);
+                f |= (fl ? 1u : 0u) << (i & 31);
+            }
+        }
+        a.mask[t] = f;
+        a.prop[t] = a.spins[t] ^ f;
+        a.qfw[t] = lq;
+    }
+}
+
+// Re log psi without the constant: bias + sum ln|cosh theta| - T ln 2
+template <int E>
+__device__ __forceinline__ double log_amp(const MachineDev& m, const uint32_t sp[4], int lane) {
+    C2<double> th[E];
+    theta_fp64<E, double>(m, m.W64, m.perm, lane, sp, th);
+    double acc = 0;
+#pragma unroll
+    for (int e = 0; e < E; e++)
+        if (slot_valid(lane, e, m.T)) acc += lnc_re<double>(th[e].x, th[e].y);
+    // visible bias (rbm_base.cpp:294-296, rbm_symmetry.cpp:138-147)
+    const int nb = m.symmetric ? m.n_vb * m.S : m.n_vb;
+    for (int q = lane; q < nb; q += 32) {
+        const int i = m.symmetric ? q / m.S : q;
+        const int site = m.symmetric ? (int)m.orbit[q] : q;
+        acc += m.vb[i].x * (spin_bit(sp, site) ? -1.0 : 1.0);
+    }
+    return warp_sum(acc);
+}
+
+template <int E>
+__global__ void __launch_bounds__(256) learned_accept(const LearnedArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (c >= a.n_chains) return;
+    const int n = a.m.n;
+    // log q(s|s') from the proposed configuration's logits, same mask
+    float lq = 0.f;
+    for (int i = lane; i < n; i += 32) {
+        const float p = clamp_prob(a.logits[(size_t)c * a.ldl + i], a.pmin);
+        const bool fl = (a.mask[4 * c + (i >> 5)] >> (i & 31)) & 1u;
+        lq += __logf(fl ? p : 1.f - p);
+    }
+    const float qrev = warp_sum(lq);
+    const float qfwd = a.qfw[4 * c] + a.qfw[4 * c + 1] + a.qfw[4 * c + 2] + a.qfw[4 * c + 3];
+    uint32_t s0[4], s1[4];
+#pragma unroll
+    for (int w = 0; w < 4; w++) {
+        s0[w] = a.spins[4 * c + w];
+        s1[w] = a.prop[4 * c + w];
+    }
+    const double d = log_amp<E>(a.m, s1, lane) - log_amp<E>(a.m, s0, lane);
+    const uint2 key = make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32));
+    const uint4 r = philox4x32(make_uint4(a.move, a.ctl[0], (uint32_t)c, 4), key);
+    // accept with min(1, |psi'/psi|^2 q(s|s') / q(s'|s))
+    const double lu = log((double)unit24<double>(r.x));
+    const bool acc = lu < 2.0 * d + (double)qrev - (double)qfwd;
+    if (lane < 4 && acc) a.spins[4 * c + lane] = s1[lane];
+    if (lane == 0) {
+        a.n_acc[c] += acc ? 1u : 0u;
+        a.n_try[c] += 1u;
+    }
+}
+
+__global__ void record_kernel(const uint32_t* spins, int n_chains, int spc, int j, uint32_t* samples) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 4 * n_chains; t += gridDim.x * blockDim.x) {
+        const int c = t >> 2, w = t & 3;
+        samples[4 * ((size_t)c * spc + j) + w] = spins[t];
+    }
+}
+
+__global__ void pair_targets(const uint32_t* samples, int N, uint32_t* targets) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 4 * N; t += gridDim.x * blockDim.x) {
+        const int i = t >> 2, w = t & 3;
+        targets[t] = samples[t] ^ samples[4 * ((i + N / 2) % N) + w];
+    }
+}
+
+__global__ void learned_rate(const uint32_t* n_acc, const uint32_t* n_try, int n, double* out) {
+    __shared__ double ra[32], rt[32];
+    double sa = 0, st = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        sa += n_acc[i];
+        st += n_try[i];
+    }
+    sa = warp_sum(sa);
+    st = warp_sum(st);
+    if ((threadIdx.x & 31) == 0) {
+        ra[threadIdx.x >> 5] = sa;
+        rt[threadIdx.x >> 5] = st;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double A = 0, Tt = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            A += ra[w];
+            Tt += rt[w];
+        }
+        *out = Tt > 0 ? A / Tt : 0.0;
+    }
+}
+
+cudaError_t launch_learned_propose(const LearnedArgs& a, cudaStream_t st) {
+    const int total = 4 * a.n_chains;
+    learned_propose<<<std::min(148 * 8, (total + 255) / 256), 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_learned_accept(const LearnedArgs& a, cudaStream_t st) {
+    const int blocks = (a.n_chains + 7) / 8;
+    switch (elements_per_lane(a.m.T)) {
+        case 1: learned_accept<1><<<blocks, 256, 0, st>>>(a); break;
+        case 2: learned_accept<2><<<blocks, 256, 0, st>>>(a); break;
+        case 4: learned_accept<4><<<blocks, 256, 0, st>>>(a); break;
+        case 8: learned_accept<8><<<blocks, 256, 0, st>>>(a); break;
+        case 16: learned_accept<16><<<blocks, 256, 0, st>>>(a); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_record(const uint32_t* spins, int n_chains, int spc, int j, uint32_t* samples, cudaStream_t st) {
+    record_kernel<<<std::min(148 * 4, (4 * n_chains + 255) / 256), 256, 0, st>>>(spins, n_chains, spc, j, samples);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pair_targets(const uint32_t* samples, int N, uint32_t* targets, cudaStream_t st) {
+    pair_targets<<<std::min(148 * 4, (4 * N + 255) / 256), 256, 0, st>>>(samples, N, targets);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_learned_rate(const uint32_t* n_acc, const uint32_t* n_try, int n_chains, double* out,
+                                cudaStream_t st) {
+    learned_rate<<<1, 1024, 0, st>>>(n_acc, n_try, n_chains, out);
+    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------

@@ -73,6 +73,11 @@ struct SamplerArgs {
     uint32_t* n_acc;  // [n_chains]
     uint32_t* n_prop; // [n_chains]
     SmemPlan plan;
+    // a launch may run a segment of the epoch's sweeps (learned proposals
+    // run between segments): sweeps [sweep0, sweep0 + nsweeps) (nsweeps 0 =
+    // all), recording samples only when record != 0; chains start fresh only
+    // in the segment at sweep 0, and the counters accumulate over segments
+    int sweep0 = 0, nsweeps = 0, record = 1;
 };
 
 struct EvalArgs {
@@ -90,6 +95,38 @@ struct EvalArgs {
     double2* ratio;         // ratio mode output (log psi'/psi)
     SmemPlan plan;
 };
+
+// Learned-proposal move for every chain: propose draws the flip mask
+// (independent sites, probability clamp(sigmoid(logit), pmin, 1 - pmin)) from
+// the network's logits of the current configurations and records log
+// q(s'|s); accept takes the logits of the proposed configurations, forms
+// log q(s|s') and log|psi(s')/psi(s)| (FP64 theta of both) and applies the
+// Metropolis-Hastings test.
+struct LearnedArgs {
+    MachineDev m;
+    int n_chains;
+    uint32_t* spins;        // [n_chains][4] current configurations
+    uint32_t* prop;         // [n_chains][4] proposed configurations
+    uint32_t* mask;         // [n_chains][4] flip masks
+    float* qfw;             // [n_chains][4] log q(s'|s) per 32-site word
+    const float* logits;    // [n_chains][ldl] network output
+    int ldl;
+    const uint32_t* ctl;    // {epoch, init}
+    uint64_t seed;
+    uint32_t move;          // move index within the epoch (Philox counter)
+    uint32_t* n_acc;        // [n_chains] accepted learned moves (epoch)
+    uint32_t* n_try;        // [n_chains] learned moves tried (epoch)
+    float pmin;
+};
+cudaError_t launch_learned_propose(const LearnedArgs& a, cudaStream_t st);
+cudaError_t launch_learned_accept(const LearnedArgs& a, cudaStream_t st);
+// samples[c * spc + j] = spins[c]
+cudaError_t launch_record(const uint32_t* spins, int n_chains, int spc, int j, uint32_t* samples, cudaStream_t st);
+// targets[i] = samples[i] ^ samples[(i + N / 2) % N] (pairs of independent samples)
+cudaError_t launch_pair_targets(const uint32_t* samples, int N, uint32_t* targets, cudaStream_t st);
+// acceptance of the learned moves -> *out (device)
+cudaError_t launch_learned_rate(const uint32_t* n_acc, const uint32_t* n_try, int n_chains, double* out,
+                                cudaStream_t st);
 
 // Launch helpers implemented in sampler.cu
 int sampler_smem_bytes(const MachineDev& m, int fp64, int warps, const SmemPlan& plan, int n_bonds);

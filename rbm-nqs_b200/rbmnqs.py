@@ -39,18 +39,22 @@ class Config(C.Structure):
         ("lr", C.c_double * 3), ("reg1", C.c_double * 3), ("reg2", C.c_double * 3),
         ("deltareg1", C.c_double * 3), ("max_iterations", C.c_int32), ("rtol", C.c_double),
         ("precision", C.c_int32), ("n_updates", C.c_int32), ("gram", C.c_int32),
+        ("proposal", C.c_int32), ("learned_steps", C.c_int32), ("learned_train", C.c_int32),
+        ("learned_hidden", C.c_int32), ("learned_lr", C.c_double),
     ]
 
 
 class SampleStats(C.Structure):
     _fields_ = [("energy", C.c_double * 2), ("energy_var", C.c_double), ("energy_stddev", C.c_double),
                 ("tau", C.c_double), ("acceptance", C.c_double), ("n_samples", C.c_int64),
-                ("n_bins", C.c_int32), ("status", C.c_int32)]
+                ("n_bins", C.c_int32), ("status", C.c_int32), ("learned_acceptance", C.c_double),
+                ("learned_loss", C.c_double)]
 
     def as_dict(self):
         return dict(energy=complex(self.energy[0], self.energy[1]), var=self.energy_var,
                     stddev=self.energy_stddev, tau=self.tau, acceptance=self.acceptance,
-                    n_samples=self.n_samples, n_bins=self.n_bins, status=self.status)
+                    n_samples=self.n_samples, n_bins=self.n_bins, status=self.status,
+                    learned_acceptance=self.learned_acceptance, learned_loss=self.learned_loss)
 
 
 class SrStats(C.Structure):
