@@ -56,6 +56,17 @@ WORKLOADS = {
     "kitaev128_symm_a4": dict(model="kitaev", n_cells=8, rbm_type=1, alpha=4, symmetry=0.5, n_chains=16384,
                               samples_per_chain=1, warmup=63, step=1, bond_flips=0.5, std=1e-4,
                               reg2=(1e-4, 1e-4, 1.0), precision=0, gram=0),
+    # the 128-spin lattice as a time series (persistent chains, 16 samples per
+    # chain, 4 sweeps apart) for tau_int of E_loc: plain single-spin / bond
+    # Metropolis against the learned multi-spin proposals at 1 sweep + 1
+    # learned move per sample (network trained on the chains' own samples)
+    "kitaev128_plain_ts": dict(model="kitaev", n_cells=8, rbm_type=1, alpha=4, symmetry=0.5, n_chains=16384,
+                               samples_per_chain=16, warmup=0, step=4, bond_flips=0.5, std=1e-4,
+                               reg2=(1e-4, 1e-4, 1.0), precision=0, gram=0),
+    "kitaev128_learned_ts": dict(model="kitaev", n_cells=8, rbm_type=1, alpha=4, symmetry=0.5, n_chains=16384,
+                                 samples_per_chain=16, warmup=0, step=1, bond_flips=0.5, std=1e-4,
+                                 reg2=(1e-4, 1e-4, 1.0), precision=0, gram=0, proposal=1, learned_steps=1,
+                                 learned_train=2, learned_lr=1e-3),
     # 48 independent toric-code trainings (L = 3..8, 8 each, basic RBM
     # alpha=2, 1024 chains each) advanced by one CUDA-graph launch per epoch;
     # launch shapes autotuned per L; matrix-free CG capped at 100 iterations
@@ -128,6 +139,9 @@ def describe(wl, P):
          "sr": "CG reg2=1e-4 reg1=(1,1e-4,0.9) lr=1e-2"}
     if wl.get("pfaffian"):
         d["pfaffian_refresh"] = wl["pf_refresh"]
+    if wl.get("proposal"):
+        d["proposal"] = "learned (MLP %d-256-256-%d, BF16), %d move(s) per sample, %d Adam step(s) per epoch" % (
+            2 * wl["n_cells"] ** 2, 2 * wl["n_cells"] ** 2, wl["learned_steps"], wl["learned_train"])
     return d
 
 
@@ -195,7 +209,9 @@ def run_ours(args, rank, world, local):
                                 bond_flips=wl["bond_flips"], seed=1234 + rank, precision=wl["precision"],
                                 gram=wl["gram"], reinit_chains=0, reg2=wl["reg2"],
                                 pfaffian=wl.get("pfaffian", 0), pfaffian_symmetry=wl.get("pf_symmetry", 0.5),
-                                pfaffian_refresh=wl.get("pf_refresh", 0))
+                                pfaffian_refresh=wl.get("pf_refresh", 0), proposal=wl.get("proposal", 0),
+                                learned_steps=wl.get("learned_steps", 1), learned_train=wl.get("learned_train", 1),
+                                learned_lr=wl.get("learned_lr", 1e-3))
     sess = rbmnqs.Session(model, cfg)
     P, N = sess.n_params, sess.N
     w0 = make_weights(P, wl["std"], 99 + rank, sess.n_neural, wl.get("pf_std"))
@@ -217,7 +233,7 @@ def run_ours(args, rank, world, local):
     # ---- device-timed region: K epochs, each bracketed by events on the
     # library's stream, L2 flushed between epochs (outside the events)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    taus, energies, accs, its = [], [], [], []
+    taus, energies, accs, its, errs, laccs = [], [], [], [], [], []
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -230,6 +246,9 @@ def run_ours(args, rank, world, local):
             taus.append(st["tau"])
             energies.append(st["energy"].real)
             accs.append(st["acceptance"])
+            errs.append(st["stddev"])
+            if wl.get("proposal"):
+                laccs.append(st["learned_acceptance"])
             its.append(sr["iterations"])
         torch.cuda.synchronize()
     if world > 1:
@@ -286,6 +305,8 @@ def run_ours(args, rank, world, local):
                            l2="256 MiB L2 flush between timed epochs (outside the event pairs)"),
             "sr_epochs_per_s": world * args.steps / (t_ms * 1e-3),
             "tau": tau, "energy_per_site": float(np.mean(energies)) / model.n, "acceptance": acc,
+            "energy_per_site_stderr": float(np.sqrt(np.mean(np.square(errs))) / np.sqrt(len(errs))) / model.n,
+            "learned_acceptance": float(np.mean(laccs)) if laccs else None,
             "cg_iterations": float(np.mean(its)),
             "stage_ms_per_epoch": {nm: stage_ms[i] / max(1, stage_cnt[i]) for i, nm in
                                    enumerate(["sampler", "eval", "moments+stats", "gram+regularise", "cg",

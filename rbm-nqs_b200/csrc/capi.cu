@@ -303,12 +303,13 @@ struct rbmnqs_handle {
         }
         ck(rbmnqs::launch_learned_rate(lacc.p, ltry.p, cfg.n_chains, lrate.p, st), "learned rate");
     }
-    // the network learns the flip pattern between independent samples of the epoch
+    // the network learns the flip pattern between independent configurations:
+    // the chains' final states, chain c paired with chain c + n_chains / 2
     void enqueue_learned_training() {
-        ck(rbmnqs::launch_pair_targets(samples.p, N, ltgt.p, st), "pair targets");
-        const int B = std::min(N, net->max_batch());
+        ck(rbmnqs::launch_pair_targets(spins.p, cfg.n_chains, ltgt.p, st), "pair targets");
         for (int t = 0; t < cfg.learned_train; t++)
-            ck(net->train_step(samples.p, ltgt.p, B, (float)cfg.learned_lr, st, lloss.p, true), "proposal training");
+            ck(net->train_step(spins.p, ltgt.p, cfg.n_chains, (float)cfg.learned_lr, st, lloss.p, true),
+               "proposal training");
     }
     void enqueue_sample() {
         const rbmnqs::SamplerArgs a = sampler_args();

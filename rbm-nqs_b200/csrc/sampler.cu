@@ -108,10 +108,22 @@ __device__ __forceinline__ double2 bias_delta_smem(const MachineDev& m, const ui
 // (wth) and the per-entry ln cosh cache (cre, cu) of the current theta, all
 // in the warp's shared scratch.  Returns the real log-magnitude sum (without
 // bias) and the phase product.
+// Entry e of this lane is theta[k + nh s] with t = lane + 32 e; the pair
+// (k, s) is packed as (s << 16) | k once per sample (no division per term).
+template <int E>
+__device__ __forceinline__ void entry_index(const MachineDev& m, int lane, uint32_t (&ks)[E]) {
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+        const int t = lane + 32 * e;
+        ks[e] = t < m.T ? ((uint32_t)(t / m.nh) << 16) | (uint32_t)(t % m.nh) : 0u;
+    }
+}
+
 template <int E, typename R>
 __device__ __forceinline__ void ratio_terms(const MachineDev& m, const uint8_t* sPerm, const C2<R>* W,
                                             const C2<R>* wth, const uint32_t* wsp, const int* fl, int nf,
-                                            const R* cre, const C2<R>* cu, int lane, R& dre, C2<R>& ph) {
+                                            const R* cre, const C2<R>* cu, int lane, R& dre, C2<R>& ph,
+                                            const uint32_t (&ks)[E]) {
     R sgn2[6];
     for (int q = 0; q < nf; q++) sgn2[q] = smem_bit(wsp, fl[q]) ? (R)2 : (R)-2;  // -2 sigma_f
     dre = 0;
@@ -119,7 +131,7 @@ __device__ __forceinline__ void ratio_terms(const MachineDev& m, const uint8_t* 
 #pragma unroll
     for (int e = 0; e < E; e++) {
         if (!slot_valid(lane, e, m.T)) continue;
-        const int t = lane + 32 * e, k = t % m.nh, s = t / m.nh;
+        const int t = lane + 32 * e, k = ks[e] & 0xffffu, s = ks[e] >> 16;
         C2<R> x = wth[t];
         for (int q = 0; q < nf; q++) {
             const C2<R> u = W[urow<R>(m, sPerm, fl[q], s) * m.nh + k];
@@ -169,6 +181,8 @@ __device__ __noinline__ void evaluate(const MachineDev* __restrict__ mp, const H
                                       double2* Eout, C2<R>* Orow, PfStage* pst, const double2* pA) {
     const MachineDev m = *mp;
     const HamDev H = *hp;
+    uint32_t ks[E];
+    entry_index<E>(m, lane, ks);
     // ln cosh cache of the current theta
 #pragma unroll
     for (int e = 0; e < E; e++) {
@@ -200,7 +214,7 @@ __device__ __noinline__ void evaluate(const MachineDev* __restrict__ mp, const H
                     if ((mask >> i) & 1) fl[nf++] = op.sites[i];
                 R dre;
                 C2<R> ph;
-                ratio_terms<E, R>(m, sPerm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph);
+                ratio_terms<E, R>(m, sPerm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph, ks);
                 const double2 b = bias_delta_smem(m, wsp, fl, nf);
                 const double mag = exp((double)dre + b.x);
                 double sb, cb;
@@ -997,7 +1011,9 @@ __global__ void __launch_bounds__(256) eval_kernel(const EvalArgs a) {
         for (int q = 0; q < nf; q++) fl[q] = a.flips[b * nf + q];
         R dre;
         C2<R> ph;
-        ratio_terms<E, R>(m, sm.perm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph);
+        uint32_t ks[E];
+        entry_index<E>(m, lane, ks);
+        ratio_terms<E, R>(m, sm.perm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph, ks);
         double2 lr = make_double2(0.0, 0.0);
         if constexpr (PF) {
             const double2 c2 = pf_ratio_any(m.pf, sp[0], fl, nf, lane, *pst, pA);
@@ -1061,9 +1077,10 @@ __global__ void learned_propose(const LearnedArgs a) {
 
 // Re log psi without the constant: bias + sum ln|cosh theta| - T ln 2
 template <int E>
-__device__ __forceinline__ double log_amp(const MachineDev& m, const uint32_t sp[4], int lane) {
+__device__ __forceinline__ double log_amp(const MachineDev& m, const double2* W64, const uint8_t* perm,
+                                          const uint32_t sp[4], int lane) {
     C2<double> th[E];
-    theta_fp64<E, double>(m, m.W64, m.perm, lane, sp, th);
+    theta_fp64<E, double>(m, W64, perm, lane, sp, th);
     double acc = 0;
 #pragma unroll
     for (int e = 0; e < E; e++)
@@ -1079,11 +1096,25 @@ __device__ __forceinline__ double log_amp(const MachineDev& m, const uint32_t sp
 }
 
 template <int E>
-__global__ void __launch_bounds__(256) learned_accept(const LearnedArgs a) {
+__global__ void __launch_bounds__(256) learned_accept(const LearnedArgs a, int tables_in_smem) {
+    extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
+    const int n = a.m.n;
+    // W (FP64, site-major) and the symmetry table in shared memory when they fit
+    const double2* W64 = a.m.W64;
+    const uint8_t* perm = a.m.perm;
+    if (tables_in_smem) {
+        double2* sW = reinterpret_cast<double2*>(smem);
+        uint8_t* sP = reinterpret_cast<uint8_t*>(sW + (size_t)n * a.m.nh);
+        for (int i = threadIdx.x; i < n * a.m.nh; i += blockDim.x) sW[i] = a.m.W64[i];
+        if (a.m.symmetric)
+            for (int i = threadIdx.x; i < n * a.m.S; i += blockDim.x) sP[i] = a.m.perm[i];
+        __syncthreads();
+        W64 = sW;
+        perm = a.m.symmetric ? sP : a.m.perm;
+    }
     const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (c >= a.n_chains) return;
-    const int n = a.m.n;
     // log q(s|s') from the proposed configuration's logits, same mask
     float lq = 0.f;
     for (int i = lane; i < n; i += 32) {
@@ -1099,7 +1130,7 @@ __global__ void __launch_bounds__(256) learned_accept(const LearnedArgs a) {
         s0[w] = a.spins[4 * c + w];
         s1[w] = a.prop[4 * c + w];
     }
-    const double d = log_amp<E>(a.m, s1, lane) - log_amp<E>(a.m, s0, lane);
+    const double d = log_amp<E>(a.m, W64, perm, s1, lane) - log_amp<E>(a.m, W64, perm, s0, lane);
     const uint2 key = make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32));
     const uint4 r = philox4x32(make_uint4(a.move, a.ctl[0], (uint32_t)c, 4), key);
     // accept with min(1, |psi'/psi|^2 q(s|s') / q(s'|s))
@@ -1158,15 +1189,24 @@ cudaError_t launch_learned_propose(const LearnedArgs& a, cudaStream_t st) {
 
 cudaError_t launch_learned_accept(const LearnedArgs& a, cudaStream_t st) {
     const int blocks = (a.n_chains + 7) / 8;
+    const size_t tb = (size_t)a.m.n * a.m.nh * 16 + (a.m.symmetric ? (size_t)a.m.n * a.m.S : 0);
+    const int in_smem = tb <= 96 * 1024;
+    const int smem = in_smem ? (int)tb : 0;
+    const void* fn = nullptr;
     switch (elements_per_lane(a.m.T)) {
-        case 1: learned_accept<1><<<blocks, 256, 0, st>>>(a); break;
-        case 2: learned_accept<2><<<blocks, 256, 0, st>>>(a); break;
-        case 4: learned_accept<4><<<blocks, 256, 0, st>>>(a); break;
-        case 8: learned_accept<8><<<blocks, 256, 0, st>>>(a); break;
-        case 16: learned_accept<16><<<blocks, 256, 0, st>>>(a); break;
+        case 1: fn = reinterpret_cast<const void*>(learned_accept<1>); break;
+        case 2: fn = reinterpret_cast<const void*>(learned_accept<2>); break;
+        case 4: fn = reinterpret_cast<const void*>(learned_accept<4>); break;
+        case 8: fn = reinterpret_cast<const void*>(learned_accept<8>); break;
+        case 16: fn = reinterpret_cast<const void*>(learned_accept<16>); break;
         default: return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
+    cudaError_t e = ensure_dynamic_smem(fn, smem);
+    if (e != cudaSuccess) return e;
+    LearnedArgs aa = a;
+    int flag = in_smem;
+    void* args[] = {&aa, &flag};
+    return cudaLaunchKernel(fn, dim3(blocks), dim3(256), args, smem, st);
 }
 
 cudaError_t launch_record(const uint32_t* spins, int n_chains, int spc, int j, uint32_t* samples, cudaStream_t st) {
