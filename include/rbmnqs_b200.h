@@ -119,6 +119,10 @@ typedef struct {
     int32_t learned_train;
     int32_t learned_hidden;    /* width of both hidden layers (64..256) */
     double learned_lr;
+    int32_t solver;            /* optimizer.sr.method: 0 = cg (cg_solver), 1 =
+                                  minresqlp (MINRES from x0 = 0; rtol is then
+                                  the relative residual, max_iterations
+                                  defaults to 4 n_params) */
 } rbmnqs_config;
 
 /* Fills the reference defaults (src/tools/ini.cpp:38-120). */

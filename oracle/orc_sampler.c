@@ -389,6 +389,82 @@ int orc_cg_solve(const double complex* O, const double complex* d, double norm,
     return itn;
 }
 
+/* MINRES (Paige & Saunders 1975; the MINRES phase of MINRES-QLP, Choi,
+ * Paige & Saunders 2011, which the reference calls through
+ * minresqlp_adapter.cpp:40-110) on the same operator as cg1:
+ * (S + r1 diag (+ rd non-neural) + r2 max(diag)) x = F, x0 = 0 as the
+ * adapter starts, at most itnlim iterations (max_iterations, default 4 P,
+ * minresqlp_adapter.cpp:89), stopping when the recurred residual norm falls
+ * to rtol * ||F|| (default rtol 1e-16) or the Lanczos process ends
+ * (beta = 0).  For Hermitian S the Lanczos coefficients are real, so the
+ * rotations are the real ones of the published algorithm.  Returns the
+ * iteration count. */
+int orc_minres_solve(const double complex* O, const double complex* d, double norm,
+                     int N, int P, int n_neural, const double complex* F,
+                     double complex* x, double r1, double r2, double rd,
+                     const double* diag, int max_iterations, double rtol,
+                     double* rnorm_out) {
+    int itnlim = max_iterations > 0 ? max_iterations : 4 * P;
+    if (rtol <= 0) rtol = 1e-16;
+    double max_diag = diag[0];
+    for (int k = 1; k < P; k++)
+        if (diag[k] > max_diag) max_diag = diag[k];
+    size_t sz = sizeof(double complex) * P;
+    double complex *v = malloc(sz), *y = malloc(sz), *R1 = malloc(sz), *R2 = malloc(sz);
+    double complex *w = calloc(P, sizeof(double complex)), *w1 = calloc(P, sizeof(double complex));
+    double complex *w2 = calloc(P, sizeof(double complex)), *tmp = malloc(sizeof(double complex) * N);
+    for (int k = 0; k < P; k++) x[k] = 0;
+    memcpy(R1, F, sz);
+    memcpy(R2, F, sz);
+    memcpy(y, F, sz);
+    double beta1 = 0;
+    for (int k = 0; k < P; k++) beta1 += creal(F[k]) * creal(F[k]) + cimag(F[k]) * cimag(F[k]);
+    beta1 = sqrt(beta1);
+    double oldb = 0, beta = beta1, dbar = 0, epsln = 0, phibar = beta1, cs = -1, sn = 0;
+    int itn = 0;
+    if (beta1 > 0) {
+        for (itn = 1; itn <= itnlim; itn++) {
+            double s = 1.0 / beta;
+            for (int k = 0; k < P; k++) v[k] = s * y[k];
+            aprod(O, d, norm, N, P, n_neural, r1, r2, rd, diag, max_diag, v, y, tmp);
+            if (itn >= 2)
+                for (int k = 0; k < P; k++) y[k] -= (beta / oldb) * R1[k];
+            double alfa = 0;
+            for (int k = 0; k < P; k++) alfa += creal(conj(v[k]) * y[k]);
+            for (int k = 0; k < P; k++) y[k] -= (alfa / beta) * R2[k];
+            memcpy(R1, R2, sz);
+            memcpy(R2, y, sz);
+            oldb = beta;
+            beta = 0;
+            for (int k = 0; k < P; k++) beta += creal(R2[k]) * creal(R2[k]) + cimag(R2[k]) * cimag(R2[k]);
+            beta = sqrt(beta);
+            double oldeps = epsln;
+            double delta = cs * dbar + sn * alfa;
+            double gbar = sn * dbar - cs * alfa;
+            epsln = sn * beta;
+            dbar = -cs * beta;
+            double gamma = sqrt(gbar * gbar + beta * beta);
+            if (gamma < 2.2250738585072014e-308) gamma = 2.2250738585072014e-308;
+            cs = gbar / gamma;
+            sn = beta / gamma;
+            double phi = cs * phibar;
+            phibar = sn * phibar;
+            double denom = 1.0 / gamma;
+            for (int k = 0; k < P; k++) {
+                double complex wn = (v[k] - oldeps * w1[k] - delta * w2[k]) * denom;
+                w1[k] = w2[k];
+                w2[k] = wn;
+                x[k] += phi * wn;
+            }
+            if (phibar <= rtol * beta1 || beta == 0) break;
+        }
+        if (itn > itnlim) itn = itnlim;
+    }
+    if (rnorm_out) *rnorm_out = phibar;
+    free(v), free(y), free(R1), free(R2), free(w), free(w1), free(w2), free(tmp);
+    return itn;
+}
+
 /* decay_t, abstract_optimizer.cpp:27-54 */
 void orc_decay_init(orc_decay* d, double initial, double min, double decay,
                     uint64_t offset) {

@@ -337,7 +337,11 @@ struct rbmnqs_handle {
         ck(rbmnqs::launch_schedule(sched.p, st), "schedule");
         int max_it = std::min(2 * P, cfg.max_iterations);
         if (max_it == 0) max_it = 2 * P;
-        const double rtol = cfg.rtol == 0 ? 1e-16 : cfg.rtol;
+        double rtol = cfg.rtol == 0 ? 1e-16 : cfg.rtol;
+        if (cfg.solver == 1) {  // minresqlp semantics (minresqlp_adapter.cpp:86-112)
+            max_it = cfg.max_iterations > 0 ? cfg.max_iterations : 4 * P;
+            rtol = cfg.rtol > 0 ? cfg.rtol : 1e-16;
+        }
         if (mfree) {
             // diag = var(O) straight from O; CG on the operator (cg_solver.cpp aprod)
             ck(rbmnqs::launch_var_diag(O.p, fp64, d.p, N, P, mfp, mfw, diag.p, maxdiag.p, st), "var diag");
@@ -357,9 +361,9 @@ struct rbmnqs_handle {
                "regularize");
             mark(4);
             if (coop_dense && cg_after) ck(cudaStreamWaitEvent(st, cg_after, 0), "cg order");
-            if (coop_dense)
+            if (coop_dense || cfg.solver == 1)
                 ck(rbmnqs::launch_cg_dense_coop(Sreg.p, F.p, x.p, P, max_it, rtol, mfp, mfw, cgres.p, st),
-                   "cooperative cg");
+                   "cooperative solve");
             else
                 ck(rbmnqs::launch_cg(Sreg.p, F.p, x.p, P, max_it, rtol, cgres.p, st), "cg");
             if (coop_dense && cg_done) ck(cudaEventRecord(cg_done, st), "cg order");
@@ -515,6 +519,7 @@ int rbmnqs_config_default(rbmnqs_config* c) {
         c->learned_train = 1;
         c->learned_hidden = 256;
         c->learned_lr = 1e-3;
+        c->solver = 0;
     });
 }
 
@@ -671,12 +676,14 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         h->F.alloc(h->P);
         h->emean.alloc(1);
         h->gram_tc = !h->fp64 && cfg->gram == 0 && !h->mfree;
-        h->coop_dense = !h->mfree && !rbmnqs::cg_cluster_fits(h->P);
+        require(cfg->solver == 0 || cfg->solver == 1, "solver must be 0 (cg) or 1 (minresqlp)");
+        h->coop_dense = !h->mfree && (!rbmnqs::cg_cluster_fits(h->P) || cfg->solver == 1);
         if (h->mfree || h->coop_dense) {
             const int nn = h->mfree ? h->N : 1;
             ck(rbmnqs::mfree_plan(nn, h->P, &h->mfp), "cooperative CG plan");
             h->mfbuf.alloc(rbmnqs::mfree_work_bytes(nn, h->P, h->mfp));
             h->mfw = rbmnqs::mfree_carve(h->mfbuf.p, nn, h->P, h->mfp);
+            h->mfw.minres = cfg->solver == 1;
         }
         if (h->mfree) {
         } else if (h->gram_tc) {
@@ -1055,14 +1062,20 @@ int rbmnqs_sr_solve(rbmnqs_handle* h, const double* O, int32_t N, const double* 
         ck(cudaMemcpyAsync(ddiag.p, diag, P * sizeof(double), cudaMemcpyHostToDevice, h->st), "c");
         int max_it = std::min(2 * P, h->cfg.max_iterations);
         if (max_it == 0) max_it = 2 * P;
-        const double rtol = h->cfg.rtol == 0 ? 1e-16 : h->cfg.rtol;
+        double rtol = h->cfg.rtol == 0 ? 1e-16 : h->cfg.rtol;
+        const bool minres = h->cfg.solver == 1;
+        if (minres) {
+            max_it = h->cfg.max_iterations > 0 ? h->cfg.max_iterations : 4 * P;
+            rtol = h->cfg.rtol > 0 ? h->cfg.rtol : 1e-16;
+        }
         if (P > kDenseMax) {
             // the operator form (cg_solver.cpp aprod) on the given O, d, norm
             rbmnqs::MfreePlan pl{};
             ck(rbmnqs::mfree_plan(N, P, &pl), "matrix-free plan");
             DevBuf<unsigned char> wb;
             wb.alloc(rbmnqs::mfree_work_bytes(N, P, pl));
-            const rbmnqs::MfreeWork wk = rbmnqs::mfree_carve(wb.p, N, P, pl);
+            rbmnqs::MfreeWork wk = rbmnqs::mfree_carve(wb.p, N, P, pl);
+            wk.minres = minres;
             dmax.alloc(1);
             ck(rbmnqs::launch_max_diag(ddiag.p, P, dmax.p, h->st), "max diag");
             ck(rbmnqs::launch_cg_mfree(dO.p, 1, dd.p, norm, N, P, h->P_neural, dF.p, dx.p, ddiag.p, dmax.p, nullptr,
@@ -1077,7 +1090,19 @@ int rbmnqs_sr_solve(rbmnqs_handle* h, const double* O, int32_t N, const double* 
             ck(rbmnqs::launch_gram_fp64(dO.p, 1, nullptr, N, P, ks, part.p, G.p, h->st), "gram");
             ck(rbmnqs::launch_solve_prep(G.p, N, norm, dd.p, ddiag.p, P, h->P_neural, r1, r2, rd, Sreg.p, h->st),
                "prep");
-            ck(rbmnqs::launch_cg(Sreg.p, dF.p, dx.p, P, max_it, rtol, res.p, h->st), "cg");
+            if (minres) {
+                rbmnqs::MfreePlan pl{};
+                ck(rbmnqs::mfree_plan(1, P, &pl), "cooperative plan");
+                DevBuf<unsigned char> wb;
+                wb.alloc(rbmnqs::mfree_work_bytes(1, P, pl));
+                rbmnqs::MfreeWork wk = rbmnqs::mfree_carve(wb.p, 1, P, pl);
+                wk.minres = 1;
+                ck(rbmnqs::launch_cg_dense_coop(Sreg.p, dF.p, dx.p, P, max_it, rtol, pl, wk, res.p, h->st),
+                   "minres");
+                ck(cudaStreamSynchronize(h->st), "sync");  // before wb goes out of scope
+            } else {
+                ck(rbmnqs::launch_cg(Sreg.p, dF.p, dx.p, P, max_it, rtol, res.p, h->st), "cg");
+            }
         }
         rbmnqs::CgResultDev r{};
         ck(cudaMemcpyAsync(x_io, dx.p, P * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "c");

@@ -286,6 +286,102 @@ __global__ void __launch_bounds__(kThreads) cg_mfree_kernel(const TO* __restrict
         return true;
     };
 
+    if (w.minres) {
+        // MINRES (Paige & Saunders 1975; the MINRES phase of MINRES-QLP,
+        // minresqlp_adapter.cpp:40-110): Lanczos on A with real coefficients
+        // (A Hermitian), QR by Givens rotations, x0 = 0, stop when the
+        // recurred residual norm reaches rtol ||F|| or beta vanishes.
+        double bl = 0;
+        for (int q = gt; q < P; q += nthreads) {
+            const double2 f = F[q];
+            w.R1[q] = f;
+            w.R2[q] = f;
+            w.w1[q] = make_double2(0, 0);
+            w.w2[q] = make_double2(0, 0);
+            x[q] = make_double2(0, 0);
+            bl += f.x * f.x + f.y * f.y;
+        }
+        bl = bsum(bl, redd);
+        if (tid == 0) w.dpart[blk] = bl;
+        bool mok = grid_barrier(w.sync, G);
+        const double beta1 = mok ? sqrt(sum_parts(w.dpart, G, redd)) : 0.0;
+        double oldb = 0, beta = beta1, dbar = 0, epsln = 0, phibar = beta1, cs = -1, sn = 0;
+        int itn = 0;
+        if (mok && beta1 > 0) {
+            for (itn = 1; itn <= max_it; itn++) {
+                const double s = 1.0 / beta;
+                for (int q = gt; q < P; q += nthreads) {
+                    const double2 r2 = cg_ld(w.R2 + q);
+                    w.p[q] = make_double2(s * r2.x, s * r2.y);  // v
+                }
+                if (!(mok = grid_barrier(w.sync, G))) break;
+                if (!(mok = aprod(w.p, false, nullptr))) break;
+                // y = A v - (beta / oldb) r1;  alfa = Re(v^H y)
+                double al = 0;
+                const double cb = itn >= 2 ? beta / oldb : 0.0;
+                for (int q = gt; q < P; q += nthreads) {
+                    double2 y = cg_ld(w.Ap + q);
+                    const double2 r1 = cg_ld(w.R1 + q), v = cg_ld(w.p + q);
+                    y.x -= cb * r1.x;
+                    y.y -= cb * r1.y;
+                    w.r[q] = y;
+                    al += v.x * y.x + v.y * y.y;
+                }
+                al = bsum(al, redd);
+                if (tid == 0) w.dpart[blk] = al;
+                if (!(mok = grid_barrier(w.sync, G))) break;
+                const double alfa = sum_parts(w.dpart, G, redd);
+                // y -= (alfa / beta) r2;  r1 = r2;  r2 = y;  beta = ||r2||
+                double bb = 0;
+                for (int q = gt; q < P; q += nthreads) {
+                    double2 y = cg_ld(w.r + q);
+                    const double2 r2 = cg_ld(w.R2 + q);
+                    y.x -= (alfa / beta) * r2.x;
+                    y.y -= (alfa / beta) * r2.y;
+                    w.R1[q] = r2;
+                    w.R2[q] = y;
+                    bb += y.x * y.x + y.y * y.y;
+                }
+                bb = bsum(bb, redd);
+                if (tid == 0) w.zpart[blk] = make_double2(bb, 0);
+                if (!(mok = grid_barrier(w.sync, G))) break;
+                oldb = beta;
+                beta = sqrt(sum_parts(w.zpart, G, redz).x);
+                const double oldeps = epsln;
+                const double delta = cs * dbar + sn * alfa;
+                const double gbar = sn * dbar - cs * alfa;
+                epsln = sn * beta;
+                dbar = -cs * beta;
+                double gamma = sqrt(gbar * gbar + beta * beta);
+                if (gamma < 2.2250738585072014e-308) gamma = 2.2250738585072014e-308;
+                cs = gbar / gamma;
+                sn = beta / gamma;
+                const double phi = cs * phibar;
+                phibar = sn * phibar;
+                const double den = 1.0 / gamma;
+                for (int q = gt; q < P; q += nthreads) {
+                    const double2 v = cg_ld(w.p + q), a1 = cg_ld(w.w1 + q), a2 = cg_ld(w.w2 + q);
+                    const double2 wn = make_double2((v.x - oldeps * a1.x - delta * a2.x) * den,
+                                                    (v.y - oldeps * a1.y - delta * a2.y) * den);
+                    w.w1[q] = a2;
+                    w.w2[q] = wn;
+                    double2 xq = cg_ld(x + q);
+                    xq.x += phi * wn.x;
+                    xq.y += phi * wn.y;
+                    x[q] = xq;
+                }
+                if (phibar <= rtol * beta1 || beta == 0) break;
+            }
+            if (itn > max_it) itn = max_it;
+        }
+        if (blk == 0 && tid == 0) {
+            res->iterations = itn;
+            res->residual = phibar;
+            if (!mok) res->status = -2;
+        }
+        return;
+    }
+
     bool ok = aprod(x, false, nullptr);
     // r = F - A x0, p = r
     double rl = 0;
@@ -423,7 +519,7 @@ cudaError_t mfree_plan(int N, int P, MfreePlan* pl) {
 }
 
 size_t mfree_work_bytes(int N, int P, const MfreePlan& pl) {
-    return ((size_t)3 * P + N + (size_t)pl.nseg * N + 2 * (size_t)pl.blocks) * sizeof(double2) +
+    return ((size_t)8 * P + N + (size_t)pl.nseg * N + 2 * (size_t)pl.blocks) * sizeof(double2) +
            (size_t)pl.blocks * sizeof(double) * 2 + sizeof(MfreeSync) + 256;
 }
 
@@ -433,7 +529,12 @@ MfreeWork mfree_carve(void* base, int N, int P, const MfreePlan& pl) {
     w.r = z;
     w.p = w.r + P;
     w.Ap = w.p + P;
-    w.tmpN = w.Ap + P;
+    w.R1 = w.Ap + P;
+    w.R2 = w.R1 + P;
+    w.w1 = w.R2 + P;
+    w.w2 = w.w1 + P;
+    w.v = w.w2 + P;
+    w.tmpN = w.v + P;
     w.partA = w.tmpN + N;
     w.zpart = w.partA + (size_t)pl.nseg * N;
     auto* dd = reinterpret_cast<double*>(w.zpart + 2 * (size_t)pl.blocks);

@@ -56,7 +56,9 @@ struct MfreePlan {
 };
 struct MfreeWork {
     const double2* S;  // formed regularised S (dense cooperative mode) or null
+    int minres;        // 0: CG (cg1), 1: MINRES from x0 = 0 (rtol relative to ||F||)
     double2 *r, *p, *Ap, *tmpN, *partA, *zpart;
+    double2 *R1, *R2, *w1, *w2, *v;  // MINRES vectors
     double *dpart, *maxpart;
     MfreeSync* sync;
     int nseg, lseg;

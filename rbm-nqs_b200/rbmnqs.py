@@ -40,7 +40,7 @@ class Config(C.Structure):
         ("deltareg1", C.c_double * 3), ("max_iterations", C.c_int32), ("rtol", C.c_double),
         ("precision", C.c_int32), ("n_updates", C.c_int32), ("gram", C.c_int32),
         ("proposal", C.c_int32), ("learned_steps", C.c_int32), ("learned_train", C.c_int32),
-        ("learned_hidden", C.c_int32), ("learned_lr", C.c_double),
+        ("learned_hidden", C.c_int32), ("learned_lr", C.c_double), ("solver", C.c_int32),
     ]
 
 

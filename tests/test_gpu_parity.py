@@ -330,3 +330,28 @@ def test_matrix_free_epochs_match_oracle():
     assert rel(diag, O.sr_moments(Om, E)[2]) < TOL64
     with pytest.raises(rbmnqs.RbmNqsError):
         s.sr_moments(with_S=True)  # S is not formed above 2048 parameters
+
+
+@pytest.mark.parametrize("model,L,kind,alpha", [("kitaev", 3, 0, 1), ("toric", 4, 0, 2), ("kitaev", 2, 1, 4)])
+def test_minres_solve_matches_oracle(model, L, kind, alpha):
+    """optimizer.sr.method = minresqlp: MINRES from x0 = 0 on the SR operator
+    (dense S for 360 / 20 parameters, the matrix-free operator for 2144)
+    against the oracle's MINRES, and against CG on the same system."""
+    rng = np.random.default_rng(8)
+    om = O.Model.kitaev(L) if model == "kitaev" else O.Model.toric(L)
+    symm = 0.5 if model == "kitaev" else 1.0
+    mach = O.Machine(om, "symmetry" if kind else "basic", alpha, symm=symm).init_random(rng, 0.05)
+    gm = rbmnqs.Model.kitaev(L) if model == "kitaev" else rbmnqs.Model.toric(L, symmetry=symm)
+    cfg = rbmnqs.default_config(rbm_type=kind, alpha=alpha, n_chains=16, samples_per_chain=12, warmup=3, seed=9,
+                                precision=1, solver=1, rtol=1e-12, max_iterations=400)
+    s = rbmnqs.Session(gm, cfg)
+    s.set_weights(mach.params())
+    s.sample()
+    E, Om = s.samples()
+    d, F, diag = O.sr_moments(Om, E)
+    xo, ito, rno = O.minres_solve(Om, d, F, 0.9, 9e-4, 1e-2, diag, max_iterations=400, rtol=1e-12)
+    xg, itg, rng_ = s.sr_solve(Om, d, F, np.zeros(mach.n_params), 0.9, 9e-4, 1e-2, diag)
+    assert abs(itg - ito) <= max(2, ito // 20)
+    assert rel(xg, xo) < 1e-8
+    xc, _, _ = O.cg_solve(Om, d, F, np.zeros(mach.n_params), 0.9, 9e-4, 1e-2, diag)
+    assert rel(xg, xc) < 1e-6
