@@ -233,6 +233,19 @@ int rbmnqs_graph_kernels(rbmnqs_handle* h, int32_t* kernel_nodes);
 /* The handle's cudaStream_t, for callers that order work against it. */
 void* rbmnqs_stream(rbmnqs_handle* h);
 
+/* ------------------------------------------------------------ checkpoints */
+/* The reference's .rbm file (rbm_base::save / load, rbm_base.cpp:219-288,
+ * matrices as eigen_fstream.cpp:25-51: rows, cols as 8-byte size_t, then the
+ * column-major complex128 data): W (n x n_hidden), h (n_hidden x 1), v (n_vb x
+ * 1), n_updates (size_t), then the Pfaffian fs_ (n_indep x 4) when present.
+ * `path` is the full file name.  Loading sets the weights and the update
+ * count, and restarts the decay_t schedules at that count
+ * (abstract_optimizer.cpp:27-54). */
+int rbmnqs_save(rbmnqs_handle* h, const char* path);
+int rbmnqs_load(rbmnqs_handle* h, const char* path);
+/* SR updates applied so far, counting the config's n_updates offset */
+int rbmnqs_n_updates(const rbmnqs_handle* h, int64_t* n_updates);
+
 /* ---------------------------------------------- learned proposal network */
 /* The proposal network n_in -> h1 -> h2 -> n_out (GELU, BF16 weights and
  * activations, FP32 accumulation; forward, backward and Adam on the GPU)

@@ -164,6 +164,7 @@ struct rbmnqs_handle {
     int n_ops = 0, n_prop_bonds = 0;
     uint32_t epoch = 0;
     bool sampled = false;
+    int64_t n_updates = 0;  // rbm_base::n_updates_ (offset + applied SR updates)
 
     cudaGraphExec_t graph = nullptr;
     int graph_kernels = 0;
@@ -389,6 +390,8 @@ struct rbmnqs_handle {
 
 // ---------------------------------------------------------------------------
 extern "C" {
+
+static void set_schedules(rbmnqs_handle* h, int64_t n_updates);
 
 const char* rbmnqs_last_error(void) { return g_err.c_str(); }
 
@@ -709,15 +712,8 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         h->cgres.alloc(1);
         h->stats.alloc(1);
         // decay_t schedules with the n_updates offset
-        rbmnqs::ScheduleDev sd{};
-        const double* src[4] = {cfg->lr, cfg->reg1, cfg->reg2, cfg->deltareg1};
-        for (int i = 0; i < 4; i++) {
-            sd.value[i] = std::pow(src[i][2], (double)cfg->n_updates) * src[i][0];
-            sd.min[i] = src[i][1];
-            sd.decay[i] = src[i][2];
-            sd.min_reached[i] = src[i][2] == 1.0;
-        }
-        ck(cudaMemcpy(h->sched.p, &sd, sizeof(sd), cudaMemcpyHostToDevice), "c");
+        h->n_updates = cfg->n_updates;
+        set_schedules(h.get(), h->n_updates);
         // device copies of the machine / Hamiltonian descriptors
         h->mdev.alloc(1);
         h->hdev.alloc(1);
@@ -802,6 +798,22 @@ int rbmnqs_get_weights(rbmnqs_handle* h, double* w) {
     });
 }
 
+// decay_t (abstract_optimizer.cpp:27-54) for lr, reg1, reg2, deltareg1,
+// constructed with an update offset
+static void set_schedules(rbmnqs_handle* h, int64_t n_updates) {
+    rbmnqs::ScheduleDev sd{};
+    const auto& c = h->cfg;
+    const double* src[4] = {c.lr, c.reg1, c.reg2, c.deltareg1};
+    for (int i = 0; i < 4; i++) {
+        sd.value[i] = std::pow(src[i][2], (double)n_updates) * src[i][0];
+        sd.min[i] = src[i][1];
+        sd.decay[i] = src[i][2];
+        sd.min_reached[i] = src[i][2] == 1.0;
+    }
+    ck(cudaMemcpyAsync(h->sched.p, &sd, sizeof(sd), cudaMemcpyHostToDevice, h->st), "copy");
+    ck(cudaStreamSynchronize(h->st), "sync");
+}
+
 static int count_kernel_nodes(cudaGraph_t g) {
     size_t nn = 0;
     ck(cudaGraphGetNodes(g, nullptr, &nn), "graph nodes");
@@ -853,6 +865,7 @@ static void read_sr_stats(rbmnqs_handle* h, rbmnqs_sr_stats* out) {
     if (h->gram_tc) ck(cudaMemcpyAsync(&gerr, h->gerr.p, sizeof(int), cudaMemcpyDeviceToHost, h->st), "copy");
     ck(cudaStreamSynchronize(h->st), "sync");
     if (gerr) throw Fail{RBMNQS_ERR_CUDA, "tensor-core Gram: pipeline wait timed out (code " + std::to_string(gerr) + ")"};
+    if (r.status == 0) h->n_updates++;
     if (out) {
         out->iterations = r.iterations;
         out->status = r.status;
@@ -1569,5 +1582,85 @@ int rbmnqs_mlp_intermediate(rbmnqs_mlp* m, int32_t which, int32_t B, float* out,
 }
 
 void rbmnqs_mlp_destroy(rbmnqs_mlp* m) { delete m; }
+
+}  // extern "C"
+
+// ----------------------------------------------------------- checkpoints --
+namespace {
+void write_mat(std::FILE* f, const cplx* data, uint64_t rows, uint64_t cols) {
+    require(std::fwrite(&rows, 8, 1, f) == 1 && std::fwrite(&cols, 8, 1, f) == 1 &&
+                std::fwrite(data, sizeof(cplx), rows * cols, f) == rows * cols,
+            "checkpoint write failed");
+}
+void read_mat(std::FILE* f, cplx* data, uint64_t rows, uint64_t cols) {
+    uint64_t r = 0, c = 0;
+    require(std::fread(&r, 8, 1, f) == 1 && std::fread(&c, 8, 1, f) == 1, "checkpoint truncated");
+    require(r == rows && c == cols, "checkpoint dimension mismatch: file " + std::to_string(r) + " x " +
+                                        std::to_string(c) + ", machine " + std::to_string(rows) + " x " +
+                                        std::to_string(cols));
+    require(std::fread(data, sizeof(cplx), rows * cols, f) == rows * cols, "checkpoint truncated");
+}
+}  // namespace
+
+extern "C" {
+
+int rbmnqs_save(rbmnqs_handle* h, const char* path) {
+    return guard([&] {
+        require(h && path, "null argument");
+        std::vector<cplx> w(h->P);
+        ck(cudaMemcpyAsync(w.data(), h->params.p, h->P * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "copy");
+        ck(cudaStreamSynchronize(h->st), "sync");
+        std::FILE* f = std::fopen(path, "wb");
+        require(f != nullptr, std::string("cannot open ") + path);
+        try {
+            const int nvb = h->n_vb, nh = h->nh, n = h->n;
+            // rbm_base::save order: weights_, h_bias_, v_bias_, n_updates_, pfaffian fs_
+            write_mat(f, w.data() + nvb + nh, n, nh);
+            write_mat(f, w.data() + nvb, nh, 1);
+            write_mat(f, w.data(), nvb, 1);
+            const uint64_t nu = (uint64_t)h->n_updates;
+            require(std::fwrite(&nu, 8, 1, f) == 1, "checkpoint write failed");
+            if (h->pf_n) write_mat(f, w.data() + h->P_neural, h->pf_indep, 4);
+        } catch (...) {
+            std::fclose(f);
+            throw;
+        }
+        require(std::fclose(f) == 0, "checkpoint write failed");
+    });
+}
+
+int rbmnqs_load(rbmnqs_handle* h, const char* path) {
+    return guard([&] {
+        require(h && path, "null argument");
+        std::vector<cplx> w(h->P);
+        std::FILE* f = std::fopen(path, "rb");
+        require(f != nullptr, std::string("cannot open ") + path);
+        uint64_t nu = 0;
+        try {
+            const int nvb = h->n_vb, nh = h->nh, n = h->n;
+            read_mat(f, w.data() + nvb + nh, n, nh);
+            read_mat(f, w.data() + nvb, nh, 1);
+            read_mat(f, w.data(), nvb, 1);
+            require(std::fread(&nu, 8, 1, f) == 1, "checkpoint truncated");
+            if (h->pf_n) read_mat(f, w.data() + h->P_neural, h->pf_indep, 4);
+        } catch (...) {
+            std::fclose(f);
+            throw;
+        }
+        std::fclose(f);
+        ck(cudaMemcpyAsync(h->params.p, w.data(), h->P * sizeof(double2), cudaMemcpyHostToDevice, h->st), "copy");
+        ck(rbmnqs::launch_unpack(h->params.p, h->n, h->n_vb, h->nh, h->vb.p, h->hb.p, h->W64.p, h->W32.p, h->st),
+           "unpack");
+        h->n_updates = (int64_t)nu;
+        set_schedules(h, h->n_updates);
+    });
+}
+
+int rbmnqs_n_updates(const rbmnqs_handle* h, int64_t* n_updates) {
+    return guard([&] {
+        require(h && n_updates, "null argument");
+        *n_updates = h->n_updates;
+    });
+}
 
 }  // extern "C"

@@ -108,6 +108,9 @@ def _declare(L):
         "rbmnqs_timing_reset": [VP, C.c_int32],
         "rbmnqs_graph_kernels": [VP, P_I],
         "rbmnqs_autotune": [VP, C.c_int32, P_I, P_I, P_D],
+        "rbmnqs_save": [VP, C.c_char_p],
+        "rbmnqs_load": [VP, C.c_char_p],
+        "rbmnqs_n_updates": [VP, P_I64],
         "rbmnqs_batch_create": [C.POINTER(VP), C.c_int32, C.POINTER(VP)],
         "rbmnqs_batch_epoch": [VP, VP, VP],
         "rbmnqs_batch_graph_kernels": [VP, P_I],
@@ -400,6 +403,18 @@ class Session:
 
     def stream(self):
         return lib().rbmnqs_stream(self._h)
+
+    def save(self, path):
+        """The reference's .rbm checkpoint (rbm_base::save)."""
+        _ck(lib().rbmnqs_save(self._h, str(path).encode()))
+
+    def load(self, path):
+        _ck(lib().rbmnqs_load(self._h, str(path).encode()))
+
+    def n_updates(self):
+        n = C.c_int64()
+        _ck(lib().rbmnqs_n_updates(self._h, C.byref(n)))
+        return n.value
 
     def autotune(self, sweeps=4):
         """Launch-shape autotuning (rbmnqs_autotune): (sampler warps per
