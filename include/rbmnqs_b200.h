@@ -178,6 +178,9 @@ int rbmnqs_epoch(rbmnqs_handle* h, rbmnqs_sample_stats* s, rbmnqs_sr_stats* o);
 /* Copies of the last epoch's per-sample data: E[N] and O[N][n_params]
  * (sample-major), both interleaved complex. */
 int rbmnqs_get_samples(rbmnqs_handle* h, double* E, double* O);
+/* The sampled configurations of the last epoch [N][4] (chain-major, the
+ * order of E and O). */
+int rbmnqs_get_sample_configs(rbmnqs_handle* h, uint32_t* configs);
 /* SR moments of the last epoch: d = <O>, F, unbiased var(O), S (P x P,
  * row-major, S_kl = <conj(O_k) O_l> - conj(d_k) d_l, unregularised). */
 int rbmnqs_get_sr(rbmnqs_handle* h, double* d, double* F, double* diag, double* S);
@@ -207,8 +210,12 @@ int rbmnqs_sr_solve(rbmnqs_handle* h, const double* O, int32_t N,
 /* Exact enumeration of all 2^n configurations weighted by |psi|^2
  * (full_sampler.cpp:43-186); n <= 30.  Outputs <E>, <O>, <E O*>. */
 int rbmnqs_full_sample(rbmnqs_handle* h, double* E_mean, double* d, double* dh);
-/* Observable expectation values <W_p> of the last epoch (after
- * rbmnqs_model_add_hexagons). */
+/* Evaluation mode (main.cpp:640-671): expectation values of the model's
+ * observables (the hexagon plaquettes W_p after rbmnqs_model_add_hexagons)
+ * over the samples of the last epoch, each through the local estimator
+ * sum_l' O[l, l'] psi(l') / psi(l) (local_op.cpp:31-60) with the
+ * aggregator's statistics: values[4 i .. 4 i + 3] = Re <O_i>, Im <O_i>,
+ * binned standard deviation of the mean, tau. */
 int rbmnqs_get_observables(rbmnqs_handle* h, double* values);
 
 /* ----------------------------------------------------------- timing ---- */

@@ -110,6 +110,16 @@ HamHost build_ham(const std::vector<rbmnqs::local_op>& ops) {
 
 void rbmnqs::set_last_error(const std::string& msg) { g_err = msg; }
 
+// One observable (evaluation mode) as a one-operator Hamiltonian table.
+struct ObsDev {
+    DevBuf<rbmnqs::OpDev> ops;
+    DevBuf<int> rowptr;
+    DevBuf<uint32_t> mask;
+    DevBuf<double2> val;
+    DevBuf<rbmnqs::HamDev> hd;
+    rbmnqs::HamDev H{};
+};
+
 struct rbmnqs_handle {
     rbmnqs_config cfg{};
     rbmnqs::model model;
@@ -144,6 +154,10 @@ struct rbmnqs_handle {
     rbmnqs::MfreePlan mfp{};
     rbmnqs::MfreeWork mfw{};
     DevBuf<unsigned char> mfbuf;
+    // evaluation-mode observables, their per-sample values and statistics
+    std::vector<std::unique_ptr<ObsDev>> obs;
+    DevBuf<double2> obsE, obsMean;
+    DevBuf<rbmnqs::EpochStatsDev> obsStats;
     // learned proposals: network, proposed configurations, masks, counters
     std::unique_ptr<rbmnqs::Mlp> net;
     DevBuf<uint32_t> lprop, lmask, lacc, ltry, ltgt;
@@ -650,6 +664,27 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         ck(cudaMemcpy(h->rowptr.p, hh.rowptr.data(), hh.rowptr.size() * sizeof(int), cudaMemcpyHostToDevice), "c");
         ck(cudaMemcpy(h->emask.p, hh.mask.data(), hh.mask.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "c");
         ck(cudaMemcpy(h->eval.p, hh.val.data(), hh.val.size() * sizeof(double2), cudaMemcpyHostToDevice), "c");
+        // observables (evaluation mode), one table each
+        for (const auto& op : m.observables) {
+            auto od = std::make_unique<ObsDev>();
+            HamHost oh = build_ham({op});
+            od->ops.alloc(oh.ops.size());
+            od->rowptr.alloc(oh.rowptr.size());
+            od->mask.alloc(oh.mask.size());
+            od->val.alloc(oh.val.size());
+            ck(cudaMemcpy(od->ops.p, oh.ops.data(), oh.ops.size() * sizeof(rbmnqs::OpDev), cudaMemcpyHostToDevice), "c");
+            ck(cudaMemcpy(od->rowptr.p, oh.rowptr.data(), oh.rowptr.size() * sizeof(int), cudaMemcpyHostToDevice), "c");
+            ck(cudaMemcpy(od->mask.p, oh.mask.data(), oh.mask.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "c");
+            ck(cudaMemcpy(od->val.p, oh.val.data(), oh.val.size() * sizeof(double2), cudaMemcpyHostToDevice), "c");
+            od->H.n_ops = 1;
+            od->H.ops = od->ops.p;
+            od->H.rowptr = od->rowptr.p;
+            od->H.ent_mask = od->mask.p;
+            od->H.ent_val = od->val.p;
+            od->hd.alloc(1);
+            ck(cudaMemcpy(od->hd.p, &od->H, sizeof(od->H), cudaMemcpyHostToDevice), "c");
+            h->obs.push_back(std::move(od));
+        }
         // bond proposals: bonds of type != 2 (metropolis_sampler.cpp:145-166)
         std::vector<int2> pb;
         if (m.kind == "kitaev")
@@ -963,6 +998,14 @@ int rbmnqs_get_sr(rbmnqs_handle* h, double* d, double* F, double* diag, double* 
     });
 }
 
+int rbmnqs_get_sample_configs(rbmnqs_handle* h, uint32_t* configs) {
+    return guard([&] {
+        require(h && configs, "null argument");
+        ck(cudaMemcpyAsync(configs, h->samples.p, (size_t)h->N * 16, cudaMemcpyDeviceToHost, h->st), "c");
+        ck(cudaStreamSynchronize(h->st), "sync");
+    });
+}
+
 int rbmnqs_get_spins(rbmnqs_handle* h, uint32_t* spins) {
     return guard([&] {
         require(h && spins, "null argument");
@@ -1187,9 +1230,36 @@ int rbmnqs_full_sample(rbmnqs_handle* h, double* E_mean, double* dm, double* dh)
 
 int rbmnqs_get_observables(rbmnqs_handle* h, double* values) {
     return guard([&] {
-        (void)h;
-        (void)values;
-        throw Fail{RBMNQS_ERR_UNSUPPORTED, "observables are evaluated with rbmnqs_eval_batch in this build"};
+        require(h && values, "null argument");
+        require(!h->obs.empty(), "the model has no observables (rbmnqs_model_add_hexagons)");
+        require(h->sampled, "rbmnqs_get_observables needs a preceding sample or epoch");
+        const int no = (int)h->obs.size();
+        if (!h->obsE.p) {
+            h->obsE.alloc(h->N);
+            h->obsMean.alloc(no);
+            h->obsStats.alloc(no);
+        }
+        for (int i = 0; i < no; i++) {
+            rbmnqs::EvalArgs ea = h->eval_args();
+            ea.H = h->obs[i]->H;
+            ea.hd = h->obs[i]->hd.p;
+            ea.O = nullptr;
+            ea.eloc = h->obsE.p;
+            ck(rbmnqs::launch_eval(ea, h->fp64, h->wpb, h->st), "observable evaluation");
+            ck(rbmnqs::launch_mean(h->obsE.p, h->N, h->obsMean.p + i, h->st), "observable mean");
+            ck(rbmnqs::launch_energy_stats(h->obsE.p, h->N, h->n_bins, h->obsMean.p + i, h->nacc.p, h->nprop.p,
+                                           h->cfg.n_chains, h->obsStats.p + i, h->st),
+               "observable statistics");
+        }
+        std::vector<rbmnqs::EpochStatsDev> st(no);
+        ck(cudaMemcpyAsync(st.data(), h->obsStats.p, no * sizeof(st[0]), cudaMemcpyDeviceToHost, h->st), "copy");
+        ck(cudaStreamSynchronize(h->st), "sync");
+        for (int i = 0; i < no; i++) {
+            values[4 * i] = st[i].energy.x;
+            values[4 * i + 1] = st[i].energy.y;
+            values[4 * i + 2] = st[i].stddev;
+            values[4 * i + 3] = st[i].tau;
+        }
     });
 }
 

@@ -769,6 +769,20 @@ cudaError_t launch_moments(const void* O, int fp64, const double2* E, int N, int
     return cudaGetLastError();
 }
 
+// mean of E[N] (complex) into *mu, one block
+__global__ void cmean_kernel(const double2* E, int N, double2* mu) {
+    __shared__ double2 red[32];
+    double2 s = make_double2(0, 0);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) s = add2(s, E[i]);
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) *mu = make_double2(s.x / N, s.y / N);
+}
+
+cudaError_t launch_mean(const double2* E, int N, double2* mu, cudaStream_t st) {
+    cmean_kernel<<<1, 1024, 0, st>>>(E, N, mu);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_energy_stats(const double2* E, int N, int n_bins, const double2* emean, const uint32_t* nacc,
                                 const uint32_t* nprop, int n_chains, EpochStatsDev* out, cudaStream_t st) {
     energy_stats<<<1, 1024, 0, st>>>(E, N, n_bins, emean, nacc, nprop, n_chains, out);

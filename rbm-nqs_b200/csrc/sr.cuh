@@ -34,6 +34,7 @@ cudaError_t launch_moments(const void* O, int fp64, const double2* E, int N, int
                            double2* pf, double2* pe, double2* d, double2* F, double2* emean, cudaStream_t st);
 cudaError_t launch_energy_stats(const double2* E, int N, int n_bins, const double2* emean, const uint32_t* nacc,
                                 const uint32_t* nprop, int n_chains, EpochStatsDev* out, cudaStream_t st);
+cudaError_t launch_mean(const double2* E, int N, double2* mu, cudaStream_t st);
 int gram_splits(int N, int P);
 cudaError_t launch_gram_fp64(const void* O, int fp64, const double2* d, int N, int P, int nks, double2* part,
                              double2* S, cudaStream_t st);

@@ -97,6 +97,7 @@ def _declare(L):
         "rbmnqs_get_samples": [VP, P_D, P_D],
         "rbmnqs_get_sr": [VP, P_D, P_D, P_D, P_D],
         "rbmnqs_get_spins": [VP, P_U32],
+        "rbmnqs_get_sample_configs": [VP, P_U32],
         "rbmnqs_set_spins": [VP, P_U32],
         "rbmnqs_eval_batch": [VP, P_U32, C.c_int32, P_D, P_D, P_D],
         "rbmnqs_log_psi_over_psi": [VP, P_U32, P_I, C.c_int32, C.c_int32, P_D],
@@ -322,6 +323,12 @@ class Session:
                                      _p(O.view(np.float64), P_D) if with_O else None))
         return E, O
 
+    def sample_configs(self):
+        """configurations of the last epoch's samples [N][4] (the order of samples())"""
+        c = np.zeros((self.N, 4), np.uint32)
+        _ck(lib().rbmnqs_get_sample_configs(self._h, _p(c, P_U32)))
+        return c
+
     def sr_moments(self, with_S=None):
         """d, F, diag and (when formed: n_params <= 2048, or with_S) S."""
         P = self.n_params
@@ -377,6 +384,13 @@ class Session:
                                   _p(x.view(np.float64), P_D), r1, r2, rd, _p(diag, P_D), C.byref(it),
                                   C.byref(rs)))
         return x, it.value, rs.value
+
+    def observables(self):
+        """Evaluation mode: [n_obs] rows of (Re <O>, Im <O>, stddev, tau) over the
+        last epoch's samples (hexagon W_p after Model.add_hexagons)."""
+        v = np.zeros(4 * self.model.n_obs, np.float64)
+        _ck(lib().rbmnqs_get_observables(self._h, _p(v, P_D)))
+        return v.reshape(-1, 4)
 
     def full_sample(self):
         P = self.n_params

@@ -355,3 +355,30 @@ def test_minres_solve_matches_oracle(model, L, kind, alpha):
     assert rel(xg, xo) < 1e-8
     xc, _, _ = O.cg_solve(Om, d, F, np.zeros(mach.n_params), 0.9, 9e-4, 1e-2, diag)
     assert rel(xg, xc) < 1e-6
+
+
+@pytest.mark.parametrize("precision,tol", [(1, TOL64), (0, TOL32)])
+def test_observables_match_oracle(precision, tol):
+    """Evaluation mode (main.cpp:640-671): <W_p> of every hexagon over the
+    epoch's samples against the oracle's local estimator on the same samples."""
+    rng = np.random.default_rng(2)
+    om = O.Model.kitaev(3)
+    mach = O.Machine(om, "symmetry", 2, symm=0.5).init_random(rng, 0.2)
+    gm = rbmnqs.Model.kitaev(3)
+    gm.add_hexagons()
+    cfg = rbmnqs.default_config(rbm_type=1, alpha=2, n_chains=32, samples_per_chain=16, warmup=4, seed=4,
+                                precision=precision)
+    s = rbmnqs.Session(gm, cfg)
+    s.set_weights(mach.params())
+    s.sample()
+    vals = s.observables()
+    hx = O.Model.hexagons(3)
+    assert vals.shape == (hx.n_ops, 4)
+    # per hexagon: the oracle's local values on the GPU's configurations
+    conf = s.sample_configs()
+    for o in range(hx.n_ops):
+        one = O.Model(hx.n, hx.k[o:o + 1], hx.sites[o:o + 1], np.array([0], np.int32),
+                      hx.mats[2 * hx.mat_off[o]: 2 * (hx.mat_off[o] + 64 * 64)])
+        _, lo, _ = O.eval_batch(mach, one, conf, with_O=False)
+        assert abs(vals[o, 0] - lo.real.mean()) < tol * max(1.0, abs(lo.real.mean()))
+        assert abs(vals[o, 1] - lo.imag.mean()) < tol * max(1.0, abs(lo.real.mean()))
