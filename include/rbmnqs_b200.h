@@ -123,6 +123,15 @@ typedef struct {
                                   minresqlp (MINRES from x0 = 0; rtol is then
                                   the relative residual, max_iterations
                                   defaults to 4 n_params) */
+    int32_t optimizer_type;    /* optimizer.type: 0 = SR, 1 = SGD
+                                  (gradient_descent.cpp:42-60) */
+    double sgd_real_factor;    /* optimizer.sgd.real_factor */
+    int32_t plugin;            /* optimizer.plugin: 0 none, 1 adam, 2 momentum,
+                                  3 heun (plugin.cpp:29-115; heun samples
+                                  and solves a second time every epoch) */
+    double adam_beta1, adam_beta2, adam_eps;  /* optimizer.adam.* */
+    double mom_alpha, mom_dialup;             /* optimizer.mom.* */
+    double heun_eps;                          /* optimizer.heun.eps */
 } rbmnqs_config;
 
 /* Fills the reference defaults (src/tools/ini.cpp:38-120). */

@@ -515,6 +515,90 @@ class Decay:
         return self.value
 
 
+class AdamPlugin:
+    """adam_plugin (optimizer/plugin.cpp:29-59): first moment complex, second
+    moment split into real and imaginary parts, bias-corrected with t counted
+    from 1; the result is scaled by lr."""
+
+    def __init__(self, P, beta1=0.9, beta2=0.999, eps=1e-8):
+        self.b1, self.b2, self.eps, self.t = beta1, beta2, eps, 1
+        self.m = np.zeros(P, np.complex128)
+        self.wr = np.zeros(P)
+        self.wi = np.zeros(P)
+
+    def apply(self, dw, lr):
+        self.m = self.b1 * self.m + (1 - self.b1) * dw
+        self.wr = self.b2 * self.wr + (1 - self.b2) * dw.real ** 2
+        self.wi = self.b2 * self.wi + (1 - self.b2) * dw.imag ** 2
+        m = self.m / (1 - self.b1 ** self.t)
+        wr = self.wr / (1 - self.b2 ** self.t)
+        wi = self.wi / (1 - self.b2 ** self.t)
+        self.t += 1
+        out = m.real / (np.sqrt(wr) + self.eps) + 1j * (m.imag / (np.sqrt(wi) + self.eps))
+        return out * lr
+
+
+class MomentumPlugin:
+    """momentum_plugin (optimizer/plugin.cpp:61-85): a zero momentum starts at
+    dw; with dialup != 1 the momentum factor ramps up as alpha * dup, dup
+    starting at 1e-3 and multiplied by dialup every step until it reaches 1."""
+
+    def __init__(self, P, alpha=0.9, dialup=1.0):
+        self.alpha, self.dialup = alpha, dialup
+        self.dup = 1.0 if dialup == 1.0 else 1e-3
+        self.m = np.zeros(P, np.complex128)
+
+    def apply(self, dw, lr):
+        ax = self.alpha
+        if np.all(np.abs(self.m) <= 1e-12):
+            self.m = dw.copy()
+        if self.dup < 1.0:
+            self.dup *= self.dialup
+            ax *= self.dup
+        self.m = ax * self.m + (1 - ax) * dw
+        return lr * self.m
+
+
+def heun_begin(x1, lr):
+    """heun_plugin::apply (optimizer/plugin.cpp:87-91), first half: the
+    weights move by delta = (lr/2) x1 (update_weights_nc, no update counted)
+    before the second sample; returns delta."""
+    return 0.5 * lr * x1
+
+
+def heun_finish(delta, x2, lr, eps, O=None, d=None):
+    """heun_plugin::apply (optimizer/plugin.cpp:92-115), second half, with x2
+    the step direction of the second gradient() call.  SR registers the
+    metric (O of the second sample, <O>; stochastic_reconfiguration.cpp:
+    111-113), giving err = sqrt(sum_s |sum_k delta_k O_sk - d.delta|^2) / P;
+    SGD has none, giving err = |delta|.  Returns the step x2 (cbrt(eps/err)
+    - 1/2) lr."""
+    delta = (delta - 0.5 * lr * x2) / 6
+    if O is not None:
+        e = np.asarray(O) @ delta - np.dot(d, delta)
+        err = np.sqrt(np.sum(np.abs(e) ** 2)) / delta.size
+    else:
+        err = np.linalg.norm(delta)
+    xx = (eps / err) ** (1.0 / 3)
+    return x2 * ((xx - 0.5) * lr)
+
+
+def sgd_direction(F, real_factor=1.0):
+    """gradient_descent::gradient (optimizer/gradient_descent.cpp:42-60): the
+    SR force F = <conj(O) E> - conj(<O>) <E> with its real part divided by
+    real_factor."""
+    F = _c128(F)
+    return F.real / real_factor + 1j * F.imag
+
+
+def optimize_tail(dw, lr, plugin=None):
+    """abstract_optimizer::optimize tail (abstract_optimizer.cpp:157-176): None
+    when max|dw| > 30 (no update), else the plugin's step or lr * dw."""
+    if np.max(np.abs(dw)) > 30:
+        return None
+    return plugin.apply(dw, lr) if plugin is not None else dw * lr
+
+
 def pf_context(machine, spins):
     n = machine.n
     inv = np.zeros(n * n, np.complex128)

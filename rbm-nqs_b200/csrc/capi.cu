@@ -147,6 +147,11 @@ struct rbmnqs_handle {
     DevBuf<rbmnqs::MachineDev> mdev;
     DevBuf<rbmnqs::HamDev> hdev;
     DevBuf<rbmnqs::CgResultDev> cgres;
+    // update plugin (adam / momentum) state
+    DevBuf<rbmnqs::PluginDev> plug;
+    DevBuf<double2> plug_m;
+    DevBuf<double> plug_wr, plug_wi, plug_part;
+    DevBuf<rbmnqs::EpochStatsDev> stats_first;
     DevBuf<rbmnqs::EpochStatsDev> stats;
     // matrix-free SR (n_params above the dense limit): no S is formed
     bool mfree = false;
@@ -326,30 +331,59 @@ struct rbmnqs_handle {
             ck(net->train_step(spins.p, ltgt.p, cfg.n_chains, (float)cfg.learned_lr, st, lloss.p, true),
                "proposal training");
     }
-    void enqueue_sample() {
+    // tm: record the stage timing events (off for the second sample of a
+    // Heun step, which runs inside the optimisation stage)
+    void enqueue_sample(bool tm = true) {
         const rbmnqs::SamplerArgs a = sampler_args();
-        mark(0);
+        if (tm) mark(0);
         if (net)
             enqueue_learned_sampling();
         else
             ck(rbmnqs::launch_sampler(a, fp64, shape, st), "sampler kernel");
-        mark(1);
+        if (tm) mark(1);
         // E_loc and O_k of every sample (local_op::evaluate, derivative)
         ck(rbmnqs::launch_eval(eval_args(), fp64, wpb, st), "eval kernel");
-        mark(2);
+        if (tm) mark(2);
         ck(rbmnqs::launch_moments(O.p, fp64, E.p, N, P, mom_blocks, pd.p, pf.p, pe.p, d.p, F.p, emean.p, st),
            "moments");
         ck(rbmnqs::launch_energy_stats(E.p, N, n_bins, emean.p, nacc.p, nprop.p, cfg.n_chains, stats.p, st),
            "energy stats");
         if (net) enqueue_learned_training();
         ck(rbmnqs::launch_advance(ctl.p, cfg.reinit_chains, st), "advance");
-        mark(3);
+        if (tm) mark(3);
     }
     // cg_after / cg_done: optional events ordering the matrix-free CG (a
     // cooperative launch) after another session's, so that two grid-wide
     // solves never compete for residency inside one batch graph.
     void enqueue_optimize(cudaEvent_t cg_after = nullptr, cudaEvent_t cg_done = nullptr) {
         ck(rbmnqs::launch_schedule(sched.p, st), "schedule");
+        if (cfg.plugin != 3) {
+            enqueue_solve(cg_after, cg_done, true);
+            ck(rbmnqs::launch_update(params.p, x.p, P, sched.p, cgres.p, plug.p, st), "update");
+        } else {
+            // heun_plugin::apply (plugin.cpp:87-115): half step, second
+            // sample and gradient() (the regularisation schedules decay
+            // again, the learning rate does not), then the combined step.
+            // The sample statistics reported are the first sample's.
+            enqueue_solve(cg_after, nullptr, true);
+            ck(rbmnqs::launch_heun_begin(params.p, x.p, P, sched.p, cgres.p, plug.p, st), "heun");
+            ck(rbmnqs::launch_unpack(params.p, n, n_vb, nh, vb.p, hb.p, W64.p, W32.p, st), "unpack");
+            ck(cudaMemcpyAsync(stats_first.p, stats.p, sizeof(rbmnqs::EpochStatsDev), cudaMemcpyDeviceToDevice, st),
+               "copy");
+            enqueue_sample(false);
+            ck(cudaMemcpyAsync(stats.p, stats_first.p, sizeof(rbmnqs::EpochStatsDev), cudaMemcpyDeviceToDevice, st),
+               "copy");
+            if (cfg.optimizer_type == 0) ck(rbmnqs::launch_schedule_regs(sched.p, st), "schedule");
+            enqueue_solve(nullptr, cg_done, false);
+            ck(rbmnqs::launch_heun_finish(params.p, x.p, P, sched.p, cgres.p, plug.p, O.p, fp64, d.p, N,
+                                          cfg.optimizer_type == 0, st),
+               "heun");
+        }
+        ck(rbmnqs::launch_unpack(params.p, n, n_vb, nh, vb.p, hb.p, W64.p, W32.p, st), "unpack");
+        mark(6);
+    }
+    // the step direction x: SR solve (warm start x) or the SGD gradient
+    void enqueue_solve(cudaEvent_t cg_after, cudaEvent_t cg_done, bool tm) {
         int max_it = std::min(2 * P, cfg.max_iterations);
         if (max_it == 0) max_it = 2 * P;
         double rtol = cfg.rtol == 0 ? 1e-16 : cfg.rtol;
@@ -357,16 +391,24 @@ struct rbmnqs_handle {
             max_it = cfg.max_iterations > 0 ? cfg.max_iterations : 4 * P;
             rtol = cfg.rtol > 0 ? cfg.rtol : 1e-16;
         }
-        if (mfree) {
+        auto mk = [&](int i) {
+            if (tm) mark(i);
+        };
+        if (cfg.optimizer_type == 1) {
+            // SGD: the gradient itself is the step direction
+            mk(4);
+            ck(rbmnqs::launch_sgd_direction(F.p, x.p, P, cfg.sgd_real_factor, cgres.p, st), "sgd direction");
+            mk(5);
+        } else if (mfree) {
             // diag = var(O) straight from O; CG on the operator (cg_solver.cpp aprod)
             ck(rbmnqs::launch_var_diag(O.p, fp64, d.p, N, P, mfp, mfw, diag.p, maxdiag.p, st), "var diag");
-            mark(4);
+            mk(4);
             if (cg_after) ck(cudaStreamWaitEvent(st, cg_after, 0), "cg order");
             ck(rbmnqs::launch_cg_mfree(O.p, fp64, d.p, (double)N, N, P, P_neural, F.p, x.p, diag.p, maxdiag.p,
                                        sched.p, 0, 0, 0, max_it, rtol, mfp, mfw, cgres.p, st),
                "matrix-free cg");
             if (cg_done) ck(cudaEventRecord(cg_done, st), "cg order");
-            mark(5);
+            mk(5);
         } else {
             if (gram_tc)
                 ck(rbmnqs::launch_gram_tc(gtc, O.p, fp64, d.p, gpart.p, gerr.p, Sm.p, st), "tensor-core gram");
@@ -374,7 +416,7 @@ struct rbmnqs_handle {
                 ck(rbmnqs::launch_gram_fp64(O.p, fp64, d.p, N, P, gram_ks, part.p, Sm.p, st), "gram");
             ck(rbmnqs::launch_regularize(Sm.p, P, P_neural, N, sched.p, diag.p, Sreg.p, maxdiag.p, st),
                "regularize");
-            mark(4);
+            mk(4);
             if (coop_dense && cg_after) ck(cudaStreamWaitEvent(st, cg_after, 0), "cg order");
             if (coop_dense || cfg.solver == 1)
                 ck(rbmnqs::launch_cg_dense_coop(Sreg.p, F.p, x.p, P, max_it, rtol, mfp, mfw, cgres.p, st),
@@ -382,17 +424,12 @@ struct rbmnqs_handle {
             else
                 ck(rbmnqs::launch_cg(Sreg.p, F.p, x.p, P, max_it, rtol, cgres.p, st), "cg");
             if (coop_dense && cg_done) ck(cudaEventRecord(cg_done, st), "cg order");
-            mark(5);
+            mk(5);
         }
-        ck(rbmnqs::launch_update(params.p, x.p, P, sched.p, cgres.p, st), "update");
-        ck(rbmnqs::launch_unpack(params.p, n, n_vb, nh, vb.p, hb.p, W64.p, W32.p, st), "unpack");
-        mark(6);
     }
     void collect_timing(int first, int last) {
         if (!timing) return;
         ck(cudaEventSynchronize(ev[last]), "event sync");
-        const int stage_of[kStages] = {0, 1, 2, 3, 4, 5};
-        (void)stage_of;
         for (int i = first; i < last; i++) {
             float ms = 0;
             ck(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]), "elapsed");
@@ -537,6 +574,15 @@ int rbmnqs_config_default(rbmnqs_config* c) {
         c->learned_hidden = 256;
         c->learned_lr = 1e-3;
         c->solver = 0;
+        c->optimizer_type = 0;
+        c->sgd_real_factor = 1.0;
+        c->plugin = 0;
+        c->adam_beta1 = 0.9;
+        c->adam_beta2 = 0.999;
+        c->adam_eps = 1e-8;
+        c->mom_alpha = 0.9;
+        c->mom_dialup = 1.0;
+        c->heun_eps = 1e-3;
     });
 }
 
@@ -745,6 +791,41 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         h->maxdiag.alloc(1);
         h->sched.alloc(1);
         h->cgres.alloc(1);
+        {
+            require(cfg->optimizer_type == 0 || cfg->optimizer_type == 1, "optimizer.type must be 0 (SR) or 1 (SGD)");
+            require(cfg->plugin >= 0 && cfg->plugin <= 3,
+                    "optimizer.plugin must be 0, 1 (adam), 2 (momentum) or 3 (heun)");
+            require(cfg->plugin != 3 || cfg->heun_eps > 0, "optimizer.heun.eps must be positive");
+            require(cfg->sgd_real_factor != 0, "optimizer.sgd.real_factor must be nonzero");
+            rbmnqs::PluginDev pd{};
+            pd.type = cfg->plugin;
+            pd.beta1 = cfg->adam_beta1;
+            pd.beta2 = cfg->adam_beta2;
+            pd.eps = cfg->adam_eps;
+            pd.alpha = cfg->mom_alpha;
+            pd.dialup = cfg->mom_dialup;
+            pd.dup = cfg->mom_dialup == 1.0 ? 1.0 : 1e-3;  // plugin.cpp:64
+            pd.t = 1;
+            pd.heps = cfg->heun_eps;
+            if (cfg->plugin == 3) {
+                h->plug_part.alloc(rbmnqs::kHeunBlocks);
+                h->stats_first.alloc(1);
+                pd.part = h->plug_part.p;
+            }
+            if (cfg->plugin) {
+                h->plug_m.alloc(h->P);
+                h->plug_wr.alloc(h->P);
+                h->plug_wi.alloc(h->P);
+                ck(cudaMemsetAsync(h->plug_m.p, 0, h->P * sizeof(double2), h->st), "memset");
+                ck(cudaMemsetAsync(h->plug_wr.p, 0, h->P * sizeof(double), h->st), "memset");
+                ck(cudaMemsetAsync(h->plug_wi.p, 0, h->P * sizeof(double), h->st), "memset");
+                pd.m = h->plug_m.p;
+                pd.wr = h->plug_wr.p;
+                pd.wi = h->plug_wi.p;
+            }
+            h->plug.alloc(1);
+            ck(cudaMemcpyAsync(h->plug.p, &pd, sizeof(pd), cudaMemcpyHostToDevice, h->st), "copy");
+        }
         h->stats.alloc(1);
         // decay_t schedules with the n_updates offset
         h->n_updates = cfg->n_updates;

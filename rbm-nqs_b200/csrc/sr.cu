@@ -250,8 +250,8 @@ __global__ void gram_finalize(const double2* part, int nks, int N, int P, double
 
 // ------------------------------------------------------ schedule / reg ---
 // decay_t::get for the four schedules (abstract_optimizer.cpp:27-54).
-__global__ void schedule_step(ScheduleDev* s) {
-    if (threadIdx.x < 4) {
+__global__ void schedule_step(ScheduleDev* s, int first) {
+    if (threadIdx.x >= first && threadIdx.x < 4) {
         const int i = threadIdx.x;
         if (!s->min_reached[i]) {
             s->value[i] *= s->decay[i];
@@ -708,9 +708,11 @@ __global__ void __cluster_dims__(kClusterCta, 1, 1) __launch_bounds__(256)
 }
 
 // ---------------------------------------------------------------- update --
-// abstract_optimizer::optimize tail (abstract_optimizer.cpp:157-176):
-// abort on max|x| > 30, else x *= lr (the next warm start) and w -= x.
-__global__ void sr_update(double2* params, double2* x, int P, const ScheduleDev* sch, CgResultDev* res) {
+// abstract_optimizer::optimize tail (abstract_optimizer.cpp:150-177): the
+// max|dw| > 30 guard, then the plugin (plugin.cpp:43-85) or dw *= lr, then
+// w -= dw (rbm_base.cpp:117-131).  x keeps dw as the next warm start.
+__global__ void sr_update(double2* params, double2* x, int P, const ScheduleDev* sch, CgResultDev* res,
+                          PluginDev* plug) {
     __shared__ double red[32];
     if (res->status == -2) return;  // the solve itself failed (matrix-free CG barrier timeout)
     double mx = 0;
@@ -729,14 +731,217 @@ __global__ void sr_update(double2* params, double2* x, int P, const ScheduleDev*
     }
     if (status != 0) return;
     const double lr = sch->value[0];
+    const int type = plug ? plug->type : 0;
+    if (type == 1) {
+        // adam_plugin::apply: second moment split into real and imaginary parts
+        const int t = plug->t;
+        const double b1 = plug->beta1, b2 = plug->beta2, eps = plug->eps;
+        const double c1 = 1.0 - pow(b1, (double)t), c2 = 1.0 - pow(b2, (double)t);
+        for (int i = threadIdx.x; i < P; i += blockDim.x) {
+            const double2 g = x[i];
+            double2 m = plug->m[i];
+            m = make_double2(b1 * m.x + (1 - b1) * g.x, b1 * m.y + (1 - b1) * g.y);
+            const double wr = b2 * plug->wr[i] + (1 - b2) * g.x * g.x;
+            const double wi = b2 * plug->wi[i] + (1 - b2) * g.y * g.y;
+            plug->m[i] = m;
+            plug->wr[i] = wr;
+            plug->wi[i] = wi;
+            x[i] = make_double2((m.x / c1) / (sqrt(wr / c2) + eps) * lr, (m.y / c1) / (sqrt(wi / c2) + eps) * lr);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) plug->t = t + 1;
+    } else if (type == 2) {
+        // momentum_plugin::apply: a momentum that is zero (every |m_i| <=
+        // 1e-12, Eigen's isZero) starts at dw
+        double nz = 0;
+        for (int i = threadIdx.x; i < P; i += blockDim.x) {
+            const double2 m = plug->m[i];
+            if (m.x * m.x + m.y * m.y > 1e-24) nz = 1;
+        }
+        nz = block_max(nz, red);
+        double ax = plug->alpha;
+        const double dup = plug->dup;
+        double dnew = dup;
+        if (dup < 1.0) {
+            dnew = dup * plug->dialup;
+            ax *= dnew;
+        }
+        for (int i = threadIdx.x; i < P; i += blockDim.x) {
+            const double2 g = x[i];
+            const double2 m0 = nz > 0 ? plug->m[i] : g;
+            const double2 m = make_double2(ax * m0.x + (1 - ax) * g.x, ax * m0.y + (1 - ax) * g.y);
+            plug->m[i] = m;
+            x[i] = make_double2(lr * m.x, lr * m.y);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) plug->dup = dnew;
+    } else {
+        for (int i = threadIdx.x; i < P; i += blockDim.x) {
+            double2 v = x[i];
+            v.x *= lr;
+            v.y *= lr;
+            x[i] = v;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        const double2 v = x[i];
+        params[i].x -= v.x;
+        params[i].y -= v.y;
+    }
+}
+
+// ------------------------------------------------------------------ heun --
+// heun_plugin::apply (plugin.cpp:87-115).  The first step guards x1 like
+// abstract_optimizer::optimize (abstract_optimizer.cpp:157), then moves the
+// weights by delta = (lr/2) x1 without counting an update (update_weights_nc).
+__global__ void heun_begin(double2* params, const double2* x, int P, const ScheduleDev* sch, CgResultDev* res,
+                           PluginDev* plug) {
+    __shared__ double red[32];
+    if (res->status == -2) {
+        if (threadIdx.x == 0) plug->gstat = -2;
+        return;
+    }
+    double mx = 0;
+    int bad = 0;
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        const double2 v = x[i];
+        if (!isfinite(v.x) || !isfinite(v.y)) bad = 1;
+        mx = fmax(mx, sqrt(v.x * v.x + v.y * v.y));
+    }
+    mx = block_max(mx, red);
+    const double nbad = block_sum((double)bad, red);
+    const int status = nbad > 0 ? -5 : (mx > 30.0 ? -4 : 0);
+    if (threadIdx.x == 0) {
+        res->max_dw = mx;
+        res->status = status;
+        plug->gstat = status;
+        plug->gmax = mx;
+    }
+    if (status != 0) return;
+    const double hl = 0.5 * sch->value[0];
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        const double2 v = x[i];
+        const double2 dl = make_double2(hl * v.x, hl * v.y);
+        plug->m[i] = dl;
+        params[i].x -= dl.x;
+        params[i].y -= dl.y;
+    }
+}
+
+// delta = (delta - (lr/2) x2) / 6; dd = d^T delta (no conjugate); |delta|^2.
+__global__ void heun_delta(const double2* x, int P, const ScheduleDev* sch, const double2* d, PluginDev* plug) {
+    __shared__ double red[32];
+    if (plug->gstat != 0) return;
+    const double hl = 0.5 * sch->value[0];
+    double ddr = 0, ddi = 0, n2 = 0;
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        const double2 v = x[i];
+        const double2 m = plug->m[i];
+        const double2 dl = make_double2((m.x - hl * v.x) / 6.0, (m.y - hl * v.y) / 6.0);
+        plug->m[i] = dl;
+        if (d) {
+            const double2 a = d[i];
+            ddr += a.x * dl.x - a.y * dl.y;
+            ddi += a.x * dl.y + a.y * dl.x;
+        }
+        n2 += dl.x * dl.x + dl.y * dl.y;
+    }
+    ddr = block_sum(ddr, red);
+    ddi = block_sum(ddi, red);
+    n2 = block_sum(n2, red);
+    if (threadIdx.x == 0) {
+        plug->dd = make_double2(ddr, ddi);
+        plug->nrm2 = n2;
+    }
+}
+
+// Per block: sum over its samples s of |sum_k delta_k O_sk - dd|^2 (the
+// metric of the SR plugin hook, stochastic_reconfiguration.cpp:111-113).
+// One warp per sample; sample-major O [N][P].
+template <typename TO>
+__global__ void heun_metric(const TO* O, int N, int P, PluginDev* plug) {
+    __shared__ double red[32];
+    if (plug->gstat != 0) return;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const double2* dl = plug->m;
+    const double2 dd = plug->dd;
+    double acc = 0;
+    for (int sIdx = blockIdx.x * nw + wib; sIdx < N; sIdx += gridDim.x * nw) {
+        const TO* row = O + (size_t)sIdx * P;
+        double er = 0, ei = 0;
+        for (int k = lane; k < P; k += 32) {
+            const TO o = row[k];
+            const double2 a = dl[k];
+            er += a.x * (double)o.x - a.y * (double)o.y;
+            ei += a.x * (double)o.y + a.y * (double)o.x;
+        }
+        for (int off = 16; off; off >>= 1) {
+            er += __shfl_xor_sync(0xffffffffu, er, off);
+            ei += __shfl_xor_sync(0xffffffffu, ei, off);
+        }
+        er -= dd.x;
+        ei -= dd.y;
+        acc += er * er + ei * ei;  // identical in every lane
+    }
+    if (lane != 0) acc = 0;
+    acc = block_sum(acc, red);
+    if (threadIdx.x == 0) plug->part[blockIdx.x] = acc;
+}
+
+// err = sqrt(sum)/P (SR metric) or |delta| (SGD); dw = x2 (cbrt-like factor)
+__global__ void heun_end(double2* params, double2* x, int P, const ScheduleDev* sch, CgResultDev* res,
+                         PluginDev* plug, int metric) {
+    if (plug->gstat != 0) {
+        if (threadIdx.x == 0) {
+            res->status = plug->gstat;
+            res->max_dw = plug->gmax;
+        }
+        return;
+    }
+    if (res->status == -2) return;  // the second solve failed
+    double err;
+    if (metric) {
+        double sm = 0;
+        for (int b = 0; b < kHeunBlocks; b++) sm += plug->part[b];  // fixed order
+        err = sqrt(sm) / (double)P;
+    } else {
+        err = sqrt(plug->nrm2);
+    }
+    const double xx = pow(plug->heps / err, 1.0 / 3.0);
+    const double f = (xx - 0.5) * sch->value[0];
     for (int i = threadIdx.x; i < P; i += blockDim.x) {
         double2 v = x[i];
-        v.x *= lr;
-        v.y *= lr;
+        v.x *= f;
+        v.y *= f;
         x[i] = v;
         params[i].x -= v.x;
         params[i].y -= v.y;
     }
+    if (threadIdx.x == 0) {
+        res->status = 0;
+        res->max_dw = plug->gmax;
+    }
+}
+
+cudaError_t launch_heun_begin(double2* params, const double2* x, int P, const ScheduleDev* sch, CgResultDev* res,
+                              PluginDev* plug, cudaStream_t st) {
+    heun_begin<<<1, 1024, 0, st>>>(params, x, P, sch, res, plug);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_heun_finish(double2* params, double2* x, int P, const ScheduleDev* sch, CgResultDev* res,
+                               PluginDev* plug, const void* O, int fp64, const double2* d, int N, int metric,
+                               cudaStream_t st) {
+    heun_delta<<<1, 1024, 0, st>>>(x, P, sch, metric ? d : nullptr, plug);
+    if (metric) {
+        if (fp64)
+            heun_metric<double2><<<kHeunBlocks, 256, 0, st>>>(static_cast<const double2*>(O), N, P, plug);
+        else
+            heun_metric<float2><<<kHeunBlocks, 256, 0, st>>>(static_cast<const float2*>(O), N, P, plug);
+    }
+    heun_end<<<1, 1024, 0, st>>>(params, x, P, sch, res, plug, metric);
+    return cudaGetLastError();
 }
 
 // Parameter vector -> kernel layouts (site-major W in FP64 and FP32).
@@ -811,7 +1016,12 @@ cudaError_t launch_gram_fp64(const void* O, int fp64, const double2* d, int N, i
 }
 
 cudaError_t launch_schedule(ScheduleDev* s, cudaStream_t st) {
-    schedule_step<<<1, 32, 0, st>>>(s);
+    schedule_step<<<1, 32, 0, st>>>(s, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_schedule_regs(ScheduleDev* s, cudaStream_t st) {
+    schedule_step<<<1, 32, 0, st>>>(s, 1);
     return cudaGetLastError();
 }
 
@@ -852,7 +1062,31 @@ cudaError_t launch_cg(const double2* A, const double2* b, double2* x, int P, int
 
 cudaError_t launch_update(double2* params, double2* x, int P, const ScheduleDev* sch, CgResultDev* res,
                           cudaStream_t st) {
-    sr_update<<<1, 1024, 0, st>>>(params, x, P, sch, res);
+    sr_update<<<1, 1024, 0, st>>>(params, x, P, sch, res, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_update(double2* params, double2* x, int P, const ScheduleDev* sch, CgResultDev* res,
+                          PluginDev* plug, cudaStream_t st) {
+    sr_update<<<1, 1024, 0, st>>>(params, x, P, sch, res, plug);
+    return cudaGetLastError();
+}
+
+__global__ void sgd_direction(const double2* F, double2* x, int P, double real_factor, CgResultDev* res) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
+        const double2 f = F[i];
+        x[i] = make_double2(f.x / real_factor, f.y);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        res->iterations = 0;
+        res->residual = 0;
+        res->status = 0;
+    }
+}
+
+cudaError_t launch_sgd_direction(const double2* F, double2* x, int P, double real_factor, CgResultDev* res,
+                                 cudaStream_t st) {
+    sgd_direction<<<(P + 255) / 256, 256, 0, st>>>(F, x, P, real_factor, res);
     return cudaGetLastError();
 }
 

@@ -45,6 +45,41 @@ cudaError_t launch_regularize(const double2* S, int P, int n_neural, int N, cons
                               double2* Sreg, double* max_diag, cudaStream_t st);
 cudaError_t launch_cg(const double2* A, const double2* b, double2* x, int P, int max_it, double rtol,
                       CgResultDev* res, cudaStream_t st);
+// Update-step plugins (optimizer/plugin.cpp:29-115): state on the device.
+struct PluginDev {
+    int type;            // 0 none, 1 adam, 2 momentum, 3 heun
+    double beta1, beta2, eps;  // adam
+    double alpha, dialup;      // momentum
+    double dup;                // momentum dial-up factor state
+    int t;                     // adam step counter (starts at 1)
+    double2* m;                // [P] first moment / momentum / heun delta
+    double* wr;                // [P] adam second moment, real parts
+    double* wi;                // [P] adam second moment, imaginary parts
+    // heun
+    double heps;               // optimizer.heun.eps
+    int gstat;                 // guard status of the first step
+    double gmax;               // its max |dw|
+    double2 dd;                // d^T delta
+    double nrm2;               // |delta|^2
+    double* part;              // [kHeunBlocks] partial sums of |O delta - d^T delta|^2
+};
+constexpr int kHeunBlocks = 296;
+// heun_plugin::apply (plugin.cpp:87-115) around a second sample + solve:
+// begin: guard on x1, delta = lr/2 x1, w -= delta;
+// finish: delta = (delta - lr/2 x2) / 6, err from O (metric, SR) or |delta|
+// (SGD), x = x2 (cbrt(eps / err) - 1/2) lr, w -= x.
+cudaError_t launch_heun_begin(double2* params, const double2* x, int P, const ScheduleDev* sch, CgResultDev* res,
+                              PluginDev* plug, cudaStream_t st);
+cudaError_t launch_heun_finish(double2* params, double2* x, int P, const ScheduleDev* sch, CgResultDev* res,
+                               PluginDev* plug, const void* O, int fp64, const double2* d, int N, int metric,
+                               cudaStream_t st);
+// decay the regularisation schedules only (a second gradient() call)
+cudaError_t launch_schedule_regs(ScheduleDev* s, cudaStream_t st);
+// SGD direction (gradient_descent.cpp:42-60): x = F with Re(x) / real_factor
+cudaError_t launch_sgd_direction(const double2* F, double2* x, int P, double real_factor, CgResultDev* res,
+                                 cudaStream_t st);
+cudaError_t launch_update(double2* params, double2* x, int P, const ScheduleDev* sch, CgResultDev* res,
+                          PluginDev* plug, cudaStream_t st);
 cudaError_t launch_update(double2* params, double2* x, int P, const ScheduleDev* sch, CgResultDev* res,
                           cudaStream_t st);
 // Matrix-free CG (cg_mfree.cu) for parameter counts without a formed S.

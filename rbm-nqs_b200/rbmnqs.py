@@ -41,6 +41,9 @@ class Config(C.Structure):
         ("precision", C.c_int32), ("n_updates", C.c_int32), ("gram", C.c_int32),
         ("proposal", C.c_int32), ("learned_steps", C.c_int32), ("learned_train", C.c_int32),
         ("learned_hidden", C.c_int32), ("learned_lr", C.c_double), ("solver", C.c_int32),
+        ("optimizer_type", C.c_int32), ("sgd_real_factor", C.c_double), ("plugin", C.c_int32),
+        ("adam_beta1", C.c_double), ("adam_beta2", C.c_double), ("adam_eps", C.c_double),
+        ("mom_alpha", C.c_double), ("mom_dialup", C.c_double), ("heun_eps", C.c_double),
     ]
 
 
