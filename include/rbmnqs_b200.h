@@ -122,7 +122,10 @@ typedef struct {
     int32_t solver;            /* optimizer.sr.method: 0 = cg (cg_solver), 1 =
                                   minresqlp (MINRES from x0 = 0; rtol is then
                                   the relative residual, max_iterations
-                                  defaults to 4 n_params) */
+                                  defaults to 4 n_params), 2 = direct
+                                  (direct_solver.cpp:31-59: multiplicative
+                                  diagonal regularisation, exact solve;
+                                  n_params <= 2048) */
     int32_t optimizer_type;    /* optimizer.type: 0 = SR, 1 = SGD
                                   (gradient_descent.cpp:42-60) */
     double sgd_real_factor;    /* optimizer.sgd.real_factor */

@@ -496,6 +496,25 @@ def minres_solve(O, d, F, r1, r2, rd, diag, n_neural=None, max_iterations=0, rto
     return x, it, rn.value
 
 
+def direct_solve(O, d, F, r1, r2, rd, diag, n_neural=None, norm=None):
+    """direct_solver::solve (optimizer/direct_solver.cpp:31-59): S =
+    conj(O)^T O / norm - conj(d) d^T, the diagonal scaled by (1 + r1)
+    ((1 + r1) + rd on non-neural parameters), plus r2 max|diag| I, solved
+    for the minimum-norm least-squares x (what Eigen's complete orthogonal
+    decomposition returns)."""
+    O = _c128(O)
+    N, P = O.shape
+    nn = P if n_neural is None else n_neural
+    S = O.conj().T @ O / float(N if norm is None else norm)
+    S -= np.outer(np.conj(d), d)
+    idx = np.arange(P)
+    S[idx[:nn], idx[:nn]] *= 1 + r1
+    if P > nn:
+        S[idx[nn:], idx[nn:]] *= 1 + r1 + rd
+    S[idx, idx] += r2 * np.max(np.abs(diag))
+    return np.linalg.lstsq(S, _c128(F), rcond=None)[0]
+
+
 class Decay:
     """decay_t (abstract_optimizer.cpp:27-54): decays before first use."""
 

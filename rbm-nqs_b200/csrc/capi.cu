@@ -152,6 +152,9 @@ struct rbmnqs_handle {
     DevBuf<double2> plug_m;
     DevBuf<double> plug_wr, plug_wi, plug_part;
     DevBuf<rbmnqs::EpochStatsDev> stats_first;
+    // direct solver: barrier state and triangular-solve work vector
+    DevBuf<rbmnqs::MfreeSync> dsync;
+    DevBuf<double2> dwork;
     DevBuf<rbmnqs::EpochStatsDev> stats;
     // matrix-free SR (n_params above the dense limit): no S is formed
     bool mfree = false;
@@ -382,6 +385,8 @@ struct rbmnqs_handle {
         ck(rbmnqs::launch_unpack(params.p, n, n_vb, nh, vb.p, hb.p, W64.p, W32.p, st), "unpack");
         mark(6);
     }
+    // solves that are cooperative launches (ordered one after another in a batch graph)
+    bool coop_solve() const { return mfree || coop_dense || cfg.solver == 2; }
     // the step direction x: SR solve (warm start x) or the SGD gradient
     void enqueue_solve(cudaEvent_t cg_after, cudaEvent_t cg_done, bool tm) {
         int max_it = std::min(2 * P, cfg.max_iterations);
@@ -414,16 +419,20 @@ struct rbmnqs_handle {
                 ck(rbmnqs::launch_gram_tc(gtc, O.p, fp64, d.p, gpart.p, gerr.p, Sm.p, st), "tensor-core gram");
             else
                 ck(rbmnqs::launch_gram_fp64(O.p, fp64, d.p, N, P, gram_ks, part.p, Sm.p, st), "gram");
-            ck(rbmnqs::launch_regularize(Sm.p, P, P_neural, N, sched.p, diag.p, Sreg.p, maxdiag.p, st),
+            ck(rbmnqs::launch_regularize(Sm.p, P, P_neural, N, sched.p, diag.p, Sreg.p, maxdiag.p, st,
+                                         cfg.solver == 2),
                "regularize");
             mk(4);
-            if (coop_dense && cg_after) ck(cudaStreamWaitEvent(st, cg_after, 0), "cg order");
-            if (coop_dense || cfg.solver == 1)
+            const bool coop = coop_solve();
+            if (coop && cg_after) ck(cudaStreamWaitEvent(st, cg_after, 0), "cg order");
+            if (cfg.solver == 2)
+                ck(rbmnqs::launch_direct_solve(Sreg.p, F.p, x.p, P, dwork.p, dsync.p, cgres.p, st), "direct solve");
+            else if (coop_dense || cfg.solver == 1)
                 ck(rbmnqs::launch_cg_dense_coop(Sreg.p, F.p, x.p, P, max_it, rtol, mfp, mfw, cgres.p, st),
                    "cooperative solve");
             else
                 ck(rbmnqs::launch_cg(Sreg.p, F.p, x.p, P, max_it, rtol, cgres.p, st), "cg");
-            if (coop_dense && cg_done) ck(cudaEventRecord(cg_done, st), "cg order");
+            if (coop && cg_done) ck(cudaEventRecord(cg_done, st), "cg order");
             mk(5);
         }
     }
@@ -760,8 +769,15 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         h->F.alloc(h->P);
         h->emean.alloc(1);
         h->gram_tc = !h->fp64 && cfg->gram == 0 && !h->mfree;
-        require(cfg->solver == 0 || cfg->solver == 1, "solver must be 0 (cg) or 1 (minresqlp)");
-        h->coop_dense = !h->mfree && (!rbmnqs::cg_cluster_fits(h->P) || cfg->solver == 1);
+        require(cfg->solver >= 0 && cfg->solver <= 2, "solver must be 0 (cg), 1 (minresqlp) or 2 (direct)");
+        require(cfg->solver != 2 || !h->mfree,
+                "the direct solver needs the formed S (at most " + std::to_string(kDenseMax) + " parameters)",
+                RBMNQS_ERR_UNSUPPORTED);
+        h->coop_dense = !h->mfree && cfg->solver != 2 && (!rbmnqs::cg_cluster_fits(h->P) || cfg->solver == 1);
+        if (cfg->solver == 2) {
+            h->dsync.alloc(1);
+            h->dwork.alloc(h->P);
+        }
         if (h->mfree || h->coop_dense) {
             const int nn = h->mfree ? h->N : 1;
             ck(rbmnqs::mfree_plan(nn, h->P, &h->mfp), "cooperative CG plan");
@@ -1201,10 +1217,12 @@ int rbmnqs_sr_solve(rbmnqs_handle* h, const double* O, int32_t N, const double* 
         if (max_it == 0) max_it = 2 * P;
         double rtol = h->cfg.rtol == 0 ? 1e-16 : h->cfg.rtol;
         const bool minres = h->cfg.solver == 1;
+        const bool direct = h->cfg.solver == 2;
         if (minres) {
             max_it = h->cfg.max_iterations > 0 ? h->cfg.max_iterations : 4 * P;
             rtol = h->cfg.rtol > 0 ? h->cfg.rtol : 1e-16;
         }
+        require(!direct || P <= kDenseMax, "the direct solver needs the formed S", RBMNQS_ERR_UNSUPPORTED);
         if (P > kDenseMax) {
             // the operator form (cg_solver.cpp aprod) on the given O, d, norm
             rbmnqs::MfreePlan pl{};
@@ -1225,9 +1243,17 @@ int rbmnqs_sr_solve(rbmnqs_handle* h, const double* O, int32_t N, const double* 
             const int ks = rbmnqs::gram_splits(N, P);
             part.alloc((size_t)ks * P * P);
             ck(rbmnqs::launch_gram_fp64(dO.p, 1, nullptr, N, P, ks, part.p, G.p, h->st), "gram");
-            ck(rbmnqs::launch_solve_prep(G.p, N, norm, dd.p, ddiag.p, P, h->P_neural, r1, r2, rd, Sreg.p, h->st),
+            ck(rbmnqs::launch_solve_prep(G.p, N, norm, dd.p, ddiag.p, P, h->P_neural, r1, r2, rd, Sreg.p, h->st,
+                                         direct),
                "prep");
-            if (minres) {
+            if (direct) {
+                DevBuf<double2> wk;
+                DevBuf<rbmnqs::MfreeSync> sy;
+                wk.alloc(P);
+                sy.alloc(1);
+                ck(rbmnqs::launch_direct_solve(Sreg.p, dF.p, dx.p, P, wk.p, sy.p, res.p, h->st), "direct solve");
+                ck(cudaStreamSynchronize(h->st), "sync");  // before wk, sy go out of scope
+            } else if (minres) {
                 rbmnqs::MfreePlan pl{};
                 ck(rbmnqs::mfree_plan(1, P, &pl), "cooperative plan");
                 DevBuf<unsigned char> wb;
@@ -1546,7 +1572,7 @@ int rbmnqs_batch_epoch(rbmnqs_batch* b, rbmnqs_sample_stats* s, rbmnqs_sr_stats*
                     rbmnqs_handle* h = b->hs[i];
                     ck(cudaStreamWaitEvent(h->st, b->fork, 0), "fork wait");
                     h->enqueue_sample();
-                    if (h->mfree || h->coop_dense) {
+                    if (h->coop_solve()) {
                         h->enqueue_optimize(prev_cg, b->cg_done[i]);
                         prev_cg = b->cg_done[i];
                     } else {

@@ -15,6 +15,7 @@
 #include <cooperative_groups.h>
 
 #include "common.cuh"
+#include "coop.cuh"
 #include "sr.cuh"
 
 namespace rbmnqs {
@@ -22,7 +23,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kColTile = 64;  // columns per block in the O^H v pass (4 row groups)
-constexpr uint32_t kBarrierSpin = 1u << 24;
 
 __device__ __forceinline__ double2 zld(const float2* O, size_t i) {
     const float2 v = __ldg(O + i);
@@ -33,39 +33,6 @@ __device__ __forceinline__ double2 zld(const double2* O, size_t i) { return __ld
 // Data written by other blocks of the same launch is read through L2
 // (ld.global.cg): the SMs' L1 caches are not coherent with each other.
 template <typename T> __device__ __forceinline__ T cg_ld(const T* p) { return __ldcg(p); }
-
-// Grid barrier with a bounded wait.  Returns false (on every thread of the
-// block) if this block gave up or another block already did.
-__device__ bool grid_barrier(MfreeSync* sync, uint32_t nblocks) {
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        ok = 1;
-        volatile uint32_t* gen = &sync->gen;
-        volatile int* bad = &sync->bad;
-        const uint32_t g = *gen;
-        __threadfence();
-        if (atomicAdd(&sync->count, 1u) == nblocks - 1) {
-            sync->count = 0;
-            __threadfence();
-            atomicAdd(&sync->gen, 1u);
-        } else {
-            uint32_t spins = 0;
-            while (*gen == g) {
-                if (++spins > kBarrierSpin || *bad) {
-                    ok = 0;
-                    atomicExch(&sync->bad, 1);
-                    break;
-                }
-                __nanosleep(32);
-            }
-        }
-        __threadfence();
-        if (*bad) ok = 0;
-    }
-    __syncthreads();
-    return ok != 0;
-}
 
 template <typename T> __device__ T bsum(T v, T* red);
 template <> __device__ double bsum<double>(double v, double* red) {

@@ -264,9 +264,11 @@ __global__ void schedule_step(ScheduleDev* s, int first) {
 }
 
 // diag = var(O) = N/(N-1) S_pp; S_reg = S + r1 diag (+ rd on non-neural
-// parameters) + r2 max(diag) (cg_solver.cpp:301-318).
+// parameters) + r2 max(diag) (cg_solver.cpp:301-318).  direct: S_pp (1 + r1)
+// ((1 + r1) + rd on non-neural parameters) + r2 max|diag|
+// (direct_solver.cpp:42-49).
 __global__ void regularize(const double2* S, int P, int n_neural, int N, const ScheduleDev* sch, double* diag,
-                           double2* Sreg, double* max_diag_out) {
+                           double2* Sreg, double* max_diag_out, int direct) {
     __shared__ double red[32];
     const double r1 = sch->value[1], r2 = sch->value[2], rd = sch->value[3];
     double mx = 0;
@@ -281,8 +283,13 @@ __global__ void regularize(const double2* S, int P, int n_neural, int N, const S
     for (size_t i = threadIdx.x; i < total; i += blockDim.x) Sreg[i] = S[i];
     __syncthreads();
     for (int p = threadIdx.x; p < P; p += blockDim.x) {
-        const double f = diag[p] * (p < n_neural ? r1 : r1 + rd) + mx * r2;
-        Sreg[(size_t)p * P + p].x += f;
+        double2& s = Sreg[(size_t)p * P + p];
+        if (direct) {
+            const double g = p < n_neural ? 1.0 + r1 : (1.0 + r1) + rd;
+            s = make_double2(s.x * g + r2 * mx, s.y * g);
+        } else {
+            s.x += diag[p] * (p < n_neural ? r1 : r1 + rd) + mx * r2;
+        }
     }
 }
 
@@ -290,7 +297,7 @@ __global__ void regularize(const double2* S, int P, int n_neural, int N, const S
 // conj(d) d^T + diag(r1 diag (+rd) + r2 max(diag)), where G = sum conj(O) O^T
 // was accumulated with weights already folded into O (cg_solver.cpp:301-318).
 __global__ void solve_prep(const double2* G, int N, double norm, const double2* d, const double* diag, int P,
-                           int n_neural, double r1, double r2, double rd, double2* Sreg) {
+                           int n_neural, double r1, double r2, double rd, double2* Sreg, int direct) {
     __shared__ double red[32];
     double mx = -1e300;
     for (int p = threadIdx.x; p < P; p += blockDim.x) mx = fmax(mx, diag[p]);
@@ -303,14 +310,22 @@ __global__ void solve_prep(const double2* G, int N, double norm, const double2* 
         // conj(d_k) d_l
         const double cx = dk.x * dl.x + dk.y * dl.y, cy = dk.x * dl.y - dk.y * dl.x;
         double2 v = make_double2(g.x * scale - cx, g.y * scale - cy);
-        if (k == l) v.x += diag[k] * (k < n_neural ? r1 : r1 + rd) + mx * r2;
+        if (k == l) {
+            if (direct) {
+                const double gk = k < n_neural ? 1.0 + r1 : (1.0 + r1) + rd;
+                v = make_double2(v.x * gk + r2 * mx, v.y * gk);
+            } else {
+                v.x += diag[k] * (k < n_neural ? r1 : r1 + rd) + mx * r2;
+            }
+        }
         Sreg[i] = v;
     }
 }
 
 cudaError_t launch_solve_prep(const double2* G, int N, double norm, const double2* d, const double* diag, int P,
-                              int n_neural, double r1, double r2, double rd, double2* Sreg, cudaStream_t st) {
-    solve_prep<<<1, 1024, 0, st>>>(G, N, norm, d, diag, P, n_neural, r1, r2, rd, Sreg);
+                              int n_neural, double r1, double r2, double rd, double2* Sreg, cudaStream_t st,
+                              int direct) {
+    solve_prep<<<1, 1024, 0, st>>>(G, N, norm, d, diag, P, n_neural, r1, r2, rd, Sreg, direct);
     return cudaGetLastError();
 }
 
@@ -1026,8 +1041,8 @@ cudaError_t launch_schedule_regs(ScheduleDev* s, cudaStream_t st) {
 }
 
 cudaError_t launch_regularize(const double2* S, int P, int n_neural, int N, const ScheduleDev* sch, double* diag,
-                              double2* Sreg, double* max_diag, cudaStream_t st) {
-    regularize<<<1, 1024, 0, st>>>(S, P, n_neural, N, sch, diag, Sreg, max_diag);
+                              double2* Sreg, double* max_diag, cudaStream_t st, int direct) {
+    regularize<<<1, 1024, 0, st>>>(S, P, n_neural, N, sch, diag, Sreg, max_diag, direct);
     return cudaGetLastError();
 }
 

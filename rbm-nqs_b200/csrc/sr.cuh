@@ -38,11 +38,14 @@ cudaError_t launch_mean(const double2* E, int N, double2* mu, cudaStream_t st);
 int gram_splits(int N, int P);
 cudaError_t launch_gram_fp64(const void* O, int fp64, const double2* d, int N, int P, int nks, double2* part,
                              double2* S, cudaStream_t st);
+// direct != 0: the direct solver's regularisation (direct_solver.cpp:42-49),
+// the diagonal scaled by (1 + r1) ((1 + r1) + rd) instead of adding r1 diag
 cudaError_t launch_solve_prep(const double2* G, int N, double norm, const double2* d, const double* diag, int P,
-                              int n_neural, double r1, double r2, double rd, double2* Sreg, cudaStream_t st);
+                              int n_neural, double r1, double r2, double rd, double2* Sreg, cudaStream_t st,
+                              int direct = 0);
 cudaError_t launch_schedule(ScheduleDev* s, cudaStream_t st);
 cudaError_t launch_regularize(const double2* S, int P, int n_neural, int N, const ScheduleDev* sch, double* diag,
-                              double2* Sreg, double* max_diag, cudaStream_t st);
+                              double2* Sreg, double* max_diag, cudaStream_t st, int direct = 0);
 cudaError_t launch_cg(const double2* A, const double2* b, double2* x, int P, int max_it, double rtol,
                       CgResultDev* res, cudaStream_t st);
 // Update-step plugins (optimizer/plugin.cpp:29-115): state on the device.
@@ -87,6 +90,11 @@ struct MfreeSync {
     uint32_t count, gen;
     int bad;
 };
+// Direct solve (direct.cu, direct_solver.cpp:31-59) of the regularised
+// Hermitian positive definite Sreg (P x P, overwritten by its Cholesky
+// factor): x = Sreg^-1 F.  work: P entries; sync: barrier state.
+cudaError_t launch_direct_solve(double2* Sreg, const double2* F, double2* x, int P, double2* work, MfreeSync* sync,
+                                CgResultDev* res, cudaStream_t st);
 struct MfreePlan {
     int blocks, nseg, lseg, diag_blocks;
 };
