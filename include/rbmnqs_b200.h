@@ -135,6 +135,14 @@ typedef struct {
     double adam_beta1, adam_beta2, adam_eps;  /* optimizer.adam.* */
     double mom_alpha, mom_dialup;             /* optimizer.mom.* */
     double heun_eps;                          /* optimizer.heun.eps */
+    int32_t sampler_type;      /* sampler.type: 0 = metropolis, 1 = full
+                                  (full_sampler.cpp:43-186: all 2^n states
+                                  weighted by |psi|^2; n_chains,
+                                  samples_per_chain, warmup, step and
+                                  bond_flips are unused; n_samples = 2^n) */
+    int32_t full_parallel_bits;  /* sampler.full.n_parallel_bits: the
+                                  enumeration order (blocks of the low bits,
+                                  Gray code over the rest) */
 } rbmnqs_config;
 
 /* Fills the reference defaults (src/tools/ini.cpp:38-120). */
@@ -229,6 +237,12 @@ int rbmnqs_full_sample(rbmnqs_handle* h, double* E_mean, double* d, double* dh);
  * aggregator's statistics: values[4 i .. 4 i + 3] = Re <O_i>, Im <O_i>,
  * binned standard deviation of the mean, tau. */
 int rbmnqs_get_observables(rbmnqs_handle* h, double* values);
+
+/* Full enumeration only: the normalised state vector psi[2^n] (complex,
+ * interleaved re, im) indexed by the state number (bit i set <=> site i
+ * down) of the last sample -- full_sampler::sample(keep_state = true)
+ * (full_sampler.cpp:112-159), returned instead of written to a file. */
+int rbmnqs_full_state(rbmnqs_handle* h, double* psi);
 
 /* ----------------------------------------------------------- timing ---- */
 /* Device time (ms, CUDA events on the handle's stream) accumulated per stage

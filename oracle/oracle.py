@@ -416,6 +416,51 @@ def metropolis(machine, model, n_chains, spc, warmup=0, step=1, bond_flips=0.0, 
     return E, O, acc, spins
 
 
+def full_order(n, bits=2):
+    """State numbers in full_sampler::sample's visiting order (one process,
+    full_sampler.cpp:63-136): block b over the low `bits` bits, and within
+    it the Gray code gray(i) = i ^ (i >> 1) over the high n - bits bits."""
+    hb = n - bits
+    k = np.arange(1 << n, dtype=np.int64)
+    b, i = k >> hb, k & ((1 << hb) - 1)
+    return b | ((i ^ (i >> 1)) << bits)
+
+
+def weighted_aggregate(x, w, n_bins):
+    """aggregator::aggregate / finalize (operators/aggregator.cpp:84-239, one
+    process) for a scalar observable with weights w and n_bins bins:
+    the weighted Welford mean and M2, the bin recurrences, tau and the binned
+    standard deviation of the mean."""
+    result, wsum, wsum2, var = 0j, 0.0, 0.0, 0.0
+    bin_, wsum_bin, cur, rb, vb = 0j, 0.0, 0, 0j, 0.0
+    bs = len(x) // n_bins
+    for xi, wi in zip(x, w):
+        wsum += wi
+        wsum2 += wi * wi
+        delta = wi * (xi - result)
+        result += delta / wsum
+        var += (np.conj(xi - result) * delta).real
+        if n_bins > 1:
+            cur += 1
+            wsum_bin += wi
+            bin_ += wi * xi
+            if cur == bs:
+                cur = 0
+                bin_ /= wsum_bin
+                delta = wsum_bin * (bin_ - rb)
+                rb += delta / wsum
+                vb += (np.conj(delta) * (bin_ - rb)).real
+                bin_, wsum_bin = 0j, 0.0
+    tau = 0.0
+    if n_bins > 1 and not (var == 0 and vb == 0):
+        tau = 0.5 * (max(bs * vb / var, 1.0) - 1)
+    den = wsum - wsum2 / wsum
+    vb = max(vb / den, 0.0)
+    var = max(var / den, 0.0)
+    sd = np.sqrt(vb / n_bins) if n_bins > 1 else np.sqrt(var / len(x))
+    return dict(mean=result, var=var, var_binned=vb, tau=tau, stddev=sd)
+
+
 def full(machine, model, threads=0, with_O=True):
     P = machine.n_params
     pt = C.c_double()

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -152,6 +153,19 @@ struct rbmnqs_handle {
     DevBuf<double2> plug_m;
     DevBuf<double> plug_wr, plug_wi, plug_part;
     DevBuf<rbmnqs::EpochStatsDev> stats_first;
+    // full enumeration: log psi, weights p, reduction partials, totals, a zero d
+    bool full = false;
+    DevBuf<double2> lpsi, dzero;
+    DevBuf<double> pw, fpart;
+    DevBuf<rbmnqs::FullStatsDev> fstat;
+    const double* fstat_W() const {
+        return reinterpret_cast<const double*>(reinterpret_cast<const char*>(fstat.p) +
+                                               offsetof(rbmnqs::FullStatsDev, W));
+    }
+    const double* fstat_vfac() const {
+        return reinterpret_cast<const double*>(reinterpret_cast<const char*>(fstat.p) +
+                                               offsetof(rbmnqs::FullStatsDev, vfac));
+    }
     // direct solver: barrier state and triangular-solve work vector
     DevBuf<rbmnqs::MfreeSync> dsync;
     DevBuf<double2> dwork;
@@ -336,7 +350,27 @@ struct rbmnqs_handle {
     }
     // tm: record the stage timing events (off for the second sample of a
     // Heun step, which runs inside the optimisation stage)
+    // full_sampler::sample: every state (the list is fixed at creation),
+    // weights p = |psi|^2, weighted aggregators
+    void enqueue_full_sample(bool tm) {
+        if (tm) mark(0);
+        if (tm) mark(1);
+        rbmnqs::EvalArgs ea = eval_args();
+        ea.logpsi = lpsi.p;
+        ck(rbmnqs::launch_eval(ea, fp64, wpb, st), "eval kernel");
+        if (tm) mark(2);
+        ck(rbmnqs::launch_full_weights(lpsi.p, N, pw.p, fpart.p, fstat.p, st), "full weights");
+        ck(rbmnqs::launch_moments(O.p, fp64, E.p, N, P, mom_blocks, pd.p, pf.p, pe.p, d.p, F.p, emean.p, st, pw.p,
+                                  fstat_W()),
+           "moments");
+        ck(rbmnqs::launch_energy_stats_weighted(E.p, pw.p, N, n_bins, emean.p, fstat.p, stats.p, st), "energy stats");
+        if (tm) mark(3);
+    }
     void enqueue_sample(bool tm = true) {
+        if (full) {
+            enqueue_full_sample(tm);
+            return;
+        }
         const rbmnqs::SamplerArgs a = sampler_args();
         if (tm) mark(0);
         if (net)
@@ -399,6 +433,14 @@ struct rbmnqs_handle {
         auto mk = [&](int i) {
             if (tm) mark(i);
         };
+        // full enumeration: O becomes sqrt(N p / W) (O - d), whose plain Gram
+        // is S = sum p conj(O - d)(O - d)^T / W (the reference's sqrt(p) O
+        // store with norm W, aggregator.cpp:274-289); d is then zero for the
+        // solve and the variance factor is W / (W - W2 / W)
+        const double2* dS = full ? dzero.p : d.p;
+        const double* vf = full ? fstat_vfac() : nullptr;
+        if (cfg.optimizer_type != 1 && full)
+            ck(rbmnqs::launch_full_center(O.p, fp64, pw.p, fstat.p, d.p, N, P, st), "full centring");
         if (cfg.optimizer_type == 1) {
             // SGD: the gradient itself is the step direction
             mk(4);
@@ -406,21 +448,21 @@ struct rbmnqs_handle {
             mk(5);
         } else if (mfree) {
             // diag = var(O) straight from O; CG on the operator (cg_solver.cpp aprod)
-            ck(rbmnqs::launch_var_diag(O.p, fp64, d.p, N, P, mfp, mfw, diag.p, maxdiag.p, st), "var diag");
+            ck(rbmnqs::launch_var_diag(O.p, fp64, dS, N, P, mfp, mfw, diag.p, maxdiag.p, st, vf), "var diag");
             mk(4);
             if (cg_after) ck(cudaStreamWaitEvent(st, cg_after, 0), "cg order");
-            ck(rbmnqs::launch_cg_mfree(O.p, fp64, d.p, (double)N, N, P, P_neural, F.p, x.p, diag.p, maxdiag.p,
+            ck(rbmnqs::launch_cg_mfree(O.p, fp64, dS, (double)N, N, P, P_neural, F.p, x.p, diag.p, maxdiag.p,
                                        sched.p, 0, 0, 0, max_it, rtol, mfp, mfw, cgres.p, st),
                "matrix-free cg");
             if (cg_done) ck(cudaEventRecord(cg_done, st), "cg order");
             mk(5);
         } else {
             if (gram_tc)
-                ck(rbmnqs::launch_gram_tc(gtc, O.p, fp64, d.p, gpart.p, gerr.p, Sm.p, st), "tensor-core gram");
+                ck(rbmnqs::launch_gram_tc(gtc, O.p, fp64, dS, gpart.p, gerr.p, Sm.p, st), "tensor-core gram");
             else
-                ck(rbmnqs::launch_gram_fp64(O.p, fp64, d.p, N, P, gram_ks, part.p, Sm.p, st), "gram");
+                ck(rbmnqs::launch_gram_fp64(O.p, fp64, dS, N, P, gram_ks, part.p, Sm.p, st), "gram");
             ck(rbmnqs::launch_regularize(Sm.p, P, P_neural, N, sched.p, diag.p, Sreg.p, maxdiag.p, st,
-                                         cfg.solver == 2),
+                                         cfg.solver == 2, vf),
                "regularize");
             mk(4);
             const bool coop = coop_solve();
@@ -592,6 +634,8 @@ int rbmnqs_config_default(rbmnqs_config* c) {
         c->mom_alpha = 0.9;
         c->mom_dialup = 1.0;
         c->heun_eps = 1e-3;
+        c->sampler_type = 0;
+        c->full_parallel_bits = 2;
     });
 }
 
@@ -647,7 +691,22 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
                 RBMNQS_ERR_UNSUPPORTED);
         // dense S up to kDenseMax parameters, the matrix-free operator above
         h->mfree = h->P > kDenseMax;
-        h->N = cfg->n_chains * cfg->samples_per_chain;
+        require(cfg->sampler_type == 0 || cfg->sampler_type == 1, "sampler_type must be 0 (metropolis) or 1 (full)");
+        h->full = cfg->sampler_type == 1;
+        if (h->full) {
+            // full_sampler.cpp:36-41: every state once (the device holds N x P
+            // derivatives, so n is bounded by memory, not by 64)
+            require(h->n <= 30 && cfg->full_parallel_bits >= 0 && cfg->full_parallel_bits <= h->n,
+                    "full enumeration needs n <= 30 and 0 <= full_parallel_bits <= n", RBMNQS_ERR_UNSUPPORTED);
+            require((double)(int64_t(1) << h->n) * h->P * (cfg->precision == 1 ? 16 : 8) <= 64.0 * (1ull << 30),
+                    "full enumeration: 2^n x n_params derivatives exceed 64 GiB", RBMNQS_ERR_UNSUPPORTED);
+            require(cfg->proposal == 0, "full enumeration has no proposals", RBMNQS_ERR_UNSUPPORTED);
+            require(cfg->plugin != 3, "the heun plugin is not supported with full enumeration",
+                    RBMNQS_ERR_UNSUPPORTED);
+            h->N = 1 << h->n;
+        } else {
+            h->N = cfg->n_chains * cfg->samples_per_chain;
+        }
         require(h->N >= 2, "need at least two samples");
         int k = 50;
         while (h->N % k) k--;
@@ -768,6 +827,15 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         h->d.alloc(h->P);
         h->F.alloc(h->P);
         h->emean.alloc(1);
+        if (h->full) {
+            h->lpsi.alloc(h->N);
+            h->pw.alloc(h->N);
+            h->fpart.alloc(3 * rbmnqs::kFullBlocks);
+            h->fstat.alloc(1);
+            h->dzero.alloc(h->P);
+            ck(cudaMemsetAsync(h->dzero.p, 0, h->P * sizeof(double2), h->st), "memset");
+            ck(rbmnqs::launch_full_states(h->samples.p, h->n, cfg->full_parallel_bits, h->st), "full states");
+        }
         h->gram_tc = !h->fp64 && cfg->gram == 0 && !h->mfree;
         require(cfg->solver >= 0 && cfg->solver <= 2, "solver must be 0 (cg), 1 (minresqlp) or 2 (direct)");
         require(cfg->solver != 2 || !h->mfree,
@@ -1335,6 +1403,19 @@ int rbmnqs_full_sample(rbmnqs_handle* h, double* E_mean, double* dm, double* dh)
     });
 }
 
+int rbmnqs_full_state(rbmnqs_handle* h, double* psi) {
+    return guard([&] {
+        require(h && psi, "null argument");
+        require(h->full, "rbmnqs_full_state needs sampler_type 1 (full enumeration)", RBMNQS_ERR_UNSUPPORTED);
+        require(h->sampled, "rbmnqs_full_state needs a preceding sample or epoch");
+        DevBuf<double2> v;
+        v.alloc(h->N);
+        ck(rbmnqs::launch_full_state_vector(h->lpsi.p, h->samples.p, h->N, h->fstat.p, v.p, h->st), "state vector");
+        ck(cudaMemcpyAsync(psi, v.p, (size_t)h->N * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "copy");
+        ck(cudaStreamSynchronize(h->st), "sync");
+    });
+}
+
 int rbmnqs_get_observables(rbmnqs_handle* h, double* values) {
     return guard([&] {
         require(h && values, "null argument");
@@ -1353,6 +1434,14 @@ int rbmnqs_get_observables(rbmnqs_handle* h, double* values) {
             ea.O = nullptr;
             ea.eloc = h->obsE.p;
             ck(rbmnqs::launch_eval(ea, h->fp64, h->wpb, h->st), "observable evaluation");
+            if (h->full) {
+                ck(rbmnqs::launch_wmean(h->obsE.p, h->pw.p, h->N, h->fstat.p, h->obsMean.p + i, h->st),
+                   "observable mean");
+                ck(rbmnqs::launch_energy_stats_weighted(h->obsE.p, h->pw.p, h->N, h->n_bins, h->obsMean.p + i,
+                                                        h->fstat.p, h->obsStats.p + i, h->st),
+                   "observable statistics");
+                continue;
+            }
             ck(rbmnqs::launch_mean(h->obsE.p, h->N, h->obsMean.p + i, h->st), "observable mean");
             ck(rbmnqs::launch_energy_stats(h->obsE.p, h->N, h->n_bins, h->obsMean.p + i, h->nacc.p, h->nprop.p,
                                            h->cfg.n_chains, h->obsStats.p + i, h->st),

@@ -410,7 +410,8 @@ __global__ void __launch_bounds__(kThreads) cg_mfree_kernel(const TO* __restrict
 // aggregator, aggregator.cpp:84-164) and per-block maxima.
 template <typename TO>
 __global__ void __launch_bounds__(kThreads) var_diag_kernel(const TO* __restrict__ O, const double2* __restrict__ d,
-                                                            int N, int P, double* diag, double* maxpart) {
+                                                            int N, int P, double* diag, double* maxpart,
+                                                            const double* vfac) {
     __shared__ double colred[kThreads];
     __shared__ double red[kThreads / 32];
     const int tid = threadIdx.x, c = tid % kColTile, rg = tid / kColTile, ngr = kThreads / kColTile;
@@ -432,7 +433,10 @@ __global__ void __launch_bounds__(kThreads) var_diag_kernel(const TO* __restrict
         if (rg == 0 && q < P) {
             double t = 0;
             for (int g = 0; g < ngr; g++) t += colred[g * kColTile + c];
-            t /= (double)N - 1.0;
+            if (vfac)
+                t = t / (double)N * *vfac;
+            else
+                t /= (double)N - 1.0;
             diag[q] = t;
             mx = fmax(mx, t);
         }
@@ -539,11 +543,13 @@ cudaError_t launch_cg_dense_coop(const double2* A, const double2* b, double2* x,
 }
 
 cudaError_t launch_var_diag(const void* O, int fp64, const double2* d, int N, int P, const MfreePlan& pl,
-                            const MfreeWork& w, double* diag, double* max_diag, cudaStream_t st) {
+                            const MfreeWork& w, double* diag, double* max_diag, cudaStream_t st,
+                            const double* vfac) {
     if (fp64)
-        var_diag_kernel<double2><<<pl.diag_blocks, kThreads, 0, st>>>((const double2*)O, d, N, P, diag, w.maxpart);
+        var_diag_kernel<double2>
+            <<<pl.diag_blocks, kThreads, 0, st>>>((const double2*)O, d, N, P, diag, w.maxpart, vfac);
     else
-        var_diag_kernel<float2><<<pl.diag_blocks, kThreads, 0, st>>>((const float2*)O, d, N, P, diag, w.maxpart);
+        var_diag_kernel<float2><<<pl.diag_blocks, kThreads, 0, st>>>((const float2*)O, d, N, P, diag, w.maxpart, vfac);
     max_parts_kernel<<<1, 32, 0, st>>>(w.maxpart, pl.diag_blocks, max_diag);
     return cudaGetLastError();
 }

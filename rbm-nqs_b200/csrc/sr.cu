@@ -56,16 +56,22 @@ __device__ __forceinline__ double2 ld2(const double2* O, size_t i) { return O[i]
 
 // ------------------------------------------------------------- moments ---
 // Per block over a slice of samples: sum_n O[n][p], sum_n E_n conj(O[n][p]),
-// sum_n E_n (aggregators a_d_, a_dh_, a_h_: aggregator.cpp:190-231).
+// sum_n E_n (aggregators a_d_, a_dh_, a_h_: aggregator.cpp:190-231), each
+// term weighted by w[n] when w is given (full enumeration, p = |psi|^2).
 template <typename TO>
-__global__ void moments_partial(const TO* O, const double2* E, int N, int P, double2* pd, double2* pf, double2* pe) {
+__global__ void moments_partial(const TO* O, const double2* E, int N, int P, double2* pd, double2* pf, double2* pe,
+                                const double* w) {
     __shared__ double2 red[32];
     const int nb = gridDim.x;
     const int n0 = (int)((long)N * blockIdx.x / nb), n1 = (int)((long)N * (blockIdx.x + 1) / nb);
     for (int p = threadIdx.x; p < P; p += blockDim.x) {
         double sx = 0, sy = 0, fx = 0, fy = 0;
         for (int n = n0; n < n1; n++) {
-            const double2 o = ld2(O, (size_t)n * P + p);
+            double2 o = ld2(O, (size_t)n * P + p);
+            if (w) {
+                const double wn = w[n];
+                o = make_double2(wn * o.x, wn * o.y);
+            }
             const double2 e = E[n];
             sx += o.x;
             sy += o.y;
@@ -76,15 +82,20 @@ __global__ void moments_partial(const TO* O, const double2* E, int N, int P, dou
         pf[(size_t)blockIdx.x * P + p] = make_double2(fx, fy);
     }
     double2 es = make_double2(0, 0);
-    for (int n = n0 + threadIdx.x; n < n1; n += blockDim.x) es = add2(es, E[n]);
+    for (int n = n0 + threadIdx.x; n < n1; n += blockDim.x) {
+        const double2 e = E[n];
+        es = add2(es, w ? make_double2(w[n] * e.x, w[n] * e.y) : e);
+    }
     es = block_sum(es, red);
     if (threadIdx.x == 0) pe[blockIdx.x] = es;
 }
 
-// d = <O>, F = <E O*> - <E> conj(<O>) (stochastic_reconfiguration.cpp:102)
-__global__ void moments_final(const double2* pd, const double2* pf, const double2* pe, int nb, int N, int P,
-                              double2* d, double2* F, double2* emean) {
+// d = <O>, F = <E O*> - <E> conj(<O>) (stochastic_reconfiguration.cpp:102);
+// the sums are divided by *wsum (the total weight) when given, else by N.
+__global__ void moments_final(const double2* pd, const double2* pf, const double2* pe, int nb, int N_, int P,
+                              double2* d, double2* F, double2* emean, const double* wsum) {
     __shared__ double2 em;
+    const double N = wsum ? *wsum : (double)N_;
     if (threadIdx.x == 0) {
         double2 s = make_double2(0, 0);
         for (int b = 0; b < nb; b++) s = add2(s, pe[b]);
@@ -268,12 +279,14 @@ __global__ void schedule_step(ScheduleDev* s, int first) {
 // ((1 + r1) + rd on non-neural parameters) + r2 max|diag|
 // (direct_solver.cpp:42-49).
 __global__ void regularize(const double2* S, int P, int n_neural, int N, const ScheduleDev* sch, double* diag,
-                           double2* Sreg, double* max_diag_out, int direct) {
+                           double2* Sreg, double* max_diag_out, int direct, const double* vfac) {
     __shared__ double red[32];
     const double r1 = sch->value[1], r2 = sch->value[2], rd = sch->value[3];
+    // unbiased variance factor: N / (N - 1), or W / (W - W2 / W) for weights
+    const double vf = vfac ? *vfac : (double)N / ((double)N - 1.0);
     double mx = 0;
     for (int p = threadIdx.x; p < P; p += blockDim.x) {
-        const double v = S[(size_t)p * P + p].x * (double)N / ((double)N - 1.0);
+        const double v = S[(size_t)p * P + p].x * vf;
         diag[p] = v;
         mx = fmax(mx, v);
     }
@@ -980,12 +993,13 @@ __global__ void unpack_weights(const double2* params, int n, int n_vb, int nh, d
 
 // ---------------------------------------------------------------- launch --
 cudaError_t launch_moments(const void* O, int fp64, const double2* E, int N, int P, int nblk, double2* pd,
-                           double2* pf, double2* pe, double2* d, double2* F, double2* emean, cudaStream_t st) {
+                           double2* pf, double2* pe, double2* d, double2* F, double2* emean, cudaStream_t st,
+                           const double* w, const double* wsum) {
     if (fp64)
-        moments_partial<double2><<<nblk, 256, 0, st>>>((const double2*)O, E, N, P, pd, pf, pe);
+        moments_partial<double2><<<nblk, 256, 0, st>>>((const double2*)O, E, N, P, pd, pf, pe, w);
     else
-        moments_partial<float2><<<nblk, 256, 0, st>>>((const float2*)O, E, N, P, pd, pf, pe);
-    moments_final<<<(P + 255) / 256, 256, 0, st>>>(pd, pf, pe, nblk, N, P, d, F, emean);
+        moments_partial<float2><<<nblk, 256, 0, st>>>((const float2*)O, E, N, P, pd, pf, pe, w);
+    moments_final<<<(P + 255) / 256, 256, 0, st>>>(pd, pf, pe, nblk, N, P, d, F, emean, wsum);
     return cudaGetLastError();
 }
 
@@ -1041,8 +1055,8 @@ cudaError_t launch_schedule_regs(ScheduleDev* s, cudaStream_t st) {
 }
 
 cudaError_t launch_regularize(const double2* S, int P, int n_neural, int N, const ScheduleDev* sch, double* diag,
-                              double2* Sreg, double* max_diag, cudaStream_t st, int direct) {
-    regularize<<<1, 1024, 0, st>>>(S, P, n_neural, N, sch, diag, Sreg, max_diag, direct);
+                              double2* Sreg, double* max_diag, cudaStream_t st, int direct, const double* vfac) {
+    regularize<<<1, 1024, 0, st>>>(S, P, n_neural, N, sch, diag, Sreg, max_diag, direct, vfac);
     return cudaGetLastError();
 }
 

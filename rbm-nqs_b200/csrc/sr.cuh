@@ -30,8 +30,10 @@ struct CgResultDev {
     double max_dw;
 };
 
+// w: optional per-sample weights, wsum: their total (device scalar)
 cudaError_t launch_moments(const void* O, int fp64, const double2* E, int N, int P, int nblk, double2* pd,
-                           double2* pf, double2* pe, double2* d, double2* F, double2* emean, cudaStream_t st);
+                           double2* pf, double2* pe, double2* d, double2* F, double2* emean, cudaStream_t st,
+                           const double* w = nullptr, const double* wsum = nullptr);
 cudaError_t launch_energy_stats(const double2* E, int N, int n_bins, const double2* emean, const uint32_t* nacc,
                                 const uint32_t* nprop, int n_chains, EpochStatsDev* out, cudaStream_t st);
 cudaError_t launch_mean(const double2* E, int N, double2* mu, cudaStream_t st);
@@ -44,8 +46,10 @@ cudaError_t launch_solve_prep(const double2* G, int N, double norm, const double
                               int n_neural, double r1, double r2, double rd, double2* Sreg, cudaStream_t st,
                               int direct = 0);
 cudaError_t launch_schedule(ScheduleDev* s, cudaStream_t st);
+// vfac: optional device scalar replacing the N / (N - 1) variance factor
 cudaError_t launch_regularize(const double2* S, int P, int n_neural, int N, const ScheduleDev* sch, double* diag,
-                              double2* Sreg, double* max_diag, cudaStream_t st, int direct = 0);
+                              double2* Sreg, double* max_diag, cudaStream_t st, int direct = 0,
+                              const double* vfac = nullptr);
 cudaError_t launch_cg(const double2* A, const double2* b, double2* x, int P, int max_it, double rtol,
                       CgResultDev* res, cudaStream_t st);
 // Update-step plugins (optimizer/plugin.cpp:29-115): state on the device.
@@ -95,6 +99,37 @@ struct MfreeSync {
 // factor): x = Sreg^-1 F.  work: P entries; sync: barrier state.
 cudaError_t launch_direct_solve(double2* Sreg, const double2* F, double2* x, int P, double2* work, MfreeSync* sync,
                                 CgResultDev* res, cudaStream_t st);
+// Full enumeration (full_sampler.cpp:43-186): every state once, weighted by
+// p = |psi|^2 (scaled by exp(-max 2 Re log psi), which the normalisation
+// removes).  full.cu.
+struct FullStatsDev {
+    double mx;    // max over states of 2 Re log psi
+    double W;     // sum p
+    double W2;    // sum p^2
+    double vfac;  // W / (W - W2 / W): the weighted unbiased-variance factor
+};
+// samples[k] = state k of the enumeration order: blocks b < 2^bits of the
+// low bits, Gray code over the high n - bits bits within each block
+cudaError_t launch_full_states(uint32_t* samples, int n, int bits, cudaStream_t st);
+// p[k] from log psi, and the totals; part: 2 * kFullBlocks doubles
+constexpr int kFullBlocks = 296;
+cudaError_t launch_full_weights(const double2* logpsi, int64_t N, double* p, double* part, FullStatsDev* fs,
+                                cudaStream_t st);
+// O[k] <- sqrt(N p_k / W) (O[k] - d): the weighted, centred samples whose
+// plain Gram (1/N) O^H O is S
+cudaError_t launch_full_center(void* O, int fp64, const double* p, const FullStatsDev* fs, const double2* d,
+                               int64_t N, int P, cudaStream_t st);
+// energy aggregator with weights (aggregator.cpp:190-239): mean, weighted
+// unbiased variance, binned variance over n_bins consecutive blocks, tau
+cudaError_t launch_energy_stats_weighted(const double2* E, const double* p, int64_t N, int n_bins,
+                                         const double2* emean, const FullStatsDev* fs, EpochStatsDev* out,
+                                         cudaStream_t st);
+// weighted mean sum p E / W into *mu
+cudaError_t launch_wmean(const double2* E, const double* p, int64_t N, const FullStatsDev* fs, double2* mu,
+                         cudaStream_t st);
+// normalised state vector psi[num(state k)] = exp(log psi_k - mx / 2) / sqrt(W)
+cudaError_t launch_full_state_vector(const double2* logpsi, const uint32_t* samples, int64_t N,
+                                     const FullStatsDev* fs, double2* psi, cudaStream_t st);
 struct MfreePlan {
     int blocks, nseg, lseg, diag_blocks;
 };
@@ -111,8 +146,10 @@ cudaError_t mfree_plan(int N, int P, MfreePlan* pl);
 size_t mfree_work_bytes(int N, int P, const MfreePlan& pl);
 MfreeWork mfree_carve(void* base, int N, int P, const MfreePlan& pl);
 // diag = unbiased var(O) per parameter and its maximum (device scalar)
+// vfac: optional device scalar: diag = (sum |O - d|^2 / N) vfac instead of / (N - 1)
 cudaError_t launch_var_diag(const void* O, int fp64, const double2* d, int N, int P, const MfreePlan& pl,
-                            const MfreeWork& w, double* diag, double* max_diag, cudaStream_t st);
+                            const MfreeWork& w, double* diag, double* max_diag, cudaStream_t st,
+                            const double* vfac = nullptr);
 // CG on a formed regularised S (P x P) with the cooperative kernel: for P
 // whose S does not fit the shared-memory cluster solve.  Work from
 // mfree_plan(1, P) / mfree_carve.

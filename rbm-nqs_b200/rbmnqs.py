@@ -44,6 +44,7 @@ class Config(C.Structure):
         ("optimizer_type", C.c_int32), ("sgd_real_factor", C.c_double), ("plugin", C.c_int32),
         ("adam_beta1", C.c_double), ("adam_beta2", C.c_double), ("adam_eps", C.c_double),
         ("mom_alpha", C.c_double), ("mom_dialup", C.c_double), ("heun_eps", C.c_double),
+        ("sampler_type", C.c_int32), ("full_parallel_bits", C.c_int32),
     ]
 
 
@@ -108,6 +109,7 @@ def _declare(L):
                             P_D, P_I, P_D],
         "rbmnqs_full_sample": [VP, P_D, P_D, P_D],
         "rbmnqs_get_observables": [VP, P_D],
+        "rbmnqs_full_state": [VP, P_D],
         "rbmnqs_timing": [VP, P_D, P_I64, C.c_int32],
         "rbmnqs_timing_reset": [VP, C.c_int32],
         "rbmnqs_graph_kernels": [VP, P_I],
@@ -285,7 +287,8 @@ class Session:
         self.n_params, self.n_neural, self.n_vb, self.n_hidden, self.n_symm = \
             P.value, Pn.value, nvb.value, nh.value, S.value
         self.n = model.n
-        self.N = cfg.n_chains * cfg.samples_per_chain
+        # samples per epoch: 2^n states for full enumeration
+        self.N = (1 << model.n) if cfg.sampler_type == 1 else cfg.n_chains * cfg.samples_per_chain
 
     def close(self):
         if getattr(self, "_h", None):
@@ -394,6 +397,13 @@ class Session:
         v = np.zeros(4 * self.model.n_obs, np.float64)
         _ck(lib().rbmnqs_get_observables(self._h, _p(v, P_D)))
         return v.reshape(-1, 4)
+
+    def full_state(self):
+        """Full enumeration (sampler_type 1): the normalised psi over all 2^n
+        states, indexed by the state number, of the last sample."""
+        psi = np.zeros(1 << self.model.n, np.complex128)
+        _ck(lib().rbmnqs_full_state(self._h, _p(psi.view(np.float64), P_D)))
+        return psi
 
     def full_sample(self):
         P = self.n_params
