@@ -30,6 +30,11 @@ template <> struct Wsel<double> {
     static __device__ __forceinline__ const double2* get(const MachineDev& m, const float2*) { return m.W64; }
 };
 
+// word i of the configuration with constant indices only (a runtime index
+// would place the array in local memory)
+__device__ __forceinline__ uint32_t spin_word(const uint32_t sp[4], int i) {
+    return i == 0 ? sp[0] : (i == 1 ? sp[1] : (i == 2 ? sp[2] : sp[3]));
+}
 __device__ __forceinline__ int spin_bit(const uint32_t sp[4], int i) {
     const uint32_t w = i < 32 ? sp[0] : (i < 64 ? sp[1] : (i < 96 ? sp[2] : sp[3]));
     return (w >> (i & 31)) & 1;
@@ -283,7 +288,7 @@ __device__ __noinline__ void evaluate(const MachineDev* __restrict__ mp, const H
 template <int E, typename R>
 __device__ __forceinline__ void stage(const MachineDev& m, const uint32_t sp[4], const C2<R> th[E], uint32_t* wsp,
                                       C2<R>* wth, int lane) {
-    if (lane < 4) wsp[lane] = sp[lane];
+    if (lane < 4) wsp[lane] = spin_word(sp, lane);
 #pragma unroll
     for (int e = 0; e < E; e++)
         if (slot_valid(lane, e, m.T)) wth[lane + 32 * e] = th[e];
@@ -466,7 +471,7 @@ __device__ __forceinline__ int sample_slot(const SamplerArgs& a, int st) {
 
 __device__ __forceinline__ void chain_finish(const SamplerArgs& a, int chain, int lane, const uint32_t sp[4],
                                              uint32_t nacc, uint32_t prop) {
-    if (lane < 4) a.spins[4 * chain + lane] = sp[lane];
+    if (lane < 4) a.spins[4 * chain + lane] = spin_word(sp, lane);
     if (lane == 0) {
         const uint32_t made = prop - prop_base(a);
         a.n_acc[chain] = (a.sweep0 ? a.n_acc[chain] : 0u) + nacc;
@@ -620,7 +625,7 @@ __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, 
         for (int e = 0; e < E; e++) L[e] = slot_valid(lane, e, m.T) ? lnc_re<R>(th[e].x, th[e].y) : (R)0;
         if (const int j = sample_slot(a, st); j >= 0) {
             const size_t idx = (size_t)chain * a.spc + j;
-            if (lane < 4) a.samples[4 * idx + lane] = sp[lane];
+            if (lane < 4) a.samples[4 * idx + lane] = spin_word(sp, lane);
         }
     }
     chain_finish(a, chain, lane, sp, nacc, prop);
@@ -635,12 +640,33 @@ __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, 
 // except for transitions at configurations of vanishing amplitude.  The
 // hardware cosine takes the argument in revolutions, so 2b needs no
 // separate range reduction for the accuracy the acceptance test needs.
+//
+// The three MUFU operations are issued in their flush-to-zero forms: the
+// non-flushing forms add a denormal test and rescale around each one.  A
+// flushed z (|a| > 43) leaves m2 = 1, the exact limit; a flushed m2 (a zero
+// of cosh to FP32 precision) gives ln|cosh| = -inf, i.e. a proposal of
+// vanishing amplitude that is rejected either way.
+__device__ __forceinline__ float ex2_ftz(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float lg2_ftz(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float cos_ftz(float x) {
+    float y;
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
 __device__ __forceinline__ float lnc_sweep(float2 t) {
     const float aa = fabsf(t.x);
-    const float z = __expf(-2.f * aa);
-    const float c2 = __cosf(2.f * t.y);
-    const float m2 = fmaf(2.f * z, c2, fmaf(z, z, 1.f));
-    return fmaf(0.346573590279972655f, __log2f(m2), aa);  // aa + 0.5 ln(m2)
+    const float z = ex2_ftz(aa * -2.88539008177792681f);  // e^{-2|a|} = 2^{-2|a| log2 e}
+    const float c2 = cos_ftz(2.f * t.y);
+    const float m2 = fmaf(z, fmaf(2.f, c2, z), 1.f);       // 1 + z (2 cos 2b + z)
+    return fmaf(0.346573590279972655f, lg2_ftz(m2), aa);  // aa + 0.5 ln(m2)
 }
 
 // FP32 sweep path with the expanded flip table in shared memory.  Proposals
@@ -648,8 +674,10 @@ __device__ __forceinline__ float lnc_sweep(float2 t) {
 // into a packed (f0, f1, bond) code and 0.5 ln u, so a proposal costs two
 // shuffles; a single-site proposal uses the all-zero pad row n as its second
 // flip, which keeps the update branch-free; acceptance compares
-// 0.5 ln u < log|psi'/psi| (the same test as u < |psi'/psi|^2).
-template <int E>
+// 0.5 ln u < log|psi'/psi| (the same test as u < |psi'/psi|^2).  NW = 1
+// when all sites fit in the first configuration word (n <= 32): the bit
+// lookups then need no word selection.
+template <int E, int NW>
 __device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem& sm, int chain, int lane) {
     const MachineDev& m = a.m;
     const int n = m.n, TP = 32 * E;
@@ -657,6 +685,18 @@ __device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem&
     const uint32_t epoch = a.ctl[0];
     uint32_t sp[4];
     chain_start(a, chain, key, epoch, sp);
+    auto sbit = [&](int i) -> bool {
+        if constexpr (NW == 1)
+            return (sp[0] >> i) & 1u;
+        else
+            return spin_bit(sp, i);
+    };
+    auto sflip = [&](int i) {
+        if constexpr (NW == 1)
+            sp[0] ^= 1u << i;
+        else
+            flip_bit(sp, i);
+    };
 
     float2 th[E];
     float SL = 0.f;  // this lane's sum of ln|cosh theta_e| (current state)
@@ -670,7 +710,7 @@ __device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem&
             }
             const double2* col = sm.U64 + lane;
             for (int f = 0; f < n; f++, col += TP) {
-                const double sg = spin_bit(sp, f) ? -1.0 : 1.0;
+                const double sg = sbit(f) ? -1.0 : 1.0;
 #pragma unroll
                 for (int e = 0; e < E; e++) {
                     const double2 w = col[32 * e];
@@ -711,7 +751,7 @@ __device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem&
                     bond = 0;
                 }
                 pcode = f0 | (f1 << 8) | (bond << 16);
-                plu = 0.5f * __logf(unit24<float>(r.z));
+                plu = 0.346573590279972655f * lg2_ftz(unit24<float>(r.z));  // 0.5 ln u
             }
             const int src = prop & 31u;
             const uint32_t code = __shfl_sync(kFull, pcode, src);
@@ -720,8 +760,8 @@ __device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem&
             const int f0 = code & 255u, f1 = (code >> 8) & 255u;
             const bool bond = (code >> 16) != 0;
             slot += bond ? 2 : 1;
-            const float g0 = spin_bit(sp, f0) ? 2.f : -2.f;  // -2 sigma_f
-            const float g1 = (bond && spin_bit(sp, f1)) ? 2.f : -2.f;
+            const float g0 = sbit(f0) ? 2.f : -2.f;  // -2 sigma_f
+            const float g1 = (bond && sbit(f1)) ? 2.f : -2.f;
             const float2 G0 = make_float2(g0, g0), G1 = make_float2(g1, g1);
             const float2* u0 = sm.U + f0 * TP + lane;
             const float2* u1 = sm.U + f1 * TP + lane;
@@ -738,15 +778,15 @@ __device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem&
 #pragma unroll
                 for (int e = 0; e < E; e++) th[e] = __ffma2_rn(G1, u1[32 * e], __ffma2_rn(G0, u0[32 * e], th[e]));
                 SL = sp_new;
-                flip_bit(sp, f0);
-                if (bond) flip_bit(sp, f1);
+                sflip(f0);
+                if (bond) sflip(f1);
                 nacc++;
             }
         }
         recompute();  // FP64 recompute of theta once per sweep
         if (const int j = sample_slot(a, st); j >= 0) {
             const size_t idx = (size_t)chain * a.spc + j;
-            if (lane < 4) a.samples[4 * idx + lane] = sp[lane];
+            if (lane < 4) a.samples[4 * idx + lane] = spin_word(sp, lane);
         }
     }
     chain_finish(a, chain, lane, sp, nacc, prop);
@@ -843,7 +883,7 @@ __device__ __forceinline__ void run_chain_gather(const SamplerArgs& a, const Sme
                     bond = 0;
                 }
                 pcode = f0 | (f1 << 8) | (bond << 16);
-                plu = 0.5f * __logf(unit24<float>(r.z));
+                plu = 0.346573590279972655f * lg2_ftz(unit24<float>(r.z));  // 0.5 ln u
             }
             const int src = prop & 31u;
             const uint32_t code = __shfl_sync(kFull, pcode, src);
@@ -877,7 +917,7 @@ __device__ __forceinline__ void run_chain_gather(const SamplerArgs& a, const Sme
         recompute();  // FP64 recompute of theta once per sweep
         if (const int j = sample_slot(a, st); j >= 0) {
             const size_t idx = (size_t)chain * a.spc + j;
-            if (lane < 4) a.samples[4 * idx + lane] = sp[lane];
+            if (lane < 4) a.samples[4 * idx + lane] = spin_word(sp, lane);
         }
     }
     chain_finish(a, chain, lane, sp, nacc, prop);
@@ -910,7 +950,10 @@ __global__ void __launch_bounds__(FAST == 2 ? MaxThreads<E, PF>::gather : MaxThr
     const int total_warps = (blockDim.x >> 5) * gridDim.x;
     for (int chain = warp * gridDim.x + blockIdx.x; chain < a.n_chains; chain += total_warps) {
         if constexpr (FAST == 1)
-            run_chain_fast<E>(a, sm, chain, lane);
+            if (a.m.n <= 32)
+                run_chain_fast<E, 1>(a, sm, chain, lane);
+            else
+                run_chain_fast<E, 4>(a, sm, chain, lane);
         else if constexpr (FAST == 2) {
             if (a.m.symmetric)
                 run_chain_gather<E, true>(a, sm, chain, lane);
