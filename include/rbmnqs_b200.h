@@ -252,13 +252,23 @@ int rbmnqs_full_state(rbmnqs_handle* h, double* psi);
 int rbmnqs_timing(rbmnqs_handle* h, double* ms, int64_t* launches, int32_t n);
 int rbmnqs_timing_reset(rbmnqs_handle* h, int32_t enable);
 /* Launch-shape autotuner: times the sweep kernel over `sweeps` sweeps (one
- * recorded sample) for each candidate warps-per-block of the planned shape
- * and halvings of it, and the evaluation kernel for 1..8 warps per block;
+ * recorded sample) for one and (where the expanded-table path allows it)
+ * two chains per warp, each with up to five warps-per-block caps, and the
+ * evaluation kernel for 1..8 warps per block;
  * keeps the fastest of each (the session's chains, weights and statistics
  * are left as they were; the epoch graph is re-captured).  No reference
  * counterpart (the reference has no launch shapes).  Outputs may be NULL. */
 int rbmnqs_autotune(rbmnqs_handle* h, int32_t sweeps, int32_t* sampler_warps_per_block,
                     int32_t* eval_warps_per_block, double* sampler_ms);
+
+/* Sets the sweep launch shape: warps per block (0 = planned) and chains per
+ * warp (1, or 2 for the FP32 expanded-table path with n <= 32 sites, whose
+ * two-chain sweep is bit-identical to the one-chain sweep).  The epoch
+ * graph is re-captured.  No reference counterpart.  RBMNQS_ERR_UNSUPPORTED
+ * when two chains per warp is not available for the session. */
+int rbmnqs_set_sweep_shape(rbmnqs_handle* h, int32_t warps_per_block, int32_t chains_per_warp);
+/* The current sweep shape (outputs may be NULL). */
+int rbmnqs_get_sweep_shape(rbmnqs_handle* h, int32_t* warps_per_block, int32_t* chains_per_warp);
 
 /* Number of kernel launches one rbmnqs_epoch performs (kernel nodes of the
  * captured epoch graph; 0 before the first rbmnqs_epoch). */

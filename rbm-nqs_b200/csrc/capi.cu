@@ -257,8 +257,16 @@ struct rbmnqs_handle {
     }
     size_t osize() const { return fp64 ? sizeof(double2) : sizeof(float2); }
 
+    // stage timing event: an external event node inside a graph capture, a
+    // plain record on the stream otherwise
     void mark(int i) {
-        if (timing) ck(cudaEventRecordWithFlags(ev[i], st, cudaEventRecordExternal), "event");
+        if (!timing) return;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        ck(cudaStreamIsCapturing(st, &cs), "capture status");
+        if (cs == cudaStreamCaptureStatusActive)
+            ck(cudaEventRecordWithFlags(ev[i], st, cudaEventRecordExternal), "event");
+        else
+            ck(cudaEventRecord(ev[i], st), "event");
     }
 
     // --- the epoch pieces -------------------------------------------------
@@ -1092,7 +1100,7 @@ int rbmnqs_optimize(rbmnqs_handle* h, rbmnqs_sr_stats* out) {
     return guard([&] {
         require(h != nullptr, "null handle");
         require(h->sampled, "rbmnqs_optimize needs a preceding rbmnqs_sample");
-        if (h->timing) ck(cudaEventRecordWithFlags(h->ev[3], h->st, cudaEventRecordExternal), "event");
+        h->mark(3);
         h->enqueue_optimize();
         h->collect_timing(3, 6);
         read_sr_stats(h, out);
@@ -1552,26 +1560,31 @@ int rbmnqs_autotune(rbmnqs_handle* h, int32_t sweeps, int32_t* sampler_wpb, int3
         if (!h->pf_n) {  // the Pfaffian buffers are sized for the planned shape
             rbmnqs::SamplerShape best = h->shape;
             best_ms = -1;
-            std::vector<int> tried;
-            for (int cap = h->shape.warps_per_block; cap >= 1; cap /= 2) {
-                rbmnqs::SamplerShape sh{};
-                ck(rbmnqs::plan_sampler(h->machine(), h->fp64, h->cfg.n_chains, h->n_prop_bonds, &sh, cap),
-                   "sampler plan");
-                if (std::find(tried.begin(), tried.end(), sh.warps_per_block) != tried.end()) continue;
-                tried.push_back(sh.warps_per_block);
-                const double ms = timed([&] {
-                    ck(cudaMemcpyAsync(h->spins.p, saved.p, sb, cudaMemcpyDeviceToDevice, h->st), "restore");
-                    ck(rbmnqs::launch_sampler(args, h->fp64, sh, h->st), "sampler kernel");
-                });
-                if (best_ms < 0 || ms < best_ms) {
-                    best_ms = ms;
-                    best = sh;
+            // one or two chains per warp, then the warps per block
+            for (int pm = 0; pm <= 1; pm++) {
+                std::vector<int> tried;
+                const int top = std::max(h->shape.warps_per_block, 32);
+                for (int cap = top; cap >= 1; cap /= 2) {
+                    rbmnqs::SamplerShape sh{};
+                    ck(rbmnqs::plan_sampler(h->machine(), h->fp64, h->cfg.n_chains, h->n_prop_bonds, &sh, cap, pm),
+                       "sampler plan");
+                    if (sh.plan.pair != pm) break;  // two chains per warp not possible here
+                    if (std::find(tried.begin(), tried.end(), sh.warps_per_block) != tried.end()) continue;
+                    tried.push_back(sh.warps_per_block);
+                    const double ms = timed([&] {
+                        ck(cudaMemcpyAsync(h->spins.p, saved.p, sb, cudaMemcpyDeviceToDevice, h->st), "restore");
+                        ck(rbmnqs::launch_sampler(args, h->fp64, sh, h->st), "sampler kernel");
+                    });
+                    if (best_ms < 0 || ms < best_ms) {
+                        best_ms = ms;
+                        best = sh;
+                    }
+                    if (tried.size() >= 5) break;
                 }
-                if (tried.size() >= 5) break;
             }
             rbmnqs::SamplerShape chk{};
             ck(rbmnqs::plan_sampler(h->machine(), h->fp64, h->cfg.n_chains, h->n_prop_bonds, &chk,
-                                    best.warps_per_block),
+                                    best.warps_per_block, best.plan.pair),
                "sampler plan");
             h->shape = chk;
         }
@@ -1602,6 +1615,32 @@ int rbmnqs_autotune(rbmnqs_handle* h, int32_t sweeps, int32_t* sampler_wpb, int3
         if (sampler_wpb) *sampler_wpb = h->shape.warps_per_block;
         if (eval_wpb) *eval_wpb = h->wpb;
         if (sampler_ms) *sampler_ms = best_ms;
+    });
+}
+
+int rbmnqs_set_sweep_shape(rbmnqs_handle* h, int32_t warps_per_block, int32_t chains_per_warp) {
+    return guard([&] {
+        require(h && warps_per_block >= 0 && (chains_per_warp == 1 || chains_per_warp == 2), "bad arguments");
+        require(!h->pf_n, "the Pfaffian buffers are sized for the planned shape", RBMNQS_ERR_UNSUPPORTED);
+        rbmnqs::SamplerShape sh{};
+        ck(rbmnqs::plan_sampler(h->machine(), h->fp64, h->cfg.n_chains, h->n_prop_bonds, &sh, warps_per_block,
+                                chains_per_warp == 2 ? 1 : 0),
+           "sampler plan");
+        require(sh.plan.pair == (chains_per_warp == 2),
+                "two chains per warp needs the FP32 expanded-table sweep with n <= 32", RBMNQS_ERR_UNSUPPORTED);
+        h->shape = sh;
+        if (h->graph) {
+            cudaGraphExecDestroy(h->graph);
+            h->graph = nullptr;
+        }
+    });
+}
+
+int rbmnqs_get_sweep_shape(rbmnqs_handle* h, int32_t* warps_per_block, int32_t* chains_per_warp) {
+    return guard([&] {
+        require(h != nullptr, "null handle");
+        if (warps_per_block) *warps_per_block = h->shape.warps_per_block;
+        if (chains_per_warp) *chains_per_warp = h->shape.plan.pair ? 2 : 1;
     });
 }
 

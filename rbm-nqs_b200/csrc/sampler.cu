@@ -669,6 +669,21 @@ __device__ __forceinline__ float lnc_sweep(float2 t) {
     return fmaf(0.346573590279972655f, lg2_ftz(m2), aa);  // aa + 0.5 ln(m2)
 }
 
+// Sum over the warp of the lanes' ln|cosh| differences for the acceptance
+// test.  The partials are summed as fixed-point integers (2^-22 steps, one
+// redux.sync instead of a five-level shuffle butterfly) when every lane's
+// partial is below 16 in magnitude, which keeps the 32-lane total inside
+// int32; otherwise the FP32 butterfly.  The quantisation (2.4e-7) is that of
+// an FP32 sum of this size, so decisions differ from the FP64 chains only at
+// ties, as with any FP32 sum.
+constexpr float kFixScale = 4194304.f;  // 2^22
+__device__ __forceinline__ int fix22(float v) { return __float2int_rn(v * kFixScale); }
+__device__ __forceinline__ float sweep_sum(float v) {
+    const int isum = __reduce_add_sync(kFull, fix22(v));
+    if (__any_sync(kFull, !(fabsf(v) < 16.f))) return warp_sum(v);
+    return (float)isum * (1.f / kFixScale);
+}
+
 // FP32 sweep path with the expanded flip table in shared memory.  Proposals
 // are decoded lane-parallel: with each Philox batch, lane j turns its draw
 // into a packed (f0, f1, bond) code and 0.5 ln u, so a proposal costs two
@@ -771,7 +786,7 @@ __device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem&
                 const float2 t = __ffma2_rn(G1, u1[32 * e], __ffma2_rn(G0, u0[32 * e], th[e]));
                 sp_new += lnc_sweep(t);
             }
-            float d = warp_sum(sp_new - SL);
+            float d = sweep_sum(sp_new - SL);
             d = fmaf(g0, sm.bre[f0], d);
             d = fmaf(g1, sm.bre[f1], d);
             if (lu < d) {
@@ -790,6 +805,156 @@ __device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem&
         }
     }
     chain_finish(a, chain, lane, sp, nacc, prop);
+}
+
+// Two chains per warp (FP32 expanded-table path, n <= 32, theta tables of
+// at most 32 E entries): lanes 0-15 run chain 2 pair, lanes 16-31 chain
+// 2 pair + 1.  Lane h of a half holds the entries that lanes h and h + 16
+// hold in run_chain_fast, t = h + 16 j + 32 k (j = 0, 1; k < E), and keeps
+// their two ln|cosh| sums apart, so that adding them reproduces the first
+// level of run_chain_fast's butterfly and the remaining 16-lane reduction
+// its other levels: every sum, decision and configuration is bit-identical
+// to the one-chain-per-warp sweep.  The per-proposal work that does not
+// scale with the entries (decoding, bias, acceptance, bit updates, loop
+// control) is issued once for both chains.  Each chain keeps its proposal
+// counter and slot count; a chain whose sweep is complete waits (its lanes
+// compute but apply nothing) until the other's is, and both then take the
+// FP64 recompute.  Proposals are drawn 16 at a time (lane j of the half
+// draws proposal prop + j): the same Philox counters as 32 at a time.
+template <int E>
+__device__ __forceinline__ void run_chain_pair(const SamplerArgs& a, const Smem& sm, int pair, int lane) {
+    const MachineDev& m = a.m;
+    const int n = m.n, TP = 32 * E;
+    const int half = lane >> 4, hl = lane & 15;
+    const int chain = 2 * pair + half;
+    const bool live = chain < a.n_chains;
+    const uint2 key = make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32));
+    const uint32_t epoch = a.ctl[0];
+    uint32_t sp[4];
+    chain_start(a, live ? chain : 2 * pair, key, epoch, sp);
+    uint32_t s0 = sp[0];  // n <= 32: the whole configuration
+
+    float2 th[2 * E];  // entry 2 k + j is t = hl + 16 j + 32 k
+    float SA = 0.f, SB = 0.f;  // sums over j = 0 and j = 1 (current state)
+    auto recompute = [&]() {
+        double2 acc[2 * E];
+#pragma unroll
+        for (int e = 0; e < 2 * E; e++) {
+            const int t = hl + 16 * (e & 1) + 32 * (e >> 1);
+            acc[e] = t < m.T ? m.hb[t % m.nh] : make_double2(0, 0);
+        }
+        const double2* col = sm.U64 + hl;
+        for (int f = 0; f < n; f++, col += TP) {
+            const double sg = (s0 >> f) & 1u ? -1.0 : 1.0;
+#pragma unroll
+            for (int e = 0; e < 2 * E; e++) {
+                const double2 w = col[16 * (e & 1) + 32 * (e >> 1)];
+                acc[e].x = fma(sg, w.x, acc[e].x);
+                acc[e].y = fma(sg, w.y, acc[e].y);
+            }
+        }
+        SA = 0.f;
+        SB = 0.f;
+#pragma unroll
+        for (int k = 0; k < E; k++) {
+            th[2 * k] = make_float2((float)acc[2 * k].x, (float)acc[2 * k].y);
+            th[2 * k + 1] = make_float2((float)acc[2 * k + 1].x, (float)acc[2 * k + 1].y);
+            SA += lnc_sweep(th[2 * k]);
+            SB += lnc_sweep(th[2 * k + 1]);
+        }
+    };
+    recompute();
+
+    const int2* bonds = sm.bonds ? sm.bonds : a.prop_bonds;
+    const int total = segment_sweeps(a);
+    const uint32_t thr = a.bond_thr24;
+    uint32_t prop = prop_base(a), nacc = 0, pcode = 0;
+    float plu = 0.f;
+    for (int st = 0; st < total; st++) {
+        int slot = live ? 0 : n;
+        while (__any_sync(kFull, slot < n)) {
+            const bool on = slot < n;
+            if (on && (prop & 15u) == 0) {
+                const uint4 r = philox4x32(make_uint4(prop + hl, epoch, (uint32_t)chain, 0), key);
+                uint32_t f0, f1, bond;
+                if ((r.x >> 8) < thr) {
+                    const int2 b = bonds[pick(r.y, (uint32_t)a.n_prop_bonds)];
+                    f0 = (uint32_t)b.x;
+                    f1 = (uint32_t)b.y;
+                    bond = 1;
+                } else {
+                    f0 = pick(r.y, (uint32_t)n);
+                    f1 = (uint32_t)n;
+                    bond = 0;
+                }
+                pcode = f0 | (f1 << 8) | (bond << 16);
+                plu = 0.346573590279972655f * lg2_ftz(unit24<float>(r.z));  // 0.5 ln u
+            }
+            const int src = prop & 15u;
+            const uint32_t code = __shfl_sync(kFull, pcode, src, 16);
+            const float lu = __shfl_sync(kFull, plu, src, 16);
+            const int f0 = code & 255u, f1 = (code >> 8) & 255u;
+            const bool bond = (code >> 16) != 0;
+            const float g0 = (s0 >> f0) & 1u ? 2.f : -2.f;  // -2 sigma_f
+            const float g1 = (bond && ((s0 >> f1) & 1u)) ? 2.f : -2.f;
+            const float2 G0 = make_float2(g0, g0), G1 = make_float2(g1, g1);
+            const float2* u0 = sm.U + f0 * TP + hl;
+            const float2* u1 = sm.U + f1 * TP + hl;
+            float2 tn[2 * E];
+            float nA = 0.f, nB = 0.f;
+#pragma unroll
+            for (int k = 0; k < E; k++) {
+                tn[2 * k] = __ffma2_rn(G1, u1[32 * k], __ffma2_rn(G0, u0[32 * k], th[2 * k]));
+                nA += lnc_sweep(tn[2 * k]);
+                tn[2 * k + 1] = __ffma2_rn(G1, u1[16 + 32 * k], __ffma2_rn(G0, u0[16 + 32 * k], th[2 * k + 1]));
+                nB += lnc_sweep(tn[2 * k + 1]);
+            }
+            // the one-chain sweep's sum: lanes h and h + 16 of it are this
+            // lane's two partials (integer sums are exact in any order)
+            const float vA = nA - SA, vB = nB - SB;
+            const int iv = fix22(vA) + fix22(vB);
+            const int ilo = __reduce_add_sync(kFull, hl == lane ? iv : 0);
+            const int ihi = __reduce_add_sync(kFull, hl == lane ? 0 : iv);
+            const bool big = !(fabsf(vA) < 16.f) || !(fabsf(vB) < 16.f);
+            const unsigned bigm = __ballot_sync(kFull, big);
+            float d;
+            if (bigm & (half ? 0xffff0000u : 0x0000ffffu)) {
+                d = vA + vB;
+#pragma unroll
+                for (int o = 8; o > 0; o >>= 1) d += __shfl_xor_sync(kFull, d, o);
+            } else {
+                d = (float)(half ? ihi : ilo) * (1.f / kFixScale);
+            }
+            d = fmaf(g0, sm.bre[f0], d);
+            d = fmaf(g1, sm.bre[f1], d);
+            if (on) {
+                prop++;
+                slot += bond ? 2 : 1;
+                if (lu < d) {
+#pragma unroll
+                    for (int e = 0; e < 2 * E; e++) th[e] = tn[e];
+                    SA = nA;
+                    SB = nB;
+                    s0 ^= 1u << f0;
+                    if (bond) s0 ^= 1u << f1;
+                    nacc++;
+                }
+            }
+        }
+        recompute();  // FP64 recompute of theta once per sweep
+        if (const int j = sample_slot(a, st); live && j >= 0) {
+            const size_t idx = (size_t)chain * a.spc + j;
+            if (hl < 4) a.samples[4 * idx + hl] = hl == 0 ? s0 : 0u;
+        }
+    }
+    if (live) {
+        if (hl < 4) a.spins[4 * chain + hl] = hl == 0 ? s0 : 0u;
+        if (hl == 0) {
+            const uint32_t made = prop - prop_base(a);
+            a.n_acc[chain] = (a.sweep0 ? a.n_acc[chain] : 0u) + nacc;
+            a.n_prop[chain] = (a.sweep0 ? a.n_prop[chain] : 0u) + made;
+        }
+    }
 }
 
 // FP32 sweep path with gathered flip rows, for theta tables whose expanded
@@ -902,7 +1067,7 @@ __device__ __forceinline__ void run_chain_gather(const SamplerArgs& a, const Sme
                 tn[e] = __ffma2_rn(G1, urd(f1, e), __ffma2_rn(G0, urd(f0, e), th[e]));
                 sp_new += lnc_sweep(tn[e]);
             }
-            float d = warp_sum(sp_new - SL);
+            float d = sweep_sum(sp_new - SL);
             d = fmaf(g0, sm.bre[f0], d);
             d = fmaf(g1, sm.bre[f1], d);
             if (lu < d) {
@@ -928,6 +1093,7 @@ __device__ __forceinline__ void run_chain_gather(const SamplerArgs& a, const Sme
 template <int E, bool PF = false> struct MaxThreads {
     static constexpr int v = PF ? 256 : (E <= 2 ? 1024 : (E <= 4 ? 896 : (E <= 8 ? 512 : 256)));
     static constexpr int gather = E <= 4 ? 896 : (E <= 8 ? 640 : 384);
+    static constexpr int pair = E <= 1 ? 1024 : (E <= 2 ? 768 : 512);  // 2 E entries per lane
 };
 
 // All chains at once, persistent warps: global warp g = warp * gridDim.x +
@@ -935,8 +1101,9 @@ template <int E, bool PF = false> struct MaxThreads {
 // on different SMs and every block holds the tables once.  FAST selects the
 // FP32 expanded-table path.
 template <int E, typename R, int FAST, bool PF>
-__global__ void __launch_bounds__(FAST == 2 ? MaxThreads<E, PF>::gather : MaxThreads<E, PF>::v, 1)
-    sampler_kernel(const SamplerArgs a) {
+__global__ void __launch_bounds__(FAST == 2 ? MaxThreads<E, PF>::gather
+                                            : (FAST == 3 ? MaxThreads<E, PF>::pair : MaxThreads<E, PF>::v),
+                                  1) sampler_kernel(const SamplerArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int fp64 = sizeof(R) == 8;
     Smem sm = carve(smem, a.m, fp64, a.plan, a.n_prop_bonds, sweep_warp_bytes(a.m.T, sizeof(R), PF));
@@ -948,6 +1115,12 @@ __global__ void __launch_bounds__(FAST == 2 ? MaxThreads<E, PF>::gather : MaxThr
     double2* pscr = PF ? a.m.pf.scratch + (size_t)(blockIdx.x * (blockDim.x >> 5) + warp) * kPfMaxSites * kPfMaxSites
                        : nullptr;
     const int total_warps = (blockDim.x >> 5) * gridDim.x;
+    if constexpr (FAST == 3) {
+        // two chains per warp (the chain-pair loop bound is warp-uniform)
+        const int pairs = (a.n_chains + 1) / 2;
+        for (int pair = warp * gridDim.x + blockIdx.x; pair < pairs; pair += total_warps)
+            run_chain_pair<E>(a, sm, pair, lane);
+    } else
     for (int chain = warp * gridDim.x + blockIdx.x; chain < a.n_chains; chain += total_warps) {
         if constexpr (FAST == 1)
             if (a.m.n <= 32)
@@ -1324,7 +1497,13 @@ template <int E, typename R, int FAST, bool PF> static const void* sampler_fn() 
 
 // The Pfaffian variants exist for theta tables up to 128 entries (32 sites,
 // alpha <= 4); they take the general (non-table) sweep.
-static const void* pick_sampler(int E, int fp64, int exp_table, int pf, int gather) {
+static const void* pick_sampler(int E, int fp64, int exp_table, int pf, int gather, int pair) {
+    if (pair && !fp64 && !pf && exp_table) {
+        if (E == 1) return sampler_fn<1, float, 3, false>();
+        if (E == 2) return sampler_fn<2, float, 3, false>();
+        if (E == 4) return sampler_fn<4, float, 3, false>();
+        return nullptr;
+    }
     if (pf) {
 #define RBMNQS_PICK_PF(EE) \
     if (E == EE) return fp64 ? sampler_fn<EE, double, 0, true>() : sampler_fn<EE, float, 0, true>();
@@ -1343,7 +1522,8 @@ static const void* pick_sampler(int E, int fp64, int exp_table, int pf, int gath
     return nullptr;
 }
 
-cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bonds, SamplerShape* out, int max_wpb) {
+static cudaError_t plan_sampler_impl(const MachineDev& m, int fp64, int n_chains, int n_bonds, SamplerShape* out,
+                                     int max_wpb, int pair_mode) {
     const int E = elements_per_lane(m.T);
     if (E < 0) return cudaErrorInvalidValue;
     int dev = 0, sms = 0, smem_max = 0;
@@ -1366,14 +1546,21 @@ cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bond
     pl.w32 = !fp64 && !pl.use_u && !pl.gather && m.n * m.nh * 8 <= 64 * 1024;
     pl.w64 = m.n * m.nh * 16 <= 32 * 1024;
     pl.bonds = n_bonds > 0 && n_bonds * 8 <= 8 * 1024;
-    const void* fn = pick_sampler(E, fp64, pl.use_u, pf, pl.gather);
+    // two chains per warp for small configurations with both expanded
+    // tables (entries per lane 2 E <= 8): fewer instructions per chain but
+    // half the resident warps and more registers per thread, which measured
+    // slower on the 32-spin alpha = 4 shape at 4096 and 16384 chains; so
+    // only on request (pair_mode 1, e.g. by the autotuner)
+    pl.pair = pl.use_u && pl.u64 && m.n <= 32 && E <= 4 && pair_mode == 1;
+    const void* fn = pick_sampler(E, fp64, pl.use_u, pf, pl.gather, pl.pair);
     if (!fn) return cudaErrorInvalidValue;
     cudaFuncAttributes fa;
     err = cudaFuncGetAttributes(&fa, fn);
     if (err != cudaSuccess) return err;
     // warps per block: enough for one block per SM to hold every chain,
     // limited by the kernel's thread bound, registers and shared memory
-    const int want = (n_chains + sms - 1) / sms;
+    const int units = pl.pair ? (n_chains + 1) / 2 : n_chains;  // warps' work items
+    const int want = (units + sms - 1) / sms;
     int wpb = fa.maxThreadsPerBlock / 32;
     const int regs = fa.numRegs > 0 ? fa.numRegs : 64;
     const int reg_warps = 65536 / (regs * 32);
@@ -1381,7 +1568,10 @@ cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bond
     if (wpb > want) wpb = want;
     if (max_wpb > 0 && wpb > max_wpb) wpb = max_wpb;
     if (wpb < 1) wpb = 1;
-    if (pl.u64 && sampler_smem_bytes(m, fp64, wpb, pl, n_bonds) > budget) pl.u64 = 0;
+    if (pl.u64 && sampler_smem_bytes(m, fp64, wpb, pl, n_bonds) > budget) {
+        if (pl.pair) return plan_sampler_impl(m, fp64, n_chains, n_bonds, out, max_wpb, 0);
+        pl.u64 = 0;
+    }
     while (wpb > 1 && sampler_smem_bytes(m, fp64, wpb, pl, n_bonds) > budget) wpb--;
     const int smem = sampler_smem_bytes(m, fp64, wpb, pl, n_bonds);
     if (smem > budget) return cudaErrorInvalidValue;
@@ -1391,13 +1581,18 @@ cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bond
     err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 32 * wpb, smem);
     if (err != cudaSuccess) return err;
     if (per_sm < 1) per_sm = 1;
-    long blocks = ((long)n_chains + wpb - 1) / wpb;
+    long blocks = ((long)units + wpb - 1) / wpb;
     if (blocks > (long)sms * per_sm) blocks = (long)sms * per_sm;
     out->plan = pl;
     out->warps_per_block = wpb;
     out->blocks = (int)blocks;
     out->smem = smem;
     return cudaSuccess;
+}
+
+cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bonds, SamplerShape* out, int max_wpb,
+                         int pair_mode) {
+    return plan_sampler_impl(m, fp64, n_chains, n_bonds, out, max_wpb, pair_mode);
 }
 
 cudaError_t ensure_dynamic_smem(const void* fn, int bytes) {
@@ -1415,7 +1610,7 @@ cudaError_t launch_sampler(const SamplerArgs& a0, int fp64, const SamplerShape& 
     SamplerArgs a = a0;
     a.plan = sh.plan;
     const int E = elements_per_lane(a.m.T);
-    const void* fn = pick_sampler(E, fp64, sh.plan.use_u, a.m.pf.n > 0, sh.plan.gather);
+    const void* fn = pick_sampler(E, fp64, sh.plan.use_u, a.m.pf.n > 0, sh.plan.gather, sh.plan.pair);
     if (!fn) return cudaErrorInvalidValue;
     const cudaError_t e = ensure_dynamic_smem(fn, sh.smem);
     if (e != cudaSuccess) return e;

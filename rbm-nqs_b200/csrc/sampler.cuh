@@ -48,6 +48,7 @@ struct SmemPlan {
     int bonds;  // proposal bond list
     int gather; // FP32 sweep with gathered flip rows (the expanded table does not fit)
     int wg;     // gather path: W32 with its zero pad row in shared memory
+    int pair;   // table path with two chains per warp
 };
 
 struct SamplerArgs {
@@ -140,9 +141,11 @@ struct SamplerShape {
     int blocks;
     int smem;
 };
-// max_wpb > 0 caps the warps per block (launch-shape autotuning).
+// max_wpb > 0 caps the warps per block (launch-shape autotuning); pair_mode
+// 1 asks for two chains per warp where the table path allows it (else, and
+// by default, one chain per warp).
 cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bonds, SamplerShape* out,
-                         int max_wpb = 0);
+                         int max_wpb = 0, int pair_mode = -1);
 cudaError_t launch_sampler(const SamplerArgs& a, int fp64, const SamplerShape& shape, cudaStream_t st);
 cudaError_t launch_eval(const EvalArgs& a, int fp64, int warps_per_block, cudaStream_t st);
 int elements_per_lane(int T);

@@ -110,6 +110,8 @@ def _declare(L):
         "rbmnqs_full_sample": [VP, P_D, P_D, P_D],
         "rbmnqs_get_observables": [VP, P_D],
         "rbmnqs_full_state": [VP, P_D],
+        "rbmnqs_set_sweep_shape": [VP, C.c_int32, C.c_int32],
+        "rbmnqs_get_sweep_shape": [VP, P_I, P_I],
         "rbmnqs_timing": [VP, P_D, P_I64, C.c_int32],
         "rbmnqs_timing_reset": [VP, C.c_int32],
         "rbmnqs_graph_kernels": [VP, P_I],
@@ -397,6 +399,14 @@ class Session:
         v = np.zeros(4 * self.model.n_obs, np.float64)
         _ck(lib().rbmnqs_get_observables(self._h, _p(v, P_D)))
         return v.reshape(-1, 4)
+
+    def set_sweep_shape(self, warps_per_block=0, chains_per_warp=1):
+        _ck(lib().rbmnqs_set_sweep_shape(self._h, warps_per_block, chains_per_warp))
+
+    def sweep_shape(self):
+        w, c = C.c_int32(), C.c_int32()
+        _ck(lib().rbmnqs_get_sweep_shape(self._h, C.byref(w), C.byref(c)))
+        return w.value, c.value
 
     def full_state(self):
         """Full enumeration (sampler_type 1): the normalised psi over all 2^n

@@ -109,6 +109,59 @@ def test_metropolis_fp32_statistics_agree():
     assert abs(st["energy"].real - ex) < 5 * st["stddev"] + 1e-3
 
 
+@pytest.mark.parametrize("L,kind,alpha,model,chains", [
+    (4, "symmetry", 4, "kitaev", 17),  # 32 sites, 128 entries: 8 per lane, two chains per warp, one half idle
+    (4, "symmetry", 4, "kitaev", 64),
+    (2, "basic", 1, "kitaev", 9),      # 8 sites, 8 entries
+    (3, "symmetry", 2, "toric", 12),   # 18 sites, 18 entries
+])
+def test_table_sweep_fp32_follows_fp64_chains(L, kind, alpha, model, chains):
+    """The FP32 expanded-table sweep (two chains per warp for n <= 32)
+    against the FP64 oracle chains on the same Philox streams: samples
+    coincide except after acceptance ties; the acceptance rates agree."""
+    rng = np.random.default_rng(6)
+    symm = 0.5 if model == "kitaev" else 1.0
+    om = O.Model.kitaev(L) if model == "kitaev" else O.Model.toric(L)
+    mach = O.Machine(om, kind, alpha, symm=symm).init_random(rng, 0.1)
+    gm = rbmnqs.Model.kitaev(L, symmetry=symm) if model == "kitaev" else rbmnqs.Model.toric(L, symmetry=symm)
+    bf = 0.5 if model == "kitaev" else 0.0
+    cfg = rbmnqs.default_config(rbm_type=1 if kind == "symmetry" else 0, alpha=alpha, n_chains=chains,
+                                samples_per_chain=8, warmup=5, bond_flips=bf, seed=31, precision=0)
+    s = rbmnqs.Session(gm, cfg)
+    s.set_weights(mach.params())
+    st = s.sample()
+    Eg, Og = s.samples()
+    Eo, Oo, acc, spo = O.metropolis(mach, om, chains, 8, warmup=5, bond_flips=bf, seed=31)
+    same = np.abs(Eg - Eo) < 1e-4 * np.maximum(1, np.abs(Eo))
+    assert np.mean(same) > 0.9
+    assert rel(Og[same], Oo[same]) < TOL32
+    assert abs(st["acceptance"] - acc.mean()) < 0.02
+    assert np.mean(np.all(s.spins() == spo, axis=1)) > 0.8
+
+
+@pytest.mark.parametrize("spec", [("kitaev4_symm_a4", 33, 0.5), ("kitaev3_basic_a1", 64, 0.5),
+                                  ("toric3_symm_a2", 10, 0.0)])
+def test_two_chains_per_warp_is_bit_identical(spec):
+    """The two-chains-per-warp sweep reproduces the one-chain sweep bit for
+    bit (same sums in the same order): samples, energies, O_k, spins and
+    weights after two epochs, for odd and even chain counts."""
+    case, chains, bf = spec
+    _, _, a, _ = make_pair(case, precision=0, chains=chains, spc=8, warmup=3, bond_flips=bf, std=0.2)
+    _, _, b, _ = make_pair(case, precision=0, chains=chains, spc=8, warmup=3, bond_flips=bf, std=0.2)
+    a.set_sweep_shape(0, 1)
+    b.set_sweep_shape(0, 2)
+    assert a.sweep_shape()[1] == 1 and b.sweep_shape()[1] == 2
+    for _ in range(2):
+        sa, _ = a.epoch()
+        sb, _ = b.epoch()
+        assert sa["acceptance"] == sb["acceptance"]
+    Ea, Oa = a.samples()
+    Eb, Ob = b.samples()
+    assert np.array_equal(Ea, Eb) and np.array_equal(Oa, Ob)
+    assert np.array_equal(a.spins(), b.spins())
+    assert np.array_equal(a.get_weights(), b.get_weights())
+
+
 @pytest.mark.parametrize("L,kind,alpha,model", [
     (8, "symmetry", 4, "kitaev"),   # 128 sites, 512 theta entries (16 per lane), W in shared memory
     (5, "symmetry", 4, "kitaev"),   # 50 sites, 200 entries (8 per lane)
@@ -260,6 +313,17 @@ def test_timing_counters():
     s.timing_reset(True)
     for _ in range(2):
         s.epoch()
+    ms, cnt = s.timing()
+    assert (cnt[:6] == 2).all() and (ms[:6] > 0).all()
+
+
+def test_timing_counters_eager_calls():
+    """Stage timing also for rbmnqs_sample / rbmnqs_optimize outside a graph."""
+    _, _, s, _ = make_pair("kitaev4_symm_a4", precision=0, chains=32, spc=8, warmup=1)
+    s.timing_reset(True)
+    for _ in range(2):
+        s.sample()
+        s.optimize()
     ms, cnt = s.timing()
     assert (cnt[:6] == 2).all() and (ms[:6] > 0).all()
 
