@@ -76,12 +76,48 @@ __device__ __forceinline__ float reduce_2pi(float b) {
     return fmaf(-k, -1.74845553146951e-07f, r);
 }
 
-__device__ __forceinline__ void sincos_r(float b, float* s, float* c) { __sincosf(reduce_2pi(b), s, c); }
+// The FP32 forms issue the hardware approximations in their flush-to-zero
+// variants (the non-flushing ones add a denormal test and rescale around
+// each): a denormal z = e^{-2|a|} (|a| > 43) becomes 0, the exact limit; a
+// denormal argument of the log (a zero of cosh to FP32 precision) gives
+// -inf, a state of vanishing amplitude.
+__device__ __forceinline__ float ftz_ex2(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ftz_lg2(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ftz_sin(float x) {
+    float y;
+    asm("sin.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ftz_cos(float x) {
+    float y;
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ftz_rsqrt(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ void sincos_r(float b, float* s, float* c) {
+    const float r = reduce_2pi(b);
+    *s = ftz_sin(r);
+    *c = ftz_cos(r);
+}
 __device__ __forceinline__ void sincos_r(double b, double* s, double* c) { sincos(b, s, c); }
-__device__ __forceinline__ float exp_r(float x) { return __expf(x); }
+__device__ __forceinline__ float exp_r(float x) { return ftz_ex2(x * 1.44269504088896341f); }
 __device__ __forceinline__ double exp_r(double x) { return exp(x); }
-__device__ __forceinline__ float log_r(float x) { return __logf(x); }
+__device__ __forceinline__ float log_r(float x) { return ftz_lg2(x) * 0.693147180559945309f; }
 __device__ __forceinline__ double log_r(double x) { return log(x); }
+__device__ __forceinline__ float rsqrt_r(float x) { return ftz_rsqrt(x); }
+__device__ __forceinline__ double rsqrt_r(double x) { return rsqrt(x); }
 
 // Real part only (Metropolis acceptance needs |psi'/psi|).
 template <typename R> __device__ __forceinline__ R lnc_re(R a, R b) {
@@ -103,7 +139,7 @@ template <typename R> __device__ __forceinline__ void lnc_full(R a, R b, R& re, 
     const R Y = copysign((R)1 - z, a) * s;
     const R m2 = X * X + Y * Y;
     re = aa + (R)0.5 * log_r(m2);
-    const R inv = m2 > (R)0 ? rsqrt(m2) : (R)0;
+    const R inv = m2 > (R)0 ? rsqrt_r(m2) : (R)0;
     ux = X * inv;
     uy = Y * inv;
 }
