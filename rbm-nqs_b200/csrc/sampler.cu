@@ -221,11 +221,23 @@ __device__ __noinline__ void evaluate(const MachineDev* __restrict__ mp, const H
                 C2<R> ph;
                 ratio_terms<E, R>(m, sPerm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph, ks);
                 const double2 b = bias_delta_smem(m, wsp, fl, nf);
-                const double mag = exp((double)dre + b.x);
-                double sb, cb;
-                sincos(b.y, &sb, &cb);
-                double rx = mag * ((double)ph.x * cb - (double)ph.y * sb);
-                double ry = mag * ((double)ph.x * sb + (double)ph.y * cb);
+                double rx, ry;
+                const double lm = (double)dre + b.x;  // ln|psi'/psi| of the RBM part
+                if (sizeof(R) == 4 && fabs(lm) < 80.0) {
+                    // FP32 path: the ratio to FP32 accuracy in FP32 arithmetic
+                    // (its inputs carry FP32 rounding already)
+                    const float mag = exp_r((float)lm);
+                    float sb, cb;
+                    sincos_r((float)b.y, &sb, &cb);
+                    rx = (double)(mag * ((float)ph.x * cb - (float)ph.y * sb));
+                    ry = (double)(mag * ((float)ph.x * sb + (float)ph.y * cb));
+                } else {
+                    const double mag = exp(lm);
+                    double sb, cb;
+                    sincos(b.y, &sb, &cb);
+                    rx = mag * ((double)ph.x * cb - (double)ph.y * sb);
+                    ry = mag * ((double)ph.x * sb + (double)ph.y * cb);
+                }
                 if constexpr (PF) {
                     const double2 c2 = pf_ratio_any(m.pf, wsp[0], fl, nf, lane, *pst, pA);
                     const double2 r = zmul(make_double2(rx, ry), c2);
