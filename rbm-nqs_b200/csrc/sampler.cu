@@ -124,13 +124,18 @@ __device__ __forceinline__ void entry_index(const MachineDev& m, int lane, uint3
     }
 }
 
-template <int E, typename R>
+// NF > 0: a compile-time flip count (the flips and their signs stay in
+// registers); NF = 0: nf flips at run time.
+template <int E, typename R, int NF = 0>
 __device__ __forceinline__ void ratio_terms(const MachineDev& m, const uint8_t* sPerm, const C2<R>* W,
-                                            const C2<R>* wth, const uint32_t* wsp, const int* fl, int nf,
+                                            const C2<R>* wth, const uint32_t* wsp, const int* fl, int nf_,
                                             const R* cre, const C2<R>* cu, int lane, R& dre, C2<R>& ph,
                                             const uint32_t (&ks)[E]) {
-    R sgn2[6];
-    for (int q = 0; q < nf; q++) sgn2[q] = smem_bit(wsp, fl[q]) ? (R)2 : (R)-2;  // -2 sigma_f
+    const int nf = NF > 0 ? NF : nf_;
+    R sgn2[NF > 0 ? NF : 6];
+#pragma unroll
+    for (int q = 0; q < (NF > 0 ? NF : 6); q++)
+        if (q < nf) sgn2[q] = smem_bit(wsp, fl[q]) ? (R)2 : (R)-2;  // -2 sigma_f
     dre = 0;
     ph = mk<R>(1, 0);
 #pragma unroll
@@ -138,7 +143,9 @@ __device__ __forceinline__ void ratio_terms(const MachineDev& m, const uint8_t* 
         if (!slot_valid(lane, e, m.T)) continue;
         const int t = lane + 32 * e, k = ks[e] & 0xffffu, s = ks[e] >> 16;
         C2<R> x = wth[t];
-        for (int q = 0; q < nf; q++) {
+#pragma unroll
+        for (int q = 0; q < (NF > 0 ? NF : 6); q++) {
+            if (q >= nf) break;
             const C2<R> u = W[urow<R>(m, sPerm, fl[q], s) * m.nh + k];
             x.x = fma(sgn2[q], u.x, x.x);
             x.y = fma(sgn2[q], u.y, x.y);
@@ -184,8 +191,8 @@ __device__ __noinline__ void evaluate(const MachineDev* __restrict__ mp, const H
                                       const uint8_t* sPerm, const uint8_t* sInv, const C2<R>* W, const C2<R>* wth,
                                       const uint32_t* wsp, R* cre, C2<R>* cu, const C2<R>* tn, int lane,
                                       double2* Eout, C2<R>* Orow, PfStage* pst, const double2* pA) {
-    const MachineDev m = *mp;
-    const HamDev H = *hp;
+    const MachineDev& m = *mp;
+    const HamDev& H = *hp;
     uint32_t ks[E];
     entry_index<E>(m, lane, ks);
     // ln cosh cache of the current theta
@@ -202,10 +209,11 @@ __device__ __noinline__ void evaluate(const MachineDev* __restrict__ mp, const H
     if (Eout) {
         double ex = 0, ey = 0;
         for (int o = 0; o < H.n_ops; o++) {
-            const OpDev op = H.ops[o];
+            const OpDev* op = H.ops + o;
+            const int k = op->k;
             int loc = 0;
-            for (int i = 0; i < op.k; i++) loc |= smem_bit(wsp, op.sites[i]) << i;
-            const int q0 = H.rowptr[op.rp + loc], q1 = H.rowptr[op.rp + loc + 1];
+            for (int i = 0; i < k; i++) loc |= smem_bit(wsp, op->sites[i]) << i;
+            const int q0 = H.rowptr[op->rp + loc], q1 = H.rowptr[op->rp + loc + 1];
             for (int q = q0; q < q1; q++) {
                 const uint32_t mask = H.ent_mask[q];
                 const double2 val = H.ent_val[q];
@@ -214,12 +222,28 @@ __device__ __noinline__ void evaluate(const MachineDev* __restrict__ mp, const H
                     ey += val.y;
                     continue;
                 }
-                int fl[6], nf = 0;
-                for (int i = 0; i < op.k; i++)
-                    if ((mask >> i) & 1) fl[nf++] = op.sites[i];
+                const int nf = __popc(mask);
+                int fl[6];
+                {
+                    uint32_t mm = mask;
+                    for (int j = 0; j < nf; j++) {
+                        fl[j] = op->sites[__ffs(mm) - 1];
+                        mm &= mm - 1;
+                    }
+                }
                 R dre;
                 C2<R> ph;
-                ratio_terms<E, R>(m, sPerm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph, ks);
+                // one- and two-site flips (every bond operator) with the flips
+                // in registers; larger flips with run-time loops
+                if (nf == 2) {
+                    const int f2[2] = {fl[0], fl[1]};
+                    ratio_terms<E, R, 2>(m, sPerm, W, wth, wsp, f2, 2, cre, cu, lane, dre, ph, ks);
+                } else if (nf == 1) {
+                    const int f1[1] = {fl[0]};
+                    ratio_terms<E, R, 1>(m, sPerm, W, wth, wsp, f1, 1, cre, cu, lane, dre, ph, ks);
+                } else {
+                    ratio_terms<E, R>(m, sPerm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph, ks);
+                }
                 const double2 b = bias_delta_smem(m, wsp, fl, nf);
                 double rx, ry;
                 const double lm = (double)dre + b.x;  // ln|psi'/psi| of the RBM part
@@ -1153,7 +1177,7 @@ __global__ void __launch_bounds__(FAST == 2 ? MaxThreads<E, PF>::gather
 // Batched evaluation at given configurations: log psi, E_loc, O_k, or the
 // log psi ratio for given flips (parity entry points).
 template <int E, typename R, bool PF>
-__global__ void __launch_bounds__(256) eval_kernel(const EvalArgs a) {
+__global__ void __launch_bounds__(256, 3) eval_kernel(const EvalArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const MachineDev& m = a.m;
     const int fp64 = sizeof(R) == 8;
