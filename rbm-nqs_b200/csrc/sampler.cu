@@ -354,7 +354,13 @@ struct Smem {
 };
 
 __host__ __device__ inline int align16(int x) { return (x + 15) & ~15; }
-__host__ __device__ inline int padded_T(int T) { return 32 * ((T + 31) / 32); }
+// Row length of the per-entry tables: 32 lanes x the entries per lane that
+// the kernels use (elements_per_lane: 1, 2, 4, 8 or 16), so that the tables'
+// layout and the kernels' indexing t = lane + 32 e agree for every T.
+__host__ __device__ inline int padded_T(int T) {
+    const int e = (T + 31) / 32;
+    return 32 * (e <= 1 ? 1 : e <= 2 ? 2 : e <= 4 ? 4 : e <= 8 ? 8 : 16);
+}
 
 // per-warp scratch.  Evaluation: spins (16 B) | theta [T] | ln cosh re [T] |
 // phase [T] | tanh theta [T] (evaluated in FP64 from the FP64 theta, so

@@ -114,6 +114,7 @@ def test_metropolis_fp32_statistics_agree():
     (4, "symmetry", 4, "kitaev", 64),
     (2, "basic", 1, "kitaev", 9),      # 8 sites, 8 entries
     (3, "symmetry", 2, "toric", 12),   # 18 sites, 18 entries
+    (3, "basic", 4, "kitaev", 12),     # 18 sites, 72 entries: rows padded to 4 per lane
 ])
 def test_table_sweep_fp32_follows_fp64_chains(L, kind, alpha, model, chains):
     """The FP32 expanded-table sweep (two chains per warp for n <= 32)
