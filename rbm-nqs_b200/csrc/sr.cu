@@ -584,12 +584,15 @@ __global__ void __launch_bounds__(1024) cg_packed(const double2* A, const double
 
 // The same iteration spread over one thread-block cluster of kClusterCta
 // CTAs on as many SMs.  CTA c owns rows [c*rp, (c+1)*rp) of S_reg (full rows
-// in its shared memory) and the matching slices of x, r, Ap; every CTA keeps
-// a full copy of p.  Per iteration: local mat-vec and p^H Ap partial, partial
-// pushed into every CTA's shared memory (DSMEM store), cluster barrier;
-// alpha, x/r update and ||r||^2 partial, pushed, barrier; beta, new p rows
-// pushed to every CTA's copy, barrier.  The operator, the arithmetic order
-// within a row and the stopping rule are those of cg_packed.
+// in its shared memory) and the matching slices of x, Ap; every CTA keeps
+// full copies of p and r.  Per iteration: local mat-vec and p^H Ap partial,
+// partial pushed into every CTA's shared memory (DSMEM store), cluster
+// barrier; alpha, x/r update of the own rows, the new r rows and the
+// ||r||^2 partial pushed to every CTA, barrier; beta and the whole new p
+// computed by every CTA from its full r and p (the same arithmetic on the
+// same data in every CTA, so the copies agree).  Two cluster barriers per
+// iteration.  The operator, the arithmetic order within a row and the
+// stopping rule are those of cg_packed.
 constexpr int kClusterCta = 8;
 
 __global__ void __cluster_dims__(kClusterCta, 1, 1) __launch_bounds__(256)
@@ -602,8 +605,8 @@ __global__ void __cluster_dims__(kClusterCta, 1, 1) __launch_bounds__(256)
     double2* Srow = reinterpret_cast<double2*>(sm);  // [rp][P]
     double2* p = Srow + (size_t)rp * P;              // [P] full copy
     double2* x = p + P;                              // [rp]
-    double2* r = x + rp;                             // [rp]
-    double2* Ap = r + rp;                            // [rp]
+    double2* rf = x + rp;                            // [P] full copy of r
+    double2* Ap = rf + P;                            // [rp]
     __shared__ double2 partA[kClusterCta], partB[kClusterCta];
     __shared__ double2 wred[8];
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
@@ -679,17 +682,13 @@ __global__ void __cluster_dims__(kClusterCta, 1, 1) __launch_bounds__(256)
     double rl0 = 0;
     for (int i = tid; i < nr; i += nt) {
         const double2 ri = make_double2(b[r0 + i].x - Ap[i].x, b[r0 + i].y - Ap[i].y);
-        r[i] = ri;
+        for (int c = 0; c < kClusterCta; c++) cl.map_shared_rank(rf, c)[r0 + i] = ri;
         rl0 += ri.x * ri.x + ri.y * ri.y;
     }
     push(partB, cta_sum(make_double2(rl0, 0)));
-    cl.sync();  // every CTA has finished reading p = x0
-    // p = r: one thread per own row publishes it to every CTA's copy
-    for (int q = tid; q < nr; q += nt) {
-        const double2 v = r[q];
-        for (int c = 0; c < kClusterCta; c++) cl.map_shared_rank(p, c)[r0 + q] = v;
-    }
-    cl.sync();
+    cl.sync();  // all of r is in every CTA; every CTA has finished reading p = x0
+    for (int i = tid; i < P; i += nt) p[i] = rf[i];  // p = r
+    __syncthreads();
     double rsold = total(partB).x;
     double rs = rsold;
     int itn = 0;
@@ -706,26 +705,23 @@ __global__ void __cluster_dims__(kClusterCta, 1, 1) __launch_bounds__(256)
             xi.x += ax * pi.x - ay * pi.y;
             xi.y += ax * pi.y + ay * pi.x;
             x[i] = xi;
-            double2 ri = r[i];
+            double2 ri = rf[r0 + i];
             ri.x -= ax * api.x - ay * api.y;
             ri.y -= ax * api.y + ay * api.x;
-            r[i] = ri;
+            for (int c = 0; c < kClusterCta; c++) cl.map_shared_rank(rf, c)[r0 + i] = ri;
             rl += ri.x * ri.x + ri.y * ri.y;
         }
         push(partB, cta_sum(make_double2(rl, 0)));
-        cl.sync();
+        cl.sync();  // the new r is complete in every CTA
         rs = total(partB).x;
         if (rs < rtol) break;
         const double beta = rs / rsold;
-        // new p rows: one thread per own row reads the old value once and
-        // writes the new one to every CTA's copy (its own included)
-        for (int q = tid; q < nr; q += nt) {
-            const double2 ri = r[q], pi = p[r0 + q];
-            const double2 v = make_double2(ri.x + beta * pi.x, ri.y + beta * pi.y);
-            for (int c = 0; c < kClusterCta; c++) cl.map_shared_rank(p, c)[r0 + q] = v;
+        for (int i = tid; i < P; i += nt) {
+            const double2 ri = rf[i], pi = p[i];
+            p[i] = make_double2(ri.x + beta * pi.x, ri.y + beta * pi.y);
         }
         rsold = rs;
-        cl.sync();
+        __syncthreads();
     }
     for (int i = tid; i < nr; i += nt) xg[r0 + i] = x[i];
     if (rank == 0 && tid == 0) {
@@ -1062,13 +1058,13 @@ cudaError_t launch_regularize(const double2* S, int P, int n_neural, int N, cons
 
 bool cg_cluster_fits(int P) {
     const int rp = (P + kClusterCta - 1) / kClusterCta;
-    return ((size_t)rp * P + P + 3 * (size_t)rp) * sizeof(double2) <= 200 * 1024;
+    return ((size_t)rp * P + 2 * (size_t)P + 2 * (size_t)rp) * sizeof(double2) <= 200 * 1024;
 }
 
 cudaError_t launch_cg(const double2* A, const double2* b, double2* x, int P, int max_it, double rtol, CgResultDev* res,
                       cudaStream_t st) {
     const int rp = (P + kClusterCta - 1) / kClusterCta;
-    const size_t csm = ((size_t)rp * P + P + 3 * (size_t)rp) * sizeof(double2);
+    const size_t csm = ((size_t)rp * P + 2 * (size_t)P + 2 * (size_t)rp) * sizeof(double2);
     if (csm <= 200 * 1024) {
         cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(cg_cluster), (int)csm);
         if (e != cudaSuccess) return e;
