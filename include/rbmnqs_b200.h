@@ -75,6 +75,17 @@ int rbmnqs_model_symmetry(const rbmnqs_model* m, int32_t* S, int32_t* n_vb,
  * (bs may be NULL) and the number of classes n_indep.  Host only. */
 int rbmnqs_model_pfaffian_classes(const rbmnqs_model* m, double symmetry,
                                   int32_t* bs, int32_t* n_indep);
+/* Exact diagonalisation on the GPU (n <= 28 sites): the lowest eigenvalue of
+ * the model's Hamiltonian by Lanczos on the full 2^n basis, stopping when it
+ * changed by at most tol (relative) over three iterations or after max_iter
+ * iterations; psi (2^n complex, interleaved re, im, may be NULL) receives
+ * the normalised eigenvector, indexed by the state number (bit i set <=>
+ * site i down).  The reference diagonalises small systems in Python
+ * (python_adapter/rbm/__init__.py:16-41, scipy); this is the same
+ * Hamiltonian and basis convention.  Allocates 3 (4 with psi) device
+ * vectors of 2^n x 16 bytes for the duration of the call. */
+int rbmnqs_model_ground_state(const rbmnqs_model* m, int32_t max_iter, double tol, uint64_t seed,
+                              double* energy, int32_t* iterations, double* psi);
 void rbmnqs_model_destroy(rbmnqs_model* m);
 
 /* ----------------------------------------------------------- config ---- */

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../host/model.hpp"
+#include "ed.cuh"
 #include "rbmnqs_b200.h"
 #include "gram_tc.cuh"
 #include "mlp.cuh"
@@ -582,6 +583,44 @@ int rbmnqs_model_symmetry(const rbmnqs_model* m, int32_t* S, int32_t* n_vb, int3
                 for (int i = 0; i < m->m.n; i++) perm[s * m->m.n + i] = m->m.perm[s][i];
         if (basis)
             for (size_t i = 0; i < m->m.basis.size(); i++) basis[i] = m->m.basis[i];
+    });
+}
+
+int rbmnqs_model_ground_state(const rbmnqs_model* m, int32_t max_iter, double tol, uint64_t seed, double* energy,
+                              int32_t* iterations, double* psi) {
+    return guard([&] {
+        require(m && energy && max_iter >= 1 && tol >= 0, "rbmnqs_model_ground_state: bad arguments");
+        const int n = m->m.n;
+        require(n >= 1 && n <= 28, "exact diagonalisation needs 1 <= n <= 28 sites", RBMNQS_ERR_UNSUPPORTED);
+        HamHost hh = build_ham(m->m.hamiltonian);
+        DevBuf<rbmnqs::OpDev> ops;
+        DevBuf<int> rowptr;
+        DevBuf<uint32_t> mask;
+        DevBuf<double2> val;
+        ops.alloc(hh.ops.size());
+        rowptr.alloc(hh.rowptr.size());
+        mask.alloc(std::max<size_t>(1, hh.mask.size()));
+        val.alloc(std::max<size_t>(1, hh.val.size()));
+        ck(cudaMemcpy(ops.p, hh.ops.data(), hh.ops.size() * sizeof(rbmnqs::OpDev), cudaMemcpyHostToDevice), "c");
+        ck(cudaMemcpy(rowptr.p, hh.rowptr.data(), hh.rowptr.size() * sizeof(int), cudaMemcpyHostToDevice), "c");
+        if (!hh.mask.empty()) {
+            ck(cudaMemcpy(mask.p, hh.mask.data(), hh.mask.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "c");
+            ck(cudaMemcpy(val.p, hh.val.data(), hh.val.size() * sizeof(double2), cudaMemcpyHostToDevice), "c");
+        }
+        rbmnqs::HamDev H{};
+        H.n_ops = (int)hh.ops.size();
+        H.ops = ops.p;
+        H.rowptr = rowptr.p;
+        H.ent_mask = mask.p;
+        H.ent_val = val.p;
+        cudaStream_t st;
+        ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+        int it = 0;
+        const cudaError_t e =
+            rbmnqs::ed_ground_state(H, n, max_iter, tol, seed, st, energy, &it, reinterpret_cast<double2*>(psi));
+        cudaStreamDestroy(st);
+        ck(e, "exact diagonalisation");
+        if (iterations) *iterations = it;
     });
 }
 

@@ -94,25 +94,41 @@ __global__ void moments_partial(const TO* O, const double2* E, int N, int P, dou
 // the sums are divided by *wsum (the total weight) when given, else by N.
 __global__ void moments_final(const double2* pd, const double2* pf, const double2* pe, int nb, int N_, int P,
                               double2* d, double2* F, double2* emean, const double* wsum) {
+    // one warp per parameter, lanes over the partial blocks (fixed order)
     __shared__ double2 em;
     const double N = wsum ? *wsum : (double)N_;
-    if (threadIdx.x == 0) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    auto wsum2 = [&](double2 v) {
+        for (int o = 16; o > 0; o >>= 1) {
+            v.x += __shfl_xor_sync(kFull, v.x, o);
+            v.y += __shfl_xor_sync(kFull, v.y, o);
+        }
+        return v;
+    };
+    if (w == 0) {
         double2 s = make_double2(0, 0);
-        for (int b = 0; b < nb; b++) s = add2(s, pe[b]);
-        em = make_double2(s.x / N, s.y / N);
-        if (blockIdx.x == 0) *emean = em;
+        for (int b = lane; b < nb; b += 32) s = add2(s, pe[b]);
+        s = wsum2(s);
+        if (lane == 0) {
+            em = make_double2(s.x / N, s.y / N);
+            if (blockIdx.x == 0) *emean = em;
+        }
     }
     __syncthreads();
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+    for (int p = blockIdx.x * nw + w; p < P; p += gridDim.x * nw) {
         double2 sd = make_double2(0, 0), sf = make_double2(0, 0);
-        for (int b = 0; b < nb; b++) {
+        for (int b = lane; b < nb; b += 32) {
             sd = add2(sd, pd[(size_t)b * P + p]);
             sf = add2(sf, pf[(size_t)b * P + p]);
         }
-        const double2 dd = make_double2(sd.x / N, sd.y / N);
-        d[p] = dd;
-        // F = dh - h * conj(d)
-        F[p] = make_double2(sf.x / N - (em.x * dd.x + em.y * dd.y), sf.y / N - (em.y * dd.x - em.x * dd.y));
+        sd = wsum2(sd);
+        sf = wsum2(sf);
+        if (lane == 0) {
+            const double2 dd = make_double2(sd.x / N, sd.y / N);
+            d[p] = dd;
+            // F = dh - h * conj(d)
+            F[p] = make_double2(sf.x / N - (em.x * dd.x + em.y * dd.y), sf.y / N - (em.y * dd.x - em.x * dd.y));
+        }
     }
 }
 
@@ -995,7 +1011,7 @@ cudaError_t launch_moments(const void* O, int fp64, const double2* E, int N, int
         moments_partial<double2><<<nblk, 256, 0, st>>>((const double2*)O, E, N, P, pd, pf, pe, w);
     else
         moments_partial<float2><<<nblk, 256, 0, st>>>((const float2*)O, E, N, P, pd, pf, pe, w);
-    moments_final<<<(P + 255) / 256, 256, 0, st>>>(pd, pf, pe, nblk, N, P, d, F, emean, wsum);
+    moments_final<<<(P + 7) / 8, 256, 0, st>>>(pd, pf, pe, nblk, N, P, d, F, emean, wsum);
     return cudaGetLastError();
 }
 

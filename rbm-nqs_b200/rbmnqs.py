@@ -110,6 +110,7 @@ def _declare(L):
         "rbmnqs_full_sample": [VP, P_D, P_D, P_D],
         "rbmnqs_get_observables": [VP, P_D],
         "rbmnqs_full_state": [VP, P_D],
+        "rbmnqs_model_ground_state": [VP, C.c_int32, C.c_double, C.c_uint64, P_D, P_I, P_D],
         "rbmnqs_set_sweep_shape": [VP, C.c_int32, C.c_int32],
         "rbmnqs_get_sweep_shape": [VP, P_I, P_I],
         "rbmnqs_timing": [VP, P_D, P_I64, C.c_int32],
@@ -221,6 +222,15 @@ class Model:
         out = VP()
         _ck(lib().rbmnqs_model_toric(n_cells, J, symmetry, C.byref(out)))
         return Model(out, "toric")
+
+    def ground_state(self, max_iter=400, tol=1e-13, seed=1, vector=False):
+        """Exact diagonalisation on the GPU (Lanczos, n <= 28): (E0,
+        iterations[, psi over the 2^n states])."""
+        e, it = C.c_double(), C.c_int32()
+        psi = np.zeros(1 << self.n, np.complex128) if vector else None
+        _ck(lib().rbmnqs_model_ground_state(self._h, max_iter, tol, seed, C.byref(e), C.byref(it),
+                                            _p(psi.view(np.float64), P_D) if vector else None))
+        return (e.value, it.value, psi) if vector else (e.value, it.value)
 
     def bonds(self):
         a = np.zeros((self.n_bonds, 3), np.int32)
