@@ -124,10 +124,17 @@ __device__ __forceinline__ void entry_index(const MachineDev& m, int lane, uint3
     }
 }
 
+// The machine sizes the ratio loop reads, held in registers (the machine
+// descriptor itself is in global memory).
+struct RatioDims {
+    int T, nh, S, symmetric;
+};
+__device__ __forceinline__ RatioDims ratio_dims(const MachineDev& m) { return RatioDims{m.T, m.nh, m.S, m.symmetric}; }
+
 // NF > 0: a compile-time flip count (the flips and their signs stay in
 // registers); NF = 0: nf flips at run time.
 template <int E, typename R, int NF = 0>
-__device__ __forceinline__ void ratio_terms(const MachineDev& m, const uint8_t* sPerm, const C2<R>* W,
+__device__ __forceinline__ void ratio_terms(const RatioDims m, const uint8_t* sPerm, const C2<R>* W,
                                             const C2<R>* wth, const uint32_t* wsp, const int* fl, int nf_,
                                             const R* cre, const C2<R>* cu, int lane, R& dre, C2<R>& ph,
                                             const uint32_t (&ks)[E]) {
@@ -146,7 +153,8 @@ __device__ __forceinline__ void ratio_terms(const MachineDev& m, const uint8_t* 
 #pragma unroll
         for (int q = 0; q < (NF > 0 ? NF : 6); q++) {
             if (q >= nf) break;
-            const C2<R> u = W[urow<R>(m, sPerm, fl[q], s) * m.nh + k];
+            const int row = m.symmetric ? (int)sPerm[fl[q] * m.S + s] : fl[q];
+            const C2<R> u = W[row * m.nh + k];
             x.x = fma(sgn2[q], u.x, x.x);
             x.y = fma(sgn2[q], u.y, x.y);
         }
@@ -161,8 +169,6 @@ __device__ __forceinline__ void ratio_terms(const MachineDev& m, const uint8_t* 
 
 // E_loc and O_k of the configuration in the warp's scratch (wsp bits, wth
 // theta): local_op.cpp:31-60, rbm_base.cpp:194-217, rbm_symmetry.cpp:97-130.
-// Kept out of line: it runs once per sample, the sweep loop keeps its
-// registers.
 // Pfaffian factor (PF): term ratios multiply by the rank-2m ratio from the
 // warp's X^{-1} in shared memory (pA, leading dimension kPfLd), the O_k of
 // the pair parameters are gathered from it.
@@ -187,12 +193,13 @@ __device__ __noinline__ double2 pf_ratio_any(const PfDev& p, uint32_t bits, cons
 }
 
 template <int E, typename R, bool PF>
-__device__ __noinline__ void evaluate(const MachineDev* __restrict__ mp, const HamDev* __restrict__ hp,
+__device__ __forceinline__ void evaluate(const MachineDev* __restrict__ mp, const HamDev* __restrict__ hp,
                                       const uint8_t* sPerm, const uint8_t* sInv, const C2<R>* W, const C2<R>* wth,
                                       const uint32_t* wsp, R* cre, C2<R>* cu, const C2<R>* tn, int lane,
                                       double2* Eout, C2<R>* Orow, PfStage* pst, const double2* pA) {
     const MachineDev& m = *mp;
     const HamDev& H = *hp;
+    const RatioDims rd = ratio_dims(m);
     uint32_t ks[E];
     entry_index<E>(m, lane, ks);
     // ln cosh cache of the current theta
@@ -224,25 +231,29 @@ __device__ __noinline__ void evaluate(const MachineDev* __restrict__ mp, const H
                 }
                 const int nf = __popc(mask);
                 int fl[6];
-                {
+                // one- and two-site flips (every bond operator) with the flips
+                // in registers; larger flips with run-time loops
+                R dre;
+                C2<R> ph;
+                if (nf <= 2) {
+                    const int i0 = __ffs(mask) - 1;
+                    const int i1 = nf == 2 ? __ffs(mask & (mask - 1)) - 1 : i0;
+                    fl[0] = op->sites[i0];
+                    fl[1] = op->sites[i1];
+                    if (nf == 2) {
+                        const int f2[2] = {fl[0], fl[1]};
+                        ratio_terms<E, R, 2>(rd, sPerm, W, wth, wsp, f2, 2, cre, cu, lane, dre, ph, ks);
+                    } else {
+                        const int f1[1] = {fl[0]};
+                        ratio_terms<E, R, 1>(rd, sPerm, W, wth, wsp, f1, 1, cre, cu, lane, dre, ph, ks);
+                    }
+                } else {
                     uint32_t mm = mask;
                     for (int j = 0; j < nf; j++) {
                         fl[j] = op->sites[__ffs(mm) - 1];
                         mm &= mm - 1;
                     }
-                }
-                R dre;
-                C2<R> ph;
-                // one- and two-site flips (every bond operator) with the flips
-                // in registers; larger flips with run-time loops
-                if (nf == 2) {
-                    const int f2[2] = {fl[0], fl[1]};
-                    ratio_terms<E, R, 2>(m, sPerm, W, wth, wsp, f2, 2, cre, cu, lane, dre, ph, ks);
-                } else if (nf == 1) {
-                    const int f1[1] = {fl[0]};
-                    ratio_terms<E, R, 1>(m, sPerm, W, wth, wsp, f1, 1, cre, cu, lane, dre, ph, ks);
-                } else {
-                    ratio_terms<E, R>(m, sPerm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph, ks);
+                    ratio_terms<E, R>(rd, sPerm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph, ks);
                 }
                 const double2 b = bias_delta_smem(m, wsp, fl, nf);
                 double rx, ry;
@@ -1183,7 +1194,7 @@ __global__ void __launch_bounds__(FAST == 2 ? MaxThreads<E, PF>::gather
 // Batched evaluation at given configurations: log psi, E_loc, O_k, or the
 // log psi ratio for given flips (parity entry points).
 template <int E, typename R, bool PF>
-__global__ void __launch_bounds__(256, 3) eval_kernel(const EvalArgs a) {
+__global__ void __launch_bounds__(256, E <= 4 ? 3 : 2) eval_kernel(const EvalArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const MachineDev& m = a.m;
     const int fp64 = sizeof(R) == 8;
@@ -1271,7 +1282,7 @@ __global__ void __launch_bounds__(256, 3) eval_kernel(const EvalArgs a) {
         C2<R> ph;
         uint32_t ks[E];
         entry_index<E>(m, lane, ks);
-        ratio_terms<E, R>(m, sm.perm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph, ks);
+        ratio_terms<E, R>(ratio_dims(m), sm.perm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph, ks);
         double2 lr = make_double2(0.0, 0.0);
         if constexpr (PF) {
             const double2 c2 = pf_ratio_any(m.pf, sp[0], fl, nf, lane, *pst, pA);
