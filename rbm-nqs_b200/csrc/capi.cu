@@ -254,6 +254,8 @@ struct rbmnqs_handle {
         H.rowptr = rowptr.p;
         H.ent_mask = emask.p;
         H.ent_val = eval.p;
+        H.n_rows = (int)rowptr.n;
+        H.n_ents = (int)emask.n;
         return H;
     }
     size_t osize() const { return fp64 ? sizeof(double2) : sizeof(float2); }
@@ -292,6 +294,14 @@ struct rbmnqs_handle {
         a.n_prop = nprop.p;
         return a;
     }
+    // evaluation tables: W in shared memory when it fits, the operator
+    // tables staged in shared memory when they fit
+    rbmnqs::SmemPlan eval_plan() const {
+        rbmnqs::SmemPlan p{};
+        p.w32 = w_in_smem;
+        p.ham = rbmnqs::ham_stage_bytes(ham());
+        return p;
+    }
     rbmnqs::EvalArgs eval_args() const {
         rbmnqs::EvalArgs ea{};
         ea.m = machine();
@@ -302,7 +312,7 @@ struct rbmnqs_handle {
         ea.B = N;
         ea.eloc = E.p;
         ea.O = O.p;
-        ea.plan = rbmnqs::SmemPlan{0, w_in_smem, 0, 0, 0};
+        ea.plan = eval_plan();
         return ea;
     }
     rbmnqs::LearnedArgs learned_args() const {
@@ -842,6 +852,8 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
             od->H.rowptr = od->rowptr.p;
             od->H.ent_mask = od->mask.p;
             od->H.ent_val = od->val.p;
+            od->H.n_rows = (int)oh.rowptr.size();
+            od->H.n_ents = (int)oh.mask.size();
             od->hd.alloc(1);
             ck(cudaMemcpy(od->hd.p, &od->H, sizeof(od->H), cudaMemcpyHostToDevice), "c");
             h->obs.push_back(std::move(od));
@@ -1004,7 +1016,7 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         h->w_in_smem = (size_t)n * nh * 8 <= 64 * 1024 ? 1 : 0;
         h->wpb = 8;
         {
-            rbmnqs::SmemPlan pl{0, h->w_in_smem, 0, 0, 0};
+            const rbmnqs::SmemPlan pl = h->eval_plan();
             while (h->wpb > 1 && rbmnqs::eval_smem_bytes(h->machine(), h->fp64, h->wpb, pl) > 200 * 1024)
                 h->wpb >>= 1;
         }
@@ -1477,6 +1489,7 @@ int rbmnqs_get_observables(rbmnqs_handle* h, double* values) {
         for (int i = 0; i < no; i++) {
             rbmnqs::EvalArgs ea = h->eval_args();
             ea.H = h->obs[i]->H;
+            ea.plan.ham = rbmnqs::ham_stage_bytes(ea.H);
             ea.hd = h->obs[i]->hd.p;
             ea.O = nullptr;
             ea.eloc = h->obsE.p;
@@ -1630,7 +1643,7 @@ int rbmnqs_autotune(rbmnqs_handle* h, int32_t sweeps, int32_t* sampler_wpb, int3
         // evaluation kernel: 1..8 warps per block within the smem budget
         {
             rbmnqs::EvalArgs ea = h->eval_args();
-            rbmnqs::SmemPlan pl{0, h->w_in_smem, 0, 0, 0};
+            const rbmnqs::SmemPlan pl = h->eval_plan();
             double best = -1;
             int bw = h->wpb;
             for (int w = 1; w <= 8; w *= 2) {

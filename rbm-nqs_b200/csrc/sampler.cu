@@ -193,12 +193,11 @@ __device__ __noinline__ double2 pf_ratio_any(const PfDev& p, uint32_t bits, cons
 }
 
 template <int E, typename R, bool PF>
-__device__ __forceinline__ void evaluate(const MachineDev* __restrict__ mp, const HamDev* __restrict__ hp,
+__device__ __forceinline__ void evaluate(const MachineDev* __restrict__ mp, const HamDev H,
                                       const uint8_t* sPerm, const uint8_t* sInv, const C2<R>* W, const C2<R>* wth,
                                       const uint32_t* wsp, R* cre, C2<R>* cu, const C2<R>* tn, int lane,
                                       double2* Eout, C2<R>* Orow, PfStage* pst, const double2* pA) {
     const MachineDev& m = *mp;
-    const HamDev& H = *hp;
     const RatioDims rd = ratio_dims(m);
     uint32_t ks[E];
     entry_index<E>(m, lane, ks);
@@ -360,6 +359,7 @@ struct Smem {
     int2* bonds;    // proposal bonds
     float2* Wg;     // gather path: [n+1][nh] FP32 W, row n = 0 (shared or global)
     uint8_t* Pg;    // gather path, symmetric: [n+1][S] P_s(f), row n = n
+    unsigned char* ham;  // evaluation: staged Hamiltonian tables
     unsigned char* warp0;
     int warp_bytes;
 };
@@ -399,6 +399,7 @@ __host__ __device__ inline int table_bytes(const MachineDev& m, int fp64, const 
     if (pl.bonds) b += align16(n_bonds * 8);
     if (pl.gather && pl.wg) b += align16((m.n + 1) * m.nh * 8);
     if (pl.gather && m.symmetric) b += align16((m.n + 1) * m.S);
+    b += align16(pl.ham);
     return b;
 }
 
@@ -447,6 +448,8 @@ __device__ inline Smem carve(unsigned char* base, const MachineDev& m, int fp64,
             off += align16((m.n + 1) * m.S);
         }
     }
+    s.ham = base + off;
+    off += align16(pl.ham);
     s.warp0 = base + off;
     s.warp_bytes = warp_bytes;
     return s;
@@ -1200,6 +1203,32 @@ __global__ void __launch_bounds__(256, E <= 4 ? 3 : 2) eval_kernel(const EvalArg
     const int fp64 = sizeof(R) == 8;
     Smem sm = carve(smem, m, fp64, a.plan, 0, eval_warp_bytes(m.T, sizeof(R), PF));
     load_tables(m, sm, fp64, a.plan, nullptr, 0);
+    // the operator tables in shared memory: every term of E_loc walks them
+    // in a chain of dependent loads
+    HamDev H = a.H;
+    if (a.plan.ham) {
+        unsigned char* hb = sm.ham;
+        OpDev* sops = reinterpret_cast<OpDev*>(hb);
+        hb += align16(H.n_ops * (int)sizeof(OpDev));
+        int* srow = reinterpret_cast<int*>(hb);
+        hb += align16(H.n_rows * 4);
+        uint32_t* smask = reinterpret_cast<uint32_t*>(hb);
+        hb += align16(H.n_ents * 4);
+        double2* sval = reinterpret_cast<double2*>(hb);
+        const int ow = H.n_ops * (int)(sizeof(OpDev) / 4);
+        for (int i = threadIdx.x; i < ow; i += blockDim.x)
+            reinterpret_cast<int*>(sops)[i] = reinterpret_cast<const int*>(H.ops)[i];
+        for (int i = threadIdx.x; i < H.n_rows; i += blockDim.x) srow[i] = H.rowptr[i];
+        for (int i = threadIdx.x; i < H.n_ents; i += blockDim.x) {
+            smask[i] = H.ent_mask[i];
+            sval[i] = H.ent_val[i];
+        }
+        __syncthreads();
+        H.ops = sops;
+        H.rowptr = srow;
+        H.ent_mask = smask;
+        H.ent_val = sval;
+    }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b = blockIdx.x * (blockDim.x >> 5) + warp;
     if (b >= a.B) return;
@@ -1296,7 +1325,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 3 : 2) eval_kernel(const EvalArg
     }
     if (a.eloc || a.O) {
         C2<R>* Orow = a.O ? reinterpret_cast<C2<R>*>(a.O) + (size_t)b * m.P : nullptr;
-        evaluate<E, R, PF>(a.md, a.hd, sm.perm, sm.inv, W, wth, wsp, cre, cu, tn, lane,
+        evaluate<E, R, PF>(a.md, H, sm.perm, sm.inv, W, wth, wsp, cre, cu, tn, lane,
                            a.eloc ? a.eloc + b : nullptr, Orow, pst, pA);
         if constexpr (PF)
             if (Orow) pf_derivative(m.pf, sp[0], lane, pA, Orow + m.P_neural);
@@ -1538,6 +1567,13 @@ int elements_per_lane(int T) {
 
 int sampler_smem_bytes(const MachineDev& m, int fp64, int warps, const SmemPlan& plan, int n_bonds) {
     return table_bytes(m, fp64, plan, n_bonds) + warps * sweep_warp_bytes(m.T, fp64 ? 8 : 4, m.pf.n > 0);
+}
+
+int ham_stage_bytes(const HamDev& H) {
+    if (H.n_rows <= 0) return 0;
+    const int b = align16(H.n_ops * (int)sizeof(OpDev)) + align16(H.n_rows * 4) + align16(H.n_ents * 4) +
+                  align16(H.n_ents * 16);
+    return b <= 48 * 1024 ? b : 0;
 }
 
 int eval_smem_bytes(const MachineDev& m, int fp64, int warps, const SmemPlan& plan) {

@@ -37,7 +37,10 @@ struct HamDev {
     const int* rowptr;
     const uint32_t* ent_mask;
     const double2* ent_val;
+    int n_rows, n_ents;  // lengths of rowptr and of the entry arrays
 };
+// Bytes of a HamDev's tables staged in shared memory (0: too large to stage).
+int ham_stage_bytes(const HamDev& H);
 
 // Which tables live in shared memory (decided on the host from their sizes).
 struct SmemPlan {
@@ -49,6 +52,7 @@ struct SmemPlan {
     int gather; // FP32 sweep with gathered flip rows (the expanded table does not fit)
     int wg;     // gather path: W32 with its zero pad row in shared memory
     int pair;   // table path with two chains per warp
+    int ham;    // evaluation: bytes of the Hamiltonian tables staged in shared memory (0: read from L2)
 };
 
 struct SamplerArgs {
