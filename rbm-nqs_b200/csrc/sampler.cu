@@ -1023,7 +1023,23 @@ __device__ __forceinline__ void run_chain_pair(const SamplerArgs& a, const Smem&
 // kept in registers and becomes theta on acceptance.  Otherwise the same
 // proposal decoding, running ln|cosh| sum and FP64 recompute per sweep as
 // run_chain_fast.
-template <int E, bool SYM>
+// Shared-memory loads by 32-bit shared address: the gather tables may also
+// live in global memory, so their generic pointers would otherwise compile
+// to generic loads.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ float2 lds_f2(uint32_t addr) {
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+    return v;
+}
+__device__ __forceinline__ uint32_t lds_u8(uint32_t addr) {
+    uint32_t v;
+    asm volatile("ld.shared.u8 %0, [%1];" : "=r"(v) : "r"(addr));
+    return v;
+}
+
+// WS: the FP32 flip rows (with their zero pad row) are in shared memory.
+template <int E, bool SYM, bool WS>
 __device__ __forceinline__ void run_chain_gather(const SamplerArgs& a, const Smem& sm, int chain, int lane) {
     const MachineDev& m = a.m;
     const int n = m.n, nh = m.nh, S = m.S;
@@ -1044,9 +1060,17 @@ __device__ __forceinline__ void run_chain_gather(const SamplerArgs& a, const Sme
     }
     const float2* Wg = sm.Wg;
     const uint8_t* Pg = sm.Pg;
+    const uint32_t wsa = WS ? smem_addr(Wg) : 0u, psa = SYM ? smem_addr(Pg) : 0u;
     auto row = [&](int f, uint32_t en) -> int { return SYM ? (int)Pg[f * S + (en >> 16)] : f; };
     auto urd = [&](int f, int e) -> float2 {
-        const float2 u = Wg[row(f, ent[e]) * nh + (ent[e] & 0xffffu)];
+        const uint32_t en = ent[e];
+        float2 u;
+        if constexpr (WS) {
+            const int r = SYM ? (int)lds_u8(psa + (uint32_t)(f * S + (en >> 16))) : f;
+            u = lds_f2(wsa + 8u * (uint32_t)(r * nh + (en & 0xffffu)));
+        } else {
+            u = Wg[row(f, en) * nh + (en & 0xffffu)];
+        }
         return ((vmask >> e) & 1u) ? u : make_float2(0.f, 0.f);
     };
 
@@ -1184,10 +1208,17 @@ __global__ void __launch_bounds__(FAST == 2 ? MaxThreads<E, PF>::gather
             else
                 run_chain_fast<E, 4>(a, sm, chain, lane);
         else if constexpr (FAST == 2) {
-            if (a.m.symmetric)
-                run_chain_gather<E, true>(a, sm, chain, lane);
-            else
-                run_chain_gather<E, false>(a, sm, chain, lane);
+            if (a.m.symmetric) {
+                if (a.plan.wg)
+                    run_chain_gather<E, true, true>(a, sm, chain, lane);
+                else
+                    run_chain_gather<E, true, false>(a, sm, chain, lane);
+            } else {
+                if (a.plan.wg)
+                    run_chain_gather<E, false, true>(a, sm, chain, lane);
+                else
+                    run_chain_gather<E, false, false>(a, sm, chain, lane);
+            }
         } else
             run_chain<E, R, PF>(a, sm, chain, lane, wlp, pst, pA, pscr);
     }
