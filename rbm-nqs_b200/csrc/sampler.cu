@@ -30,6 +30,21 @@ template <> struct Wsel<double> {
     static __device__ __forceinline__ const double2* get(const MachineDev& m, const float2*) { return m.W64; }
 };
 
+// Shared-memory loads by 32-bit shared address: the gather tables may also
+// live in global memory, so their generic pointers would otherwise compile
+// to generic loads.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ float2 lds_f2(uint32_t addr) {
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+    return v;
+}
+__device__ __forceinline__ uint32_t lds_u8(uint32_t addr) {
+    uint32_t v;
+    asm volatile("ld.shared.u8 %0, [%1];" : "=r"(v) : "r"(addr));
+    return v;
+}
+
 // word i of the configuration with constant indices only (a runtime index
 // would place the array in local memory)
 __device__ __forceinline__ uint32_t spin_word(const uint32_t sp[4], int i) {
@@ -133,7 +148,9 @@ __device__ __forceinline__ RatioDims ratio_dims(const MachineDev& m) { return Ra
 
 // NF > 0: a compile-time flip count (the flips and their signs stay in
 // registers); NF = 0: nf flips at run time.
-template <int E, typename R, int NF = 0>
+// WS (FP32): W and the symmetry table are in shared memory, read by shared
+// addresses.
+template <int E, typename R, int NF = 0, bool WS = false>
 __device__ __forceinline__ void ratio_terms(const RatioDims m, const uint8_t* sPerm, const C2<R>* W,
                                             const C2<R>* wth, const uint32_t* wsp, const int* fl, int nf_,
                                             const R* cre, const C2<R>* cu, int lane, R& dre, C2<R>& ph,
@@ -153,8 +170,15 @@ __device__ __forceinline__ void ratio_terms(const RatioDims m, const uint8_t* sP
 #pragma unroll
         for (int q = 0; q < (NF > 0 ? NF : 6); q++) {
             if (q >= nf) break;
-            const int row = m.symmetric ? (int)sPerm[fl[q] * m.S + s] : fl[q];
-            const C2<R> u = W[row * m.nh + k];
+            C2<R> u;
+            if constexpr (WS && sizeof(R) == 4) {
+                const int row = m.symmetric ? (int)lds_u8(smem_addr(sPerm) + (uint32_t)(fl[q] * m.S + s)) : fl[q];
+                const float2 v = lds_f2(smem_addr(W) + 8u * (uint32_t)(row * m.nh + k));
+                u = mk<R>(v.x, v.y);
+            } else {
+                const int row = m.symmetric ? (int)sPerm[fl[q] * m.S + s] : fl[q];
+                u = W[row * m.nh + k];
+            }
             x.x = fma(sgn2[q], u.x, x.x);
             x.y = fma(sgn2[q], u.y, x.y);
         }
@@ -192,7 +216,7 @@ __device__ __noinline__ double2 pf_ratio_any(const PfDev& p, uint32_t bits, cons
     }
 }
 
-template <int E, typename R, bool PF>
+template <int E, typename R, bool PF, bool WS>
 __device__ __forceinline__ void evaluate(const MachineDev* __restrict__ mp, const HamDev H,
                                       const uint8_t* sPerm, const uint8_t* sInv, const C2<R>* W, const C2<R>* wth,
                                       const uint32_t* wsp, R* cre, C2<R>* cu, const C2<R>* tn, int lane,
@@ -241,10 +265,10 @@ __device__ __forceinline__ void evaluate(const MachineDev* __restrict__ mp, cons
                     fl[1] = op->sites[i1];
                     if (nf == 2) {
                         const int f2[2] = {fl[0], fl[1]};
-                        ratio_terms<E, R, 2>(rd, sPerm, W, wth, wsp, f2, 2, cre, cu, lane, dre, ph, ks);
+                        ratio_terms<E, R, 2, WS>(rd, sPerm, W, wth, wsp, f2, 2, cre, cu, lane, dre, ph, ks);
                     } else {
                         const int f1[1] = {fl[0]};
-                        ratio_terms<E, R, 1>(rd, sPerm, W, wth, wsp, f1, 1, cre, cu, lane, dre, ph, ks);
+                        ratio_terms<E, R, 1, WS>(rd, sPerm, W, wth, wsp, f1, 1, cre, cu, lane, dre, ph, ks);
                     }
                 } else {
                     uint32_t mm = mask;
@@ -252,7 +276,7 @@ __device__ __forceinline__ void evaluate(const MachineDev* __restrict__ mp, cons
                         fl[j] = op->sites[__ffs(mm) - 1];
                         mm &= mm - 1;
                     }
-                    ratio_terms<E, R>(rd, sPerm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph, ks);
+                    ratio_terms<E, R, 0, WS>(rd, sPerm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph, ks);
                 }
                 const double2 b = bias_delta_smem(m, wsp, fl, nf);
                 double rx, ry;
@@ -1023,21 +1047,6 @@ __device__ __forceinline__ void run_chain_pair(const SamplerArgs& a, const Smem&
 // kept in registers and becomes theta on acceptance.  Otherwise the same
 // proposal decoding, running ln|cosh| sum and FP64 recompute per sweep as
 // run_chain_fast.
-// Shared-memory loads by 32-bit shared address: the gather tables may also
-// live in global memory, so their generic pointers would otherwise compile
-// to generic loads.
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ float2 lds_f2(uint32_t addr) {
-    float2 v;
-    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
-    return v;
-}
-__device__ __forceinline__ uint32_t lds_u8(uint32_t addr) {
-    uint32_t v;
-    asm volatile("ld.shared.u8 %0, [%1];" : "=r"(v) : "r"(addr));
-    return v;
-}
-
 // WS: the FP32 flip rows (with their zero pad row) are in shared memory.
 template <int E, bool SYM, bool WS>
 __device__ __forceinline__ void run_chain_gather(const SamplerArgs& a, const Smem& sm, int chain, int lane) {
@@ -1356,8 +1365,12 @@ __global__ void __launch_bounds__(256, E <= 4 ? 3 : 2) eval_kernel(const EvalArg
     }
     if (a.eloc || a.O) {
         C2<R>* Orow = a.O ? reinterpret_cast<C2<R>*>(a.O) + (size_t)b * m.P : nullptr;
-        evaluate<E, R, PF>(a.md, H, sm.perm, sm.inv, W, wth, wsp, cre, cu, tn, lane,
-                           a.eloc ? a.eloc + b : nullptr, Orow, pst, pA);
+        if (sizeof(R) == 4 && sm.W32)
+            evaluate<E, R, PF, true>(a.md, H, sm.perm, sm.inv, W, wth, wsp, cre, cu, tn, lane,
+                               a.eloc ? a.eloc + b : nullptr, Orow, pst, pA);
+        else
+            evaluate<E, R, PF, false>(a.md, H, sm.perm, sm.inv, W, wth, wsp, cre, cu, tn, lane,
+                               a.eloc ? a.eloc + b : nullptr, Orow, pst, pA);
         if constexpr (PF)
             if (Orow) pf_derivative(m.pf, sp[0], lane, pA, Orow + m.P_neural);
     }
