@@ -741,12 +741,31 @@ __device__ __forceinline__ float cos_ftz(float x) {
     asm("cos.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
-__device__ __forceinline__ float lnc_sweep(float2 t) {
-    const float aa = fabsf(t.x);
-    const float z = ex2_ftz(aa * -2.88539008177792681f);  // e^{-2|a|} = 2^{-2|a| log2 e}
-    const float c2 = cos_ftz(2.f * t.y);
-    const float m2 = fmaf(z, fmaf(2.f, c2, z), 1.f);       // 1 + z (2 cos 2b + z)
-    return fmaf(0.346573590279972655f, lg2_ftz(m2), aa);  // aa + 0.5 ln(m2)
+
+// Sum of ln|cosh| (the form above) over a lane's E entries: the |a| terms
+// add up and the factors 1 + z^2 + 2 z cos 2b (each in [0, 4]) multiply in
+// groups of four, one lg2 per group instead of one per entry.  A group's
+// product stays within FP32 range unless its states have vanishing
+// amplitude (then ln|cosh| is -inf either way).  Same order of operations
+// for a given group of entries wherever it is formed.
+template <int E> __device__ __forceinline__ float lnc_sweep_sum(const float2 (&t)[E]) {
+    float sa = 0.f, lg = 0.f;
+#pragma unroll
+    for (int g = 0; g < E; g += 4) {
+        float pm = 1.f;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (g + q >= E) break;
+            const float2 x = t[g + q];
+            const float aa = fabsf(x.x);
+            const float z = ex2_ftz(aa * -2.88539008177792681f);
+            const float c2 = cos_ftz(2.f * x.y);
+            pm *= fmaf(z, fmaf(2.f, c2, z), 1.f);
+            sa += aa;
+        }
+        lg += lg2_ftz(pm);
+    }
+    return fmaf(0.346573590279972655f, lg, sa);
 }
 
 // Sum over the warp of the lanes' ln|cosh| differences for the acceptance
@@ -818,9 +837,7 @@ __device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem&
         } else {
             theta_fp64<E, float>(m, sm.W64 ? sm.W64 : m.W64, sm.perm, lane, sp, th);
         }
-        SL = 0.f;
-#pragma unroll
-        for (int e = 0; e < E; e++) SL += lnc_sweep(th[e]);
+        SL = lnc_sweep_sum<E>(th);
     };
     recompute();
 
@@ -860,12 +877,10 @@ __device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem&
             const float2 G0 = make_float2(g0, g0), G1 = make_float2(g1, g1);
             const float2* u0 = sm.U + f0 * TP + lane;
             const float2* u1 = sm.U + f1 * TP + lane;
-            float sp_new = 0.f;
+            float2 tq[E];
 #pragma unroll
-            for (int e = 0; e < E; e++) {
-                const float2 t = __ffma2_rn(G1, u1[32 * e], __ffma2_rn(G0, u0[32 * e], th[e]));
-                sp_new += lnc_sweep(t);
-            }
+            for (int e = 0; e < E; e++) tq[e] = __ffma2_rn(G1, u1[32 * e], __ffma2_rn(G0, u0[32 * e], th[e]));
+            const float sp_new = lnc_sweep_sum<E>(tq);
             float d = sweep_sum(sp_new - SL);
             d = fmaf(g0, sm.bre[f0], d);
             d = fmaf(g1, sm.bre[f1], d);
@@ -933,15 +948,16 @@ __device__ __forceinline__ void run_chain_pair(const SamplerArgs& a, const Smem&
                 acc[e].y = fma(sg, w.y, acc[e].y);
             }
         }
-        SA = 0.f;
-        SB = 0.f;
+        float2 tA[E], tB[E];
 #pragma unroll
         for (int k = 0; k < E; k++) {
             th[2 * k] = make_float2((float)acc[2 * k].x, (float)acc[2 * k].y);
             th[2 * k + 1] = make_float2((float)acc[2 * k + 1].x, (float)acc[2 * k + 1].y);
-            SA += lnc_sweep(th[2 * k]);
-            SB += lnc_sweep(th[2 * k + 1]);
+            tA[k] = th[2 * k];
+            tB[k] = th[2 * k + 1];
         }
+        SA = lnc_sweep_sum<E>(tA);
+        SB = lnc_sweep_sum<E>(tB);
     };
     recompute();
 
@@ -980,15 +996,15 @@ __device__ __forceinline__ void run_chain_pair(const SamplerArgs& a, const Smem&
             const float2 G0 = make_float2(g0, g0), G1 = make_float2(g1, g1);
             const float2* u0 = sm.U + f0 * TP + hl;
             const float2* u1 = sm.U + f1 * TP + hl;
-            float2 tn[2 * E];
-            float nA = 0.f, nB = 0.f;
+            float2 tn[2 * E], tA[E], tB[E];
 #pragma unroll
             for (int k = 0; k < E; k++) {
                 tn[2 * k] = __ffma2_rn(G1, u1[32 * k], __ffma2_rn(G0, u0[32 * k], th[2 * k]));
-                nA += lnc_sweep(tn[2 * k]);
                 tn[2 * k + 1] = __ffma2_rn(G1, u1[16 + 32 * k], __ffma2_rn(G0, u0[16 + 32 * k], th[2 * k + 1]));
-                nB += lnc_sweep(tn[2 * k + 1]);
+                tA[k] = tn[2 * k];
+                tB[k] = tn[2 * k + 1];
             }
+            const float nA = lnc_sweep_sum<E>(tA), nB = lnc_sweep_sum<E>(tB);
             // the one-chain sweep's sum: lanes h and h + 16 of it are this
             // lane's two partials (integer sums are exact in any order)
             const float vA = nA - SA, vB = nB - SB;
@@ -1109,9 +1125,7 @@ __device__ __forceinline__ void run_chain_gather(const SamplerArgs& a, const Sme
             for (int q = 0; q < 4; q++)
                 if (c + q < E) th[c + q] = make_float2((float)acc[q].x, (float)acc[q].y);
         }
-        SL = 0.f;
-#pragma unroll
-        for (int e = 0; e < E; e++) SL += lnc_sweep(th[e]);
+        SL = lnc_sweep_sum<E>(th);
     };
     recompute();
 
@@ -1150,12 +1164,9 @@ __device__ __forceinline__ void run_chain_gather(const SamplerArgs& a, const Sme
             const float g1 = (bond && spin_bit(sp, f1)) ? 2.f : -2.f;
             const float2 G0 = make_float2(g0, g0), G1 = make_float2(g1, g1);
             float2 tn[E];
-            float sp_new = 0.f;
 #pragma unroll
-            for (int e = 0; e < E; e++) {
-                tn[e] = __ffma2_rn(G1, urd(f1, e), __ffma2_rn(G0, urd(f0, e), th[e]));
-                sp_new += lnc_sweep(tn[e]);
-            }
+            for (int e = 0; e < E; e++) tn[e] = __ffma2_rn(G1, urd(f1, e), __ffma2_rn(G0, urd(f0, e), th[e]));
+            const float sp_new = lnc_sweep_sum<E>(tn);
             float d = sweep_sum(sp_new - SL);
             d = fmaf(g0, sm.bre[f0], d);
             d = fmaf(g1, sm.bre[f1], d);
