@@ -384,6 +384,7 @@ struct Smem {
     float2* Wg;     // gather path: [n+1][nh] FP32 W, row n = 0 (shared or global)
     uint8_t* Pg;    // gather path, symmetric: [n+1][S] P_s(f), row n = n
     unsigned char* ham;  // evaluation: staged Hamiltonian tables
+    double2* base64;     // [TP] hb + sum_f W[P_s(f), k]: theta of the all-up configuration (FP64)
     unsigned char* warp0;
     int warp_bytes;
 };
@@ -424,6 +425,7 @@ __host__ __device__ inline int table_bytes(const MachineDev& m, int fp64, const 
     if (pl.gather && pl.wg) b += align16((m.n + 1) * m.nh * 8);
     if (pl.gather && m.symmetric) b += align16((m.n + 1) * m.S);
     b += align16(pl.ham);
+    if (pl.u64 || pl.gather) b += align16(TP * 16);
     return b;
 }
 
@@ -474,6 +476,10 @@ __device__ inline Smem carve(unsigned char* base, const MachineDev& m, int fp64,
     }
     s.ham = base + off;
     off += align16(pl.ham);
+    if (pl.u64 || pl.gather) {
+        s.base64 = reinterpret_cast<double2*>(base + off);
+        off += align16(TP * 16);
+    }
     s.warp0 = base + off;
     s.warp_bytes = warp_bytes;
     return s;
@@ -511,6 +517,26 @@ __device__ inline void load_tables(const MachineDev& m, const Smem& s, int fp64,
             if (pl.use_u) s.U[i] = make_float2((float)w.x, (float)w.y);
             if (pl.u64 && f < m.n) s.U64[i] = w;
         }
+    __syncthreads();
+    // theta of the all-up configuration per entry; a recompute then subtracts
+    // 2 W over the down spins only: theta = base - 2 sum_{f down} W[P_s(f), k]
+    if (pl.u64 || pl.gather) {
+        const double2* W64 = pl.w64 ? s.W64 : m.W64;
+        for (int t = tid; t < TP; t += nt) {
+            double2 acc = make_double2(0, 0);
+            if (t < m.T) {
+                const int k = t % m.nh, sy = t / m.nh;
+                acc = m.hb[k];
+                for (int f = 0; f < m.n; f++) {
+                    const double2 w = pl.u64 ? s.U64[f * TP + t]
+                                             : W64[(m.symmetric ? (int)s.perm[f * m.S + sy] : f) * m.nh + k];
+                    acc.x += w.x;
+                    acc.y += w.y;
+                }
+            }
+            s.base64[t] = acc;
+        }
+    }
     __syncthreads();
 }
 
@@ -818,18 +844,21 @@ __device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem&
         if (sm.U64) {
             double2 acc[E];
 #pragma unroll
-            for (int e = 0; e < E; e++) {
-                const int t = lane + 32 * e;
-                acc[e] = t < m.T ? m.hb[t % m.nh] : make_double2(0, 0);
-            }
-            const double2* col = sm.U64 + lane;
-            for (int f = 0; f < n; f++, col += TP) {
-                const double sg = sbit(f) ? -1.0 : 1.0;
+            for (int e = 0; e < E; e++) acc[e] = sm.base64[lane + 32 * e];
+            // down spins in increasing order
 #pragma unroll
-                for (int e = 0; e < E; e++) {
-                    const double2 w = col[32 * e];
-                    acc[e].x = fma(sg, w.x, acc[e].x);
-                    acc[e].y = fma(sg, w.y, acc[e].y);
+            for (int wd = 0; wd < NW; wd++) {
+                uint32_t bits = spin_word(sp, wd);
+                while (bits) {
+                    const int f = 32 * wd + __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    const double2* col = sm.U64 + f * TP + lane;
+#pragma unroll
+                    for (int e = 0; e < E; e++) {
+                        const double2 w = col[32 * e];
+                        acc[e].x = fma(-2.0, w.x, acc[e].x);
+                        acc[e].y = fma(-2.0, w.y, acc[e].y);
+                    }
                 }
             }
 #pragma unroll
@@ -934,18 +963,14 @@ __device__ __forceinline__ void run_chain_pair(const SamplerArgs& a, const Smem&
     auto recompute = [&]() {
         double2 acc[2 * E];
 #pragma unroll
-        for (int e = 0; e < 2 * E; e++) {
-            const int t = hl + 16 * (e & 1) + 32 * (e >> 1);
-            acc[e] = t < m.T ? m.hb[t % m.nh] : make_double2(0, 0);
-        }
-        const double2* col = sm.U64 + hl;
-        for (int f = 0; f < n; f++, col += TP) {
-            const double sg = (s0 >> f) & 1u ? -1.0 : 1.0;
+        for (int e = 0; e < 2 * E; e++) acc[e] = sm.base64[hl + 16 * (e & 1) + 32 * (e >> 1)];
+        for (uint32_t bits = s0; bits; bits &= bits - 1) {  // down spins in increasing order
+            const double2* col = sm.U64 + (__ffs(bits) - 1) * TP + hl;
 #pragma unroll
             for (int e = 0; e < 2 * E; e++) {
                 const double2 w = col[16 * (e & 1) + 32 * (e >> 1)];
-                acc[e].x = fma(sg, w.x, acc[e].x);
-                acc[e].y = fma(sg, w.y, acc[e].y);
+                acc[e].x = fma(-2.0, w.x, acc[e].x);
+                acc[e].y = fma(-2.0, w.y, acc[e].y);
             }
         }
         float2 tA[E], tB[E];
@@ -1109,16 +1134,22 @@ __device__ __forceinline__ void run_chain_gather(const SamplerArgs& a, const Sme
             double2 acc[4];
 #pragma unroll
             for (int q = 0; q < 4; q++)
-                acc[q] = (c + q < E && ((vmask >> (c + q)) & 1u)) ? m.hb[ent[c + q] & 0xffffu] : make_double2(0, 0);
-            for (int f = 0; f < n; f++) {
-                const double sg = spin_bit(sp, f) ? -1.0 : 1.0;
+                acc[q] = (c + q < E && ((vmask >> (c + q)) & 1u)) ? sm.base64[lane + 32 * (c + q)]
+                                                                   : make_double2(0, 0);
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    if (c + q >= E || !((vmask >> (c + q)) & 1u)) continue;
-                    const uint32_t en = ent[c + q];
-                    const double2 w = W64[row(f, en) * nh + (en & 0xffffu)];
-                    acc[q].x = fma(sg, w.x, acc[q].x);
-                    acc[q].y = fma(sg, w.y, acc[q].y);
+            for (int wd = 0; wd < 4; wd++) {  // down spins in increasing order
+                uint32_t bits = spin_word(sp, wd);
+                while (bits) {
+                    const int f = 32 * wd + __ffs(bits) - 1;
+                    bits &= bits - 1;
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        if (c + q >= E || !((vmask >> (c + q)) & 1u)) continue;
+                        const uint32_t en = ent[c + q];
+                        const double2 w = W64[row(f, en) * nh + (en & 0xffffu)];
+                        acc[q].x = fma(-2.0, w.x, acc[q].x);
+                        acc[q].y = fma(-2.0, w.y, acc[q].y);
+                    }
                 }
             }
 #pragma unroll
