@@ -907,15 +907,20 @@ __device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem&
             const float2* u0 = sm.U + f0 * TP + lane;
             const float2* u1 = sm.U + f1 * TP + lane;
             float2 tq[E];
+            if (bond) {
 #pragma unroll
-            for (int e = 0; e < E; e++) tq[e] = __ffma2_rn(G1, u1[32 * e], __ffma2_rn(G0, u0[32 * e], th[e]));
+                for (int e = 0; e < E; e++) tq[e] = __ffma2_rn(G1, u1[32 * e], __ffma2_rn(G0, u0[32 * e], th[e]));
+            } else {
+#pragma unroll
+                for (int e = 0; e < E; e++) tq[e] = __ffma2_rn(G0, u0[32 * e], th[e]);
+            }
             const float sp_new = lnc_sweep_sum<E>(tq);
             float d = sweep_sum(sp_new - SL);
             d = fmaf(g0, sm.bre[f0], d);
             d = fmaf(g1, sm.bre[f1], d);
             if (lu < d) {
 #pragma unroll
-                for (int e = 0; e < E; e++) th[e] = __ffma2_rn(G1, u1[32 * e], __ffma2_rn(G0, u0[32 * e], th[e]));
+                for (int e = 0; e < E; e++) th[e] = tq[e];
                 SL = sp_new;
                 sflip(f0);
                 if (bond) sflip(f1);
@@ -1195,8 +1200,13 @@ __device__ __forceinline__ void run_chain_gather(const SamplerArgs& a, const Sme
             const float g1 = (bond && spin_bit(sp, f1)) ? 2.f : -2.f;
             const float2 G0 = make_float2(g0, g0), G1 = make_float2(g1, g1);
             float2 tn[E];
+            if (bond) {
 #pragma unroll
-            for (int e = 0; e < E; e++) tn[e] = __ffma2_rn(G1, urd(f1, e), __ffma2_rn(G0, urd(f0, e), th[e]));
+                for (int e = 0; e < E; e++) tn[e] = __ffma2_rn(G1, urd(f1, e), __ffma2_rn(G0, urd(f0, e), th[e]));
+            } else {
+#pragma unroll
+                for (int e = 0; e < E; e++) tn[e] = __ffma2_rn(G0, urd(f0, e), th[e]);
+            }
             const float sp_new = lnc_sweep_sum<E>(tn);
             float d = sweep_sum(sp_new - SL);
             d = fmaf(g0, sm.bre[f0], d);
