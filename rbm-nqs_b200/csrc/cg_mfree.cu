@@ -483,6 +483,12 @@ cudaError_t mfree_plan(int N, int P, MfreePlan* pl) {
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     if (per_sm > 2) per_sm = 2;
     pl->blocks = sms * per_sm;
+    // formed S (N == 1): one warp per row of S is all the mat-vec can use,
+    // and fewer blocks make every grid barrier cheaper
+    if (N == 1) {
+        const int want = (P + kThreads / 32 - 1) / (kThreads / 32);
+        if (want < pl->blocks) pl->blocks = want < 1 ? 1 : want;
+    }
     pl->nseg = kThreads / 32;  // column slices of the O b pass (one per warp of a block)
     pl->lseg = (P + pl->nseg - 1) / pl->nseg;
     pl->diag_blocks = pl->blocks;
