@@ -1289,7 +1289,7 @@ __global__ void __launch_bounds__(FAST == 2 ? MaxThreads<E, PF>::gather
 // Batched evaluation at given configurations: log psi, E_loc, O_k, or the
 // log psi ratio for given flips (parity entry points).
 template <int E, typename R, bool PF>
-__global__ void __launch_bounds__(256, E <= 4 ? 3 : 2) eval_kernel(const EvalArgs a) {
+__global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) eval_kernel(const EvalArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const MachineDev& m = a.m;
     const int fp64 = sizeof(R) == 8;
