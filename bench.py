@@ -77,7 +77,7 @@ WORKLOADS = {
 METRIC = "uncorrelated samples/s (SR epoch, E_loc binning tau)"
 # DRAM bytes per sampler launch from an ncu capture of the same workload: the
 # theta tables, flip tables and chains live in shared memory and registers
-SAMPLER_DRAM_BYTES = {"kitaev32_symm_a4": 141824.0}
+SAMPLER_DRAM_BYTES = {"kitaev32_symm_a4": 136704.0}
 L2_FLUSH_BYTES = 256 << 20
 
 
