@@ -211,7 +211,19 @@ struct rbmnqs_handle {
     double stage_ms[kStages] = {};
     int64_t stage_launches[kStages] = {};
 
+    // pinned host copies of the per-epoch results, read back with one
+    // stream synchronisation
+    struct Readback {
+        rbmnqs::EpochStatsDev stats;
+        rbmnqs::CgResultDev cg;
+        rbmnqs::ScheduleDev sched;
+        int gerr;
+        double lrate;
+        float lloss;
+    };
+    Readback* rb = nullptr;
     ~rbmnqs_handle() {
+        if (rb) cudaFreeHost(rb);
         if (graph) cudaGraphExecDestroy(graph);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
@@ -1045,7 +1057,13 @@ int rbmnqs_set_weights(rbmnqs_handle* h, const double* w) {
         ck(cudaMemcpyAsync(h->params.p, w, h->P * sizeof(double2), cudaMemcpyHostToDevice, h->st), "copy");
         ck(rbmnqs::launch_unpack(h->params.p, h->n, h->n_vb, h->nh, h->vb.p, h->hb.p, h->W64.p, h->W32.p, h->st),
            "unpack");
-        ck(cudaStreamSynchronize(h->st), "sync");
+        // a pageable host buffer is free once the copy call returns (the unpack
+        // is ordered before any later work on the stream); a pinned or
+        // device-visible one only after the copy completes
+        cudaPointerAttributes pa{};
+        if (cudaPointerGetAttributes(&pa, w) != cudaSuccess || pa.type != cudaMemoryTypeUnregistered)
+            ck(cudaStreamSynchronize(h->st), "sync");
+        cudaGetLastError();  // clear a failed attribute query
     });
 }
 
@@ -1087,11 +1105,28 @@ static int count_kernel_nodes(cudaGraph_t g) {
     return k;
 }
 
-static void read_sample_stats(rbmnqs_handle* h, rbmnqs_sample_stats* out) {
-    rbmnqs::EpochStatsDev s{};
-    ck(cudaMemcpyAsync(&s, h->stats.p, sizeof(s), cudaMemcpyDeviceToHost, h->st), "copy");
+// Sample statistics (s) and SR statistics (o) of the last sample / optimize
+// step: the device results are copied into pinned host memory and read after
+// one stream synchronisation.  With sr, a successful step counts as an update.
+static void readback(rbmnqs_handle* h, bool sample, rbmnqs_sample_stats* out, bool sr, rbmnqs_sr_stats* o) {
+    if (!h->rb) ck(cudaMallocHost(&h->rb, sizeof(*h->rb)), "cudaMallocHost");
+    auto* rb = h->rb;
+    if (sample) {
+        ck(cudaMemcpyAsync(&rb->stats, h->stats.p, sizeof(rb->stats), cudaMemcpyDeviceToHost, h->st), "copy");
+        if (h->net) {
+            ck(cudaMemcpyAsync(&rb->lrate, h->lrate.p, sizeof(double), cudaMemcpyDeviceToHost, h->st), "copy");
+            ck(cudaMemcpyAsync(&rb->lloss, h->lloss.p, sizeof(float), cudaMemcpyDeviceToHost, h->st), "copy");
+        }
+    }
+    rb->gerr = 0;
+    if (sr) {
+        ck(cudaMemcpyAsync(&rb->cg, h->cgres.p, sizeof(rb->cg), cudaMemcpyDeviceToHost, h->st), "copy");
+        ck(cudaMemcpyAsync(&rb->sched, h->sched.p, sizeof(rb->sched), cudaMemcpyDeviceToHost, h->st), "copy");
+        if (h->gram_tc) ck(cudaMemcpyAsync(&rb->gerr, h->gerr.p, sizeof(int), cudaMemcpyDeviceToHost, h->st), "copy");
+    }
     ck(cudaStreamSynchronize(h->st), "sync");
-    if (out) {
+    if (sample && out) {
+        const auto& s = rb->stats;
         out->energy[0] = s.energy.x;
         out->energy[1] = s.energy.y;
         out->energy_var = s.var;
@@ -1101,39 +1136,25 @@ static void read_sample_stats(rbmnqs_handle* h, rbmnqs_sample_stats* out) {
         out->n_samples = h->N;
         out->n_bins = h->n_bins;
         out->status = s.finite ? RBMNQS_OK : RBMNQS_ERR_NONFINITE;
-        out->learned_acceptance = 0;
-        out->learned_loss = 0;
-        if (h->net) {
-            double r = 0;
-            float l = 0;
-            ck(cudaMemcpyAsync(&r, h->lrate.p, sizeof(r), cudaMemcpyDeviceToHost, h->st), "copy");
-            ck(cudaMemcpyAsync(&l, h->lloss.p, sizeof(l), cudaMemcpyDeviceToHost, h->st), "copy");
-            ck(cudaStreamSynchronize(h->st), "sync");
-            out->learned_acceptance = r;
-            out->learned_loss = l;
-        }
+        out->learned_acceptance = h->net ? rb->lrate : 0;
+        out->learned_loss = h->net ? rb->lloss : 0;
     }
-}
-
-static void read_sr_stats(rbmnqs_handle* h, rbmnqs_sr_stats* out) {
-    rbmnqs::CgResultDev r{};
-    rbmnqs::ScheduleDev sd{};
-    ck(cudaMemcpyAsync(&r, h->cgres.p, sizeof(r), cudaMemcpyDeviceToHost, h->st), "copy");
-    ck(cudaMemcpyAsync(&sd, h->sched.p, sizeof(sd), cudaMemcpyDeviceToHost, h->st), "copy");
-    int gerr = 0;
-    if (h->gram_tc) ck(cudaMemcpyAsync(&gerr, h->gerr.p, sizeof(int), cudaMemcpyDeviceToHost, h->st), "copy");
-    ck(cudaStreamSynchronize(h->st), "sync");
-    if (gerr) throw Fail{RBMNQS_ERR_CUDA, "tensor-core Gram: pipeline wait timed out (code " + std::to_string(gerr) + ")"};
-    if (r.status == 0) h->n_updates++;
-    if (out) {
-        out->iterations = r.iterations;
-        out->status = r.status;
-        out->residual = r.residual;
-        out->max_dw = r.max_dw;
-        out->lr = sd.value[0];
-        out->reg1 = sd.value[1];
-        out->reg2 = sd.value[2];
-        out->deltareg1 = sd.value[3];
+    if (sr) {
+        if (rb->gerr)
+            throw Fail{RBMNQS_ERR_CUDA,
+                       "tensor-core Gram: pipeline wait timed out (code " + std::to_string(rb->gerr) + ")"};
+        const auto& r = rb->cg;
+        if (r.status == 0) h->n_updates++;
+        if (o) {
+            o->iterations = r.iterations;
+            o->status = r.status;
+            o->residual = r.residual;
+            o->max_dw = r.max_dw;
+            o->lr = rb->sched.value[0];
+            o->reg1 = rb->sched.value[1];
+            o->reg2 = rb->sched.value[2];
+            o->deltareg1 = rb->sched.value[3];
+        }
     }
 }
 
@@ -1142,7 +1163,7 @@ int rbmnqs_sample(rbmnqs_handle* h, rbmnqs_sample_stats* out) {
         require(h != nullptr, "null handle");
         h->enqueue_sample();
         h->collect_timing(0, 3);
-        read_sample_stats(h, out);
+        readback(h, true, out, false, nullptr);
         h->sampled = true;
     });
 }
@@ -1154,7 +1175,7 @@ int rbmnqs_optimize(rbmnqs_handle* h, rbmnqs_sr_stats* out) {
         h->mark(3);
         h->enqueue_optimize();
         h->collect_timing(3, 6);
-        read_sr_stats(h, out);
+        readback(h, false, nullptr, true, out);
     });
 }
 
@@ -1178,8 +1199,7 @@ int rbmnqs_epoch(rbmnqs_handle* h, rbmnqs_sample_stats* s, rbmnqs_sr_stats* o) {
         }
         ck(cudaGraphLaunch(h->graph, h->st), "graph launch");
         h->collect_timing(0, 6);
-        read_sample_stats(h, s);
-        read_sr_stats(h, o);
+        readback(h, true, s, true, o);
         h->sampled = true;
     });
 }
@@ -1773,8 +1793,7 @@ int rbmnqs_batch_epoch(rbmnqs_batch* b, rbmnqs_sample_stats* s, rbmnqs_sr_stats*
         ck(cudaGraphLaunch(b->graph, b->st), "graph launch");
         ck(cudaStreamSynchronize(b->st), "sync");
         for (size_t i = 0; i < b->hs.size(); i++) {
-            read_sample_stats(b->hs[i], s ? s + i : nullptr);
-            read_sr_stats(b->hs[i], o ? o + i : nullptr);
+            readback(b->hs[i], true, s ? s + i : nullptr, true, o ? o + i : nullptr);
             b->hs[i]->sampled = true;
         }
     });
