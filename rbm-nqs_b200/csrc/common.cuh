@@ -144,6 +144,41 @@ template <typename R> __device__ __forceinline__ void lnc_full(R a, R b, R& re, 
     uy = Y * inv;
 }
 
+// FP32 sum of ln cosh over a lane's valid entries x[e] (e < nv): re = sum |a|
+// + ln|prod (X + i sgn(a) Y)| and u = the unit phase of that product (ln 2
+// per entry left out, as in lnc_full).  The factors are multiplied in groups
+// of four (|X + iY| <= 2, so a group's product stays in the FP32 range), with
+// one lg2 and one rsqrt per group instead of one per entry.  A group whose
+// |product|^2 is below the smallest normal float counts as a zero of cosh:
+// re = -inf, u = 0.
+template <int E> __device__ __forceinline__ void lnc_lane(const float2 (&x)[E], int nv, float& re, float2& u) {
+    float asum = 0.f, l2 = 0.f;
+    float2 P = make_float2(1.f, 0.f);
+#pragma unroll
+    for (int g = 0; g < E; g += 4) {
+        if (g >= nv) break;
+        float2 G = make_float2(1.f, 0.f);
+#pragma unroll
+        for (int j = 0; j < 4 && g + j < E; j++) {
+            if (g + j >= nv) break;
+            const float a = x[g + j].x, aa = fabsf(a);
+            const float z = exp_r(-2.f * aa);
+            float s, c;
+            sincos_r(x[g + j].y, &s, &c);
+            const float2 f = make_float2((1.f + z) * c, copysignf(1.f - z, a) * s);
+            asum += aa;
+            G = cmul(G, f);
+        }
+        const float m2 = G.x * G.x + G.y * G.y;
+        const bool ok = m2 >= 1.17549435e-38f;
+        l2 += ok ? ftz_lg2(m2) : __int_as_float(0xff800000u);  // -inf
+        const float inv = ok ? ftz_rsqrt(m2) : 0.f;
+        P = cmul(P, make_float2(G.x * inv, G.y * inv));
+    }
+    re = asum + 0.346573590279972655f * l2;  // (ln 2 / 2) lg2
+    u = P;
+}
+
 // tanh(a + ib) = [sgn(a)(1 - z^2) + i 4z sin b cos b] / (X^2 + Y^2), the
 // denominator 1 + z^2 + 2z cos 2b written as the sum of squares
 // X^2 + Y^2 = ((1+z) cos b)^2 + ((1-z) sin b)^2, which does not cancel near

@@ -150,11 +150,32 @@ __device__ __forceinline__ RatioDims ratio_dims(const MachineDev& m) { return Ra
 // registers); NF = 0: nf flips at run time.
 // WS (FP32): W and the symmetry table are in shared memory, read by shared
 // addresses.
+// FP32 (R = float): the lane's entries go through lnc_lane and the cache is
+// the lane aggregate (cl.re, cl.u) of the current theta; FP64: one ln cosh
+// per entry against the per-entry cache (cre, cu).
+template <typename R> struct LaneCache {
+    R re;
+    C2<R> u;
+};
+__device__ __forceinline__ int lane_entries(int lane, int T, int E) {
+    const int v = (T - lane + 31) >> 5;
+    return v < 0 ? 0 : (v > E ? E : v);
+}
+template <int E>
+__device__ __forceinline__ LaneCache<float> lane_cache(const float2* wth, int lane, int T) {
+    float2 x[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) x[e] = slot_valid(lane, e, T) ? wth[lane + 32 * e] : make_float2(0.f, 0.f);
+    LaneCache<float> c;
+    lnc_lane<E>(x, lane_entries(lane, T, E), c.re, c.u);
+    return c;
+}
+
 template <int E, typename R, int NF = 0, bool WS = false>
 __device__ __forceinline__ void ratio_terms(const RatioDims m, const uint8_t* sPerm, const C2<R>* W,
                                             const C2<R>* wth, const uint32_t* wsp, const int* fl, int nf_,
-                                            const R* cre, const C2<R>* cu, int lane, R& dre, C2<R>& ph,
-                                            const uint32_t (&ks)[E]) {
+                                            const R* cre, const C2<R>* cu, const LaneCache<R> cl, int lane,
+                                            R& dre, C2<R>& ph, const uint32_t (&ks)[E]) {
     const int nf = NF > 0 ? NF : nf_;
     R sgn2[NF > 0 ? NF : 6];
 #pragma unroll
@@ -162,8 +183,10 @@ __device__ __forceinline__ void ratio_terms(const RatioDims m, const uint8_t* sP
         if (q < nf) sgn2[q] = smem_bit(wsp, fl[q]) ? (R)2 : (R)-2;  // -2 sigma_f
     dre = 0;
     ph = mk<R>(1, 0);
+    C2<R> xs[E];
 #pragma unroll
     for (int e = 0; e < E; e++) {
+        xs[e] = mk<R>(0, 0);
         if (!slot_valid(lane, e, m.T)) continue;
         const int t = lane + 32 * e, k = ks[e] & 0xffffu, s = ks[e] >> 16;
         C2<R> x = wth[t];
@@ -182,10 +205,21 @@ __device__ __forceinline__ void ratio_terms(const RatioDims m, const uint8_t* sP
             x.x = fma(sgn2[q], u.x, x.x);
             x.y = fma(sgn2[q], u.y, x.y);
         }
-        R re, ux, uy;
-        lnc_full<R>(x.x, x.y, re, ux, uy);
-        dre += re - cre[t];
-        ph = cmul(ph, cmulc(mk<R>(ux, uy), cu[t]));
+        if constexpr (sizeof(R) == 4) {
+            xs[e] = x;
+        } else {
+            R re, ux, uy;
+            lnc_full<R>(x.x, x.y, re, ux, uy);
+            dre += re - cre[t];
+            ph = cmul(ph, cmulc(mk<R>(ux, uy), cu[t]));
+        }
+    }
+    if constexpr (sizeof(R) == 4) {
+        float re;
+        float2 u;
+        lnc_lane<E>(xs, lane_entries(lane, m.T, E), re, u);
+        dre = re - cl.re;
+        ph = cmulc(u, cl.u);
     }
     dre = warp_sum(dre);
     ph = warp_cprod(ph);
@@ -226,16 +260,21 @@ __device__ __forceinline__ void evaluate(const MachineDev* __restrict__ mp, cons
     uint32_t ks[E];
     entry_index<E>(m, lane, ks);
     // ln cosh cache of the current theta
+    LaneCache<R> cl{};
+    if constexpr (sizeof(R) == 4) {
+        cl = lane_cache<E>(wth, lane, m.T);
+    } else {
 #pragma unroll
-    for (int e = 0; e < E; e++) {
-        if (!slot_valid(lane, e, m.T)) continue;
-        const int t = lane + 32 * e;
-        R re, ux, uy;
-        lnc_full<R>(wth[t].x, wth[t].y, re, ux, uy);
-        cre[t] = re;
-        cu[t] = mk<R>(ux, uy);
+        for (int e = 0; e < E; e++) {
+            if (!slot_valid(lane, e, m.T)) continue;
+            const int t = lane + 32 * e;
+            R re, ux, uy;
+            lnc_full<R>(wth[t].x, wth[t].y, re, ux, uy);
+            cre[t] = re;
+            cu[t] = mk<R>(ux, uy);
+        }
+        __syncwarp();
     }
-    __syncwarp();
     if (Eout) {
         double ex = 0, ey = 0;
         for (int o = 0; o < H.n_ops; o++) {
@@ -265,10 +304,10 @@ __device__ __forceinline__ void evaluate(const MachineDev* __restrict__ mp, cons
                     fl[1] = op->sites[i1];
                     if (nf == 2) {
                         const int f2[2] = {fl[0], fl[1]};
-                        ratio_terms<E, R, 2, WS>(rd, sPerm, W, wth, wsp, f2, 2, cre, cu, lane, dre, ph, ks);
+                        ratio_terms<E, R, 2, WS>(rd, sPerm, W, wth, wsp, f2, 2, cre, cu, cl, lane, dre, ph, ks);
                     } else {
                         const int f1[1] = {fl[0]};
-                        ratio_terms<E, R, 1, WS>(rd, sPerm, W, wth, wsp, f1, 1, cre, cu, lane, dre, ph, ks);
+                        ratio_terms<E, R, 1, WS>(rd, sPerm, W, wth, wsp, f1, 1, cre, cu, cl, lane, dre, ph, ks);
                     }
                 } else {
                     uint32_t mm = mask;
@@ -276,7 +315,7 @@ __device__ __forceinline__ void evaluate(const MachineDev* __restrict__ mp, cons
                         fl[j] = op->sites[__ffs(mm) - 1];
                         mm &= mm - 1;
                     }
-                    ratio_terms<E, R, 0, WS>(rd, sPerm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph, ks);
+                    ratio_terms<E, R, 0, WS>(rd, sPerm, W, wth, wsp, fl, nf, cre, cu, cl, lane, dre, ph, ks);
                 }
                 const double2 b = bias_delta_smem(m, wsp, fl, nf);
                 double rx, ry;
@@ -1387,15 +1426,20 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) eval_kernel(const EvalArg
         if (a.ratio || a.eloc || a.O) pf_fresh(m.pf, sp[0], lane, pA, *pst, pA + kPfMaxSites * kPfLd, kPfLd);
     }
     if (a.ratio) {
+        LaneCache<R> cl{};
+        if constexpr (sizeof(R) == 4) {
+            cl = lane_cache<E>(wth, lane, m.T);
+        } else {
 #pragma unroll
-        for (int e = 0; e < E; e++) {
-            if (!slot_valid(lane, e, m.T)) continue;
-            R r, ux, uy;
-            lnc_full<R>(th[e].x, th[e].y, r, ux, uy);
-            cre[lane + 32 * e] = r;
-            cu[lane + 32 * e] = mk<R>(ux, uy);
+            for (int e = 0; e < E; e++) {
+                if (!slot_valid(lane, e, m.T)) continue;
+                R r, ux, uy;
+                lnc_full<R>(th[e].x, th[e].y, r, ux, uy);
+                cre[lane + 32 * e] = r;
+                cu[lane + 32 * e] = mk<R>(ux, uy);
+            }
+            __syncwarp();
         }
-        __syncwarp();
         int fl[6];
         const int nf = a.n_flips;
         for (int q = 0; q < nf; q++) fl[q] = a.flips[b * nf + q];
@@ -1403,7 +1447,7 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) eval_kernel(const EvalArg
         C2<R> ph;
         uint32_t ks[E];
         entry_index<E>(m, lane, ks);
-        ratio_terms<E, R>(ratio_dims(m), sm.perm, W, wth, wsp, fl, nf, cre, cu, lane, dre, ph, ks);
+        ratio_terms<E, R>(ratio_dims(m), sm.perm, W, wth, wsp, fl, nf, cre, cu, cl, lane, dre, ph, ks);
         double2 lr = make_double2(0.0, 0.0);
         if constexpr (PF) {
             const double2 c2 = pf_ratio_any(m.pf, sp[0], fl, nf, lane, *pst, pA);
