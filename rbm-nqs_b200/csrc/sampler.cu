@@ -113,15 +113,28 @@ __device__ __forceinline__ double2 bias_delta(const MachineDev& m, const uint32_
     return b;
 }
 
-__device__ __forceinline__ double2 bias_delta_smem(const MachineDev& m, const uint32_t* wsp, const int* fl, int nf) {
+// Visible-bias index f mod n_vb of site 0 <= f < n, without an integer
+// division for one bias per site (n_vb = n) and for a power-of-two basis
+// (one bias for all sites, one per sublattice, ...).
+__device__ __forceinline__ int vb_index(int f, int n_vb, int n) {
+    return n_vb == n ? f : ((n_vb & (n_vb - 1)) == 0 ? (f & (n_vb - 1)) : f % n_vb);
+}
+
+// The bias sizes passed in registers (the machine descriptor is in global
+// memory and the term loop of evaluate() calls this once per term).
+__device__ __forceinline__ double2 bias_delta_smem(const double2* vb, int n_vb, int n, const uint32_t* wsp,
+                                                   const int* fl, int nf) {
     double2 b = make_double2(0, 0);
     for (int q = 0; q < nf; q++) {
         const double sg = smem_bit(wsp, fl[q]) ? -1.0 : 1.0;
-        const double2 v = m.vb[fl[q] % m.n_vb];
+        const double2 v = vb[vb_index(fl[q], n_vb, n)];
         b.x -= 2.0 * sg * v.x;
         b.y -= 2.0 * sg * v.y;
     }
     return b;
+}
+__device__ __forceinline__ double2 bias_delta_smem(const MachineDev& m, const uint32_t* wsp, const int* fl, int nf) {
+    return bias_delta_smem(m.vb, m.n_vb, m.n, wsp, fl, nf);
 }
 
 // psi(sigma with flips)/psi(sigma) for the RBM part from the warp's theta
@@ -277,6 +290,8 @@ __device__ __forceinline__ void evaluate(const MachineDev* __restrict__ mp, cons
     }
     if (Eout) {
         double ex = 0, ey = 0;
+        const double2* vb = m.vb;
+        const int nvb = m.n_vb, nsites = m.n;
         for (int o = 0; o < H.n_ops; o++) {
             const OpDev* op = H.ops + o;
             const int k = op->k;
@@ -317,7 +332,7 @@ __device__ __forceinline__ void evaluate(const MachineDev* __restrict__ mp, cons
                     }
                     ratio_terms<E, R, 0, WS>(rd, sPerm, W, wth, wsp, fl, nf, cre, cu, cl, lane, dre, ph, ks);
                 }
-                const double2 b = bias_delta_smem(m, wsp, fl, nf);
+                const double2 b = bias_delta_smem(vb, nvb, nsites, wsp, fl, nf);
                 double rx, ry;
                 const double lm = (double)dre + b.x;  // ln|psi'/psi| of the RBM part
                 if (sizeof(R) == 4 && fabs(lm) < 80.0) {
