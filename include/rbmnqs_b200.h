@@ -366,7 +366,11 @@ int rbmnqs_probe_mufu(int32_t iters, double* ops_per_second);
  * Every call shares the array: calls that overlap on the GPU (other streams,
  * other threads) race and must be serialised by the caller.  When
  * `iterations` or `residual` is non-NULL the call waits for `stream` to read
- * them back.  Allocates nothing: no cudaMalloc, cudaFree or allocating
+ * them back.  max_iterations 0 means 2 n_params, a negative value is
+ * rejected with RBMNQS_ERR_ARG; rtol 0 means 1e-16.  The array's address is
+ * resolved once per device and kept, so the library must not outlive a
+ * cudaDeviceReset (or a release of the primary context) of a device it has
+ * solved on.  Allocates nothing: no cudaMalloc, cudaFree or allocating
  * library routine. */
 #define RBMNQS_NOALLOC_MAX_PARAMS 256
 int rbmnqs_sr_solve_noalloc(const double* O, int32_t N, int32_t n_params,

@@ -50,6 +50,8 @@ extern "C" int rbmnqs_sr_solve_noalloc(const double* O, int32_t N, int32_t P, in
                                         std::to_string(P));
     if (N < 1 || !(norm > 0) || n_neural < 0 || n_neural > P)
         return fail(RBMNQS_ERR_ARG, "rbmnqs_sr_solve_noalloc: bad N, norm or n_neural");
+    if (max_iterations < 0)
+        return fail(RBMNQS_ERR_ARG, "rbmnqs_sr_solve_noalloc: max_iterations must be >= 0 (0 = 2 n_params)");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail(RBMNQS_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));

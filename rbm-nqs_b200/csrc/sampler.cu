@@ -1840,10 +1840,15 @@ cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bond
 }
 
 cudaError_t ensure_dynamic_smem(const void* fn, int bytes) {
+    // the attribute belongs to the kernel on the current device: cache it per
+    // (device, kernel) so that a second device gets its own setting
     static std::mutex mu;
-    static std::map<const void*, int> set;
+    static std::map<std::pair<int, const void*>, int> set;
     std::lock_guard<std::mutex> lk(mu);
-    int& cur = set[fn];
+    int dev = 0;
+    const cudaError_t de = cudaGetDevice(&dev);
+    if (de != cudaSuccess) return de;
+    int& cur = set[{dev, fn}];
     if (bytes <= cur) return cudaSuccess;
     const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess) cur = bytes;
