@@ -108,9 +108,89 @@ HamHost build_ham(const std::vector<rbmnqs::local_op>& ops) {
     return h;
 }
 
+// The operators regrouped by transition for the FP32 evaluation kernel
+// (TermDev): one term per (operator, nonzero flip mask), with the matrix
+// element of every local configuration (zero where the row lacks the mask),
+// and one diagonal term per operator with diagonal entries.
+struct TermHost {
+    std::vector<rbmnqs::TermDev> terms, diag;
+    std::vector<double2> vals;
+    int nf_max = 0;
+};
+
+TermHost build_terms(const std::vector<rbmnqs::local_op>& ops) {
+    TermHost t;
+    auto pack4 = [](const int* v, int cnt) {
+        uint32_t w = 0;
+        for (int i = 0; i < cnt && i < 4; i++) w |= (uint32_t)(v[i] & 0xff) << (8 * i);
+        return w;
+    };
+    for (const auto& op : ops) {
+        const int dim = 1 << op.k;
+        int sites[6] = {0, 0, 0, 0, 0, 0};
+        for (int i = 0; i < op.k; i++) sites[i] = op.acts_on[i];
+        std::vector<uint32_t> masks;  // distinct masks in increasing order
+        for (int r = 0; r < dim; r++)
+            for (int c = 0; c < dim; c++)
+                if (op.mat[(size_t)r * dim + c] != cplx(0, 0)) masks.push_back((uint32_t)(r ^ c));
+        std::sort(masks.begin(), masks.end());
+        masks.erase(std::unique(masks.begin(), masks.end()), masks.end());
+        for (uint32_t mk : masks) {
+            rbmnqs::TermDev d{};
+            int fl[6] = {0, 0, 0, 0, 0, 0}, nf = 0;
+            for (int i = 0; i < op.k; i++)
+                if ((mk >> i) & 1u) fl[nf++] = sites[i];
+            d.flip0 = pack4(fl, 4);
+            d.flip1 = (uint32_t)(fl[4] & 0xff) | ((uint32_t)(fl[5] & 0xff) << 8) | ((uint32_t)nf << 16) |
+                      ((uint32_t)op.k << 24);
+            d.site0 = pack4(sites, 4);
+            d.site1 = (uint32_t)(sites[4] & 0xff) | ((uint32_t)(sites[5] & 0xff) << 8);
+            d.voff = (int)t.vals.size();
+            for (int r = 0; r < dim; r++) {
+                const cplx v = op.mat[(size_t)r * dim + (r ^ (int)mk)];
+                t.vals.push_back(make_double2(v.real(), v.imag()));
+            }
+            if (mk == 0) {
+                t.diag.push_back(d);
+            } else {
+                t.terms.push_back(d);
+                t.nf_max = std::max(t.nf_max, nf);
+            }
+        }
+    }
+    return t;
+}
+
 }  // namespace
 
 void rbmnqs::set_last_error(const std::string& msg) { g_err = msg; }
+
+// Device copy of a TermHost and its view for the evaluation kernel.
+struct TermBufs {
+    DevBuf<rbmnqs::TermDev> terms, diag;
+    DevBuf<double2> vals;
+    rbmnqs::TermTable tt{};
+    void upload(const TermHost& t) {
+        terms.alloc(std::max<size_t>(1, t.terms.size()));
+        diag.alloc(std::max<size_t>(1, t.diag.size()));
+        vals.alloc(std::max<size_t>(1, t.vals.size()));
+        if (!t.terms.empty())
+            ck(cudaMemcpy(terms.p, t.terms.data(), t.terms.size() * sizeof(rbmnqs::TermDev), cudaMemcpyHostToDevice),
+               "c");
+        if (!t.diag.empty())
+            ck(cudaMemcpy(diag.p, t.diag.data(), t.diag.size() * sizeof(rbmnqs::TermDev), cudaMemcpyHostToDevice),
+               "c");
+        if (!t.vals.empty())
+            ck(cudaMemcpy(vals.p, t.vals.data(), t.vals.size() * sizeof(double2), cudaMemcpyHostToDevice), "c");
+        tt.n_terms = (int)t.terms.size();
+        tt.n_diag = (int)t.diag.size();
+        tt.nf_max = t.nf_max;
+        tt.n_vals = (int)t.vals.size();
+        tt.terms = terms.p;
+        tt.diag = diag.p;
+        tt.vals = vals.p;
+    }
+};
 
 // One observable (evaluation mode) as a one-operator Hamiltonian table.
 struct ObsDev {
@@ -120,6 +200,7 @@ struct ObsDev {
     DevBuf<double2> val;
     DevBuf<rbmnqs::HamDev> hd;
     rbmnqs::HamDev H{};
+    TermBufs terms;
 };
 
 struct rbmnqs_handle {
@@ -148,6 +229,7 @@ struct rbmnqs_handle {
     DevBuf<rbmnqs::ScheduleDev> sched;
     DevBuf<rbmnqs::MachineDev> mdev;
     DevBuf<rbmnqs::HamDev> hdev;
+    TermBufs terms;  // the Hamiltonian as terms (FP32 evaluation kernel)
     DevBuf<rbmnqs::CgResultDev> cgres;
     // update plugin (adam / momentum) state
     DevBuf<rbmnqs::PluginDev> plug;
@@ -325,6 +407,7 @@ struct rbmnqs_handle {
         ea.eloc = E.p;
         ea.O = O.p;
         ea.plan = eval_plan();
+        ea.tt = terms.tt;
         return ea;
     }
     rbmnqs::LearnedArgs learned_args() const {
@@ -847,6 +930,7 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         ck(cudaMemcpy(h->rowptr.p, hh.rowptr.data(), hh.rowptr.size() * sizeof(int), cudaMemcpyHostToDevice), "c");
         ck(cudaMemcpy(h->emask.p, hh.mask.data(), hh.mask.size() * sizeof(uint32_t), cudaMemcpyHostToDevice), "c");
         ck(cudaMemcpy(h->eval.p, hh.val.data(), hh.val.size() * sizeof(double2), cudaMemcpyHostToDevice), "c");
+        h->terms.upload(build_terms(m.hamiltonian));
         // observables (evaluation mode), one table each
         for (const auto& op : m.observables) {
             auto od = std::make_unique<ObsDev>();
@@ -868,6 +952,7 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
             od->H.n_ents = (int)oh.mask.size();
             od->hd.alloc(1);
             ck(cudaMemcpy(od->hd.p, &od->H, sizeof(od->H), cudaMemcpyHostToDevice), "c");
+            od->terms.upload(build_terms({op}));
             h->obs.push_back(std::move(od));
         }
         // bond proposals: bonds of type != 2 (metropolis_sampler.cpp:145-166)
@@ -1286,6 +1371,7 @@ static void eval_common(rbmnqs_handle* h, const uint32_t* spins, int B, double* 
     a.spins = ds.p;
     a.B = B;
     a.plan = rbmnqs::SmemPlan{0, h->w_in_smem, 0, 0, 0};
+    a.tt = h->terms.tt;
     if (logpsi) {
         dl.alloc(B);
         a.logpsi = dl.p;
@@ -1511,6 +1597,7 @@ int rbmnqs_get_observables(rbmnqs_handle* h, double* values) {
             ea.H = h->obs[i]->H;
             ea.plan.ham = rbmnqs::ham_stage_bytes(ea.H);
             ea.hd = h->obs[i]->hd.p;
+            ea.tt = h->obs[i]->terms.tt;
             ea.O = nullptr;
             ea.eloc = h->obsE.p;
             ck(rbmnqs::launch_eval(ea, h->fp64, h->wpb, h->st), "observable evaluation");

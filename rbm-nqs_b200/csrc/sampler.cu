@@ -1896,8 +1896,27 @@ static cudaError_t launch_e(const EvalArgs& a, int wpb, cudaStream_t st) {
         default: return cudaErrorInvalidValue;                               \
     }
 
-cudaError_t launch_eval(const EvalArgs& a, int fp64, int wpb, cudaStream_t st) {
+static cudaError_t launch_eval_warp(const EvalArgs& a, int fp64, int wpb, cudaStream_t st) {
     RBMNQS_DISPATCH(launch_e, a)
+}
+
+// FP32 E_loc and O_k go to the term-table kernel (eloc.cu) when it supports
+// the machine; log psi, ratios, FP64 and the Pfaffian factor to eval_kernel.
+cudaError_t launch_eval(const EvalArgs& a, int fp64, int wpb, cudaStream_t st) {
+    if (!fp64 && (a.eloc || a.O) && !a.ratio && a.tt.terms && a.m.pf.n == 0) {
+        EvalArgs f = a;
+        f.logpsi = nullptr;
+        const cudaError_t e = launch_eloc_fast(f, st);
+        if (e == cudaSuccess) {
+            if (!a.logpsi) return cudaSuccess;
+            EvalArgs r = a;
+            r.eloc = nullptr;
+            r.O = nullptr;
+            return launch_eval_warp(r, fp64, wpb, st);
+        }
+        if (e != cudaErrorNotSupported) return e;
+    }
+    return launch_eval_warp(a, fp64, wpb, st);
 }
 
 }  // namespace rbmnqs

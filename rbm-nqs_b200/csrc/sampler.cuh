@@ -85,6 +85,28 @@ struct SamplerArgs {
     int sweep0 = 0, nsweeps = 0, record = 1;
 };
 
+// The Hamiltonian regrouped by transition for the FP32 evaluation kernel
+// (local_op.cpp:31-60): every (operator, flip mask) pair that appears in some
+// row of an operator's matrix is one term.  Its value for a configuration is
+// vals[voff + loc] (loc = the operator's local bits, bit i = site i of the
+// operator), zero where the row has no entry with that mask.  Diagonal
+// entries (mask 0) form one term per operator in `diag`.  Sites and flips
+// are packed one byte each.
+struct TermDev {
+    uint32_t flip0;  // flipped sites 0..3
+    uint32_t flip1;  // flipped sites 4..5, then nf, k
+    uint32_t site0;  // operator sites 0..3
+    uint32_t site1;  // operator sites 4..5
+    int voff;        // offset of the 2^k values in vals
+    int pad[3];
+};
+struct TermTable {
+    int n_terms = 0, n_diag = 0, nf_max = 0, n_vals = 0;
+    const TermDev* terms = nullptr;
+    const TermDev* diag = nullptr;
+    const double2* vals = nullptr;
+};
+
 struct EvalArgs {
     MachineDev m;
     HamDev H;
@@ -99,6 +121,7 @@ struct EvalArgs {
     int n_flips;
     double2* ratio;         // ratio mode output (log psi'/psi)
     SmemPlan plan;
+    TermTable tt;           // terms of H for the FP32 evaluation kernel (n_terms 0 with terms null: none)
 };
 
 // Learned-proposal move for every chain: propose draws the flip mask
@@ -152,6 +175,10 @@ cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bond
                          int max_wpb = 0, int pair_mode = -1);
 cudaError_t launch_sampler(const SamplerArgs& a, int fp64, const SamplerShape& shape, cudaStream_t st);
 cudaError_t launch_eval(const EvalArgs& a, int fp64, int warps_per_block, cudaStream_t st);
+// The FP32 evaluation kernel (E_loc and O_k from the term table, no Pfaffian
+// factor).  cudaErrorNotSupported when the machine or the table does not fit
+// it; launch_eval then runs eval_kernel.
+cudaError_t launch_eloc_fast(const EvalArgs& a, cudaStream_t st);
 int elements_per_lane(int T);
 cudaError_t launch_advance(uint32_t* ctl, int reinit, cudaStream_t st);
 cudaError_t launch_mufu_probe(float* out, int iters, int blocks, cudaStream_t st);
