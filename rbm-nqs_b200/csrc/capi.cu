@@ -161,6 +161,55 @@ TermHost build_terms(const std::vector<rbmnqs::local_op>& ops) {
     return t;
 }
 
+// Row order of W in the shared memory of the FP32 evaluation kernel
+// (symmetric machines).  The kernel reads 16-byte pieces of row P_s(f) for
+// the symmetry indices s of eight consecutive lanes at a time; a row of rank
+// q starts at 16-byte unit q u (u odd), i.e. in bank group (q u) mod 8.  Two
+// orders are scored by the number of load wavefronts they cost over every
+// flipped site (the ideal is one per eight lanes): the identity, and the
+// order in which the symmetry orbits of the sites enumerate the rows
+// (rank(P_s(rep)) consecutive in s), which for translation groups gives
+// consecutive lanes consecutive ranks.  The cheaper one is returned.
+std::vector<uint8_t> eval_row_order(const std::vector<std::vector<int>>& perm, int n, int nh) {
+    const int S = (int)perm.size();
+    std::vector<uint8_t> ident(n);
+    for (int r = 0; r < n; r++) ident[r] = (uint8_t)r;
+    const int kb = nh % 4 == 0 ? 4 : (nh % 2 == 0 ? 2 : 1);
+    if (kb == 1 || S == 0) return ident;
+    int u = (8 * nh + 15) / 16;
+    if ((u & 1) == 0) u++;
+    const int G = nh * S / kb, NGK = nh / kb, loads = kb == 4 ? 2 : 1;
+    auto cost = [&](const std::vector<uint8_t>& rank) {
+        long c = 0;
+        for (int f = 0; f < n; f++)
+            for (int g0 = 0; g0 < G; g0 += 8)
+                for (int h = 0; h < loads; h++) {
+                    int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0}, mx = 0;
+                    for (int g = g0; g < std::min(G, g0 + 8); g++) {
+                        const int sidx = g / NGK, k0 = (g % NGK) * kb;
+                        const int unit = rank[perm[sidx][f]] * u + (8 * k0) / 16 + h;
+                        mx = std::max(mx, ++cnt[unit & 7]);
+                    }
+                    c += mx;
+                }
+        return c;
+    };
+    std::vector<uint8_t> orb(n, 0);
+    std::vector<char> used(n, 0);
+    int next = 0;
+    for (int rep = 0; rep < n && next < n; rep++) {
+        if (used[rep]) continue;
+        for (int sidx = 0; sidx < S; sidx++) {
+            const int r = perm[sidx][rep];
+            if (!used[r]) {
+                used[r] = 1;
+                orb[r] = (uint8_t)next++;
+            }
+        }
+    }
+    return cost(orb) < cost(ident) ? orb : ident;
+}
+
 }  // namespace
 
 void rbmnqs::set_last_error(const std::string& msg) { g_err = msg; }
@@ -216,6 +265,7 @@ struct rbmnqs_handle {
     DevBuf<double2> params, vb, hb, W64, x;
     DevBuf<float2> W32;
     DevBuf<uint8_t> perm, inv, orbit;
+    DevBuf<uint8_t> wrank;  // row order of W in the FP32 evaluation kernel (symmetric machines)
     DevBuf<rbmnqs::OpDev> ops;
     DevBuf<int> rowptr;
     DevBuf<uint32_t> emask;
@@ -408,6 +458,7 @@ struct rbmnqs_handle {
         ea.O = O.p;
         ea.plan = eval_plan();
         ea.tt = terms.tt;
+        ea.wrank = wrank.p;
         return ea;
     }
     rbmnqs::LearnedArgs learned_args() const {
@@ -894,6 +945,11 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
             ck(cudaMemcpy(h->perm.p, perm.data(), perm.size(), cudaMemcpyHostToDevice), "copy");
             ck(cudaMemcpy(h->inv.p, inv.data(), inv.size(), cudaMemcpyHostToDevice), "copy");
             ck(cudaMemcpy(h->orbit.p, orbit.data(), orbit.size(), cudaMemcpyHostToDevice), "copy");
+            if (n < 255) {
+                const std::vector<uint8_t> wr = eval_row_order(m.perm, n, nh);
+                h->wrank.alloc(n);
+                ck(cudaMemcpy(h->wrank.p, wr.data(), n, cudaMemcpyHostToDevice), "copy");
+            }
         }
         if (h->pf_n) {
             const int pn = h->pf_n;
@@ -1372,6 +1428,7 @@ static void eval_common(rbmnqs_handle* h, const uint32_t* spins, int B, double* 
     a.B = B;
     a.plan = rbmnqs::SmemPlan{0, h->w_in_smem, 0, 0, 0};
     a.tt = h->terms.tt;
+    a.wrank = h->wrank.p;
     if (logpsi) {
         dl.alloc(B);
         a.logpsi = dl.p;

@@ -44,11 +44,11 @@ int blocks_per_sm(const void* fn, int threads, int smem) {
 
 cudaError_t launch_eloc_fast(const EvalArgs& a, cudaStream_t st) {
     const MachineDev& m = a.m;
-    if (m.pf.n > 0 || !a.tt.terms || a.ratio || a.tt.nf_max > 6 || m.n > 256) return cudaErrorNotSupported;
+    if (m.pf.n > 0 || !a.tt.terms || a.ratio || a.tt.nf_max > 6 || m.n > 255) return cudaErrorNotSupported;
     if (a.B == 0) return cudaSuccess;
     const int kb = m.nh % 4 == 0 ? 4 : (m.nh % 2 == 0 ? 2 : 1);
     const int G = m.T / kb;
-    int ng = 1;
+    int ng = kb == 1 ? 2 : 1;  // entries come in pairs
     while (32 * ng < G) ng *= 2;
     if (kb * ng > 16) return cudaErrorNotSupported;
     const void* fn = pick_eloc(kb, ng, m.symmetric != 0, a.tt.nf_max);

@@ -7,7 +7,6 @@ namespace eloc {
 
 const void* pick_kb1(int ng, bool sym, int nfm) {
     switch (ng) {
-        case 1: return pick3<1, 1>(sym, nfm);
         case 2: return pick3<1, 2>(sym, nfm);
         case 4: return pick3<1, 4>(sym, nfm);
         case 8: return pick3<1, 8>(sym, nfm);

@@ -122,6 +122,7 @@ struct EvalArgs {
     double2* ratio;         // ratio mode output (log psi'/psi)
     SmemPlan plan;
     TermTable tt;           // terms of H for the FP32 evaluation kernel (n_terms 0 with terms null: none)
+    const uint8_t* wrank;   // symmetric machines: row order of W in that kernel's shared memory (null: identity)
 };
 
 // Learned-proposal move for every chain: propose draws the flip mask
