@@ -119,12 +119,19 @@ typedef struct {
                                   cores when precision is 0, FP64 when 1);
                                   1 = FP64 CUDA cores in either precision */
     /* Learned proposals (no reference counterpart): 0 = plain Metropolis;
-     * 1 = after every `step` sweeps, learned_steps multi-spin moves drawn
-     * from the proposal network (independent site flips with network
-     * probabilities) and accepted by the exact Metropolis-Hastings ratio
-     * |psi'/psi|^2 q(s|s')/q(s'|s); samples are recorded after them.  The
-     * network is trained every epoch (learned_train Adam steps, learned_lr)
-     * on pairs of the epoch's samples.  Not with the Pfaffian factor. */
+     * 1 = learned_steps moves per sample after every `step` sweeps (step 0:
+     * no sweeps, the chains move by learned moves alone).  A move flips one
+     * entry of a dictionary of site sets: every single site and every
+     * distinct off-diagonal flip set of the Hamiltonian (Kitaev x / y bonds,
+     * toric-code stars; at most 256 entries).  The proposal network maps the
+     * configuration s to logits over the dictionary; the move is drawn from
+     * q(m|s) = 0.9 softmax(logits(s))_m + 0.1 / D and accepted by the exact
+     * Metropolis-Hastings ratio |psi'/psi|^2 q(m|s') / q(m|s), q(m|s') from
+     * the network at s'.  The network is trained every epoch (learned_train
+     * Adam steps, learned_lr) on the first min(n_chains, 2048) chains'
+     * configurations, towards targets proportional to
+     * min(1, |psi(s with move m)/psi(s)|^2) (softmax cross entropy).  Not
+     * with the Pfaffian factor. */
     int32_t proposal;
     int32_t learned_steps;
     int32_t learned_train;
@@ -322,6 +329,11 @@ int rbmnqs_mlp_forward(rbmnqs_mlp* m, const uint32_t* spins, int32_t B, float* l
  * takes one Adam step with learning rate lr. */
 int rbmnqs_mlp_train_step(rbmnqs_mlp* m, const uint32_t* spins, const uint32_t* targets, int32_t B, float lr,
                           int32_t apply, float* loss, float* grads);
+/* The same step on the soft-target softmax cross entropy
+ * -(1/B) sum_b sum_m t[b][m] log softmax(logits[b])_m, with targets[B][n_out]
+ * (rows summing to 1): the loss the learned proposals are trained with. */
+int rbmnqs_mlp_train_step_soft(rbmnqs_mlp* m, const uint32_t* spins, const float* targets, int32_t B, float lr,
+                               int32_t apply, float* loss, float* grads);
 /* tensor of the last pass for tests: 0 a1, 1 a2, 2 z1, 3 z2, 4 g1, 5 g2,
  * 6 g3 (dL/dlogits); [B][cols] as float (out may be NULL to query cols) */
 int rbmnqs_mlp_intermediate(rbmnqs_mlp* m, int32_t which, int32_t B, float* out, int32_t* cols);

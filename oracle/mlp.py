@@ -8,6 +8,8 @@ tests to check the CUDA forward and backward passes:
                            -> z2 = W2 a1 + b2 -> a2 = GELU(z2)  (h2)
                            -> l  = W3 a2 + b3                    (n_out flip logits)
     loss = (1/B) sum_b sum_i softplus(l_bi) - t_bi l_bi          (BCE with logits)
+    or, for the learned proposals over a move dictionary,
+    loss = -(1/B) sum_b sum_m t_bm log softmax(l_b)_m           (soft targets)
 
 GELU is the erf form.  With bf16=True the values are rounded to bfloat16
 (round to nearest even) at the points where the GPU stores them in BF16: the
@@ -77,11 +79,27 @@ def loss(logits, T):
     return float(np.sum(np.logaddexp(0.0, logits) - T * logits) / B)
 
 
-def backward(f, T, bf=True):
-    """Gradients of loss() with respect to W1..W3, b1..b3."""
+def log_softmax(logits):
+    m = logits.max(axis=1, keepdims=True)
+    return logits - m - np.log(np.exp(logits - m).sum(axis=1, keepdims=True))
+
+
+def loss_soft(logits, T):
+    """Soft-target softmax cross entropy -(1/B) sum_b sum_m T_bm log softmax(l_b)_m
+    (the learned proposals' training loss; rows of T sum to 1)."""
+    B = logits.shape[0]
+    return float(-np.sum(T * log_softmax(logits)) / B)
+
+
+def backward(f, T, bf=True, soft=False):
+    """Gradients of loss() (soft=False) or loss_soft() (soft=True) with
+    respect to W1..W3, b1..b3."""
     r = (lambda v: bf16(v)) if bf else (lambda v: v)
     B = f["logits"].shape[0]
-    g3 = r((1.0 / (1.0 + np.exp(-f["logits"])) - T) / B)
+    if soft:
+        g3 = r((np.exp(log_softmax(f["logits"])) - T) / B)
+    else:
+        g3 = r((1.0 / (1.0 + np.exp(-f["logits"])) - T) / B)
     da2 = g3 @ f["W3"]
     g2 = r(da2 * gelu_grad(f["z2"]))
     da1 = g2 @ f["W2"]

@@ -315,9 +315,13 @@ struct rbmnqs_handle {
     DevBuf<rbmnqs::EpochStatsDev> obsStats;
     // learned proposals: network, proposed configurations, masks, counters
     std::unique_ptr<rbmnqs::Mlp> net;
-    DevBuf<uint32_t> lprop, lmask, lacc, ltry, ltgt;
-    DevBuf<float> lqfw, lloss;
+    DevBuf<uint32_t> lprop, lacc, ltry;
+    DevBuf<int> lmv;
+    DevBuf<float> lqfw, lloss, ltgt;
     DevBuf<double> lrate;
+    // move dictionary: flip masks [D][4], flip lists [D][2]; training batch
+    int n_moves = 0, train_batch = 0;
+    DevBuf<uint32_t> dmask, dflip;
     // Pfaffian factor: class matrix, derivative pairs, unscramble buffers
     int pf_n = 0, pf_indep = 0;
     DevBuf<int16_t> pf_bs;
@@ -467,23 +471,32 @@ struct rbmnqs_handle {
         l.n_chains = cfg.n_chains;
         l.spins = spins.p;
         l.prop = lprop.p;
-        l.mask = lmask.p;
+        l.mv = lmv.p;
         l.qfw = lqfw.p;
         l.logits = net->logits();
         l.ldl = net->dims().out_p;
+        l.n_moves = n_moves;
+        l.mmask = dmask.p;
+        l.mflip = dflip.p;
         l.ctl = ctl.p;
         l.seed = cfg.seed ^ 0x5DEECE66DULL;
         l.n_acc = lacc.p;
         l.n_try = ltry.p;
-        l.pmin = 1e-3f;
+        l.eps = 0.1f;
+        l.targets = ltgt.p;
+        l.B = train_batch;
         return l;
     }
-    // sweeps in segments, learned moves between them, samples recorded after them
+    // sweeps in segments (step sweeps per sample, none when step is 0),
+    // learned moves after them, samples recorded after the moves
     void enqueue_learned_sampling() {
         rbmnqs::SamplerArgs a = sampler_args();
         a.record = 0;
         ck(cudaMemsetAsync(lacc.p, 0, lacc.n * sizeof(uint32_t), st), "memset");
         ck(cudaMemsetAsync(ltry.p, 0, ltry.n * sizeof(uint32_t), st), "memset");
+        // fresh chains when this epoch starts them (the sweep kernel would
+        // draw the same configurations at its first sweep)
+        ck(rbmnqs::launch_init_chains(spins.p, n, cfg.n_chains, ctl.p, cfg.seed, st), "init chains");
         if (cfg.warmup > 0) {
             a.sweep0 = 0;
             a.nsweeps = cfg.warmup;
@@ -491,9 +504,11 @@ struct rbmnqs_handle {
         }
         rbmnqs::LearnedArgs l = learned_args();
         for (int j = 0; j < cfg.samples_per_chain; j++) {
-            a.sweep0 = cfg.warmup + j * cfg.step;
-            a.nsweeps = cfg.step;
-            ck(rbmnqs::launch_sampler(a, fp64, shape, st), "sampler kernel");
+            if (cfg.step > 0) {
+                a.sweep0 = cfg.warmup + j * cfg.step;
+                a.nsweeps = cfg.step;
+                ck(rbmnqs::launch_sampler(a, fp64, shape, st), "sampler kernel");
+            }
             for (int k = 0; k < cfg.learned_steps; k++) {
                 l.move = (uint32_t)(j * cfg.learned_steps + k);
                 ck(net->forward(spins.p, cfg.n_chains, st), "proposal network");
@@ -505,12 +520,14 @@ struct rbmnqs_handle {
         }
         ck(rbmnqs::launch_learned_rate(lacc.p, ltry.p, cfg.n_chains, lrate.p, st), "learned rate");
     }
-    // the network learns the flip pattern between independent configurations:
-    // the chains' final states, chain c paired with chain c + n_chains / 2
+    // the network is trained on the chains' current configurations (the
+    // first train_batch of them) towards t_m proportional to min(1,
+    // |psi(s with move m)/psi(s)|^2)
     void enqueue_learned_training() {
-        ck(rbmnqs::launch_pair_targets(spins.p, cfg.n_chains, ltgt.p, st), "pair targets");
+        if (cfg.learned_train <= 0) return;
+        ck(rbmnqs::launch_learned_targets(learned_args(), st), "learned targets");
         for (int t = 0; t < cfg.learned_train; t++)
-            ck(net->train_step(spins.p, ltgt.p, cfg.n_chains, (float)cfg.learned_lr, st, lloss.p, true),
+            ck(net->train_step_soft(spins.p, ltgt.p, train_batch, (float)cfg.learned_lr, st, lloss.p, true),
                "proposal training");
     }
     // tm: record the stage timing events (off for the second sample of a
@@ -858,9 +875,9 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
                                        cfg->learned_hidden >= 64 && cfg->learned_hidden <= 256),
                 "learned proposals: no Pfaffian factor, <= 256 sites, hidden width 64..256 (multiple of 64)",
                 RBMNQS_ERR_UNSUPPORTED);
-        require(cfg->alpha >= 1 && cfg->n_chains >= 1 && cfg->samples_per_chain >= 1 && cfg->step >= 1 &&
-                    cfg->warmup >= 0,
-                "bad sampler/machine sizes");
+        require(cfg->alpha >= 1 && cfg->n_chains >= 1 && cfg->samples_per_chain >= 1 && cfg->warmup >= 0 &&
+                    (cfg->step >= 1 || (cfg->proposal == 1 && cfg->step == 0 && cfg->learned_steps >= 1)),
+                "bad sampler/machine sizes (step 0 needs learned proposals)");
         auto h = std::make_unique<rbmnqs_handle>();
         h->cfg = *cfg;
         h->model = mdl->m;
@@ -1139,21 +1156,61 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         // FP32 W in shared memory when it fits
         ck(rbmnqs::plan_sampler(h->machine(), h->fp64, cfg->n_chains, h->n_prop_bonds, &h->shape), "sampler plan");
         if (cfg->proposal == 1) {
+            // move dictionary: every site, then the Hamiltonian's distinct
+            // off-diagonal flip sets of two or more sites
+            std::vector<std::vector<int>> moves;
+            for (int i = 0; i < n; i++) moves.push_back({i});
+            {
+                std::vector<std::vector<int>> seen;
+                for (const auto& t : build_terms(m.hamiltonian).terms) {
+                    const int nf = (t.flip1 >> 16) & 0xff;
+                    std::vector<int> fs;
+                    for (int q = 0; q < nf; q++)
+                        fs.push_back(q < 4 ? (t.flip0 >> (8 * q)) & 0xff : (t.flip1 >> (8 * (q - 4))) & 0xff);
+                    std::sort(fs.begin(), fs.end());
+                    if (fs.size() < 2 || std::find(seen.begin(), seen.end(), fs) != seen.end()) continue;
+                    seen.push_back(fs);
+                    moves.push_back(fs);
+                }
+            }
+            require(moves.size() <= 256,
+                    "learned proposals: the move dictionary (sites + off-diagonal flip sets) exceeds 256 moves",
+                    RBMNQS_ERR_UNSUPPORTED);
+            h->n_moves = (int)moves.size();
+            std::vector<uint32_t> mk((size_t)h->n_moves * 4, 0u), fl((size_t)h->n_moves * 2, 0u);
+            for (int d = 0; d < h->n_moves; d++) {
+                const auto& fs = moves[d];
+                for (size_t q = 0; q < fs.size(); q++) {
+                    mk[4 * d + fs[q] / 32] |= 1u << (fs[q] % 32);
+                    const uint32_t b = (uint32_t)fs[q] & 0xff;
+                    if (q < 4)
+                        fl[2 * d] |= b << (8 * q);
+                    else
+                        fl[2 * d + 1] |= b << (8 * (q - 4));
+                }
+                fl[2 * d + 1] |= (uint32_t)fs.size() << 16;
+            }
+            h->dmask.alloc(mk.size());
+            h->dflip.alloc(fl.size());
+            ck(cudaMemcpy(h->dmask.p, mk.data(), mk.size() * 4, cudaMemcpyHostToDevice), "copy");
+            ck(cudaMemcpy(h->dflip.p, fl.data(), fl.size() * 4, cudaMemcpyHostToDevice), "copy");
+            h->train_batch = std::min(cfg->n_chains, 2048);
             rbmnqs::MlpDims md;
-            md.n_in = md.n_out = n;
+            md.n_in = n;
+            md.n_out = h->n_moves;
             md.h1 = md.h2 = cfg->learned_hidden;
             try {
-                h->net = std::make_unique<rbmnqs::Mlp>(md, std::max(cfg->n_chains, h->N), h->st);
+                h->net = std::make_unique<rbmnqs::Mlp>(md, std::max(cfg->n_chains, h->train_batch), h->st);
             } catch (cudaError_t e) {
                 ck(e, "proposal network");
             }
             ck(h->net->init_random(0.02f, cfg->seed), "proposal network init");
             h->lprop.alloc((size_t)cfg->n_chains * 4);
-            h->lmask.alloc((size_t)cfg->n_chains * 4);
-            h->lqfw.alloc((size_t)cfg->n_chains * 4);
+            h->lmv.alloc(cfg->n_chains);
+            h->lqfw.alloc(cfg->n_chains);
             h->lacc.alloc(cfg->n_chains);
             h->ltry.alloc(cfg->n_chains);
-            h->ltgt.alloc((size_t)h->N * 4);
+            h->ltgt.alloc((size_t)h->train_batch * h->n_moves);
             h->lloss.alloc(1);
             h->lrate.alloc(1);
             ck(cudaMemsetAsync(h->lloss.p, 0, sizeof(float), h->st), "memset");
@@ -1960,7 +2017,7 @@ struct rbmnqs_mlp {
     cudaStream_t st = nullptr;
     std::unique_ptr<rbmnqs::Mlp> net;
     DevBuf<uint32_t> spins, targets;
-    DevBuf<float> loss;
+    DevBuf<float> loss, soft;  // soft: [max_batch][n_out] targets of the softmax loss
     ~rbmnqs_mlp() {
         net.reset();
         if (st) cudaStreamDestroy(st);
@@ -2060,12 +2117,40 @@ int rbmnqs_mlp_forward(rbmnqs_mlp* m, const uint32_t* spins, int32_t B, float* l
     });
 }
 
+namespace {
+// loss and gradients of the last training step, gradients in the logical
+// flat parameter layout
+void mlp_results(rbmnqs_mlp* m, float* loss, float* grads);
+}  // namespace
+
 int rbmnqs_mlp_train_step(rbmnqs_mlp* m, const uint32_t* spins, const uint32_t* targets, int32_t B, float lr,
                           int32_t apply, float* loss, float* grads) {
     return guard([&] {
         require(m && spins && targets, "null argument");
         mlp_upload(m, spins, targets, B);
         ck(m->net->train_step(m->spins.p, m->targets.p, B, lr, m->st, m->loss.p, apply != 0), "train step");
+        mlp_results(m, loss, grads);
+    });
+}
+
+int rbmnqs_mlp_train_step_soft(rbmnqs_mlp* m, const uint32_t* spins, const float* targets, int32_t B, float lr,
+                               int32_t apply, float* loss, float* grads) {
+    return guard([&] {
+        require(m && spins && targets, "null argument");
+        mlp_upload(m, spins, nullptr, B);
+        const size_t cnt = (size_t)B * m->net->dims().n_out;
+        if (m->soft.n < cnt) m->soft.alloc((size_t)m->net->max_batch() * m->net->dims().n_out);
+        ck(cudaMemcpyAsync(m->soft.p, targets, cnt * 4, cudaMemcpyHostToDevice, m->st), "copy");
+        ck(m->net->train_step_soft(m->spins.p, m->soft.p, B, lr, m->st, m->loss.p, apply != 0), "train step");
+        mlp_results(m, loss, grads);
+    });
+}
+
+}  // extern "C"
+
+namespace {
+void mlp_results(rbmnqs_mlp* m, float* loss, float* grads) {
+    {
         float l = 0;
         ck(cudaMemcpyAsync(&l, m->loss.p, 4, cudaMemcpyDeviceToHost, m->st), "copy");
         std::vector<float> g;
@@ -2089,8 +2174,11 @@ int rbmnqs_mlp_train_step(rbmnqs_mlp* m, const uint32_t* spins, const uint32_t* 
                 src += prow[l2];
             }
         }
-    });
+    }
 }
+}  // namespace
+
+extern "C" {
 
 int rbmnqs_mlp_intermediate(rbmnqs_mlp* m, int32_t which, int32_t B, float* out, int32_t* cols) {
     return guard([&] {

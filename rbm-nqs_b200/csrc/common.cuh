@@ -49,6 +49,11 @@ template <typename R> __device__ __forceinline__ R warp_sum(R v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
     return v;
 }
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(kFull, v, o));
+    return v;
+}
 template <typename T> __device__ __forceinline__ T warp_cprod(T v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {

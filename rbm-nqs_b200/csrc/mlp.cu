@@ -213,6 +213,49 @@ __global__ void bce_grad(const float* __restrict__ L, const uint32_t* __restrict
     }
 }
 
+// Soft-target softmax cross entropy, one warp per row: with p = softmax(l)
+// over the n logical outputs, dL/dl = (p - t) / B and the loss is
+// -(1/B) sum_m t_m log p_m; targets tg[b][n] (rows sum to 1).  Padded rows
+// and columns get zero gradient.
+__global__ void softmax_ce_grad(const float* __restrict__ L, const float* __restrict__ tg, int B, int n, int rows,
+                                int cols, __nv_bfloat16* __restrict__ G, float* __restrict__ lossp) {
+    __shared__ float red[32];
+    const int lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    float acc = 0.f;
+    for (int b = blockIdx.x * wpb + (threadIdx.x >> 5); b < rows; b += gridDim.x * wpb) {
+        const float* lr = L + (size_t)b * cols;
+        __nv_bfloat16* gr = G + (size_t)b * cols;
+        if (b >= B) {
+            for (int c = lane; c < cols; c += 32) gr[c] = __float2bfloat16_rn(0.f);
+            continue;
+        }
+        float mx = -INFINITY;
+        for (int c = lane; c < n; c += 32) mx = fmaxf(mx, lr[c]);
+        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        float se = 0.f;
+        for (int c = lane; c < n; c += 32) se += expf(lr[c] - mx);
+        for (int o = 16; o > 0; o >>= 1) se += __shfl_xor_sync(0xffffffffu, se, o);
+        const float lse = mx + logf(se);
+        for (int c = lane; c < cols; c += 32) {
+            float g = 0.f;
+            if (c < n) {
+                const float lp = lr[c] - lse, t = tg[(size_t)b * n + c];
+                g = (expf(lp) - t) / (float)B;
+                acc -= t * lp / (float)B;
+            }
+            gr[c] = __float2bfloat16_rn(g);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float s = 0.f;
+        for (int w = 0; w < wpb; w++) s += red[w];
+        lossp[blockIdx.x] = s;
+    }
+}
+
 __global__ void sum_loss(const float* lossp, int n, float* out) {
     if (threadIdx.x == 0) {
         float s = 0.f;
@@ -495,11 +538,29 @@ cudaError_t Mlp::train_step(const uint32_t* spins, const uint32_t* targets, int 
     cudaError_t r = forward(spins, B, st);
     if (r != cudaSuccess) return r;
     const int M = (B + 255) / 256 * 256;  // split-K chunks of 256 samples
-    const int I = d_.in_p, H1 = d_.h1, H2 = d_.h2, Oo = d_.out_p;
     if (M > bmax_) return cudaErrorInvalidValue;
-    const int nb = grid_for((size_t)M * Oo);
-    bce_grad<<<nb, 256, 0, st>>>(L_, targets, B, d_.n_out, M, Oo, G3_, lossp_);
+    const int nb = grid_for((size_t)M * d_.out_p);
+    bce_grad<<<nb, 256, 0, st>>>(L_, targets, B, d_.n_out, M, d_.out_p, G3_, lossp_);
     if (loss_dev) sum_loss<<<1, 32, 0, st>>>(lossp_, nb, loss_dev);
+    return backward_step(B, lr, st, apply);
+}
+
+cudaError_t Mlp::train_step_soft(const uint32_t* spins, const float* targets, int B, float lr, cudaStream_t st,
+                                 float* loss_dev, bool apply) {
+    cudaError_t r = forward(spins, B, st);
+    if (r != cudaSuccess) return r;
+    const int M = (B + 255) / 256 * 256;
+    if (M > bmax_) return cudaErrorInvalidValue;
+    const int nb = std::min(148 * 4, (M + 7) / 8);
+    softmax_ce_grad<<<nb, 256, 0, st>>>(L_, targets, B, d_.n_out, M, d_.out_p, G3_, lossp_);
+    if (loss_dev) sum_loss<<<1, 32, 0, st>>>(lossp_, nb, loss_dev);
+    return backward_step(B, lr, st, apply);
+}
+
+cudaError_t Mlp::backward_step(int B, float lr, cudaStream_t st, bool apply) {
+    cudaError_t r;
+    const int M = (B + 255) / 256 * 256;
+    const int I = d_.in_p, H1 = d_.h1, H2 = d_.h2, Oo = d_.out_p;
     // dA2 = G3 W3 -> G2 = dA2 * gelu'(Z2); dA1 = G2 W2 -> G1
     Epi e{};
     e.mode = kGeluBwd;

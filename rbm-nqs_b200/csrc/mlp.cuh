@@ -41,6 +41,11 @@ class Mlp {
     // (device): loss -> *loss_dev (FP32, device scalar) when non-null.
     cudaError_t train_step(const uint32_t* spins, const uint32_t* targets, int B, float lr, cudaStream_t st,
                            float* loss_dev, bool apply);
+    // The same step on the soft-target softmax cross entropy
+    // -(1/B) sum_b sum_m t[b][m] log softmax(logits[b])_m, targets[B][n_out]
+    // (FP32, device, rows summing to 1).
+    cudaError_t train_step_soft(const uint32_t* spins, const float* targets, int B, float lr, cudaStream_t st,
+                                float* loss_dev, bool apply);
     // gradient buffers (FP32, device) in the flat parameter layout, valid after train_step
     const float* grads() const { return grad_; }
     // intermediate tensors for tests: which = 0 a1, 1 a2, 2 z1, 3 z2, 4 g1, 5 g2, 6 g3 (rows x cols as float)
@@ -71,6 +76,9 @@ class Mlp {
     size_t off_W(int l) const;
     size_t off_b(int l) const;
     cudaError_t refresh_bf16(cudaStream_t st);
+    // backward from dL/dlogits in G3 (after a forward of B rows), gradients,
+    // and the Adam step when apply
+    cudaError_t backward_step(int B, float lr, cudaStream_t st, bool apply);
 };
 
 }  // namespace rbmnqs

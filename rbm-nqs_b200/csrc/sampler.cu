@@ -1489,124 +1489,310 @@ __global__ void __launch_bounds__(256, E <= 4 ? 4 : 2) eval_kernel(const EvalArg
 
 // ---------------------------------------------------------------------------
 // Learned proposals (learned-proposal extension; no reference counterpart).
-// Random streams: Philox counter {(move << 5) | (word << 3) | group, epoch,
-// chain, 3} for the flip draws and {move, epoch, chain, 4} for the
-// acceptance draw, disjoint from the sweep streams 0 and 1.
-__device__ __forceinline__ float clamp_prob(float logit, float pmin) {
-    const float p = 1.f / (1.f + __expf(-logit));
-    return fminf(fmaxf(p, pmin), 1.f - pmin);
+// A move is one entry m of a dictionary of flip sets (every single site and
+// every off-diagonal flip set of the Hamiltonian: x / y bonds of the Kitaev
+// model, stars of the toric code).  The network maps the current
+// configuration s to logits over the dictionary; the proposal is
+// q(m|s) = (1 - eps) softmax(logits(s))_m + eps / D, and s' = s with m's
+// sites flipped.  Every move is its own inverse, so the Metropolis-Hastings
+// ratio is |psi(s')/psi(s)|^2 q(m|s') / q(m|s), q(m|s') from the network at
+// s'.  The uniform part eps / D keeps every single-site flip possible
+// (irreducible chain).  Random streams: Philox {128 move + 2 lane + k,
+// epoch, chain, 3} for the Gumbel draws, {128 move + 64, ...} for the
+// mixture draw and {move, epoch, chain, 4} for the acceptance.
+
+// The proposal's log probability from a logits row: lanes hold m = lane +
+// 32 i; returns log q(m) for the given m on every lane and log-sum-exp.
+__device__ __forceinline__ float logq_of(const float* row, int D, int m, float eps, int lane) {
+    float mx = -INFINITY;
+    for (int i = lane; i < D; i += 32) mx = fmaxf(mx, row[i]);
+    mx = warp_max(mx);
+    float se = 0.f;
+    for (int i = lane; i < D; i += 32) se += __expf(row[i] - mx);
+    se = warp_sum(se);
+    const float p = __expf(row[m] - mx) / se;
+    return __logf((1.f - eps) * p + eps / (float)D);
 }
 
+// one warp per chain: draw m ~ q(.|s), record it, log q(m|s) and s'
 __global__ void learned_propose(const LearnedArgs a) {
-    const int total = a.n_chains * 4, n = a.m.n;
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
     const uint2 key = make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32));
     const uint32_t epoch = a.ctl[0];
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-        const int c = t >> 2, w = t & 3;
-        uint32_t f = 0;
-        float lq = 0.f;
-        for (int g = 0; g < 8; g++) {
-            const int i0 = 32 * w + 4 * g;
-            if (i0 >= n) break;
-            const uint4 r = philox4x32(make_uint4((a.move << 5) | (uint32_t)(w << 3) | (uint32_t)g, epoch,
-                                                  (uint32_t)c, 3),
-                                       key);
+    const int D = a.n_moves;
+    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < a.n_chains; c += nw) {
+        const float* row = a.logits + (size_t)c * a.ldl;
+        // Gumbel-max over the softmax part: argmax_m logit_m - ln(-ln u_m)
+        float best = -INFINITY;
+        int bm = 0;
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const uint4 r = philox4x32(make_uint4(128u * a.move + 2u * lane + k, epoch, (uint32_t)c, 3), key);
             const uint32_t rr[4] = {r.x, r.y, r.z, r.w};
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                const int i = i0 + q;
-                if (i >= n) break;
-                const float p = clamp_prob(a.logits[(size_t)c * a.ldl + i], a.pmin);
-                const bool fl = unit24<float>(rr[q]) < p;
-                lq += __logf(fl ? p : 1.f - p);
-                f |= (fl ? 1u : 0u) << (i & 31);
+                const int m = lane + 32 * (4 * k + q);
+                if (m >= D) break;
+                const float u = ((float)(rr[q] >> 8) + 0.5f) * (1.f / 16777216.f);
+                const float g = row[m] - __logf(-__logf(u));
+                if (g > best) {
+                    best = g;
+                    bm = m;
+                }
             }
         }
-        a.mask[t] = f;
-        a.prop[t] = a.spins[t] ^ f;
-        a.qfw[t] = lq;
-    }
-}
-
-// Re log psi without the constant: bias + sum ln|cosh theta| - T ln 2
-template <int E>
-__device__ __forceinline__ double log_amp(const MachineDev& m, const double2* W64, const uint8_t* perm,
-                                          const uint32_t sp[4], int lane) {
-    C2<double> th[E];
-    theta_fp64<E, double>(m, W64, perm, lane, sp, th);
-    double acc = 0;
 #pragma unroll
-    for (int e = 0; e < E; e++)
-        if (slot_valid(lane, e, m.T)) acc += lnc_re<double>(th[e].x, th[e].y);
-    // visible bias (rbm_base.cpp:294-296, rbm_symmetry.cpp:138-147)
-    const int nb = m.symmetric ? m.n_vb * m.S : m.n_vb;
-    for (int q = lane; q < nb; q += 32) {
-        const int i = m.symmetric ? q / m.S : q;
-        const int site = m.symmetric ? (int)m.orbit[q] : q;
-        acc += m.vb[i].x * (spin_bit(sp, site) ? -1.0 : 1.0);
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ob = __shfl_xor_sync(kFull, best, o);
+            const int om = __shfl_xor_sync(kFull, bm, o);
+            if (ob > best || (ob == best && om < bm)) {
+                best = ob;
+                bm = om;
+            }
+        }
+        // the uniform part of the mixture
+        const uint4 r = philox4x32(make_uint4(128u * a.move + 64u, epoch, (uint32_t)c, 3), key);
+        if (unit24<float>(r.x) < a.eps) bm = (int)pick(r.y, (uint32_t)D);
+        const float lq = logq_of(row, D, bm, a.eps, lane);
+        if (lane < 4) a.prop[4 * c + lane] = a.spins[4 * c + lane] ^ a.mmask[4 * bm + lane];
+        if (lane == 0) {
+            a.mv[c] = bm;
+            a.qfw[c] = lq;
+        }
     }
-    return warp_sum(acc);
 }
 
+// Shared tables of the learned kernels: FP64 W, the symmetry table and the
+// all-up theta (theta recomputed from the configuration), FP32 W with its
+// zero row (flip rows of the ratio); each from global memory when the
+// shared copies do not fit (smem_w 0).
+struct LearnTabs {
+    const double2* W64;
+    const float2* W32;
+    const uint8_t* perm;
+    const double2* base;
+    const float* bre;  // Re v[f mod n_vb], [n] = 0
+};
+__host__ __device__ inline int learned_smem_bytes(const MachineDev& m, int smem_w) {
+    const int TP = padded_T(m.T);
+    int b = align16(TP * 16) + align16((m.n + 1) * 4);
+    if (smem_w) b += align16(m.n * m.nh * 16) + align16((m.n + 1) * m.nh * 8) + (m.symmetric ? align16(m.n * m.S) : 0);
+    return b;
+}
+__device__ LearnTabs learned_tables(const MachineDev& m, unsigned char* smem, int smem_w) {
+    const int TP = padded_T(m.T), tid = threadIdx.x, nt = blockDim.x;
+    LearnTabs L{m.W64, m.W32, m.perm, nullptr, nullptr};
+    int off = 0;
+    double2* base = reinterpret_cast<double2*>(smem + off);
+    off += align16(TP * 16);
+    float* bre = reinterpret_cast<float*>(smem + off);
+    off += align16((m.n + 1) * 4);
+    if (smem_w) {
+        double2* w64 = reinterpret_cast<double2*>(smem + off);
+        off += align16(m.n * m.nh * 16);
+        float2* w32 = reinterpret_cast<float2*>(smem + off);
+        off += align16((m.n + 1) * m.nh * 8);
+        for (int i = tid; i < m.n * m.nh; i += nt) w64[i] = m.W64[i];
+        for (int i = tid; i < (m.n + 1) * m.nh; i += nt) w32[i] = i < m.n * m.nh ? m.W32[i] : make_float2(0.f, 0.f);
+        L.W64 = w64;
+        L.W32 = w32;
+        if (m.symmetric) {
+            uint8_t* p = smem + off;
+            for (int i = tid; i < m.n * m.S; i += nt) p[i] = m.perm[i];
+            L.perm = p;
+        }
+    }
+    for (int i = tid; i <= m.n; i += nt) bre[i] = i < m.n ? (float)m.vb[i % m.n_vb].x : 0.f;
+    __syncthreads();
+    for (int t = tid; t < TP; t += nt) {
+        double2 acc = make_double2(0, 0);
+        if (t < m.T) {
+            const int k = t % m.nh, sy = t / m.nh;
+            acc = m.hb[k];
+            for (int f = 0; f < m.n; f++) {
+                const double2 w = L.W64[(m.symmetric ? (int)L.perm[f * m.S + sy] : f) * m.nh + k];
+                acc.x += w.x;
+                acc.y += w.y;
+            }
+        }
+        base[t] = acc;
+    }
+    __syncthreads();
+    L.base = base;
+    L.bre = bre;
+    return L;
+}
+
+// FP32 theta of a configuration (lane entries t = lane + 32 e, zero beyond
+// T), recomputed in FP64 as the all-up table minus 2 W over the down spins.
+// The lane's entries (k, s) of theta, t = lane + 32 e; -1 beyond T.
+template <int E> struct LaneEnt {
+    int k[E], s[E];
+    __device__ LaneEnt(const MachineDev& m, int lane) {
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            const int t = lane + 32 * e;
+            k[e] = t < m.T ? t % m.nh : -1;
+            s[e] = t < m.T ? t / m.nh : 0;
+        }
+    }
+};
+
 template <int E>
-__global__ void __launch_bounds__(256) learned_accept(const LearnedArgs a, int tables_in_smem) {
+__device__ __forceinline__ void learned_theta(const MachineDev& m, const LearnTabs& L, const LaneEnt<E>& le,
+                                              const uint32_t (&sp)[4], int lane, float2 (&th)[E]) {
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+        const int t = lane + 32 * e;
+        double2 acc = le.k[e] >= 0 ? L.base[t] : make_double2(0, 0);
+        if (le.k[e] >= 0) {
+            const int k = le.k[e], sy = le.s[e];
+#pragma unroll
+            for (int wd = 0; wd < 4; wd++) {
+                uint32_t bits = sp[wd];
+                while (bits) {
+                    const int f = 32 * wd + __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    const double2 w = L.W64[(m.symmetric ? (int)L.perm[f * m.S + sy] : f) * m.nh + k];
+                    acc.x = fma(-2.0, w.x, acc.x);
+                    acc.y = fma(-2.0, w.y, acc.y);
+                }
+            }
+        }
+        th[e] = make_float2((float)acc.x, (float)acc.y);
+    }
+}
+
+// Re log psi(s with the move's flips)/psi(s): lane partial of the ln|cosh|
+// difference (sum with sweep_sum) plus, on lane 0, the visible bias.
+template <int E>
+__device__ __forceinline__ float move_partial(const MachineDev& m, const LearnTabs& L, const LaneEnt<E>& le,
+                                              const float2 (&th)[E], float s0, const uint32_t (&sp)[4], uint32_t fw0,
+                                              uint32_t fw1, int lane) {
+    const int nf = (fw1 >> 16) & 0xff;
+    float2 tp[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) tp[e] = th[e];
+    float bias = 0.f;
+    for (int q = 0; q < nf; q++) {
+        const int f = q < 4 ? (fw0 >> (8 * q)) & 0xff : (fw1 >> (8 * (q - 4))) & 0xff;
+        const float g = spin_bit(sp, f) ? 2.f : -2.f;  // -2 sigma_f
+        bias = fmaf(g, L.bre[f], bias);
+        const float2 G2 = make_float2(g, g);
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+            if (le.k[e] < 0) continue;
+            const float2 w = L.W32[(m.symmetric ? (int)L.perm[f * m.S + le.s[e]] : f) * m.nh + le.k[e]];
+            tp[e] = __ffma2_rn(G2, w, tp[e]);
+        }
+    }
+    return lnc_sweep_sum<E>(tp) - s0 + (lane == 0 ? bias : 0.f);
+}
+
+// one warp per chain: log q(m|s') from the network at s', |psi'/psi|^2 in
+// FP32 from the FP64-recomputed theta, Metropolis-Hastings test
+template <int E>
+__global__ void __launch_bounds__(256) learned_accept(const LearnedArgs a, int smem_w) {
     extern __shared__ __align__(16) unsigned char smem[];
+    const LearnTabs L = learned_tables(a.m, smem, smem_w);
     const int lane = threadIdx.x & 31;
-    const int n = a.m.n;
-    // W (FP64, site-major) and the symmetry table in shared memory when they fit
-    const double2* W64 = a.m.W64;
-    const uint8_t* perm = a.m.perm;
-    if (tables_in_smem) {
-        double2* sW = reinterpret_cast<double2*>(smem);
-        uint8_t* sP = reinterpret_cast<uint8_t*>(sW + (size_t)n * a.m.nh);
-        for (int i = threadIdx.x; i < n * a.m.nh; i += blockDim.x) sW[i] = a.m.W64[i];
-        if (a.m.symmetric)
-            for (int i = threadIdx.x; i < n * a.m.S; i += blockDim.x) sP[i] = a.m.perm[i];
-        __syncthreads();
-        W64 = sW;
-        perm = a.m.symmetric ? sP : a.m.perm;
-    }
-    const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (c >= a.n_chains) return;
-    // log q(s|s') from the proposed configuration's logits, same mask
-    float lq = 0.f;
-    for (int i = lane; i < n; i += 32) {
-        const float p = clamp_prob(a.logits[(size_t)c * a.ldl + i], a.pmin);
-        const bool fl = (a.mask[4 * c + (i >> 5)] >> (i & 31)) & 1u;
-        lq += __logf(fl ? p : 1.f - p);
-    }
-    const float qrev = warp_sum(lq);
-    const float qfwd = a.qfw[4 * c] + a.qfw[4 * c + 1] + a.qfw[4 * c + 2] + a.qfw[4 * c + 3];
-    uint32_t s0[4], s1[4];
-#pragma unroll
-    for (int w = 0; w < 4; w++) {
-        s0[w] = a.spins[4 * c + w];
-        s1[w] = a.prop[4 * c + w];
-    }
-    const double d = log_amp<E>(a.m, W64, perm, s1, lane) - log_amp<E>(a.m, W64, perm, s0, lane);
+    const LaneEnt<E> le(a.m, lane);
+    const int nw = (gridDim.x * blockDim.x) >> 5;
     const uint2 key = make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32));
-    const uint4 r = philox4x32(make_uint4(a.move, a.ctl[0], (uint32_t)c, 4), key);
-    // accept with min(1, |psi'/psi|^2 q(s|s') / q(s'|s))
-    const double lu = log((double)unit24<double>(r.x));
-    const bool acc = lu < 2.0 * d + (double)qrev - (double)qfwd;
-    if (lane < 4 && acc) a.spins[4 * c + lane] = s1[lane];
-    if (lane == 0) {
-        a.n_acc[c] += acc ? 1u : 0u;
-        a.n_try[c] += 1u;
+    const uint32_t epoch = a.ctl[0];
+    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < a.n_chains; c += nw) {
+        const int mv = a.mv[c];
+        const float qrev = logq_of(a.logits + (size_t)c * a.ldl, a.n_moves, mv, a.eps, lane);
+        uint32_t sp[4];
+#pragma unroll
+        for (int w = 0; w < 4; w++) sp[w] = a.spins[4 * c + w];
+        float2 th[E];
+        learned_theta<E>(a.m, L, le, sp, lane, th);
+        const float s0 = lnc_sweep_sum<E>(th);
+        const float d =
+            sweep_sum(move_partial<E>(a.m, L, le, th, s0, sp, a.mflip[2 * mv], a.mflip[2 * mv + 1], lane));
+        const uint4 r = philox4x32(make_uint4(a.move, epoch, (uint32_t)c, 4), key);
+        // accept with min(1, |psi'/psi|^2 q(m|s') / q(m|s))
+        const bool acc = __logf(unit24<float>(r.x) + 0x1p-25f) < 2.f * d + qrev - a.qfw[c];
+        if (lane < 4 && acc) a.spins[4 * c + lane] = a.prop[4 * c + lane];
+        if (lane == 0) {
+            a.n_acc[c] += acc ? 1u : 0u;
+            a.n_try[c] += 1u;
+        }
     }
+}
+
+// Training targets of the proposal network at configurations spins[0..B):
+// t_m proportional to min(1, |psi(s with move m)/psi(s)|^2), a locally
+// balanced choice (g(r) = min(1, r) satisfies g(r) = r g(1/r)), so that
+// moves likely to be accepted get most of the proposal probability.
+template <int E>
+__global__ void __launch_bounds__(256) learned_targets(const LearnedArgs a, int smem_w) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const LearnTabs L = learned_tables(a.m, smem, smem_w);
+    const int lane = threadIdx.x & 31;
+    const LaneEnt<E> le(a.m, lane);
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const int D = a.n_moves;
+    for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < a.B; b += nw) {
+        uint32_t sp[4];
+#pragma unroll
+        for (int w = 0; w < 4; w++) sp[w] = a.spins[4 * b + w];
+        float2 th[E];
+        learned_theta<E>(a.m, L, le, sp, lane, th);
+        const float s0 = lnc_sweep_sum<E>(th);
+        float lg[8];  // min(0, 2 ln|psi'/psi|) of moves lane + 32 i
+#pragma unroll
+        for (int i = 0; i < 8; i++) lg[i] = -INFINITY;
+        for (int mv = 0; mv < D; mv++) {
+            const float d =
+                sweep_sum(move_partial<E>(a.m, L, le, th, s0, sp, a.mflip[2 * mv], a.mflip[2 * mv + 1], lane));
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+                if (mv == lane + 32 * i) lg[i] = fminf(0.f, 2.f * d);
+        }
+        float mx = -INFINITY;
+#pragma unroll
+        for (int i = 0; i < 8; i++) mx = fmaxf(mx, lg[i]);
+        mx = warp_max(mx);
+        float se = 0.f;
+#pragma unroll
+        for (int i = 0; i < 8; i++) se += lane + 32 * i < D ? __expf(lg[i] - mx) : 0.f;
+        se = warp_sum(se);
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+            if (lane + 32 * i < D) a.targets[(size_t)b * D + lane + 32 * i] = __expf(lg[i] - mx) / se;
+    }
+}
+
+// Fresh chains (Philox stream 1, as chain_start) when the control word asks
+// for initialisation: for epochs whose moves run without a sweep kernel.
+__global__ void init_chains(uint32_t* spins, int n, int n_chains, const uint32_t* ctl, uint64_t seed) {
+    if (!ctl[1]) return;
+    const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n_chains; c += gridDim.x * blockDim.x) {
+        const uint4 r = philox4x32(make_uint4(0, ctl[0], (uint32_t)c, 1), key);
+        const uint32_t rw[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+        for (int w = 0; w < 4; w++) {
+            const int lo = 32 * w;
+            const uint32_t mask = n >= lo + 32 ? 0xffffffffu : (n > lo ? ((1u << (n - lo)) - 1) : 0u);
+            spins[4 * c + w] = rw[w] & mask;
+        }
+    }
+}
+
+cudaError_t launch_init_chains(uint32_t* spins, int n, int n_chains, const uint32_t* ctl, uint64_t seed,
+                               cudaStream_t st) {
+    init_chains<<<std::min(148 * 4, (n_chains + 255) / 256), 256, 0, st>>>(spins, n, n_chains, ctl, seed);
+    return cudaGetLastError();
 }
 
 __global__ void record_kernel(const uint32_t* spins, int n_chains, int spc, int j, uint32_t* samples) {
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 4 * n_chains; t += gridDim.x * blockDim.x) {
         const int c = t >> 2, w = t & 3;
         samples[4 * ((size_t)c * spc + j) + w] = spins[t];
-    }
-}
-
-__global__ void pair_targets(const uint32_t* samples, int N, uint32_t* targets) {
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 4 * N; t += gridDim.x * blockDim.x) {
-        const int i = t >> 2, w = t & 3;
-        targets[t] = samples[t] ^ samples[4 * ((i + N / 2) % N) + w];
     }
 }
 
@@ -1635,40 +1821,51 @@ __global__ void learned_rate(const uint32_t* n_acc, const uint32_t* n_try, int n
 }
 
 cudaError_t launch_learned_propose(const LearnedArgs& a, cudaStream_t st) {
-    const int total = 4 * a.n_chains;
-    learned_propose<<<std::min(148 * 8, (total + 255) / 256), 256, 0, st>>>(a);
+    learned_propose<<<std::min(148 * 8, (a.n_chains + 7) / 8), 256, 0, st>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_learned_accept(const LearnedArgs& a, cudaStream_t st) {
-    const int blocks = (a.n_chains + 7) / 8;
-    const size_t tb = (size_t)a.m.n * a.m.nh * 16 + (a.m.symmetric ? (size_t)a.m.n * a.m.S : 0);
-    const int in_smem = tb <= 96 * 1024;
-    const int smem = in_smem ? (int)tb : 0;
+static cudaError_t launch_learned_kernel(const LearnedArgs& a, int which, int rows, cudaStream_t st) {
+    const int full = learned_smem_bytes(a.m, 1);
+    const int smem_w = full <= 160 * 1024;
+    const int smem = learned_smem_bytes(a.m, smem_w);
     const void* fn = nullptr;
+#define RBMNQS_LK(E)                                                                                 \
+    fn = which == 0 ? reinterpret_cast<const void*>(learned_accept<E>)                            \
+                    : reinterpret_cast<const void*>(learned_targets<E>);
     switch (elements_per_lane(a.m.T)) {
-        case 1: fn = reinterpret_cast<const void*>(learned_accept<1>); break;
-        case 2: fn = reinterpret_cast<const void*>(learned_accept<2>); break;
-        case 4: fn = reinterpret_cast<const void*>(learned_accept<4>); break;
-        case 8: fn = reinterpret_cast<const void*>(learned_accept<8>); break;
-        case 16: fn = reinterpret_cast<const void*>(learned_accept<16>); break;
+        case 1: RBMNQS_LK(1) break;
+        case 2: RBMNQS_LK(2) break;
+        case 4: RBMNQS_LK(4) break;
+        case 8: RBMNQS_LK(8) break;
+        case 16: RBMNQS_LK(16) break;
         default: return cudaErrorInvalidValue;
     }
+#undef RBMNQS_LK
     cudaError_t e = ensure_dynamic_smem(fn, smem);
     if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    const int blocks = std::max(1, std::min((rows + 7) / 8, 2 * sms));
     LearnedArgs aa = a;
-    int flag = in_smem;
+    int flag = smem_w;
     void* args[] = {&aa, &flag};
     return cudaLaunchKernel(fn, dim3(blocks), dim3(256), args, smem, st);
 }
 
-cudaError_t launch_record(const uint32_t* spins, int n_chains, int spc, int j, uint32_t* samples, cudaStream_t st) {
-    record_kernel<<<std::min(148 * 4, (4 * n_chains + 255) / 256), 256, 0, st>>>(spins, n_chains, spc, j, samples);
-    return cudaGetLastError();
+cudaError_t launch_learned_accept(const LearnedArgs& a, cudaStream_t st) {
+    return launch_learned_kernel(a, 0, a.n_chains, st);
 }
 
-cudaError_t launch_pair_targets(const uint32_t* samples, int N, uint32_t* targets, cudaStream_t st) {
-    pair_targets<<<std::min(148 * 4, (4 * N + 255) / 256), 256, 0, st>>>(samples, N, targets);
+cudaError_t launch_learned_targets(const LearnedArgs& a, cudaStream_t st) {
+    if (a.B <= 0) return cudaSuccess;
+    if (a.n_moves > 256) return cudaErrorInvalidValue;
+    return launch_learned_kernel(a, 1, a.B, st);
+}
+
+cudaError_t launch_record(const uint32_t* spins, int n_chains, int spc, int j, uint32_t* samples, cudaStream_t st) {
+    record_kernel<<<std::min(148 * 4, (4 * n_chains + 255) / 256), 256, 0, st>>>(spins, n_chains, spc, j, samples);
     return cudaGetLastError();
 }
 

@@ -125,34 +125,41 @@ struct EvalArgs {
     const uint8_t* wrank;   // symmetric machines: row order of W in that kernel's shared memory (null: identity)
 };
 
-// Learned-proposal move for every chain: propose draws the flip mask
-// (independent sites, probability clamp(sigmoid(logit), pmin, 1 - pmin)) from
-// the network's logits of the current configurations and records log
-// q(s'|s); accept takes the logits of the proposed configurations, forms
-// log q(s|s') and log|psi(s')/psi(s)| (FP64 theta of both) and applies the
-// Metropolis-Hastings test.
+// Learned-proposal move for every chain (dictionary moves): propose draws a
+// move m of the dictionary from q(.|s) = (1 - eps) softmax(logits(s)) +
+// eps / D and records log q(m|s) and s' = s with m's sites flipped; accept
+// takes the logits at s' for log q(m|s'), forms log|psi(s')/psi(s)| and
+// applies the Metropolis-Hastings test.  targets writes the network's
+// training targets at configurations spins[0..B).
 struct LearnedArgs {
     MachineDev m;
     int n_chains;
     uint32_t* spins;        // [n_chains][4] current configurations
     uint32_t* prop;         // [n_chains][4] proposed configurations
-    uint32_t* mask;         // [n_chains][4] flip masks
-    float* qfw;             // [n_chains][4] log q(s'|s) per 32-site word
-    const float* logits;    // [n_chains][ldl] network output
+    int* mv;                // [n_chains] proposed move
+    float* qfw;             // [n_chains] log q(m|s)
+    const float* logits;    // [rows][ldl] network output
     int ldl;
+    int n_moves;            // D (<= 256)
+    const uint32_t* mmask;  // [D][4] flip masks
+    const uint32_t* mflip;  // [D][2] flipped sites (bytes 0..5) and their count (byte 6)
     const uint32_t* ctl;    // {epoch, init}
     uint64_t seed;
     uint32_t move;          // move index within the epoch (Philox counter)
     uint32_t* n_acc;        // [n_chains] accepted learned moves (epoch)
     uint32_t* n_try;        // [n_chains] learned moves tried (epoch)
-    float pmin;
+    float eps;              // uniform part of the proposal
+    float* targets;         // [B][D] training targets (targets kernel)
+    int B;
 };
 cudaError_t launch_learned_propose(const LearnedArgs& a, cudaStream_t st);
 cudaError_t launch_learned_accept(const LearnedArgs& a, cudaStream_t st);
+cudaError_t launch_learned_targets(const LearnedArgs& a, cudaStream_t st);
+// chains from Philox stream 1 (as the sweep kernel's fresh start) when ctl[1] is set
+cudaError_t launch_init_chains(uint32_t* spins, int n, int n_chains, const uint32_t* ctl, uint64_t seed,
+                               cudaStream_t st);
 // samples[c * spc + j] = spins[c]
 cudaError_t launch_record(const uint32_t* spins, int n_chains, int spc, int j, uint32_t* samples, cudaStream_t st);
-// targets[i] = samples[i] ^ samples[(i + N / 2) % N] (pairs of independent samples)
-cudaError_t launch_pair_targets(const uint32_t* samples, int N, uint32_t* targets, cudaStream_t st);
 // acceptance of the learned moves -> *out (device)
 cudaError_t launch_learned_rate(const uint32_t* n_acc, const uint32_t* n_try, int n_chains, double* out,
                                 cudaStream_t st);

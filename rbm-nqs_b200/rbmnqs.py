@@ -131,6 +131,7 @@ def _declare(L):
         "rbmnqs_mlp_init": [VP, C.c_float, C.c_uint64],
         "rbmnqs_mlp_forward": [VP, P_U32, C.c_int32, P_F],
         "rbmnqs_mlp_train_step": [VP, P_U32, P_U32, C.c_int32, C.c_float, C.c_int32, P_F, P_F],
+        "rbmnqs_mlp_train_step_soft": [VP, P_U32, P_F, C.c_int32, C.c_float, C.c_int32, P_F, P_F],
         "rbmnqs_mlp_intermediate": [VP, C.c_int32, C.c_int32, P_F, P_I],
         "rbmnqs_mlp_destroy": [VP],
     }
@@ -541,6 +542,16 @@ class ProposalNet:
         g = np.zeros(self.n_params, np.float32) if grads else None
         _ck(lib().rbmnqs_mlp_train_step(self._h, _p(s, P_U32), _p(t, P_U32), s.shape[0], lr, 1 if apply else 0,
                                         C.byref(loss), _p(g, P_F)))
+        return loss.value, g
+
+    def train_step_soft(self, spins, targets, lr=1e-3, apply=True, grads=True):
+        """One step on the softmax cross entropy against soft targets [B][n_out]."""
+        s = np.ascontiguousarray(spins, dtype=np.uint32)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        loss = C.c_float()
+        g = np.zeros(self.n_params, np.float32) if grads else None
+        _ck(lib().rbmnqs_mlp_train_step_soft(self._h, _p(s, P_U32), _p(t, P_F), s.shape[0], lr, 1 if apply else 0,
+                                             C.byref(loss), _p(g, P_F)))
         return loss.value, g
 
     def intermediate(self, which, B):

@@ -33,7 +33,7 @@ def setup(dims, B, seed=3, std=0.05, max_batch=None):
     net.set_params(rbmnqs.mlp_flatten(p))
     p = rbmnqs.mlp_unflatten(net.get_params(), dims)  # the FP32 values the GPU holds
     spins = O.random_spins(rng, B, dims[0])
-    tgt = O.random_spins(rng, B, dims[3])
+    tgt = O.random_spins(rng, B, min(dims[3], 128))
     return net, p, spins, tgt
 
 
@@ -88,6 +88,29 @@ def test_backward_layers_and_gradients_match_oracle(dims, B, cap):
     # against the oracle's own BF16 backward pass from the same parameters
     f = M.forward(p, X)
     go = M.backward(f, T)
+    for k in ("W1", "W2", "W3", "b1", "b2", "b3"):
+        err = np.linalg.norm(grads[k] - go[k]) / np.linalg.norm(go[k])
+        assert err < 2e-2, (k, err)
+
+
+@pytest.mark.parametrize("dims,B", [((128, 256, 256, 256), 512), ((18, 64, 64, 27), 300)])
+def test_soft_target_gradients_match_oracle(dims, B):
+    """Softmax cross entropy over a move dictionary (the learned proposals'
+    loss): dL/dlogits and the parameter gradients against the oracle."""
+    net, p, spins, _ = setup(dims, B, max_batch=1024)
+    rng = np.random.default_rng(8)
+    T = rng.random((B, dims[3])) ** 4
+    T /= T.sum(axis=1, keepdims=True)
+    loss, g = net.train_step_soft(spins, T, apply=False)
+    L = net.forward(spins).astype(np.float64)
+    X = M.spins_to_input(spins, dims[0])
+    T32 = T.astype(np.float32).astype(np.float64)
+    assert abs(loss - M.loss_soft(L, T32)) < 1e-5 * abs(M.loss_soft(L, T32))
+    net.train_step_soft(spins, T, apply=False)
+    g3 = net.intermediate(6, B)[:, :dims[3]].astype(np.float64)
+    assert bf_close(g3, M.bf16((np.exp(M.log_softmax(L)) - T32) / B))
+    grads = rbmnqs.mlp_unflatten(g, dims)
+    go = M.backward(M.forward(p, X), T32, soft=True)
     for k in ("W1", "W2", "W3", "b1", "b2", "b3"):
         err = np.linalg.norm(grads[k] - go[k]) / np.linalg.norm(go[k])
         assert err < 2e-2, (k, err)

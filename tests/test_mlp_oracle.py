@@ -43,6 +43,32 @@ def test_backward_matches_finite_differences():
             assert abs(fd - g[k].ravel()[idx]) < 1e-7 * max(1.0, abs(fd)), (k, idx, fd, g[k].ravel()[idx])
 
 
+def test_soft_backward_matches_finite_differences():
+    """The softmax cross entropy against soft targets (the learned proposals'
+    loss over a move dictionary)."""
+    dims = (12, 64, 64, 20)
+    rng = np.random.default_rng(4)
+    p = M.init(dims, std=0.3, seed=5)
+    for k in ("b1", "b2", "b3"):
+        p[k] = rng.normal(0, 0.1, p[k].shape)
+    X = rng.choice([-1.0, 1.0], size=(7, dims[0]))
+    T = rng.random((7, dims[3]))
+    T /= T.sum(axis=1, keepdims=True)
+    g = M.backward(M.forward(p, X, bf=False), T, bf=False, soft=True)
+    eps = 1e-6
+    for k in ("W1", "b1", "W2", "b2", "W3", "b3"):
+        flat = p[k].ravel()
+        for idx in rng.choice(flat.size, 6, replace=False):
+            old = flat[idx]
+            flat[idx] = old + eps
+            lp = M.loss_soft(M.forward(p, X, bf=False)["logits"], T)
+            flat[idx] = old - eps
+            lm = M.loss_soft(M.forward(p, X, bf=False)["logits"], T)
+            flat[idx] = old
+            fd = (lp - lm) / (2 * eps)
+            assert abs(fd - g[k].ravel()[idx]) < 1e-7 * max(1.0, abs(fd)), (k, idx, fd, g[k].ravel()[idx])
+
+
 def test_spins_to_input_convention():
     bits = np.array([[0b101, 0, 0, 0]], np.uint32)
     x = M.spins_to_input(bits, 4)
