@@ -1,23 +1,27 @@
 """Benchmark of the VMC hot path (one SR epoch per step) on B200.
 
-Workload (default, the config the headline metric is quoted on):
-  Kitaev honeycomb, n_cells=4 (32 spins), J=-1, h=0; symmetric RBM
-  (translations + 180-degree rotation, symmetry 0.5), alpha=4 -> 133
-  parameters; weights complex Gaussian std 1e-4 (seeded synthetic);
-  4096 Metropolis chains x 64 sweeps per epoch (63 warm-up sweeps + 1
-  sampled sweep, one sample per chain -> O is 4096 x 133), bond flips with
-  probability 0.5, persistent chains; FP32 psi-ratio math with an FP64
-  theta recompute after every sweep; SR with S from the 4096 x 133 O matrix,
-  FP64 CG with diagonal shift reg2 = 1e-4, reg1 = (1, 1e-4, 0.9), lr = 1e-2.
+Default workload (the config the headline metric is quoted on): Kitaev
+honeycomb n_cells=8 (128 spins), J=-1, h=0; symmetric RBM (symmetry 0.5),
+alpha=4 -> 517 parameters; 16384 chains, 16 samples per chain one sweep
+apart (persistent chains), single-spin-flip sweeps; SR with CG.
 
-One step = one SR epoch: sweeps -> E_loc -> O_k -> moments/stats -> Gram S
--> regularise -> CG -> weight update, launched as one CUDA graph.
-
-Metric: uncorrelated samples/s = N / (1 + 2 tau) per epoch time, tau the
-reference's binning estimate of the E_loc autocorrelation; SR epochs/s is
-reported beside it.  `--impl reference` times the reference algorithm's CPU
-restatement (the FP64 oracle; the reference itself cannot be built here) on
-all host cores on a bounded sample of the same workload.
+The metric compares forms of the method on the same trained wavefunction:
+a checkpoint is trained first (plain FP32 SR from seeded complex Gaussian
+weights of std 1e-4, 600 epochs of 4096 chains; saved with rbmnqs_save and
+loaded by every form), then each form runs its epochs from it:
+  * learned  -- the headline `value`: mixed precision (FP32 psi ratios,
+    FP64 theta recompute, TF32x3 tensor-core Gram, FP64 CG), the whole epoch
+    as one CUDA graph, one learned move per sample after each sweep (the
+    proposal network trained every epoch);
+  * plain_fp32 -- the same without the learned moves;
+  * plain_fp64 -- plain GPU Metropolis in the reference's arithmetic (FP64
+    throughout), launched stage by stage.
+Uncorrelated samples/s = N / (1 + 2 tau) per epoch time, tau the
+reference's binning estimate of the E_loc autocorrelation along the chains;
+SR epochs/s, E/site and their differences are reported beside it.
+`--impl reference` times the reference algorithm's CPU restatement (the
+FP64 oracle; the reference itself cannot be built here) on all host cores on
+a bounded sample of the same workload.
 
 Multi-GPU: the path does not shard (one GPU, no collective); --gpus N runs N
 independent replicas, one process per GPU under torchrun, timed as the max
@@ -37,9 +41,16 @@ sys.path.insert(0, os.path.join(ROOT, "rbm-nqs_b200"))
 import numpy as np  # noqa: E402
 
 # Workloads (seeded synthetic inputs of the benchmark shapes).  The metric
-# line is quoted on kitaev32_symm_a4; the others measure the Pfaffian path and
-# the 128-spin lattice with the same harness.
+# line is quoted on kitaev128_forms; the others measure the 32-spin lattice,
+# the Pfaffian path and the batched toric problems with the same harness.
 WORKLOADS = {
+    # the metric's config: the 128-spin Kitaev lattice, forms compared on a
+    # trained checkpoint (see the module docstring)
+    "kitaev128_forms": dict(model="kitaev", n_cells=8, rbm_type=1, alpha=4, symmetry=0.5, n_chains=16384,
+                            samples_per_chain=16, warmup=0, step=1, bond_flips=0.0, std=1e-4,
+                            reg2=(1e-4, 1e-4, 1.0), precision=0, gram=0, forms=True,
+                            train=dict(n_chains=4096, warmup=15, bond_flips=0.5, epochs=600),
+                            learned=dict(proposal=1, learned_steps=1, learned_train=2, learned_lr=1e-3)),
     # Kitaev 32 spins, symmetric RBM alpha=4, 4096 chains x 64 sweeps,
     # FP32 sweep / FP64 theta recompute, TF32x3 tensor-core Gram, FP64 CG
     "kitaev32_symm_a4": dict(model="kitaev", n_cells=4, rbm_type=1, alpha=4, symmetry=0.5, n_chains=4096,
@@ -57,16 +68,10 @@ WORKLOADS = {
                               samples_per_chain=1, warmup=63, step=1, bond_flips=0.5, std=1e-4,
                               reg2=(1e-4, 1e-4, 1.0), precision=0, gram=0),
     # the 128-spin lattice as a time series (persistent chains, 16 samples per
-    # chain, 4 sweeps apart) for tau_int of E_loc: plain single-spin / bond
-    # Metropolis against the learned multi-spin proposals at 1 sweep + 1
-    # learned move per sample (network trained on the chains' own samples)
+    # chain, 4 sweeps apart), seeded weights (profiling)
     "kitaev128_plain_ts": dict(model="kitaev", n_cells=8, rbm_type=1, alpha=4, symmetry=0.5, n_chains=16384,
                                samples_per_chain=16, warmup=0, step=4, bond_flips=0.5, std=1e-4,
                                reg2=(1e-4, 1e-4, 1.0), precision=0, gram=0),
-    "kitaev128_learned_ts": dict(model="kitaev", n_cells=8, rbm_type=1, alpha=4, symmetry=0.5, n_chains=16384,
-                                 samples_per_chain=16, warmup=0, step=1, bond_flips=0.5, std=1e-4,
-                                 reg2=(1e-4, 1e-4, 1.0), precision=0, gram=0, proposal=1, learned_steps=1,
-                                 learned_train=2, learned_lr=1e-3),
     # 48 independent toric-code trainings (L = 3..8, 8 each, basic RBM
     # alpha=2, 1024 chains each) advanced by one CUDA-graph launch per epoch;
     # launch shapes autotuned per L; matrix-free CG capped at 100 iterations
@@ -75,9 +80,17 @@ WORKLOADS = {
                           std=1e-4, reg2=(1e-4, 1e-4, 1.0), precision=0, gram=0, max_iterations=100),
 }
 METRIC = "uncorrelated samples/s (SR epoch, E_loc binning tau)"
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 # DRAM bytes per sampler launch from an ncu capture of the same workload: the
 # theta tables, flip tables and chains live in shared memory and registers
 SAMPLER_DRAM_BYTES = {"kitaev32_symm_a4": 136704.0}
+# DRAM bytes per launch of the evaluation kernel: the O store written (N x P
+# FP32 complex); the capture of 32768 samples wrote 78.9 MB (the rest of its
+# 135.5 MB still in L2 when the kernel ended), scaled by 8 to the 262144
+# samples of one launch
+ELOC_DRAM_BYTES = {"kitaev128_forms": 8 * 78.9e6}
+ELOC_TRAFFIC_SOURCE = ("dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of 32768 samples "
+                       "(profiles/eloc_kernel_kitaev128_symm_a4.md), scaled to 262144 samples")
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -87,7 +100,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="kitaev32_symm_a4", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="kitaev128_forms", choices=list(WORKLOADS))
+    ap.add_argument("--train-epochs", type=int, default=0, help="override the checkpoint's training epochs")
     ap.add_argument("--cpu-baseline", type=int, default=1, help="time the CPU restatement beside our arm")
     ap.add_argument("--chains", type=int, default=0, help="override the workload's chain count (profiling)")
     ap.add_argument("--sweeps", type=int, default=0, help="override the sweeps per epoch (profiling)")
@@ -415,6 +429,235 @@ def run_batch(args, rank, world, local):
     return res if rank == 0 else None
 
 
+# ------------------------------------------------------- forms (C5) --
+def forms_config(wl, seed, form):
+    """Session config of one form of the 128-spin workload."""
+    import rbmnqs
+    kw = dict(rbm_type=wl["rbm_type"], alpha=wl["alpha"], n_chains=wl["n_chains"],
+              samples_per_chain=wl["samples_per_chain"], warmup=wl["warmup"], step=wl["step"],
+              bond_flips=wl["bond_flips"], seed=seed, precision=0, gram=0, reinit_chains=0, reg2=wl["reg2"])
+    if form == "learned":
+        kw.update(wl["learned"])
+    elif form == "plain_fp64":
+        kw["precision"] = 1
+    return rbmnqs.default_config(**kw)
+
+
+def train_checkpoint(wl, model, epochs, seed, path):
+    """Plain FP32 SR from seeded std-1e-4 weights; saved as a .rbm file."""
+    import rbmnqs
+    t = wl["train"]
+    cfg = rbmnqs.default_config(rbm_type=wl["rbm_type"], alpha=wl["alpha"], n_chains=t["n_chains"],
+                                samples_per_chain=1, warmup=t["warmup"], step=1, bond_flips=t["bond_flips"],
+                                seed=seed, precision=0, gram=0, reinit_chains=0, reg2=wl["reg2"])
+    s = rbmnqs.Session(model, cfg)
+    s.set_weights(make_weights(s.n_params, wl["std"], 99))
+    t0 = time.perf_counter()
+    es = []
+    for _ in range(epochs):
+        st, _ = s.epoch()
+        es.append(st["energy"].real / model.n)
+    s.save(path)
+    return {"epochs": epochs, "n_chains": t["n_chains"], "sweeps_per_epoch": t["warmup"] + 1,
+            "energy_per_site_last50": float(np.mean(es[-50:])), "seconds": time.perf_counter() - t0}
+
+
+def time_form(sess, graph, steps, warmup, l2_flush, stream, clk=None):
+    """Warm-up epochs, then `steps` epochs timed with CUDA events on the
+    session's stream (L2 flushed between epochs, outside the events)."""
+    import torch
+    for _ in range(max(1, warmup)):
+        sess.epoch() if graph else (sess.sample(), sess.optimize())
+    sess.timing_reset(True)
+    if graph:
+        sess.epoch()  # re-capture with the stage-timing event nodes; not timed
+        sess.timing_reset(True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    stats = []
+    torch.cuda.synchronize()
+    ctx = clk if clk is not None else _Null()
+    with ctx:
+        for k in range(steps):
+            l2_flush()
+            ev[k][0].record(stream)
+            if graph:
+                st, sr = sess.epoch()
+            else:
+                st = sess.sample()
+                sr = sess.optimize()
+            ev[k][1].record(stream)
+            stats.append((st, sr))
+        torch.cuda.synchronize()
+    t_ms = [a.elapsed_time(b) for a, b in ev]
+    ms, cnt = sess.timing()
+    return t_ms, stats, [float(m / max(1, c)) for m, c in zip(ms, cnt)]
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        pass
+
+
+def form_summary(N, n, t_ms, stats, stage_ms):
+    taus = [st["tau"] for st, _ in stats]
+    es = [st["energy"].real / n for st, _ in stats]
+    errs = [st["stddev"] / n for st, _ in stats]
+    tau = float(np.mean(taus))
+    t = float(np.sum(t_ms)) * 1e-3
+    neff = len(stats) * N / (1.0 + 2.0 * tau)
+    d = {"uncorrelated_samples_per_s": neff / t, "ms_per_epoch": 1e3 * t / len(stats),
+         "sr_epochs_per_s": len(stats) / t, "tau": tau, "energy_per_site": float(np.mean(es)),
+         "energy_per_site_stderr": float(np.sqrt(np.sum(np.square(errs)))) / len(errs),
+         "acceptance": float(np.mean([st["acceptance"] for st, _ in stats])),
+         "cg_iterations": float(np.mean([sr["iterations"] for _, sr in stats])),
+         "epochs_timed": len(stats),
+         "stage_ms_per_epoch": {nm: stage_ms[i] for i, nm in enumerate(
+             ["sampler", "eval", "moments+stats", "gram+regularise", "cg", "update"])}}
+    if any(st["learned_acceptance"] for st, _ in stats):
+        d["learned_acceptance"] = float(np.mean([st["learned_acceptance"] for st, _ in stats]))
+    return d
+
+
+def run_forms(args, rank, world, local):
+    import tempfile
+
+    import torch
+    import rbmnqs
+
+    dist = init_dist(world, "nccl")
+    torch.cuda.set_device(local)
+    wl = workload(args)
+    model = rbmnqs.Model.kitaev(wl["n_cells"], symmetry=wl["symmetry"])
+    n = model.n
+    tmp = tempfile.mkdtemp(prefix="rbmnqs_bench_")
+    ckpt = os.path.join(tmp, "kitaev128_trained.rbm")
+    train = train_checkpoint(wl, model, args.train_epochs or wl["train"]["epochs"], 77 + rank, ckpt)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def session(form):
+        s = rbmnqs.Session(model, forms_config(wl, 1234 + rank, form))
+        s.load(ckpt)
+        return s
+
+    out = {}
+    # learned form: the headline number, clocks sampled in its timed region
+    learned = session("learned")
+    lstream = torch.cuda.ExternalStream(learned.stream())
+
+    def flush_on(stream):
+        def f():
+            with torch.cuda.stream(stream):
+                flush.zero_()
+        return f
+
+    if world > 1:
+        dist.barrier()
+    clk = ClockSampler(local)
+    t_ms, stats, stage = time_form(learned, True, args.steps, args.warmup, flush_on(lstream), lstream, clk)
+    clocks = clk.summary()
+    t_learned_ms = float(np.sum(t_ms))
+    out["learned"] = form_summary(learned.N, n, t_ms, stats, stage)
+    kern_per_epoch = learned.graph_kernels()
+    # end to end through the C ABI with host buffers: weights in, epoch,
+    # weights and statistics out, every step
+    w = learned.get_weights()
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    taus2 = []
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush_on(lstream)()
+        ev2[k][0].record(lstream)
+        learned.set_weights(w)
+        st, _ = learned.epoch()
+        w = learned.get_weights()
+        ev2[k][1].record(lstream)
+        taus2.append(st["tau"])
+    torch.cuda.synchronize()
+    t2_ms = sum(a.elapsed_time(b) for a, b in ev2)
+    mufu = rbmnqs.probe_mufu() if rank == 0 else 0.0
+    T = learned.n_hidden * learned.n_symm
+    P = learned.n_params
+    del learned
+    # plain forms
+    p32 = session("plain_fp32")
+    s32 = torch.cuda.ExternalStream(p32.stream())
+    t_ms, stats, stage = time_form(p32, True, args.steps, args.warmup, flush_on(s32), s32)
+    out["plain_fp32"] = form_summary(p32.N, n, t_ms, stats, stage)
+    del p32
+    p64 = session("plain_fp64")
+    s64 = torch.cuda.ExternalStream(p64.stream())
+    steps64 = max(2, min(args.steps, 3))
+    t_ms, stats, stage = time_form(p64, False, steps64, 1, flush_on(s64), s64)
+    out["plain_fp64"] = form_summary(p64.N, n, t_ms, stats, stage)
+    del p64
+
+    if world > 1:
+        t = torch.tensor([t_learned_ms, t2_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_learned_ms, t2_ms = t.tolist()
+    if rank != 0:
+        return None
+    L = out["learned"]
+    N = wl["n_chains"] * wl["samples_per_chain"]
+    value = world * args.steps * N / (1.0 + 2.0 * L["tau"]) / (t_learned_ms * 1e-3)
+    e2e = world * args.steps * N / (1.0 + 2.0 * float(np.mean(taus2))) / (t2_ms * 1e-3)
+    # roofline of the dominant kernel (the E_loc / O_k evaluation): every
+    # off-diagonal term (the x and y bonds, n / 2 each) evaluates ln cosh of
+    # all T theta entries of theta', each one ex2, one sin and one cos (the
+    # per-four lg2 and rsqrt not counted)
+    terms = n
+    ops = float(N) * terms * T * 3.0
+    eval_ms = L["stage_ms_per_epoch"]["eval"]
+    achieved = ops / (eval_ms * 1e-3)
+    sweep_ms = L["stage_ms_per_epoch"]["sampler"]
+    dE = L["energy_per_site"] - out["plain_fp32"]["energy_per_site"]
+    dE_err = float(np.hypot(L["energy_per_site_stderr"], out["plain_fp32"]["energy_per_site_stderr"]))
+    res = {
+        "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_learned_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 psi ratios / fp64 theta+CG / tf32x3 Gram",
+        "data": "synthetic (checkpoint trained here from seeded complex Gaussian weights std 1e-4, Philox chains)",
+        "config": {"workload": args.workload, "model": f"kitaev honeycomb n_cells={wl['n_cells']} ({n} spins) J=-1",
+                   "machine": f"symmetric RBM alpha={wl['alpha']}, {P} params",
+                   "n_chains": wl["n_chains"], "samples_per_chain": wl["samples_per_chain"],
+                   "sweeps_between_samples": wl["step"], "proposals": "single-spin flips",
+                   "learned": "1 learned move per sample (dictionary of 128 sites + 128 x/y bonds, MLP "
+                              "128-256-256-256 BF16), 2 Adam steps per epoch",
+                   "sr": "CG reg2=1e-4 reg1=(1,1e-4,0.9) lr=1e-2", "checkpoint": train,
+                   "parallelism": f"replicas x{world}",
+                   "l2": "256 MiB L2 flush between timed epochs (outside the event pairs)"},
+        "sr_epochs_per_s": world * args.steps / (t_learned_ms * 1e-3),
+        "tau": L["tau"], "energy_per_site": L["energy_per_site"],
+        "energy_per_site_stderr": L["energy_per_site_stderr"],
+        "forms": out,
+        "vs_plain_fp64": value / (world * out["plain_fp64"]["uncorrelated_samples_per_s"]),
+        "vs_plain_fp32": value / (world * out["plain_fp32"]["uncorrelated_samples_per_s"]),
+        "sr_epochs_vs_plain_fp64": L["sr_epochs_per_s"] / out["plain_fp64"]["sr_epochs_per_s"],
+        "delta_energy_per_site_learned_vs_plain_fp32": {"value": dE, "stderr": dE_err},
+        "delta_energy_per_site_learned_vs_plain_fp64": {
+            "value": L["energy_per_site"] - out["plain_fp64"]["energy_per_site"],
+            "stderr": float(np.hypot(L["energy_per_site_stderr"], out["plain_fp64"]["energy_per_site_stderr"]))},
+        "roofline": {"bound": "mufu", "kernel": "eloc_kernel", "achieved": achieved / 1e9, "peak": mufu / 1e9,
+                     "unit": "Gop/s (MUFU)", "frac": achieved / mufu,
+                     "peak_source": "measured in this run by rbmnqs_probe_mufu (no MUFU figure in "
+                                    "MEASURED_PEAKS.json)",
+                     "algorithmic_ops_per_launch": ops,
+                     "ops_per_unit": "3 MUFU (ex2, sin, cos) per theta entry per off-diagonal term per sample: "
+                                     f"{N} samples x {terms} terms x {T} entries",
+                     "traffic": ELOC_DRAM_BYTES.get(args.workload),
+                     "traffic_source": ELOC_TRAFFIC_SOURCE,
+                     "sweep_kernel": {"ms_per_epoch": sweep_ms}},
+        "e2e": {"value": e2e, "unit": "samples/s", "h2d_bytes_per_step": P * 16,
+                "d2h_bytes_per_step": P * 16 + 96},
+        "gpu_launches": kern_per_epoch * args.steps,
+        "clocks": clocks,
+    }
+    return res
+
+
 # ------------------------------------------------------------ CPU arm --
 def cpu_epoch(wl, chains, seed, threads):
     """One bounded epoch of the workload on the FP64 CPU restatement:
@@ -438,6 +681,27 @@ def cpu_epoch(wl, chains, seed, threads):
     return dt, O.stats(E)["tau"], len(E)
 
 
+def cpu_forms_epoch(wl, chains, seed, threads):
+    """One bounded epoch of the 128-spin workload on the FP64 CPU
+    restatement, the reference's sampler structure: `chains` fresh chains,
+    warm-up sweeps, samples_per_chain samples one sweep apart, then the
+    matrix-free CG on their samples; seeded weights of std 1e-4 (the
+    configuration's initial weights).  Returns (seconds, tau, samples)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    om = O.Model.kitaev(wl["n_cells"])
+    mach = O.Machine(om, "symmetry", wl["alpha"], symm=wl["symmetry"])
+    mach.set_params(make_weights(mach.n_params, wl["std"], 99))
+    t0 = time.perf_counter()
+    E, Om, acc, _ = O.metropolis(mach, om, chains, wl["samples_per_chain"], warmup=wl["train"]["warmup"],
+                                 step=wl["step"], bond_flips=wl["bond_flips"], seed=seed, threads=threads)
+    d, F, diag = O.sr_moments(Om, E)
+    O.cg_solve(Om, d, F, np.zeros(mach.n_params), 0.9, wl["reg2"][0], 1e-2, diag)
+    dt = time.perf_counter() - t0
+    return dt, O.stats(E)["tau"], len(E)
+
+
 def cpu_arm(wl, steps, warmup, chains=256):
     threads = os.cpu_count() or 1
     times = []
@@ -456,6 +720,32 @@ def main():
     args = parse()
     rank, world, local = dist_env()
     wl = workload(args)
+    if args.impl == "reference" and wl.get("forms"):
+        if rank != 0:
+            return
+        threads = os.cpu_count() or 1
+        chains = 64
+        ts, taus, n = [], [], 0
+        for k in range(args.warmup + args.steps):
+            dt, tau, n = cpu_forms_epoch(wl, chains, 1234 + k, threads)
+            if k >= args.warmup:
+                ts.append(dt)
+                taus.append(tau)
+        t = float(np.mean(ts))
+        v = n / (1.0 + 2.0 * float(np.mean(taus))) / t
+        line = {"metric": METRIC, "value": v, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "fp64", "data": "synthetic", "impl": "reference",
+                "tau": float(np.mean(taus)),
+                "config": {"workload": args.workload, "parallelism": "host cores",
+                           "sample": f"{chains} of {wl['n_chains']} chains x ({wl['train']['warmup']} warm-up + "
+                                     f"{wl['samples_per_chain']}) sweeps, one sample per sweep, + CG on their "
+                                     f"samples, per step; weights std 1e-4"},
+                "cpu_baseline": {"value": v, "unit": "samples/s", "cores": threads, "kind": "port",
+                                 "sample": f"{n} samples of {chains} chains per step"},
+                "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
     if args.impl == "reference":
         if rank != 0:
             return
@@ -476,6 +766,22 @@ def main():
         res = run_batch(args, rank, world, local)
         if rank == 0:
             print(json.dumps(res))
+        return
+    if wl.get("forms"):
+        res = run_forms(args, rank, world, local)
+        if rank == 0:
+            if args.cpu_baseline and world == 1:
+                threads = os.cpu_count() or 1
+                dt, tau, n = cpu_forms_epoch(wl, 128, 4321, threads)
+                res["cpu_baseline"] = {"value": n / (1.0 + 2.0 * tau) / dt, "unit": "samples/s", "cores": threads,
+                                       "kind": "port",
+                                       "sample": f"128 of {wl['n_chains']} chains x ({wl['train']['warmup']} "
+                                                 f"warm-up + {wl['samples_per_chain']}) sweeps + CG on their "
+                                                 f"{n} samples ({dt:.1f} s), weights std 1e-4, tau {tau:.3f}"}
+            print(json.dumps(res))
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     res = run_ours(args, rank, world, local)
     if rank == 0:
