@@ -14,6 +14,8 @@
 // fixed order, so results are deterministic.
 #include <cooperative_groups.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "coop.cuh"
 #include "sr.cuh"
@@ -463,6 +465,118 @@ __global__ void max_parts_kernel(const double* maxpart, int n, double* out) {
 
 template <typename TO> const void* cg_fn() { return reinterpret_cast<const void*>(cg_mfree_kernel<TO>); }
 
+// CG (cg1 semantics, cg_solver.cpp:260-334) on a formed regularised S with
+// one grid barrier per iteration.  Every block keeps full copies of p, r and
+// x in shared memory and updates them itself, with the same sums in the same
+// order as every other block, so alpha and beta agree bit for bit across the
+// grid; the only data exchanged through global memory is A p, one row per
+// warp, written to one of two buffers by iteration parity (a block one
+// iteration ahead writes the other buffer while slower blocks still read).
+__global__ void __launch_bounds__(kThreads) cg_dense1_kernel(const double2* __restrict__ S,
+                                                             const double2* __restrict__ F, double2* x, int P,
+                                                             int max_it, double rtol, MfreeWork w, CgResultDev* res) {
+    extern __shared__ double2 sv[];
+    double2 *p = sv, *r = sv + P, *xs = sv + 2 * P;
+    __shared__ double redd[kThreads / 32];
+    __shared__ double2 redz[kThreads / 32];
+    const int tid = threadIdx.x, lane = tid & 31, G = gridDim.x, blk = blockIdx.x;
+    const int gw = blk * (kThreads / 32) + (tid >> 5), nwarps = G * (kThreads / 32);
+    if (blk == 0 && tid == 0) res->status = 0;
+    // rows of S times a shared-memory vector into a global buffer
+    auto matvec = [&](const double2* v, double2* out) {
+        for (int row = gw; row < P; row += nwarps) {
+            const double2* Sr = S + (size_t)row * P;
+            double ax = 0, ay = 0;
+            int q = lane;
+            for (; q + 96 < P; q += 128) {
+                double2 a[4], b[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    a[u] = __ldg(Sr + q + 32 * u);
+                    b[u] = v[q + 32 * u];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    ax = fma(a[u].x, b[u].x, fma(-a[u].y, b[u].y, ax));
+                    ay = fma(a[u].x, b[u].y, fma(a[u].y, b[u].x, ay));
+                }
+            }
+            for (; q < P; q += 32) {
+                const double2 a = __ldg(Sr + q), b = v[q];
+                ax = fma(a.x, b.x, fma(-a.y, b.y, ax));
+                ay = fma(a.x, b.y, fma(a.y, b.x, ay));
+            }
+            ax = warp_sum(ax);
+            ay = warp_sum(ay);
+            if (lane == 0) out[row] = make_double2(ax, ay);
+        }
+    };
+    for (int q = tid; q < P; q += kThreads) xs[q] = x[q];
+    __syncthreads();
+    matvec(xs, w.Ap);
+    bool ok = grid_barrier(w.sync, G);
+    double rs = 0.0;
+    int itn = 0;
+    if (ok) {
+        // r = F - A x0, p = r
+        double rl = 0;
+        for (int q = tid; q < P; q += kThreads) {
+            const double2 aq = cg_ld(w.Ap + q);
+            const double2 rq = make_double2(F[q].x - aq.x, F[q].y - aq.y);
+            r[q] = rq;
+            p[q] = rq;
+            rl += rq.x * rq.x + rq.y * rq.y;
+        }
+        double rsold = bsum(rl, redd);
+        rs = rsold;
+        for (itn = 0; itn < max_it; itn++) {
+            double2* ab = (itn & 1) ? w.Ap : w.R1;  // A x0 went to w.Ap
+            matvec(p, ab);
+            if (!(ok = grid_barrier(w.sync, G))) break;
+            // alpha = rsold / (p^H A p)
+            double2 pp = make_double2(0, 0);
+            for (int q = tid; q < P; q += kThreads) {
+                const double2 aq = cg_ld(ab + q), pq = p[q];
+                pp.x += pq.x * aq.x + pq.y * aq.y;
+                pp.y += pq.x * aq.y - pq.y * aq.x;
+            }
+            const double2 pap = bsum(pp, redz);
+            const double den = pap.x * pap.x + pap.y * pap.y;
+            const double ax = rsold * pap.x / den, ay = -rsold * pap.y / den;
+            double rl2 = 0;
+            for (int q = tid; q < P; q += kThreads) {
+                const double2 pq = p[q], aq = cg_ld(ab + q);
+                double2 xq = xs[q], rq = r[q];
+                xq.x += ax * pq.x - ay * pq.y;
+                xq.y += ax * pq.y + ay * pq.x;
+                rq.x -= ax * aq.x - ay * aq.y;
+                rq.y -= ax * aq.y + ay * aq.x;
+                xs[q] = xq;
+                r[q] = rq;
+                rl2 += rq.x * rq.x + rq.y * rq.y;
+            }
+            rs = bsum(rl2, redd);
+            if (rs < rtol) break;
+            const double beta = rs / rsold;
+            for (int q = tid; q < P; q += kThreads) {
+                const double2 rq = r[q], pq = p[q];
+                p[q] = make_double2(rq.x + beta * pq.x, rq.y + beta * pq.y);
+            }
+            rsold = rs;
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    if (blk == 0) {
+        for (int q = tid; q < P; q += kThreads) x[q] = xs[q];
+        if (tid == 0) {
+            res->iterations = itn;
+            res->residual = rs;
+            if (!ok) res->status = -2;
+        }
+    }
+}
+
 }  // namespace
 
 cudaError_t mfree_plan(int N, int P, MfreePlan* pl) {
@@ -532,6 +646,28 @@ cudaError_t launch_cg_dense_coop(const double2* A, const double2* b, double2* x,
                                  const MfreePlan& pl, const MfreeWork& w, CgResultDev* res, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(w.sync, 0, sizeof(MfreeSync), st);
     if (e != cudaSuccess) return e;
+    if (!w.minres) {
+        // CG: the one-barrier kernel, p, r and x of every block in shared memory
+        const int smem = 3 * P * (int)sizeof(double2);
+        const void* fn = reinterpret_cast<const void*>(cg_dense1_kernel);
+        if ((e = ensure_dynamic_smem(fn, smem)) != cudaSuccess) return e;
+        int dev = 0, sms = 148, per_sm = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_dense1_kernel, kThreads, smem)) !=
+            cudaSuccess)
+            return e;
+        if (per_sm < 1) return cudaErrorInvalidConfiguration;
+        int blocks = std::min(sms * per_sm, (P + kThreads / 32 - 1) / (kThreads / 32));
+        blocks = std::max(1, blocks);
+        MfreeWork wk = w;
+        const double2* S = A;
+        const double2* F = b;
+        double2* xo = x;
+        CgResultDev* r = res;
+        void* args[] = {&S, &F, &xo, &P, &max_it, &rtol, &wk, &r};
+        return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(kThreads), args, smem, st);
+    }
     MfreeWork wk = w;
     wk.S = A;
     const double2* O = nullptr;

@@ -1642,26 +1642,33 @@ template <int E> struct LaneEnt {
 template <int E>
 __device__ __forceinline__ void learned_theta(const MachineDev& m, const LearnTabs& L, const LaneEnt<E>& le,
                                               const uint32_t (&sp)[4], int lane, float2 (&th)[E]) {
+    // one pass over the down spins, every entry of the lane per spin
+    double2 acc[E];
+    int ro[E];  // row offset of the lane's entries in the symmetry table
 #pragma unroll
     for (int e = 0; e < E; e++) {
-        const int t = lane + 32 * e;
-        double2 acc = le.k[e] >= 0 ? L.base[t] : make_double2(0, 0);
-        if (le.k[e] >= 0) {
-            const int k = le.k[e], sy = le.s[e];
+        acc[e] = le.k[e] >= 0 ? L.base[lane + 32 * e] : make_double2(0, 0);
+        ro[e] = m.symmetric ? le.s[e] : 0;
+    }
 #pragma unroll
-            for (int wd = 0; wd < 4; wd++) {
-                uint32_t bits = sp[wd];
-                while (bits) {
-                    const int f = 32 * wd + __ffs(bits) - 1;
-                    bits &= bits - 1;
-                    const double2 w = L.W64[(m.symmetric ? (int)L.perm[f * m.S + sy] : f) * m.nh + k];
-                    acc.x = fma(-2.0, w.x, acc.x);
-                    acc.y = fma(-2.0, w.y, acc.y);
-                }
+    for (int wd = 0; wd < 4; wd++) {
+        uint32_t bits = sp[wd];
+        while (bits) {
+            const int f = 32 * wd + __ffs(bits) - 1;
+            bits &= bits - 1;
+            const int fS = f * m.S;
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+                if (le.k[e] < 0) continue;
+                const int row = m.symmetric ? (int)L.perm[fS + ro[e]] : f;
+                const double2 w = L.W64[row * m.nh + le.k[e]];
+                acc[e].x = fma(-2.0, w.x, acc[e].x);
+                acc[e].y = fma(-2.0, w.y, acc[e].y);
             }
         }
-        th[e] = make_float2((float)acc.x, (float)acc.y);
     }
+#pragma unroll
+    for (int e = 0; e < E; e++) th[e] = make_float2((float)acc[e].x, (float)acc[e].y);
 }
 
 // Re log psi(s with the move's flips)/psi(s): lane partial of the ln|cosh|
