@@ -360,6 +360,22 @@ void rbmnqs_batch_destroy(rbmnqs_batch* b);
  * counterpart in the reference (measurement helper). */
 int rbmnqs_probe_mufu(int32_t iters, double* ops_per_second);
 
+/* Test hook for failure detection (no reference counterpart; the
+ * reference's failure handling is the max|dw| guard and exceptions,
+ * abstract_optimizer.cpp:157-159, main.cpp:610-615).  Process-wide:
+ *   0  off;
+ *   1  the grid barriers of the cooperative solvers (matrix-free CG, the
+ *      formed-S cooperative CG and MINRES, the direct solver) wait for one
+ *      arrival more than the grid makes and give up after a short bounded
+ *      wait: the solve reports status RBMNQS_ERR_CUDA (rbmnqs_sr_stats) and
+ *      leaves the weights unchanged;
+ *   2  the proposal network's GEMM issues no copies and its bounded wait for
+ *      them runs out: calls that run the network fail with RBMNQS_ERR_CUDA.
+ * No copy is in flight when a wait gives up and no GPU fault is raised; the
+ * context stays usable once the hook is off again.  Captured epoch graphs
+ * keep the setting they were captured with. */
+int rbmnqs_test_fault(int32_t kind);
+
 /* ------------------------------------------ allocation-free SR solve ---- */
 /* No counterpart in the reference.  The same solve as rbmnqs_sr_solve for
  * callers that cannot allocate device memory: code inside a runtime that

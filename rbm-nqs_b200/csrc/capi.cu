@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstddef>
 #include <cstdio>
@@ -214,6 +215,11 @@ std::vector<uint8_t> eval_row_order(const std::vector<std::vector<int>>& perm, i
 
 void rbmnqs::set_last_error(const std::string& msg) { g_err = msg; }
 
+namespace {
+std::atomic<int> g_test_fault{0};
+}
+int rbmnqs::test_fault() { return g_test_fault.load(std::memory_order_relaxed); }
+
 // Device copy of a TermHost and its view for the evaluation kernel.
 struct TermBufs {
     DevBuf<rbmnqs::TermDev> terms, diag;
@@ -356,6 +362,7 @@ struct rbmnqs_handle {
         int gerr;
         double lrate;
         float lloss;
+        int nerr;  // proposal network pipeline error flag
     };
     Readback* rb = nullptr;
     ~rbmnqs_handle() {
@@ -1322,7 +1329,14 @@ static void readback(rbmnqs_handle* h, bool sample, rbmnqs_sample_stats* out, bo
         ck(cudaMemcpyAsync(&rb->sched, h->sched.p, sizeof(rb->sched), cudaMemcpyDeviceToHost, h->st), "copy");
         if (h->gram_tc) ck(cudaMemcpyAsync(&rb->gerr, h->gerr.p, sizeof(int), cudaMemcpyDeviceToHost, h->st), "copy");
     }
+    rb->nerr = 0;
+    if (h->net) ck(cudaMemcpyAsync(&rb->nerr, h->net->error_flag(), sizeof(int), cudaMemcpyDeviceToHost, h->st), "copy");
     ck(cudaStreamSynchronize(h->st), "sync");
+    if (rb->nerr) {
+        const int ne = rb->nerr;
+        ck(h->net->clear_error(h->st), "memset");
+        throw Fail{RBMNQS_ERR_CUDA, "proposal network GEMM: pipeline wait timed out (code " + std::to_string(ne) + ")"};
+    }
     if (sample && out) {
         const auto& s = rb->stats;
         out->energy[0] = s.energy.x;
@@ -1775,6 +1789,13 @@ int rbmnqs_graph_kernels(rbmnqs_handle* h, int32_t* kernel_nodes) {
     });
 }
 
+int rbmnqs_test_fault(int32_t kind) {
+    return guard([&] {
+        require(kind >= 0 && kind <= 2, "rbmnqs_test_fault: kind must be 0, 1 or 2");
+        g_test_fault.store(kind);
+    });
+}
+
 int rbmnqs_probe_mufu(int32_t iters, double* ops_per_second) {
     return guard([&] {
         require(ops_per_second && iters > 0, "bad arguments");
@@ -2033,7 +2054,11 @@ void mlp_upload(rbmnqs_mlp* m, const uint32_t* spins, const uint32_t* targets, i
 void mlp_check(rbmnqs_mlp* m) {
     ck(cudaStreamSynchronize(m->st), "sync");
     const int e = m->net->error_flag_host();
-    if (e) throw Fail{RBMNQS_ERR_CUDA, "proposal network GEMM: pipeline wait timed out (code " + std::to_string(e) + ")"};
+    if (e) {
+        ck(m->net->clear_error(m->st), "memset");
+        ck(cudaStreamSynchronize(m->st), "sync");
+        throw Fail{RBMNQS_ERR_CUDA, "proposal network GEMM: pipeline wait timed out (code " + std::to_string(e) + ")"};
+    }
 }
 }  // namespace
 

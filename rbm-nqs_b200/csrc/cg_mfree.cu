@@ -579,6 +579,20 @@ __global__ void __launch_bounds__(kThreads) cg_dense1_kernel(const double2* __re
 
 }  // namespace
 
+__global__ void init_sync_kernel(MfreeSync* sync, uint32_t extra, uint32_t cap) {
+    sync->count = 0;
+    sync->gen = 0;
+    sync->bad = 0;
+    sync->extra = extra;
+    sync->spin_cap = cap;
+}
+
+cudaError_t launch_init_sync(MfreeSync* sync, cudaStream_t st) {
+    const bool stall = test_fault() == 1;
+    init_sync_kernel<<<1, 1, 0, st>>>(sync, stall ? 1u : 0u, stall ? 1024u : 0u);
+    return cudaGetLastError();
+}
+
 cudaError_t mfree_plan(int N, int P, MfreePlan* pl) {
     int dev = 0, sms = 148, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -644,7 +658,7 @@ cudaError_t launch_max_diag(const double* diag, int P, double* max_diag, cudaStr
 
 cudaError_t launch_cg_dense_coop(const double2* A, const double2* b, double2* x, int P, int max_it, double rtol,
                                  const MfreePlan& pl, const MfreeWork& w, CgResultDev* res, cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(w.sync, 0, sizeof(MfreeSync), st);
+    cudaError_t e = launch_init_sync(w.sync, st);
     if (e != cudaSuccess) return e;
     if (!w.minres) {
         // CG: the one-barrier kernel, p, r and x of every block in shared memory
@@ -701,7 +715,7 @@ cudaError_t launch_cg_mfree(const void* O, int fp64, const double2* d, double no
                             const ScheduleDev* sch, double r1, double r2, double rd, int max_it, double rtol,
                             const MfreePlan& pl, const MfreeWork& w, CgResultDev* res, cudaStream_t st) {
     // barrier state: count 0, no failure
-    cudaError_t e = cudaMemsetAsync(w.sync, 0, sizeof(MfreeSync), st);
+    cudaError_t e = launch_init_sync(w.sync, st);
     if (e != cudaSuccess) return e;
     MfreeWork wk = w;
     CgResultDev* r = res;

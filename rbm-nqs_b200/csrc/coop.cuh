@@ -23,15 +23,17 @@ static __device__ bool grid_barrier(MfreeSync* sync, uint32_t nblocks) {
         volatile uint32_t* gen = &sync->gen;
         volatile int* bad = &sync->bad;
         const uint32_t g = *gen;
+        const uint32_t need = nblocks + sync->extra;
+        const uint32_t cap = sync->spin_cap ? sync->spin_cap : kBarrierSpin;
         __threadfence();
-        if (atomicAdd(&sync->count, 1u) == nblocks - 1) {
+        if (atomicAdd(&sync->count, 1u) == need - 1) {
             sync->count = 0;
             __threadfence();
             atomicAdd(&sync->gen, 1u);
         } else {
             uint32_t spins = 0;
             while (*gen == g) {
-                if (++spins > kBarrierSpin || *bad) {
+                if (++spins > cap || *bad) {
                     ok = 0;
                     atomicExch(&sync->bad, 1);
                     break;

@@ -235,7 +235,7 @@ cudaError_t launch_direct_solve(double2* Sreg, const double2* F, double2* x, int
     const int nb = (P + kTile - 1) / kTile;
     const int tiles = (nb - 1) * nb / 2;
     const int blocks = std::max(1, std::min(tiles, std::min(per_sm, 2) * sms));
-    e = cudaMemsetAsync(sync, 0, sizeof(MfreeSync), st);
+    e = launch_init_sync(sync, st);
     if (e != cudaSuccess) return e;
     void* args[] = {&Sreg, &P, (void*)&F, &x, &work, &sync, &res};
     return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(cholesky_solve_kernel), dim3(blocks),

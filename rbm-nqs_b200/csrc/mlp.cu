@@ -19,6 +19,7 @@
 
 #include "common.cuh"
 #include "mlp.cuh"
+#include "sr.cuh"
 #include "tc_common.cuh"
 
 namespace rbmnqs {
@@ -35,6 +36,7 @@ enum EpiMode : int { kStoreF32 = 0, kBiasGelu = 1, kBiasF32 = 2, kGeluBwd = 3 };
 
 struct Epi {
     int mode;
+    int stall;             // test fault 2: the copies are not issued, the bounded wait runs out
     float* f32;            // kStoreF32: [nsplit][Mtot][ld]; kBiasGelu: Z; kBiasF32: logits
     __nv_bfloat16* bf;     // kBiasGelu: activation; kGeluBwd: gradient
     const float* bias;     // kBiasGelu, kBiasF32
@@ -96,12 +98,16 @@ __global__ void __launch_bounds__(128, 1)
 
     if (tid == 0) {
         const uint32_t fb = smem_u32(&full_bar);
-        mbar_expect_tx(fb, (uint32_t)nchunks * (kRows * 128 + N * 128));
-        for (int c = 0; c < nchunks; c++) {
-            tma_load_2d(a_base + c * (kRows * 128), &mapA, fb, k0 + c * kChunk, m0);
-            tma_load_2d(b_base + c * (N * 128), &mapB, fb, k0 + c * kChunk, 0);
+        if (!epi.stall) {
+            mbar_expect_tx(fb, (uint32_t)nchunks * (kRows * 128 + N * 128));
+            for (int c = 0; c < nchunks; c++) {
+                tma_load_2d(a_base + c * (kRows * 128), &mapA, fb, k0 + c * kChunk, m0);
+                tma_load_2d(b_base + c * (N * 128), &mapB, fb, k0 + c * kChunk, 0);
+            }
         }
-        if (mbar_wait(fb, 0)) {
+        // under the test fault no copy is in flight and nothing arrives:
+        // the wait gives up after a short limit
+        if (epi.stall ? mbar_wait_n(fb, 0, 4096u) : mbar_wait(fb, 0)) {
             asm volatile("tcgen05.fence::after_thread_sync;");
             const uint32_t id = idesc_bf16(N);
             for (int c = 0; c < nchunks; c++)
@@ -115,7 +121,7 @@ __global__ void __launch_bounds__(128, 1)
         } else {
             ok_load = 0;
             atomicExch(err, 1);
-            (void)mbar_wait(fb, 0);  // drain the copies (bounded)
+            if (!epi.stall) (void)mbar_wait(fb, 0);  // drain the copies (bounded)
         }
     }
     __syncthreads();
@@ -347,8 +353,10 @@ int grid_for(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8);
 }  // namespace
 
 // ---------------------------------------------------------------------------
-static cudaError_t gemm(const void* mapA, const void* mapB, int M, int N, int K, int nsplit, const Epi& e, int* err,
+static cudaError_t gemm(const void* mapA, const void* mapB, int M, int N, int K, int nsplit, const Epi& e0, int* err,
                         cudaStream_t st) {
+    Epi e = e0;
+    e.stall = test_fault() == 2 ? 1 : 0;
     // M multiple of 128, N multiple of 16 (<= 256), K = nsplit * nchunks * 64
     const int nchunks = K / (kChunk * nsplit);
     if (M % kRows || N % 16 || N > kMaxN || nchunks < 1 || nchunks > kMaxChunks || nchunks * kChunk * nsplit != K)

@@ -51,6 +51,9 @@ class Mlp {
     // intermediate tensors for tests: which = 0 a1, 1 a2, 2 z1, 3 z2, 4 g1, 5 g2, 6 g3 (rows x cols as float)
     cudaError_t intermediate(int which, int B, float* host, int* cols);
     int error_flag_host();
+    // device address of the pipeline error flag, and its reset
+    const int* error_flag() const { return err_; }
+    cudaError_t clear_error(cudaStream_t st) { return cudaMemsetAsync(err_, 0, sizeof(int), st); }
 
    private:
     MlpDims d_;

@@ -769,6 +769,10 @@ __global__ void sr_update(double2* params, double2* x, int P, const ScheduleDev*
         res->max_dw = mx;
         res->status = status;
     }
+    // a non-finite direction is no warm start for the next solve (the
+    // reference stops the run here, main.cpp:610-615)
+    if (status == -5)
+        for (int i = threadIdx.x; i < P; i += blockDim.x) x[i] = make_double2(0.0, 0.0);
     if (status != 0) return;
     const double lr = sch->value[0];
     const int type = plug ? plug->type : 0;

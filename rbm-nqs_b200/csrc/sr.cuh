@@ -93,7 +93,16 @@ cudaError_t launch_update(double2* params, double2* x, int P, const ScheduleDev*
 struct MfreeSync {
     uint32_t count, gen;
     int bad;
+    uint32_t extra;     // arrivals beyond the grid's blocks a barrier waits for (0; 1 under test fault 1)
+    uint32_t spin_cap;  // polls before a waiting block gives up (0: kBarrierSpin)
 };
+// Barrier state for a cooperative launch: zero, or under test fault 1 an
+// extra arrival that never comes and a short wait limit.
+cudaError_t launch_init_sync(MfreeSync* sync, cudaStream_t st);
+// Process-wide test hook (rbmnqs_test_fault): 0 none, 1 cooperative-solve
+// barriers never complete, 2 the proposal network's GEMM copies are never
+// issued; the bounded waits then run out and the calls report an error.
+int test_fault();
 // Direct solve (direct.cu, direct_solver.cpp:31-59) of the regularised
 // Hermitian positive definite Sreg (P x P, overwritten by its Cholesky
 // factor): x = Sreg^-1 F.  work: P entries; sync: barrier state.

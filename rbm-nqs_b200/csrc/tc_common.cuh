@@ -44,6 +44,12 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
         if (mbar_try(bar, phase)) return true;
     return false;
 }
+// The same with a given limit on the polls.
+__device__ __forceinline__ bool mbar_wait_n(uint32_t bar, uint32_t phase, uint32_t polls) {
+    for (uint32_t i = 0; i < polls; i++)
+        if (mbar_try(bar, phase)) return true;
+    return false;
+}
 
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y) {
     asm volatile(

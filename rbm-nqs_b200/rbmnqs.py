@@ -143,6 +143,8 @@ def _declare(L):
     L.rbmnqs_sr_solve_noalloc.argtypes = [VP, C.c_int32, C.c_int32, C.c_int32, VP, C.c_double, VP, VP, C.c_double,
                                           C.c_double, C.c_double, VP, C.c_int32, C.c_double, VP, P_I, P_D]
     L.rbmnqs_sr_solve_noalloc.restype = C.c_int
+    L.rbmnqs_test_fault.argtypes = [C.c_int32]
+    L.rbmnqs_test_fault.restype = C.c_int
     L.rbmnqs_probe_mufu.argtypes = [C.c_int32, P_D]
     L.rbmnqs_probe_mufu.restype = C.c_int
     L.rbmnqs_last_error.restype = C.c_char_p
@@ -161,6 +163,13 @@ def lib():
         _LIB = C.CDLL(LIBPATH)
         _declare(_LIB)
     return _LIB
+
+
+def test_fault(kind):
+    """rbmnqs_test_fault: 0 off, 1 cooperative-solve barriers never complete,
+    2 the proposal network's GEMM copies are never issued (bounded waits run
+    out and the calls report RBMNQS_ERR_CUDA)."""
+    _ck(lib().rbmnqs_test_fault(kind))
 
 
 def probe_mufu(iters=4096):

@@ -330,14 +330,17 @@ def test_timing_counters_eager_calls():
 
 
 def test_massive_step_is_reported():
-    om, mach, s, rng = make_pair("kitaev3_basic_a1", precision=1, chains=4, spc=8, lr=(1.0, 1.0, 1.0),
-                                 reg1=(1e-12, 1e-12, 1.0), reg2=(1e-12, 1e-12, 1.0), std=2.0)
+    """max|dw| > 30 (abstract_optimizer.cpp:157-159): SGD direction Re F /
+    real_factor with real_factor 1e-9 trips the guard whatever the samples;
+    the status is reported and the weights stay."""
+    om, mach, s, rng = make_pair("kitaev3_basic_a1", precision=1, chains=4, spc=8, optimizer_type=1,
+                                 sgd_real_factor=1e-9, std=0.1)
     w0 = s.get_weights()
     s.sample()
     st = s.optimize()
-    if st["max_dw"] > 30:
-        assert st["status"] == rbmnqs.ERR_MASSIVE_STEP
-        assert np.array_equal(s.get_weights(), w0)
+    assert st["max_dw"] > 30
+    assert st["status"] == rbmnqs.ERR_MASSIVE_STEP
+    assert np.array_equal(s.get_weights(), w0)
 
 
 @pytest.mark.parametrize("precision", [1, 0])
