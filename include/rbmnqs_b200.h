@@ -138,8 +138,9 @@ typedef struct {
     int32_t learned_hidden;    /* width of both hidden layers (64..256) */
     double learned_lr;
     int32_t solver;            /* optimizer.sr.method: 0 = cg (cg_solver), 1 =
-                                  minresqlp (MINRES from x0 = 0; rtol is then
-                                  the relative residual, max_iterations
+                                  minresqlp (MINRES-QLP from x0 = 0; rtol
+                                  then bounds the relative residual
+                                  ||r|| / (||A|| ||x|| + ||b||), max_iterations
                                   defaults to 4 n_params), 2 = direct
                                   (direct_solver.cpp:31-59: multiplicative
                                   diagonal regularisation, exact solve;
@@ -245,6 +246,20 @@ int rbmnqs_sr_solve(rbmnqs_handle* h, const double* O, int32_t N,
                     const double* d, double norm, const double* F,
                     double* x_io, double r1, double r2, double rd,
                     const double* diag, int32_t* iterations, double* residual);
+/* The last SR solve's outcome (that of rbmnqs_sr_solve or of the last
+ * epoch's update), the getters of minresqlp_adapter.h (getItn, getRnorm,
+ * getAcond) and the istop that minresqlp_adapter::apply returns
+ * (minresqlp_adapter.cpp:104-110).  With solver = 1 (minresqlp): istop is
+ * the stopping reason of MINRES-QLP (1: beta_{k+1} < eps, 2: x is an
+ * eigenvector, 3: b = 0, 4/5: relative residual <= rtol / at machine
+ * precision, 6/7: relative normal-equation residual <= rtol / at machine
+ * precision, 8: iteration limit, 12: ||x|| reached 1e7, 13: Acond reached
+ * 1e15 or 0.1/eps, 14: the least-squares problem has no further
+ * solution), acond the condition estimate and qlp_iterations the number
+ * of steps taken with the QLP updates (Acond above 1e7).  Other solvers
+ * leave istop, acond and qlp_iterations 0.  Any output pointer may be NULL. */
+int rbmnqs_solve_info(rbmnqs_handle* h, int32_t* iterations, double* residual,
+                      int32_t* istop, double* acond, int32_t* qlp_iterations);
 /* Exact enumeration of all 2^n configurations weighted by |psi|^2
  * (full_sampler.cpp:43-186); n <= 30.  Outputs <E>, <O>, <E O*>. */
 int rbmnqs_full_sample(rbmnqs_handle* h, double* E_mean, double* d, double* dh);

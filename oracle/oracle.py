@@ -100,8 +100,9 @@ def _declare(L):
     L.orc_sr_matrix.argtypes = [P_D, P_D, C.c_int, C.c_int, P_D]
     L.orc_cg_solve.argtypes = [P_D, P_D, C.c_double, C.c_int, C.c_int, C.c_int, P_D, P_D,
                                C.c_double, C.c_double, C.c_double, P_D, C.c_int, C.c_double, P_D]
-    L.orc_minres_solve.argtypes = [P_D, P_D, C.c_double, C.c_int, C.c_int, C.c_int, P_D, P_D,
-                                   C.c_double, C.c_double, C.c_double, P_D, C.c_int, C.c_double, P_D]
+    L.orc_minresqlp_solve.argtypes = [P_D, P_D, C.c_double, C.c_int, C.c_int, C.c_int, P_D, P_D,
+                                      C.c_double, C.c_double, C.c_double, P_D, C.c_int, C.c_double, P_D,
+                                      P_I, P_D, P_I]
     L.orc_pf_context.argtypes = [C.POINTER(_Machine), P_U32, C.POINTER(_PfCtx)]
     L.orc_pf_update.argtypes = [C.POINTER(_Machine), P_U32, P_I, C.c_int, C.POINTER(_PfCtx)]
     L.orc_pf_matrix.argtypes = [C.POINTER(_Machine), P_U32, P_D]
@@ -526,8 +527,10 @@ def cg_solve(O, d, F, x0, r1, r2, rd, diag, n_neural=None, max_iterations=0, rto
     return x, it, rs.value
 
 
-def minres_solve(O, d, F, r1, r2, rd, diag, n_neural=None, max_iterations=0, rtol=0.0, norm=None):
-    """MINRES on the SR operator from x0 = 0 -> (x, iterations, residual estimate)."""
+def minres_solve(O, d, F, r1, r2, rd, diag, n_neural=None, max_iterations=0, rtol=0.0, norm=None, info=False):
+    """MINRES-QLP (zminresqlpModule.f90 through minresqlp_adapter.cpp:40-110)
+    on the SR operator from x0 = 0 -> (x, iterations, rnorm), plus
+    {"istop", "acond", "qlp"} when info is set."""
     O = _c128(O)
     N, P = O.shape
     d = _c128(d)
@@ -535,9 +538,15 @@ def minres_solve(O, d, F, r1, r2, rd, diag, n_neural=None, max_iterations=0, rto
     x = np.zeros(P, np.complex128)
     diag = np.ascontiguousarray(diag, dtype=np.float64)
     rn = C.c_double()
-    it = lib().orc_minres_solve(_p(O, P_D), _p(d, P_D), float(N if norm is None else norm), N, P,
-                                P if n_neural is None else n_neural, _p(F, P_D), _p(x, P_D), r1, r2, rd,
-                                _p(diag, P_D), max_iterations, rtol, C.byref(rn))
+    ist = C.c_int()
+    ac = C.c_double()
+    nq = C.c_int()
+    it = lib().orc_minresqlp_solve(_p(O, P_D), _p(d, P_D), float(N if norm is None else norm), N, P,
+                                   P if n_neural is None else n_neural, _p(F, P_D), _p(x, P_D), r1, r2, rd,
+                                   _p(diag, P_D), max_iterations, rtol, C.byref(rn), C.byref(ist), C.byref(ac),
+                                   C.byref(nq))
+    if info:
+        return x, it, rn.value, {"istop": ist.value, "acond": ac.value, "qlp": nq.value}
     return x, it, rn.value
 
 

@@ -185,13 +185,14 @@ int orc_cg_solve(const double complex* O, const double complex* d, double norm,
                  const double* diag, int max_iterations, double rtol,
                  double* rs_out);
 
-/* MINRES on the same operator (minresqlp_adapter.cpp:40-110 semantics,
- * x0 = 0, relative residual test); returns the iteration count. */
-int orc_minres_solve(const double complex* O, const double complex* d, double norm,
-                     int N, int P, int n_neural, const double complex* F,
-                     double complex* x, double r1, double r2, double rd,
-                     const double* diag, int max_iterations, double rtol,
-                     double* rnorm_out);
+/* MINRES-QLP on the same operator (zminresqlpModule.f90 through
+ * minresqlp_adapter.cpp:40-110): x0 = 0; rnorm, istop, Acond and the
+ * number of QLP iterations through the optional pointers. */
+int orc_minresqlp_solve(const double complex* O, const double complex* d, double norm,
+                        int N, int P, int n_neural, const double complex* F,
+                        double complex* x, double r1, double r2, double rd,
+                        const double* diag, int max_iterations, double rtol,
+                        double* rnorm_out, int* istop_out, double* acond_out, int* qlp_out);
 
 /* decay_t (abstract_optimizer.cpp:27-54) */
 typedef struct {

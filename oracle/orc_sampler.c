@@ -389,79 +389,277 @@ int orc_cg_solve(const double complex* O, const double complex* d, double norm,
     return itn;
 }
 
-/* MINRES (Paige & Saunders 1975; the MINRES phase of MINRES-QLP, Choi,
- * Paige & Saunders 2011, which the reference calls through
- * minresqlp_adapter.cpp:40-110) on the same operator as cg1:
- * (S + r1 diag (+ rd non-neural) + r2 max(diag)) x = F, x0 = 0 as the
- * adapter starts, at most itnlim iterations (max_iterations, default 4 P,
- * minresqlp_adapter.cpp:89), stopping when the recurred residual norm falls
- * to rtol * ||F|| (default rtol 1e-16) or the Lanczos process ends
- * (beta = 0).  For Hermitian S the Lanczos coefficients are real, so the
- * rotations are the real ones of the published algorithm.  Returns the
- * iteration count. */
-int orc_minres_solve(const double complex* O, const double complex* d, double norm,
-                     int N, int P, int n_neural, const double complex* F,
-                     double complex* x, double r1, double r2, double rd,
-                     const double* diag, int max_iterations, double rtol,
-                     double* rnorm_out) {
-    int itnlim = max_iterations > 0 ? max_iterations : 4 * P;
+/* MINRES-QLP (Choi, Paige & Saunders, SIAM J. Sci. Comput. 33, 2011;
+ * ACM TOMS 40, Algorithm 937, 2014), the solver behind optimizer.sr.method =
+ * minresqlp: deps/minresqlp/Src/zminresqlpModule.f90:42-1288 driven by
+ * minresqlp_adapter.cpp:40-110 (x0 = 0, no preconditioner, the operator
+ * with its shift folded in as aprod applies it).  For Hermitian operators
+ * the Lanczos coefficients alpha, beta and therefore every rotation and
+ * recurrence scalar are real; the vectors are complex.  The iteration runs
+ * MINRES updates while the condition estimate Acond stays below trancond
+ * and switches to the QLP updates after (minimum-length solutions of
+ * near-singular systems).  Stopping rules and their order follow the
+ * published routine (istop codes 1-14); maxxnorm, trancond and Acondlim
+ * are the adapter's 1e7, 1e7 and 1e15, itnlim 4 P unless given, rtol 1e-16
+ * unless given.  Returns the iteration count; rnorm, istop, Acond and the
+ * number of QLP iterations through the optional pointers. */
+static void symortho_r(double a, double b, double* c, double* s, double* r) {
+    const double aa = fabs(a), ab = fabs(b), rmin = 2.2250738585072014e-308;
+    if (ab <= rmin) {
+        *c = 1, *s = 0, *r = a;
+    } else if (aa <= rmin) {
+        *c = 0, *s = 1, *r = b;
+    } else if (ab > aa) {
+        const double t = aa / ab;
+        double cc = 1.0 / sqrt(1.0 + t * t);
+        *s = cc * ((b > 0) == (a > 0) ? 1.0 : -1.0);
+        *c = cc * t;
+        *r = b / *s;
+    } else {
+        const double t = ab / aa;
+        const double cc = 1.0 / sqrt(1.0 + t * t);
+        *c = cc;
+        *s = cc * t * ((b > 0) == (a > 0) ? 1.0 : -1.0);
+        *r = a / cc;
+    }
+}
+
+static double nrm(int n, const double* v) {
+    double s = 0;
+    for (int i = 0; i < n; i++) s += v[i] * v[i];
+    return sqrt(s);
+}
+
+int orc_minresqlp_solve(const double complex* O, const double complex* d, double norm,
+                        int N, int P, int n_neural, const double complex* F,
+                        double complex* x, double r1, double r2, double rd,
+                        const double* diag, int max_iterations, double rtol,
+                        double* rnorm_out, int* istop_out, double* acond_out, int* qlp_out) {
+    const double eps = 2.220446049250313e-16, maxxnorm = 1e7, trancond = 1e7, Acondlim = 1e15;
+    const int itnlim = max_iterations > 0 ? max_iterations : 4 * P;
     if (rtol <= 0) rtol = 1e-16;
     double max_diag = diag[0];
     for (int k = 1; k < P; k++)
         if (diag[k] > max_diag) max_diag = diag[k];
     size_t sz = sizeof(double complex) * P;
     double complex *v = malloc(sz), *y = malloc(sz), *R1 = malloc(sz), *R2 = malloc(sz);
-    double complex *w = calloc(P, sizeof(double complex)), *w1 = calloc(P, sizeof(double complex));
-    double complex *w2 = calloc(P, sizeof(double complex)), *tmp = malloc(sizeof(double complex) * N);
+    double complex *w = calloc(P, sizeof(double complex)), *wl = calloc(P, sizeof(double complex));
+    double complex *wl2 = calloc(P, sizeof(double complex)), *xl2 = calloc(P, sizeof(double complex));
+    double complex* tmp = malloc(sizeof(double complex) * N);
     for (int k = 0; k < P; k++) x[k] = 0;
+    memcpy(y, F, sz);
     memcpy(R1, F, sz);
     memcpy(R2, F, sz);
-    memcpy(y, F, sz);
     double beta1 = 0;
     for (int k = 0; k < P; k++) beta1 += creal(F[k]) * creal(F[k]) + cimag(F[k]) * cimag(F[k]);
+    int istop = beta1 == 0 ? 3 : 0;
     beta1 = sqrt(beta1);
-    double oldb = 0, beta = beta1, dbar = 0, epsln = 0, phibar = beta1, cs = -1, sn = 0;
-    int itn = 0;
-    if (beta1 > 0) {
-        for (itn = 1; itn <= itnlim; itn++) {
-            double s = 1.0 / beta;
-            for (int k = 0; k < P; k++) v[k] = s * y[k];
-            aprod(O, d, norm, N, P, n_neural, r1, r2, rd, diag, max_diag, v, y, tmp);
-            if (itn >= 2)
-                for (int k = 0; k < P; k++) y[k] -= (beta / oldb) * R1[k];
-            double alfa = 0;
-            for (int k = 0; k < P; k++) alfa += creal(conj(v[k]) * y[k]);
-            for (int k = 0; k < P; k++) y[k] -= (alfa / beta) * R2[k];
-            memcpy(R1, R2, sz);
-            memcpy(R2, y, sz);
-            oldb = beta;
-            beta = 0;
-            for (int k = 0; k < P; k++) beta += creal(R2[k]) * creal(R2[k]) + cimag(R2[k]) * cimag(R2[k]);
-            beta = sqrt(beta);
-            double oldeps = epsln;
-            double delta = cs * dbar + sn * alfa;
-            double gbar = sn * dbar - cs * alfa;
-            epsln = sn * beta;
-            dbar = -cs * beta;
-            double gamma = sqrt(gbar * gbar + beta * beta);
-            if (gamma < 2.2250738585072014e-308) gamma = 2.2250738585072014e-308;
-            cs = gbar / gamma;
-            sn = beta / gamma;
-            double phi = cs * phibar;
-            phibar = sn * phibar;
-            double denom = 1.0 / gamma;
-            for (int k = 0; k < P; k++) {
-                double complex wn = (v[k] - oldeps * w1[k] - delta * w2[k]) * denom;
-                w1[k] = w2[k];
-                w2[k] = wn;
-                x[k] += phi * wn;
-            }
-            if (phibar <= rtol * beta1 || beta == 0) break;
+    const double ieps = 0.1 / eps;
+    int itn = 0, qlp = 0, lastiter = 0;
+    double beta = 0, betal, betan = beta1, alfa, pnorm = 0;
+    double dbar, dlta = 0, epln, eplnn = 0, dltan = 0, gbar = 0, dlta_qlp;
+    double gama = 0, gamal = 0, gamal2 = 0, gamal3, gama_tmp;
+    double tau = 0, taul = 0, taul2, phi = beta1, cs = -1, sn = 0, cr1 = -1, sr1 = 0, cr2 = -1, sr2 = 0;
+    double vepln = 0, veplnl = 0, veplnl2 = 0, eta = 0, etal = 0, etal2 = 0;
+    double u = 0, ul = 0, ul2 = 0, ul3 = 0, ul4;
+    double xnorm = 0, xl2norm = 0, Axnorm = 0, Anorm = 0, Acond = 1, Acondl = 1, gmin = 0, gminl = 0, gminl2;
+    double rnorm = beta1, rnorml = beta1, relres = 1, relresl = 0, relAresl = 0, t1 = 2, t2 = 2;
+    double gamal_qlp = 0, vepln_qlp = 0, gama_qlp = 0, ul_qlp = 0, u_qlp = 0;
+    while (istop <= 0) {
+        itn++;
+        // Lanczos: v = y / beta, y = A v - (beta / betal) r1 - (alfa / beta) r2
+        betal = beta;
+        beta = betan;
+        for (int k = 0; k < P; k++) v[k] = y[k] / beta;
+        aprod(O, d, norm, N, P, n_neural, r1, r2, rd, diag, max_diag, v, y, tmp);
+        if (itn >= 2)
+            for (int k = 0; k < P; k++) y[k] -= (beta / betal) * R1[k];
+        alfa = 0;
+        for (int k = 0; k < P; k++) alfa += creal(conj(v[k]) * y[k]);
+        for (int k = 0; k < P; k++) y[k] -= (alfa / beta) * R2[k];
+        memcpy(R1, R2, sz);
+        memcpy(R2, y, sz);
+        betan = 0;
+        for (int k = 0; k < P; k++) betan += creal(y[k]) * creal(y[k]) + cimag(y[k]) * cimag(y[k]);
+        betan = sqrt(betan);
+        {
+            const double q2[2] = {alfa, betan}, q3[3] = {beta, alfa, betan};
+            pnorm = itn == 1 ? nrm(2, q2) : nrm(3, q3);
         }
-        if (itn > itnlim) itn = itnlim;
+        // previous left reflection
+        dbar = dltan;
+        dlta = cs * dbar + sn * alfa;
+        epln = eplnn;
+        gbar = sn * dbar - cs * alfa;
+        eplnn = sn * betan;
+        dltan = -cs * betan;
+        dlta_qlp = dlta;
+        // current left reflection
+        gamal3 = gamal2;
+        gamal2 = gamal;
+        gamal = gama;
+        symortho_r(gbar, betan, &cs, &sn, &gama);
+        gama_tmp = gama;
+        taul2 = taul;
+        taul = tau;
+        tau = cs * phi;
+        phi = sn * phi;
+        Axnorm = sqrt(Axnorm * Axnorm + tau * tau);
+        // previous right reflection P_{k-2,k}
+        if (itn > 2) {
+            veplnl2 = veplnl;
+            etal2 = etal;
+            etal = eta;
+            const double dt = sr2 * vepln - cr2 * dlta;
+            veplnl = cr2 * vepln + sr2 * dlta;
+            dlta = dt;
+            eta = sr2 * gama;
+            gama = -cr2 * gama;
+        }
+        // current right reflection P_{k-1,k}
+        if (itn > 1) {
+            double g;
+            symortho_r(gamal, dlta, &cr1, &sr1, &g);
+            gamal = g;
+            vepln = sr1 * gama;
+            gama = -cr1 * gama;
+        }
+        // xnorm
+        ul4 = ul3;
+        ul3 = ul2;
+        if (itn > 2) ul2 = (taul2 - etal2 * ul4 - veplnl2 * ul3) / gamal2;
+        if (itn > 1) ul = (taul - etal * ul3 - veplnl * ul2) / gamal;
+        {
+            const double q3[3] = {xl2norm, ul2, ul};
+            const double xt = nrm(3, q3);
+            if (fabs(gama) > 0 && xt < maxxnorm) {
+                u = (tau - eta * ul2 - vepln * ul) / gama;
+                const double q2[2] = {xt, u};
+                if (relAresl < relresl && nrm(2, q2) > maxxnorm) {
+                    u = 0;
+                    istop = 12;
+                }
+            } else {
+                u = 0;
+                istop = 14;
+            }
+        }
+        {
+            const double q2[2] = {xl2norm, ul2};
+            xl2norm = nrm(2, q2);
+            const double q3[3] = {xl2norm, ul, u};
+            xnorm = nrm(3, q3);
+        }
+        if (Acond < trancond && istop == 0 && qlp == 0) {
+            // MINRES updates
+            for (int k = 0; k < P; k++) {
+                const double complex a = wl[k];
+                wl2[k] = a;
+                wl[k] = w[k];
+                if (fabs(gama_tmp) > 0) w[k] = (v[k] - epln * wl2[k] - dlta_qlp * wl[k]) / gama_tmp;
+            }
+            if (xnorm < maxxnorm) {
+                for (int k = 0; k < P; k++) x[k] += tau * w[k];
+            } else {
+                istop = 12;
+                lastiter = 1;
+            }
+        } else {
+            // MINRES-QLP updates
+            qlp++;
+            if (qlp == 1) {
+                for (int k = 0; k < P; k++) xl2[k] = 0;
+                if (itn > 1) {
+                    for (int k = 0; k < P; k++) {
+                        if (itn > 3) wl2[k] = gamal3 * wl2[k] + veplnl2 * wl[k] + etal * w[k];
+                        if (itn > 2) wl[k] = gamal_qlp * wl[k] + vepln_qlp * w[k];
+                        w[k] = gama_qlp * w[k];
+                        xl2[k] = x[k] - ul_qlp * wl[k] - u_qlp * w[k];
+                    }
+                }
+            }
+            for (int k = 0; k < P; k++) {
+                if (itn == 1) {
+                    wl2[k] = wl[k];
+                    wl[k] = sr1 * v[k];
+                    w[k] = -cr1 * v[k];
+                } else if (itn == 2) {
+                    wl2[k] = wl[k];
+                    wl[k] = cr1 * w[k] + sr1 * v[k];
+                    w[k] = sr1 * w[k] - cr1 * v[k];
+                } else {
+                    wl2[k] = wl[k];
+                    wl[k] = w[k];
+                    w[k] = sr2 * wl2[k] - cr2 * v[k];
+                    wl2[k] = cr2 * wl2[k] + sr2 * v[k];
+                    v[k] = cr1 * wl[k] + sr1 * w[k];
+                    w[k] = sr1 * wl[k] - cr1 * w[k];
+                    wl[k] = v[k];
+                }
+                xl2[k] += ul2 * wl2[k];
+                x[k] = xl2[k] + ul * wl[k] + u * w[k];
+            }
+        }
+        // next right reflection P_{k-1,k+1}
+        {
+            const double gt = gamal;
+            symortho_r(gt, eplnn, &cr2, &sr2, &gamal);
+            gamal_qlp = gt;
+        }
+        vepln_qlp = vepln;
+        gama_qlp = gama;
+        ul_qlp = ul;
+        u_qlp = u;
+        // norm and condition estimates
+        const double ag = fabs(gama);
+        Anorm = fmax(fmax(Anorm, pnorm), fmax(fabs(gamal), ag));
+        if (itn == 1) {
+            gmin = ag;
+            gminl = gmin;
+        } else {
+            gminl2 = gminl;
+            gminl = gmin;
+            gmin = fmin(gminl2, fmin(fabs(gamal), ag));
+        }
+        Acondl = Acond;
+        Acond = Anorm / gmin;
+        rnorml = rnorm;
+        relresl = relres;
+        if (istop != 14) rnorm = fabs(phi);
+        relres = rnorm / (Anorm * xnorm + beta1);
+        {
+            const double q2[2] = {gbar, dltan};
+            const double rootl = nrm(2, q2);
+            relAresl = rootl / Anorm;
+        }
+        // stopping rules, in the published order
+        const double epsx = Anorm * xnorm * eps;
+        if (istop == 0 || istop == 14) {
+            t1 = 1 + relres;
+            t2 = 1 + relAresl;
+        }
+        if (t1 <= 1) istop = 5;
+        else if (t2 <= 1) istop = 7;
+        else if (relres <= rtol) istop = 4;
+        else if (relAresl <= rtol) istop = 6;
+        else if (epsx >= beta1) istop = 2;
+        else if (xnorm >= maxxnorm) istop = 12;
+        else if (Acond >= Acondlim || Acond >= ieps) istop = 13;
+        else if (itn >= itnlim) istop = 8;
+        else if (betan < eps) istop = 1;
+        if (istop == 6 || istop == 7 || istop == 12 || istop == 13) lastiter = 1;
+        if (istop != 0 && lastiter) {
+            itn--;
+            Acond = Acondl;
+            rnorm = rnorml;
+            relres = relresl;
+        }
     }
-    if (rnorm_out) *rnorm_out = phibar;
-    free(v), free(y), free(R1), free(R2), free(w), free(w1), free(w2), free(tmp);
+    if (rnorm_out) *rnorm_out = rnorm;
+    if (istop_out) *istop_out = istop;
+    if (acond_out) *acond_out = Acond;
+    if (qlp_out) *qlp_out = qlp;
+    free(v), free(y), free(R1), free(R2), free(w), free(wl), free(wl2), free(xl2), free(tmp);
     return itn;
 }
 

@@ -344,6 +344,7 @@ struct rbmnqs_handle {
     uint32_t epoch = 0;
     bool sampled = false;
     int64_t n_updates = 0;  // rbm_base::n_updates_ (offset + applied SR updates)
+    rbmnqs::CgResultDev last_solve{};  // the last SR solve's result (rbmnqs_solve_info)
 
     cudaGraphExec_t graph = nullptr;
     int graph_kernels = 0;
@@ -1356,6 +1357,7 @@ static void readback(rbmnqs_handle* h, bool sample, rbmnqs_sample_stats* out, bo
             throw Fail{RBMNQS_ERR_CUDA,
                        "tensor-core Gram: pipeline wait timed out (code " + std::to_string(rb->gerr) + ")"};
         const auto& r = rb->cg;
+        h->last_solve = r;
         if (r.status == 0) h->n_updates++;
         if (o) {
             o->iterations = r.iterations;
@@ -1632,8 +1634,23 @@ int rbmnqs_sr_solve(rbmnqs_handle* h, const double* O, int32_t N, const double* 
         ck(cudaMemcpyAsync(x_io, dx.p, P * sizeof(double2), cudaMemcpyDeviceToHost, h->st), "c");
         ck(cudaMemcpyAsync(&r, res.p, sizeof(r), cudaMemcpyDeviceToHost, h->st), "c");
         ck(cudaStreamSynchronize(h->st), "sync");
+        h->last_solve = r;
         if (iterations) *iterations = r.iterations;
         if (residual) *residual = r.residual;
+    });
+}
+
+int rbmnqs_solve_info(rbmnqs_handle* h, int32_t* iterations, double* residual, int32_t* istop, double* acond,
+                      int32_t* qlp_iterations) {
+    return guard([&] {
+        require(h != nullptr, "null handle");
+        const auto& r = h->last_solve;
+        const bool mq = h->cfg.solver == 1;
+        if (iterations) *iterations = r.iterations;
+        if (residual) *residual = r.residual;
+        if (istop) *istop = mq ? r.istop : 0;
+        if (acond) *acond = mq ? r.acond : 0.0;
+        if (qlp_iterations) *qlp_iterations = mq ? r.qlp_iterations : 0;
     });
 }
 

@@ -62,6 +62,29 @@ template <> __device__ double2 bsum<double2>(double2 v, double2* red) {
 // Sum of the per-block partials: thread t adds entries t, t + 256, ... and the
 // block reduces in a fixed order, so every block gets the same value (and the
 // loads are issued in parallel rather than as one dependent chain).
+// Stable reflection [c s; s -c] (a, b)^T = (r, 0)^T for real a, b with c >= 0
+// (SYMORTHO of MINRES-QLP, zminresqlpModule.f90): the larger of |a|, |b|
+// divides, so nothing overflows or cancels.
+__device__ __forceinline__ void symortho(double a, double b, double& c, double& s, double& r) {
+    const double aa = fabs(a), ab = fabs(b), rmin = 2.2250738585072014e-308;
+    const double sg = (a > 0) == (b > 0) ? 1.0 : -1.0;
+    if (ab <= rmin) {
+        c = 1, s = 0, r = a;
+    } else if (aa <= rmin) {
+        c = 0, s = 1, r = b;
+    } else if (ab > aa) {
+        const double t = aa / ab, cc = 1.0 / sqrt(1.0 + t * t);
+        s = cc * sg;
+        c = cc * t;
+        r = b / s;
+    } else {
+        const double t = ab / aa, cc = 1.0 / sqrt(1.0 + t * t);
+        c = cc;
+        s = cc * t * sg;
+        r = a / cc;
+    }
+}
+
 __device__ __forceinline__ double sum_parts(const double* p, int G, double* red) {
     double s = 0;
     for (int i = threadIdx.x; i < G; i += blockDim.x) s += cg_ld(p + i);
@@ -93,7 +116,12 @@ __global__ void __launch_bounds__(kThreads) cg_mfree_kernel(const TO* __restrict
     const int gt = blk * kThreads + tid, nthreads = G * kThreads;
     const double r1 = sch ? sch->value[1] : r1_, r2 = sch ? sch->value[2] : r2_, rd = sch ? sch->value[3] : rd_;
     const double mxd = max_diag ? *max_diag : 0.0;
-    if (blk == 0 && tid == 0) res->status = 0;
+    if (blk == 0 && tid == 0) {
+        res->status = 0;
+        res->istop = 0;
+        res->qlp_iterations = 0;
+        res->acond = 0;
+    }
 
     // A b into Ap (b = x at the start, p afterwards); returns false on a
     // barrier timeout.  With want_pap, also leaves sum_q conj(b_q) Ap_q.
@@ -256,10 +284,20 @@ __global__ void __launch_bounds__(kThreads) cg_mfree_kernel(const TO* __restrict
     };
 
     if (w.minres) {
-        // MINRES (Paige & Saunders 1975; the MINRES phase of MINRES-QLP,
-        // minresqlp_adapter.cpp:40-110): Lanczos on A with real coefficients
-        // (A Hermitian), QR by Givens rotations, x0 = 0, stop when the
-        // recurred residual norm reaches rtol ||F|| or beta vanishes.
+        // MINRES-QLP (Choi, Paige & Saunders; ACM TOMS 937), the solver of
+        // optimizer.sr.method = minresqlp (zminresqlpModule.f90:42-1288 driven
+        // by minresqlp_adapter.cpp:40-110): Lanczos on A with real
+        // coefficients (A Hermitian), left reflections for the QR factors,
+        // two right reflections per step for the LQ factors, MINRES updates
+        // of x while the condition estimate stays below trancond and QLP
+        // updates (minimum-length solution) after; x0 = 0.  The scalar
+        // recurrence is carried redundantly by every thread (all blocks read
+        // the same partial sums in the same order, so every copy agrees) and
+        // the vectors are updated elementwise:
+        //   v -> w.p, y -> w.Ap, r1 -> w.R1, r2 -> w.R2,
+        //   w -> w.w2, wl -> w.w1, wl2 -> w.v, xl2 -> w.r.
+        // Three grid barriers per iteration besides the operator's own.
+        const double eps = 2.220446049250313e-16, maxxnorm = 1e7, trancond = 1e7, Acondlim = 1e15;
         double bl = 0;
         for (int q = gt; q < P; q += nthreads) {
             const double2 f = F[q];
@@ -267,6 +305,8 @@ __global__ void __launch_bounds__(kThreads) cg_mfree_kernel(const TO* __restrict
             w.R2[q] = f;
             w.w1[q] = make_double2(0, 0);
             w.w2[q] = make_double2(0, 0);
+            w.v[q] = make_double2(0, 0);
+            w.r[q] = make_double2(0, 0);
             x[q] = make_double2(0, 0);
             bl += f.x * f.x + f.y * f.y;
         }
@@ -274,78 +314,239 @@ __global__ void __launch_bounds__(kThreads) cg_mfree_kernel(const TO* __restrict
         if (tid == 0) w.dpart[blk] = bl;
         bool mok = grid_barrier(w.sync, G);
         const double beta1 = mok ? sqrt(sum_parts(w.dpart, G, redd)) : 0.0;
-        double oldb = 0, beta = beta1, dbar = 0, epsln = 0, phibar = beta1, cs = -1, sn = 0;
-        int itn = 0;
-        if (mok && beta1 > 0) {
-            for (itn = 1; itn <= max_it; itn++) {
-                const double s = 1.0 / beta;
-                for (int q = gt; q < P; q += nthreads) {
-                    const double2 r2 = cg_ld(w.R2 + q);
-                    w.p[q] = make_double2(s * r2.x, s * r2.y);  // v
+        int istop = beta1 == 0 ? 3 : 0, itn = 0, qlp = 0;
+        bool lastiter = false;
+        double beta = 0, betal, betan = beta1, alfa, pnorm;
+        double dbar, dlta, epln, eplnn = 0, dltan = 0, gbar = 0, dlta_qlp;
+        double gama = 0, gamal = 0, gamal2 = 0, gamal3, gama_tmp;
+        double tau = 0, taul = 0, taul2, phi = beta1, cs = -1, sn = 0, cr1 = -1, sr1 = 0, cr2 = -1, sr2 = 0;
+        double vepln = 0, veplnl = 0, veplnl2 = 0, eta = 0, etal = 0, etal2 = 0;
+        double u = 0, ul = 0, ul2 = 0, ul3 = 0, ul4;
+        double xnorm = 0, xl2norm = 0, Anorm = 0, Acond = 1, Acondl = 1, gmin = 0, gminl = 0, gminl2;
+        double rnorm = beta1, rnorml = beta1, relres = 1, relresl = 0, relAresl = 0, t1 = 2, t2 = 2;
+        double gamal_qlp = 0, vepln_qlp = 0, gama_qlp = 0, ul_qlp = 0, u_qlp = 0;
+        if (!mok) istop = -1;
+        while (istop == 0) {
+            itn++;
+            // Lanczos step: v = y / beta, y = A v - (beta / betal) r1 - (alfa / beta) r2
+            betal = beta;
+            beta = betan;
+            const double s = 1.0 / beta;
+            for (int q = gt; q < P; q += nthreads) {
+                const double2 r2 = cg_ld(w.R2 + q);
+                w.p[q] = make_double2(s * r2.x, s * r2.y);
+            }
+            if (!(mok = grid_barrier(w.sync, G))) break;
+            if (!(mok = aprod(w.p, false, nullptr))) break;
+            double al = 0;
+            const double cb = itn >= 2 ? beta / betal : 0.0;
+            for (int q = gt; q < P; q += nthreads) {
+                double2 y = cg_ld(w.Ap + q);
+                const double2 r1 = cg_ld(w.R1 + q), v = cg_ld(w.p + q);
+                y.x -= cb * r1.x;
+                y.y -= cb * r1.y;
+                w.Ap[q] = y;
+                al += v.x * y.x + v.y * y.y;
+            }
+            al = bsum(al, redd);
+            if (tid == 0) w.dpart[blk] = al;
+            if (!(mok = grid_barrier(w.sync, G))) break;
+            alfa = sum_parts(w.dpart, G, redd);
+            double bb = 0;
+            const double ca = alfa / beta;
+            for (int q = gt; q < P; q += nthreads) {
+                double2 y = cg_ld(w.Ap + q);
+                const double2 r2 = cg_ld(w.R2 + q);
+                y.x -= ca * r2.x;
+                y.y -= ca * r2.y;
+                w.R1[q] = r2;
+                w.R2[q] = y;
+                bb += y.x * y.x + y.y * y.y;
+            }
+            bb = bsum(bb, redd);
+            if (tid == 0) w.zpart[blk] = make_double2(bb, 0);
+            if (!(mok = grid_barrier(w.sync, G))) break;
+            betan = sqrt(sum_parts(w.zpart, G, redz).x);
+            pnorm = itn == 1 ? hypot(alfa, betan) : norm3d(beta, alfa, betan);
+            // previous left reflection
+            dbar = dltan;
+            dlta = cs * dbar + sn * alfa;
+            epln = eplnn;
+            gbar = sn * dbar - cs * alfa;
+            eplnn = sn * betan;
+            dltan = -cs * betan;
+            dlta_qlp = dlta;
+            // current left reflection
+            gamal3 = gamal2;
+            gamal2 = gamal;
+            gamal = gama;
+            symortho(gbar, betan, cs, sn, gama);
+            gama_tmp = gama;
+            taul2 = taul;
+            taul = tau;
+            tau = cs * phi;
+            phi = sn * phi;
+            // previous right reflection P_{k-2,k}
+            if (itn > 2) {
+                veplnl2 = veplnl;
+                etal2 = etal;
+                etal = eta;
+                const double dt = sr2 * vepln - cr2 * dlta;
+                veplnl = cr2 * vepln + sr2 * dlta;
+                dlta = dt;
+                eta = sr2 * gama;
+                gama = -cr2 * gama;
+            }
+            // current right reflection P_{k-1,k}
+            if (itn > 1) {
+                double g;
+                symortho(gamal, dlta, cr1, sr1, g);
+                gamal = g;
+                vepln = sr1 * gama;
+                gama = -cr1 * gama;
+            }
+            // solution norm
+            ul4 = ul3;
+            ul3 = ul2;
+            if (itn > 2) ul2 = (taul2 - etal2 * ul4 - veplnl2 * ul3) / gamal2;
+            if (itn > 1) ul = (taul - etal * ul3 - veplnl * ul2) / gamal;
+            const double xt = norm3d(xl2norm, ul2, ul);
+            if (fabs(gama) > 0 && xt < maxxnorm) {
+                u = (tau - eta * ul2 - vepln * ul) / gama;
+                if (relAresl < relresl && hypot(xt, u) > maxxnorm) {
+                    u = 0;
+                    istop = 12;
                 }
-                if (!(mok = grid_barrier(w.sync, G))) break;
-                if (!(mok = aprod(w.p, false, nullptr))) break;
-                // y = A v - (beta / oldb) r1;  alfa = Re(v^H y)
-                double al = 0;
-                const double cb = itn >= 2 ? beta / oldb : 0.0;
-                for (int q = gt; q < P; q += nthreads) {
-                    double2 y = cg_ld(w.Ap + q);
-                    const double2 r1 = cg_ld(w.R1 + q), v = cg_ld(w.p + q);
-                    y.x -= cb * r1.x;
-                    y.y -= cb * r1.y;
-                    w.r[q] = y;
-                    al += v.x * y.x + v.y * y.y;
-                }
-                al = bsum(al, redd);
-                if (tid == 0) w.dpart[blk] = al;
-                if (!(mok = grid_barrier(w.sync, G))) break;
-                const double alfa = sum_parts(w.dpart, G, redd);
-                // y -= (alfa / beta) r2;  r1 = r2;  r2 = y;  beta = ||r2||
-                double bb = 0;
-                for (int q = gt; q < P; q += nthreads) {
-                    double2 y = cg_ld(w.r + q);
-                    const double2 r2 = cg_ld(w.R2 + q);
-                    y.x -= (alfa / beta) * r2.x;
-                    y.y -= (alfa / beta) * r2.y;
-                    w.R1[q] = r2;
-                    w.R2[q] = y;
-                    bb += y.x * y.x + y.y * y.y;
-                }
-                bb = bsum(bb, redd);
-                if (tid == 0) w.zpart[blk] = make_double2(bb, 0);
-                if (!(mok = grid_barrier(w.sync, G))) break;
-                oldb = beta;
-                beta = sqrt(sum_parts(w.zpart, G, redz).x);
-                const double oldeps = epsln;
-                const double delta = cs * dbar + sn * alfa;
-                const double gbar = sn * dbar - cs * alfa;
-                epsln = sn * beta;
-                dbar = -cs * beta;
-                double gamma = sqrt(gbar * gbar + beta * beta);
-                if (gamma < 2.2250738585072014e-308) gamma = 2.2250738585072014e-308;
-                cs = gbar / gamma;
-                sn = beta / gamma;
-                const double phi = cs * phibar;
-                phibar = sn * phibar;
-                const double den = 1.0 / gamma;
+            } else {
+                u = 0;
+                istop = 14;
+            }
+            xl2norm = hypot(xl2norm, ul2);
+            xnorm = norm3d(xl2norm, ul, u);
+            if (Acond < trancond && istop == 0 && qlp == 0) {
+                // MINRES updates
+                const bool upd = xnorm < maxxnorm;
+                const double ig = fabs(gama_tmp) > 0 ? 1.0 / gama_tmp : 0.0;
                 for (int q = gt; q < P; q += nthreads) {
                     const double2 v = cg_ld(w.p + q), a1 = cg_ld(w.w1 + q), a2 = cg_ld(w.w2 + q);
-                    const double2 wn = make_double2((v.x - oldeps * a1.x - delta * a2.x) * den,
-                                                    (v.y - oldeps * a1.y - delta * a2.y) * den);
+                    double2 wn = a2;
+                    if (ig != 0)
+                        wn = make_double2((v.x - epln * a1.x - dlta_qlp * a2.x) * ig,
+                                          (v.y - epln * a1.y - dlta_qlp * a2.y) * ig);
+                    w.v[q] = a1;
                     w.w1[q] = a2;
                     w.w2[q] = wn;
-                    double2 xq = cg_ld(x + q);
-                    xq.x += phi * wn.x;
-                    xq.y += phi * wn.y;
-                    x[q] = xq;
+                    if (upd) {
+                        double2 xq = cg_ld(x + q);
+                        xq.x += tau * wn.x;
+                        xq.y += tau * wn.y;
+                        x[q] = xq;
+                    }
                 }
-                if (phibar <= rtol * beta1 || beta == 0) break;
+                if (!upd) {
+                    istop = 12;
+                    lastiter = true;
+                }
+            } else {
+                // MINRES-QLP updates
+                qlp++;
+                const bool first = qlp == 1;
+                for (int q = gt; q < P; q += nthreads) {
+                    double2 W = cg_ld(w.w2 + q), WL = cg_ld(w.w1 + q), WL2 = cg_ld(w.v + q);
+                    double2 XL2 = cg_ld(w.r + q);
+                    const double2 v = cg_ld(w.p + q), xq = cg_ld(x + q);
+                    if (first) {
+                        // transfer from the MINRES vectors
+                        XL2 = make_double2(0, 0);
+                        if (itn > 1) {
+                            if (itn > 3)
+                                WL2 = make_double2(gamal3 * WL2.x + veplnl2 * WL.x + etal * W.x,
+                                                   gamal3 * WL2.y + veplnl2 * WL.y + etal * W.y);
+                            if (itn > 2)
+                                WL = make_double2(gamal_qlp * WL.x + vepln_qlp * W.x,
+                                                  gamal_qlp * WL.y + vepln_qlp * W.y);
+                            W = make_double2(gama_qlp * W.x, gama_qlp * W.y);
+                            XL2 = make_double2(xq.x - ul_qlp * WL.x - u_qlp * W.x, xq.y - ul_qlp * WL.y - u_qlp * W.y);
+                        }
+                    }
+                    if (itn == 1) {
+                        WL2 = WL;
+                        WL = make_double2(sr1 * v.x, sr1 * v.y);
+                        W = make_double2(-cr1 * v.x, -cr1 * v.y);
+                    } else if (itn == 2) {
+                        WL2 = WL;
+                        WL = make_double2(cr1 * W.x + sr1 * v.x, cr1 * W.y + sr1 * v.y);
+                        W = make_double2(sr1 * W.x - cr1 * v.x, sr1 * W.y - cr1 * v.y);
+                    } else {
+                        const double2 a = WL, b = W;
+                        const double2 wt = make_double2(sr2 * a.x - cr2 * v.x, sr2 * a.y - cr2 * v.y);
+                        WL2 = make_double2(cr2 * a.x + sr2 * v.x, cr2 * a.y + sr2 * v.y);
+                        WL = make_double2(cr1 * b.x + sr1 * wt.x, cr1 * b.y + sr1 * wt.y);
+                        W = make_double2(sr1 * b.x - cr1 * wt.x, sr1 * b.y - cr1 * wt.y);
+                    }
+                    XL2 = make_double2(XL2.x + ul2 * WL2.x, XL2.y + ul2 * WL2.y);
+                    w.w2[q] = W;
+                    w.w1[q] = WL;
+                    w.v[q] = WL2;
+                    w.r[q] = XL2;
+                    x[q] = make_double2(XL2.x + ul * WL.x + u * W.x, XL2.y + ul * WL.y + u * W.y);
+                }
             }
-            if (itn > max_it) itn = max_it;
+            // next right reflection P_{k-1,k+1}
+            gamal_qlp = gamal;
+            symortho(gamal_qlp, eplnn, cr2, sr2, gamal);
+            vepln_qlp = vepln;
+            gama_qlp = gama;
+            ul_qlp = ul;
+            u_qlp = u;
+            // norm and condition estimates
+            const double ag = fabs(gama);
+            Anorm = fmax(fmax(Anorm, pnorm), fmax(fabs(gamal), ag));
+            if (itn == 1) {
+                gmin = ag;
+                gminl = gmin;
+            } else {
+                gminl2 = gminl;
+                gminl = gmin;
+                gmin = fmin(gminl2, fmin(fabs(gamal), ag));
+            }
+            Acondl = Acond;
+            Acond = Anorm / gmin;
+            rnorml = rnorm;
+            relresl = relres;
+            if (istop != 14) rnorm = fabs(phi);
+            relres = rnorm / (Anorm * xnorm + beta1);
+            relAresl = hypot(gbar, dltan) / Anorm;
+            // stopping rules in the published order
+            const double epsx = Anorm * xnorm * eps;
+            if (istop == 0 || istop == 14) {
+                t1 = 1 + relres;
+                t2 = 1 + relAresl;
+            }
+            if (t1 <= 1) istop = 5;
+            else if (t2 <= 1) istop = 7;
+            else if (relres <= rtol) istop = 4;
+            else if (relAresl <= rtol) istop = 6;
+            else if (epsx >= beta1) istop = 2;
+            else if (xnorm >= maxxnorm) istop = 12;
+            else if (Acond >= Acondlim || Acond >= 0.1 / eps) istop = 13;
+            else if (itn >= max_it) istop = 8;
+            else if (betan < eps) istop = 1;
+            // the last step's estimates are not kept for these stops
+            if (istop == 6 || istop == 7 || istop == 12 || istop == 13) lastiter = true;
+            if (istop != 0 && lastiter) {
+                itn--;
+                Acond = Acondl;
+                rnorm = rnorml;
+                relres = relresl;
+            }
         }
         if (blk == 0 && tid == 0) {
             res->iterations = itn;
-            res->residual = phibar;
+            res->residual = rnorm;
+            res->istop = istop;
+            res->acond = Acond;
+            res->qlp_iterations = qlp;
             if (!mok) res->status = -2;
         }
         return;
@@ -481,7 +682,12 @@ __global__ void __launch_bounds__(kThreads) cg_dense1_kernel(const double2* __re
     __shared__ double2 redz[kThreads / 32];
     const int tid = threadIdx.x, lane = tid & 31, G = gridDim.x, blk = blockIdx.x;
     const int gw = blk * (kThreads / 32) + (tid >> 5), nwarps = G * (kThreads / 32);
-    if (blk == 0 && tid == 0) res->status = 0;
+    if (blk == 0 && tid == 0) {
+        res->status = 0;
+        res->istop = 0;
+        res->qlp_iterations = 0;
+        res->acond = 0;
+    }
     // rows of S times a shared-memory vector into a global buffer
     auto matvec = [&](const double2* v, double2* out) {
         for (int row = gw; row < P; row += nwarps) {

@@ -28,6 +28,11 @@ struct CgResultDev {
     int status;
     double residual;
     double max_dw;
+    // MINRES-QLP: stopping reason (istop 1-14 of zminresqlpModule.f90), the
+    // condition estimate Acond and the number of QLP iterations
+    int istop;
+    int qlp_iterations;
+    double acond;
 };
 
 // w: optional per-sample weights, wsum: their total (device scalar)
@@ -144,7 +149,7 @@ struct MfreePlan {
 };
 struct MfreeWork {
     const double2* S;  // formed regularised S (dense cooperative mode) or null
-    int minres;        // 0: CG (cg1), 1: MINRES from x0 = 0 (rtol relative to ||F||)
+    int minres;        // 0: CG (cg1), 1: MINRES-QLP from x0 = 0 (rtol bounds the relative residual)
     double2 *r, *p, *Ap, *tmpN, *partA, *zpart;
     double2 *R1, *R2, *w1, *w2, *v;  // MINRES vectors
     double *dpart, *maxpart;

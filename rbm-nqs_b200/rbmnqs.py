@@ -107,6 +107,7 @@ def _declare(L):
         "rbmnqs_log_psi_over_psi": [VP, P_U32, P_I, C.c_int32, C.c_int32, P_D],
         "rbmnqs_sr_solve": [VP, P_D, C.c_int32, P_D, C.c_double, P_D, P_D, C.c_double, C.c_double, C.c_double,
                             P_D, P_I, P_D],
+        "rbmnqs_solve_info": [VP, P_I, P_D, P_I, P_D, P_I],
         "rbmnqs_full_sample": [VP, P_D, P_D, P_D],
         "rbmnqs_get_observables": [VP, P_D],
         "rbmnqs_full_state": [VP, P_D],
@@ -412,6 +413,16 @@ class Session:
                                   _p(x.view(np.float64), P_D), r1, r2, rd, _p(diag, P_D), C.byref(it),
                                   C.byref(rs)))
         return x, it.value, rs.value
+
+    def solve_info(self):
+        """The last SR solve's outcome (minresqlp_adapter getItn / getRnorm /
+        getAcond and the istop of apply): {"iterations", "residual",
+        "istop", "acond", "qlp"}; istop, acond and qlp are 0 unless the
+        solver is minresqlp."""
+        it, rs, ist, ac, nq = C.c_int32(), C.c_double(), C.c_int32(), C.c_double(), C.c_int32()
+        _ck(lib().rbmnqs_solve_info(self._h, C.byref(it), C.byref(rs), C.byref(ist), C.byref(ac), C.byref(nq)))
+        return {"iterations": it.value, "residual": rs.value, "istop": ist.value, "acond": ac.value,
+                "qlp": nq.value}
 
     def observables(self):
         """Evaluation mode: [n_obs] rows of (Re <O>, Im <O>, stddev, tau) over the

@@ -402,9 +402,10 @@ def test_matrix_free_epochs_match_oracle():
 
 @pytest.mark.parametrize("model,L,kind,alpha", [("kitaev", 3, 0, 1), ("toric", 4, 0, 2), ("kitaev", 2, 1, 4)])
 def test_minres_solve_matches_oracle(model, L, kind, alpha):
-    """optimizer.sr.method = minresqlp: MINRES from x0 = 0 on the SR operator
-    (dense S for 360 / 20 parameters, the matrix-free operator for 2144)
-    against the oracle's MINRES, and against CG on the same system."""
+    """optimizer.sr.method = minresqlp: MINRES-QLP from x0 = 0 on the SR
+    operator (dense S for 360 / 20 parameters, the matrix-free operator for
+    2144) against the oracle's MINRES-QLP (iterations, solution, stopping
+    reason), and against CG on the same system."""
     rng = np.random.default_rng(8)
     om = O.Model.kitaev(L) if model == "kitaev" else O.Model.toric(L)
     symm = 0.5 if model == "kitaev" else 1.0
@@ -417,12 +418,54 @@ def test_minres_solve_matches_oracle(model, L, kind, alpha):
     s.sample()
     E, Om = s.samples()
     d, F, diag = O.sr_moments(Om, E)
-    xo, ito, rno = O.minres_solve(Om, d, F, 0.9, 9e-4, 1e-2, diag, max_iterations=400, rtol=1e-12)
+    xo, ito, rno, io = O.minres_solve(Om, d, F, 0.9, 9e-4, 1e-2, diag, max_iterations=400, rtol=1e-12, info=True)
     xg, itg, rng_ = s.sr_solve(Om, d, F, np.zeros(mach.n_params), 0.9, 9e-4, 1e-2, diag)
+    ig = s.solve_info()
     assert abs(itg - ito) <= max(2, ito // 20)
     assert rel(xg, xo) < 1e-8
+    assert ig["istop"] == io["istop"] and ig["iterations"] == itg and ig["qlp"] == io["qlp"] == 0
     xc, _, _ = O.cg_solve(Om, d, F, np.zeros(mach.n_params), 0.9, 9e-4, 1e-2, diag)
     assert rel(xg, xc) < 1e-6
+
+
+def qlp_system(N, P, k, scale, seed):
+    """Random O whose last k columns are scaled by scale * (1..k): S has k
+    eigenvalues near scale^2 next to a bulk of order 1."""
+    rng = np.random.default_rng(seed)
+    Om = rng.normal(size=(N, P)) + 1j * rng.normal(size=(N, P))
+    Om[:, P - k:] *= scale * (1 + np.arange(k))
+    E = rng.normal(size=N) + 1j * rng.normal(size=N)
+    d, F, diag = O.sr_moments(Om, E)
+    return Om, d, F, diag
+
+
+@pytest.mark.parametrize("model,L,alpha,N,scale,r1", [("kitaev", 2, 1, 300, 1e-5, 0.0),
+                                                      ("toric", 4, 2, 1200, 1e-5, 0.5)])
+def test_minresqlp_qlp_phase_matches_oracle(model, L, alpha, N, scale, r1):
+    """An ill-conditioned S (four eigenvalues near scale^2 beside an O(1)
+    bulk; condition 3e10 / 7e10) in the style of debug.cpp:215-262: the
+    condition estimate passes trancond = 1e7 and the QLP updates take over,
+    on the formed S (80 parameters) and on the matrix-free operator (2144
+    parameters, multiplicative regularisation r1).  The GPU's iterations,
+    stopping reason and solution agree with the oracle's, and the solution
+    with the dense solve to cond * eps."""
+    gm = rbmnqs.Model.kitaev(L) if model == "kitaev" else rbmnqs.Model.toric(L, symmetry=1.0)
+    cfg = rbmnqs.default_config(rbm_type=0, alpha=alpha, n_chains=16, samples_per_chain=4, precision=1, solver=1)
+    s = rbmnqs.Session(gm, cfg)
+    P = s.n_params
+    Om, d, F, diag = qlp_system(N, P, 4, scale, 3)
+    xo, ito, rno, io = O.minres_solve(Om, d, F, r1, 0.0, 0.0, diag, info=True)
+    xg, itg, rsg = s.sr_solve(Om, d, F, np.zeros(P), r1, 0.0, 0.0, diag)
+    ig = s.solve_info()
+    A = Om.conj().T @ Om / N - np.outer(d.conj(), d) + np.diag(diag * r1)
+    xs = np.linalg.solve(A, F)
+    assert io["qlp"] > 0 and ig["qlp"] > 0 and ig["acond"] > 1e7, (io, ig)
+    assert ig["istop"] == io["istop"] and ig["istop"] in (4, 5), (io, ig)
+    # on these systems the count follows rounding: relative perturbations of
+    # 1e-15 in F move the oracle's own count between 232 and 268 (matrix-free case)
+    assert abs(itg - ito) <= max(3, ito // 5), (itg, ito)
+    assert rel(xg, xs) < 1e-4 and rel(xg, xo) < 1e-4
+    assert np.linalg.norm(A @ xg - F) < 1e-9 * np.linalg.norm(F)
 
 
 @pytest.mark.parametrize("precision,tol", [(1, TOL64), (0, TOL32)])

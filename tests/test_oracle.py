@@ -286,6 +286,83 @@ def test_cg_solves_regularised_system():
     assert np.allclose(S, S.conj().T, atol=1e-13)
 
 
+def qlp_system(N, P, k, s, seed):
+    """Random O whose last k columns are scaled by s (1..k): S has k
+    eigenvalues near s^2 next to a bulk of order 1."""
+    rng = np.random.default_rng(seed)
+    Om = rng.normal(size=(N, P)) + 1j * rng.normal(size=(N, P))
+    if k:
+        Om[:, P - k:] *= s * (1 + np.arange(k))
+    E = rng.normal(size=N) + 1j * rng.normal(size=N)
+    d, F, diag = O.sr_moments(Om, E)
+    return Om, d, F, diag
+
+
+def sr_operator(Om, d, diag, r1, r2, rd, n_neural, norm):
+    S = Om.conj().T @ Om / norm - np.outer(d.conj(), d)
+    f = np.where(np.arange(Om.shape[1]) < n_neural, r1, r1 + rd)
+    return S + np.diag(diag * f + diag.max() * r2)
+
+
+def test_minresqlp_solves_the_regularised_system():
+    """The system of debug.cpp:215-262 (500 parameters, 500 samples, 50
+    neural parameters, norm 0.1, d = column sums / sqrt(norm), e1 = de = e2
+    = 1, itnlim 1000): the operator is indefinite (d d^H is not the outer
+    product of the mean), which MINRES-QLP handles; it stops on the
+    relative residual, in the MINRES phase (condition about 4e4)."""
+    rng = np.random.default_rng(1)
+    Om = rng.uniform(-1, 1, (500, 500)) + 1j * rng.uniform(-1, 1, (500, 500))
+    d = Om.sum(0) / np.sqrt(0.1)
+    diag = np.sum(np.abs(Om) ** 2, 0) / 0.1 - np.abs(d) ** 2
+    F = rng.uniform(-1, 1, 500) + 1j * rng.uniform(-1, 1, 500)
+    x, it, rn, info = O.minres_solve(Om, d, F, 1.0, 1.0, 1.0, diag, n_neural=50, norm=0.1, info=True,
+                                     max_iterations=1000)
+    A = sr_operator(Om, d, diag, 1.0, 1.0, 1.0, 50, 0.1)
+    scale = np.linalg.norm(A, 2) * np.linalg.norm(x) + np.linalg.norm(F)
+    assert np.linalg.norm(A @ x - F) < 1e-14 * scale  # the relative residual MINRES-QLP bounds
+    assert info["istop"] in (4, 5) and info["qlp"] == 0 and info["acond"] < 1e7
+    assert 0 < it < 1000 and rn < 1e-14 * scale
+
+
+def test_minresqlp_switches_to_qlp_on_an_ill_conditioned_system():
+    """Four eigenvalues near 1e-10 beside an O(1) bulk (condition 3e10):
+    the condition estimate passes trancond = 1e7, the QLP updates take over
+    and the solution still agrees with the dense solve to cond * eps."""
+    Om, d, F, diag = qlp_system(300, 80, 4, 1e-5, 3)
+    x, it, rn, info = O.minres_solve(Om, d, F, 0.0, 0.0, 0.0, diag, info=True)
+    A = sr_operator(Om, d, diag, 0.0, 0.0, 0.0, 80, 300)
+    xs = np.linalg.solve(A, F)
+    assert info["qlp"] > 0 and info["acond"] > 1e7 and info["istop"] in (4, 5), info
+    assert np.linalg.norm(A @ x - F) < 1e-10 * np.linalg.norm(F)
+    assert np.linalg.norm(x - xs) < 1e-4 * np.linalg.norm(xs)
+
+
+def test_minresqlp_singular_system_gives_near_minimum_length():
+    """40 samples, 120 parameters, no regularisation: S has rank 39 and F
+    lies in its range.  MINRES-QLP solves it to rounding and its solution is
+    within 1 % of the minimum-length (pseudo-inverse) solution's norm."""
+    Om, d, F, diag = qlp_system(40, 120, 0, 1.0, 4)
+    x, it, rn, info = O.minres_solve(Om, d, F, 0.0, 0.0, 0.0, diag, info=True)
+    A = sr_operator(Om, d, diag, 0.0, 0.0, 0.0, 120, 40)
+    xp = np.linalg.pinv(A, rcond=1e-10, hermitian=True) @ F
+    assert np.linalg.norm(A @ x - F) < 1e-12 * np.linalg.norm(F)
+    assert np.linalg.norm(x) < 1.01 * np.linalg.norm(xp)
+    assert info["qlp"] > 0
+
+
+def test_minresqlp_stopping_rules():
+    """itnlim reached: istop 8 after exactly max_iterations steps; a loose
+    rtol: istop 4 (relative residual <= rtol) long before rounding level;
+    b = 0: istop 3, x = 0, no iterations."""
+    Om, d, F, diag = qlp_system(300, 80, 4, 1e-5, 3)
+    x, it, rn, info = O.minres_solve(Om, d, F, 0.0, 0.0, 0.0, diag, max_iterations=7, info=True)
+    assert it == 7 and info["istop"] == 8
+    x, it, rn, info = O.minres_solve(Om, d, F, 0.0, 0.0, 0.0, diag, rtol=1e-3, info=True)
+    assert info["istop"] == 4 and it < 40
+    x, it, rn, info = O.minres_solve(Om, d, np.zeros_like(F), 0.0, 0.0, 0.0, diag, info=True)
+    assert it == 0 and info["istop"] == 3 and not np.any(x)
+
+
 def test_decay_schedule():
     d = O.Decay(1.0, 1e-4, 0.9)
     assert abs(d.get() - 0.9) < 1e-15  # decays before first use
