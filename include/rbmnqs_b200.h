@@ -319,6 +319,19 @@ void* rbmnqs_stream(rbmnqs_handle* h);
  * (abstract_optimizer.cpp:27-54). */
 int rbmnqs_save(rbmnqs_handle* h, const char* path);
 int rbmnqs_load(rbmnqs_handle* h, const char* path);
+/* Training log, logger.cpp:31-74: opens <name>.log, appending when the file
+ * exists unless `force` (rbm.force) is set.  Every applied update (by
+ * rbmnqs_epoch, rbmnqs_optimize or a batch epoch) then appends one line with
+ * the values stochastic_reconfiguration.cpp:86-91 (gradient_descent.cpp:
+ * 47-52 for SGD) and metropolis_sampler.cpp:275-277 log: energy per spin,
+ * its standard deviation per spin and the acceptance rate (not with the
+ * full sampler), as %.16g separated by ", "; the first line after opening
+ * is the header "# Energy, Energy Stddev, AccetpanceRate" (the reference's
+ * names, "EnergyStddev" for SGD).  A step rejected as massive or
+ * non-finite writes no line, as in main.cpp:600-616.  The file is closed by
+ * rbmnqs_log_close or rbmnqs_destroy. */
+int rbmnqs_log_open(rbmnqs_handle* h, const char* name, int32_t force);
+int rbmnqs_log_close(rbmnqs_handle* h);
 /* SR updates applied so far, counting the config's n_updates offset */
 int rbmnqs_n_updates(const rbmnqs_handle* h, int64_t* n_updates);
 

@@ -345,6 +345,14 @@ struct rbmnqs_handle {
     bool sampled = false;
     int64_t n_updates = 0;  // rbm_base::n_updates_ (offset + applied SR updates)
     rbmnqs::CgResultDev last_solve{};  // the last SR solve's result (rbmnqs_solve_info)
+    // training log <name>.log (rbmnqs_log_open): one line per applied update
+    struct LogFile {
+        FILE* f = nullptr;
+        bool first = true;  // the header line precedes the first line written
+        ~LogFile() {
+            if (f) fclose(f);
+        }
+    } log;
 
     cudaGraphExec_t graph = nullptr;
     int graph_kernels = 0;
@@ -1311,6 +1319,26 @@ static int count_kernel_nodes(cudaGraph_t g) {
     return k;
 }
 
+// One line of the training log (logger.cpp:53-74 with the values that
+// stochastic_reconfiguration.cpp:86-91 / gradient_descent.cpp:47-52 and
+// metropolis_sampler.cpp:275-277 log): energy per spin, its standard
+// deviation per spin and, for Metropolis sampling, the acceptance rate,
+// written as %.16g (ostream precision 16) separated by ", ", after a header
+// "# <names>" on the first line a handle writes.
+static void write_log_line(rbmnqs_handle* h, const rbmnqs::EpochStatsDev& s) {
+    FILE* f = h->log.f;
+    const bool sgd = h->cfg.optimizer_type == 1;
+    if (h->log.first) {
+        std::fprintf(f, "# Energy, %s%s\n", sgd ? "EnergyStddev" : "Energy Stddev", h->full ? "" : ", AccetpanceRate");
+        h->log.first = false;
+    }
+    const double n = h->n;
+    std::fprintf(f, "%.16g, %.16g", s.energy.x / n, s.stddev / n);
+    if (!h->full) std::fprintf(f, ", %.16g", s.acceptance);
+    std::fprintf(f, "\n");
+    std::fflush(f);
+}
+
 // Sample statistics (s) and SR statistics (o) of the last sample / optimize
 // step: the device results are copied into pinned host memory and read after
 // one stream synchronisation.  With sr, a successful step counts as an update.
@@ -1359,6 +1387,7 @@ static void readback(rbmnqs_handle* h, bool sample, rbmnqs_sample_stats* out, bo
         const auto& r = rb->cg;
         h->last_solve = r;
         if (r.status == 0) h->n_updates++;
+        if (r.status == 0 && h->log.f) write_log_line(h, rb->stats);
         if (o) {
             o->iterations = r.iterations;
             o->status = r.status;
@@ -1637,6 +1666,29 @@ int rbmnqs_sr_solve(rbmnqs_handle* h, const double* O, int32_t N, const double* 
         h->last_solve = r;
         if (iterations) *iterations = r.iterations;
         if (residual) *residual = r.residual;
+    });
+}
+
+int rbmnqs_log_open(rbmnqs_handle* h, const char* name, int32_t force) {
+    return guard([&] {
+        require(h != nullptr && name != nullptr && name[0] != 0, "null handle or empty name");
+        if (h->log.f) fclose(h->log.f);
+        h->log.f = nullptr;
+        const std::string fn = std::string(name) + ".log";
+        FILE* probe = std::fopen(fn.c_str(), "r");
+        const bool exists = probe != nullptr;
+        if (probe) fclose(probe);
+        h->log.f = std::fopen(fn.c_str(), exists && !force ? "a" : "w");
+        require(h->log.f != nullptr, "cannot open " + fn);
+        h->log.first = true;
+    });
+}
+
+int rbmnqs_log_close(rbmnqs_handle* h) {
+    return guard([&] {
+        require(h != nullptr, "null handle");
+        if (h->log.f) fclose(h->log.f);
+        h->log.f = nullptr;
     });
 }
 

@@ -108,6 +108,8 @@ def _declare(L):
         "rbmnqs_sr_solve": [VP, P_D, C.c_int32, P_D, C.c_double, P_D, P_D, C.c_double, C.c_double, C.c_double,
                             P_D, P_I, P_D],
         "rbmnqs_solve_info": [VP, P_I, P_D, P_I, P_D, P_I],
+        "rbmnqs_log_open": [VP, C.c_char_p, C.c_int32],
+        "rbmnqs_log_close": [VP],
         "rbmnqs_full_sample": [VP, P_D, P_D, P_D],
         "rbmnqs_get_observables": [VP, P_D],
         "rbmnqs_full_state": [VP, P_D],
@@ -413,6 +415,14 @@ class Session:
                                   _p(x.view(np.float64), P_D), r1, r2, rd, _p(diag, P_D), C.byref(it),
                                   C.byref(rs)))
         return x, it.value, rs.value
+
+    def log_open(self, name, force=False):
+        """Training log <name>.log (logger.cpp:31-74): one line per applied
+        update, appended to an existing file unless force."""
+        _ck(lib().rbmnqs_log_open(self._h, str(name).encode(), int(bool(force))))
+
+    def log_close(self):
+        _ck(lib().rbmnqs_log_close(self._h))
 
     def solve_info(self):
         """The last SR solve's outcome (minresqlp_adapter getItn / getRnorm /
