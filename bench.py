@@ -105,6 +105,10 @@ def parse():
     ap.add_argument("--cpu-baseline", type=int, default=1, help="time the CPU restatement beside our arm")
     ap.add_argument("--chains", type=int, default=0, help="override the workload's chain count (profiling)")
     ap.add_argument("--sweeps", type=int, default=0, help="override the sweeps per epoch (profiling)")
+    ap.add_argument("--forms", default="learned,plain_fp32,plain_fp64",
+                    help="forms of the 128-spin workload to run (profiling runs a subset; the metric line needs all)")
+    ap.add_argument("--profile-region", type=int, default=0,
+                    help="bracket each form's timed epochs with cudaProfilerStart/Stop (ncu --profile-from-start off)")
     return ap.parse_args()
 
 
@@ -462,9 +466,10 @@ def train_checkpoint(wl, model, epochs, seed, path):
             "energy_per_site_last50": float(np.mean(es[-50:])), "seconds": time.perf_counter() - t0}
 
 
-def time_form(sess, graph, steps, warmup, l2_flush, stream, clk=None):
+def time_form(sess, graph, steps, warmup, l2_flush, stream, clk=None, profile=False):
     """Warm-up epochs, then `steps` epochs timed with CUDA events on the
-    session's stream (L2 flushed between epochs, outside the events)."""
+    session's stream (L2 flushed between epochs, outside the events);
+    `profile` brackets the timed epochs with cudaProfilerStart/Stop."""
     import torch
     for _ in range(max(1, warmup)):
         sess.epoch() if graph else (sess.sample(), sess.optimize())
@@ -476,6 +481,8 @@ def time_form(sess, graph, steps, warmup, l2_flush, stream, clk=None):
     stats = []
     torch.cuda.synchronize()
     ctx = clk if clk is not None else _Null()
+    if profile:
+        torch.cuda.profiler.start()
     with ctx:
         for k in range(steps):
             l2_flush()
@@ -488,6 +495,8 @@ def time_form(sess, graph, steps, warmup, l2_flush, stream, clk=None):
             ev[k][1].record(stream)
             stats.append((st, sr))
         torch.cuda.synchronize()
+    if profile:
+        torch.cuda.profiler.stop()
     t_ms = [a.elapsed_time(b) for a, b in ev]
     ms, cnt = sess.timing()
     return t_ms, stats, [float(m / max(1, c)) for m, c in zip(ms, cnt)]
@@ -542,21 +551,35 @@ def run_forms(args, rank, world, local):
         s.load(ckpt)
         return s
 
-    out = {}
-    # learned form: the headline number, clocks sampled in its timed region
-    learned = session("learned")
-    lstream = torch.cuda.ExternalStream(learned.stream())
-
     def flush_on(stream):
         def f():
             with torch.cuda.stream(stream):
                 flush.zero_()
         return f
 
+    out = {}
+    forms = [f for f in args.forms.split(",") if f]
+    if sorted(forms) != sorted(["learned", "plain_fp32", "plain_fp64"]):
+        # a subset of the forms (profiling): each timed alone, no metric line
+        for form in forms:
+            s = session(form)
+            st = torch.cuda.ExternalStream(s.stream())
+            graph = form != "plain_fp64"
+            t_ms, stats, stage = time_form(s, graph, args.steps, args.warmup, flush_on(st), st,
+                                           profile=bool(args.profile_region))
+            out[form] = form_summary(s.N, n, t_ms, stats, stage)
+            out[form]["graph_kernels"] = s.graph_kernels() if graph else None
+            del s
+        return {"workload": args.workload, "forms_only": out, "checkpoint": train} if rank == 0 else None
+    # learned form: the headline number, clocks sampled in its timed region
+    learned = session("learned")
+    lstream = torch.cuda.ExternalStream(learned.stream())
+
     if world > 1:
         dist.barrier()
     clk = ClockSampler(local)
-    t_ms, stats, stage = time_form(learned, True, args.steps, args.warmup, flush_on(lstream), lstream, clk)
+    t_ms, stats, stage = time_form(learned, True, args.steps, args.warmup, flush_on(lstream), lstream, clk,
+                                   profile=bool(args.profile_region))
     clocks = clk.summary()
     t_learned_ms = float(np.sum(t_ms))
     out["learned"] = form_summary(learned.N, n, t_ms, stats, stage)
@@ -584,7 +607,8 @@ def run_forms(args, rank, world, local):
     # plain forms
     p32 = session("plain_fp32")
     s32 = torch.cuda.ExternalStream(p32.stream())
-    t_ms, stats, stage = time_form(p32, True, args.steps, args.warmup, flush_on(s32), s32)
+    t_ms, stats, stage = time_form(p32, True, args.steps, args.warmup, flush_on(s32), s32,
+                                   profile=bool(args.profile_region))
     out["plain_fp32"] = form_summary(p32.N, n, t_ms, stats, stage)
     del p32
     p64 = session("plain_fp64")

@@ -325,6 +325,9 @@ struct rbmnqs_handle {
     DevBuf<int> lmv;
     DevBuf<float> lqfw, lloss, ltgt;
     DevBuf<double> lrate;
+    // FP32 theta of each chain [n_chains][padded T]: handed from the sweep
+    // kernel (or the theta kernel) to the learned moves
+    DevBuf<float2> lth;
     // move dictionary: flip masks [D][4], flip lists [D][2]; training batch
     int n_moves = 0, train_batch = 0;
     DevBuf<uint32_t> dmask, dflip;
@@ -519,11 +522,21 @@ struct rbmnqs_handle {
             ck(rbmnqs::launch_sampler(a, fp64, shape, st), "sampler kernel");
         }
         rbmnqs::LearnedArgs l = learned_args();
+        // theta of the current configurations for the moves: from the sweep
+        // kernel when its path writes it, else (no sweeps) from the theta
+        // kernel once per sample; the moves keep it current
+        const bool sweep_theta = cfg.step > 0 && rbmnqs::sampler_writes_theta(machine(), fp64, shape);
+        if (!fp64 && (sweep_theta || cfg.step == 0)) {
+            a.theta_out = lth.p;
+            l.theta = lth.p;
+        }
         for (int j = 0; j < cfg.samples_per_chain; j++) {
             if (cfg.step > 0) {
                 a.sweep0 = cfg.warmup + j * cfg.step;
                 a.nsweeps = cfg.step;
                 ck(rbmnqs::launch_sampler(a, fp64, shape, st), "sampler kernel");
+            } else if (l.theta && cfg.learned_steps > 0) {
+                ck(rbmnqs::launch_learned_theta(l, st), "learned theta");
             }
             for (int k = 0; k < cfg.learned_steps; k++) {
                 l.move = (uint32_t)(j * cfg.learned_steps + k);
@@ -1227,6 +1240,7 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
             h->lacc.alloc(cfg->n_chains);
             h->ltry.alloc(cfg->n_chains);
             h->ltgt.alloc((size_t)h->train_batch * h->n_moves);
+            h->lth.alloc((size_t)cfg->n_chains * 32 * rbmnqs::elements_per_lane(h->T));
             h->lloss.alloc(1);
             h->lrate.alloc(1);
             ck(cudaMemsetAsync(h->lloss.p, 0, sizeof(float), h->st), "memset");

@@ -629,6 +629,14 @@ __device__ __forceinline__ int sample_slot(const SamplerArgs& a, int st) {
     return (sg - a.warmup) / a.step;
 }
 
+// theta_out[chain][lane + 32 e] = th[e] (coalesced per e)
+template <int E>
+__device__ __forceinline__ void store_theta(float2* out, int chain, int lane, const float2 (&th)[E]) {
+    float2* dst = out + (size_t)chain * (32 * E) + lane;
+#pragma unroll
+    for (int e = 0; e < E; e++) dst[32 * e] = th[e];
+}
+
 __device__ __forceinline__ void chain_finish(const SamplerArgs& a, int chain, int lane, const uint32_t sp[4],
                                              uint32_t nacc, uint32_t prop) {
     if (lane < 4) a.spins[4 * chain + lane] = spin_word(sp, lane);
@@ -987,6 +995,7 @@ __device__ __forceinline__ void run_chain_fast(const SamplerArgs& a, const Smem&
             if (lane < 4) a.samples[4 * idx + lane] = spin_word(sp, lane);
         }
     }
+    if (a.theta_out) store_theta<E>(a.theta_out, chain, lane, th);
     chain_finish(a, chain, lane, sp, nacc, prop);
 }
 
@@ -1280,6 +1289,7 @@ __device__ __forceinline__ void run_chain_gather(const SamplerArgs& a, const Sme
             if (lane < 4) a.samples[4 * idx + lane] = spin_word(sp, lane);
         }
     }
+    if (a.theta_out) store_theta<E>(a.theta_out, chain, lane, th);
     chain_finish(a, chain, lane, sp, nacc, prop);
 }
 
@@ -1672,13 +1682,13 @@ __device__ __forceinline__ void learned_theta(const MachineDev& m, const LearnTa
 }
 
 // Re log psi(s with the move's flips)/psi(s): lane partial of the ln|cosh|
-// difference (sum with sweep_sum) plus, on lane 0, the visible bias.
+// difference (sum with sweep_sum) plus, on lane 0, the visible bias; tp
+// receives theta of the moved configuration.
 template <int E>
 __device__ __forceinline__ float move_partial(const MachineDev& m, const LearnTabs& L, const LaneEnt<E>& le,
                                               const float2 (&th)[E], float s0, const uint32_t (&sp)[4], uint32_t fw0,
-                                              uint32_t fw1, int lane) {
+                                              uint32_t fw1, int lane, float2 (&tp)[E]) {
     const int nf = (fw1 >> 16) & 0xff;
-    float2 tp[E];
 #pragma unroll
     for (int e = 0; e < E; e++) tp[e] = th[e];
     float bias = 0.f;
@@ -1714,15 +1724,25 @@ __global__ void __launch_bounds__(256) learned_accept(const LearnedArgs a, int s
         uint32_t sp[4];
 #pragma unroll
         for (int w = 0; w < 4; w++) sp[w] = a.spins[4 * c + w];
-        float2 th[E];
-        learned_theta<E>(a.m, L, le, sp, lane, th);
+        float2 th[E], tp[E];
+        float2* tc = a.theta ? a.theta + (size_t)c * (32 * E) + lane : nullptr;
+        if (tc) {
+#pragma unroll
+            for (int e = 0; e < E; e++) th[e] = tc[32 * e];
+        } else {
+            learned_theta<E>(a.m, L, le, sp, lane, th);
+        }
         const float s0 = lnc_sweep_sum<E>(th);
         const float d =
-            sweep_sum(move_partial<E>(a.m, L, le, th, s0, sp, a.mflip[2 * mv], a.mflip[2 * mv + 1], lane));
+            sweep_sum(move_partial<E>(a.m, L, le, th, s0, sp, a.mflip[2 * mv], a.mflip[2 * mv + 1], lane, tp));
         const uint4 r = philox4x32(make_uint4(a.move, epoch, (uint32_t)c, 4), key);
         // accept with min(1, |psi'/psi|^2 q(m|s') / q(m|s))
         const bool acc = __logf(unit24<float>(r.x) + 0x1p-25f) < 2.f * d + qrev - a.qfw[c];
         if (lane < 4 && acc) a.spins[4 * c + lane] = a.prop[4 * c + lane];
+        if (tc && acc) {
+#pragma unroll
+            for (int e = 0; e < E; e++) tc[32 * e] = tp[e];
+        }
         if (lane == 0) {
             a.n_acc[c] += acc ? 1u : 0u;
             a.n_try[c] += 1u;
@@ -1753,8 +1773,9 @@ __global__ void __launch_bounds__(256) learned_targets(const LearnedArgs a, int 
 #pragma unroll
         for (int i = 0; i < 8; i++) lg[i] = -INFINITY;
         for (int mv = 0; mv < D; mv++) {
+            float2 tp[E];
             const float d =
-                sweep_sum(move_partial<E>(a.m, L, le, th, s0, sp, a.mflip[2 * mv], a.mflip[2 * mv + 1], lane));
+                sweep_sum(move_partial<E>(a.m, L, le, th, s0, sp, a.mflip[2 * mv], a.mflip[2 * mv + 1], lane, tp));
 #pragma unroll
             for (int i = 0; i < 8; i++)
                 if (mv == lane + 32 * i) lg[i] = fminf(0.f, 2.f * d);
@@ -1770,6 +1791,28 @@ __global__ void __launch_bounds__(256) learned_targets(const LearnedArgs a, int 
 #pragma unroll
         for (int i = 0; i < 8; i++)
             if (lane + 32 * i < D) a.targets[(size_t)b * D + lane + 32 * i] = __expf(lg[i] - mx) / se;
+    }
+}
+
+// theta of every chain's configuration into a.theta (FP64 recompute,
+// rounded to FP32): the starting point of learned moves that run without a
+// sweep before them.
+template <int E>
+__global__ void __launch_bounds__(256) learned_theta_init(const LearnedArgs a, int smem_w) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const LearnTabs L = learned_tables(a.m, smem, smem_w);
+    const int lane = threadIdx.x & 31;
+    const LaneEnt<E> le(a.m, lane);
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < a.n_chains; c += nw) {
+        uint32_t sp[4];
+#pragma unroll
+        for (int w = 0; w < 4; w++) sp[w] = a.spins[4 * c + w];
+        float2 th[E];
+        learned_theta<E>(a.m, L, le, sp, lane, th);
+        float2* tc = a.theta + (size_t)c * (32 * E) + lane;
+#pragma unroll
+        for (int e = 0; e < E; e++) tc[32 * e] = th[e];
     }
 }
 
@@ -1838,8 +1881,9 @@ static cudaError_t launch_learned_kernel(const LearnedArgs& a, int which, int ro
     const int smem = learned_smem_bytes(a.m, smem_w);
     const void* fn = nullptr;
 #define RBMNQS_LK(E)                                                                                 \
-    fn = which == 0 ? reinterpret_cast<const void*>(learned_accept<E>)                            \
-                    : reinterpret_cast<const void*>(learned_targets<E>);
+    fn = which == 0   ? reinterpret_cast<const void*>(learned_accept<E>)                          \
+         : which == 1 ? reinterpret_cast<const void*>(learned_targets<E>)                         \
+                      : reinterpret_cast<const void*>(learned_theta_init<E>);
     switch (elements_per_lane(a.m.T)) {
         case 1: RBMNQS_LK(1) break;
         case 2: RBMNQS_LK(2) break;
@@ -1869,6 +1913,11 @@ cudaError_t launch_learned_targets(const LearnedArgs& a, cudaStream_t st) {
     if (a.B <= 0) return cudaSuccess;
     if (a.n_moves > 256) return cudaErrorInvalidValue;
     return launch_learned_kernel(a, 1, a.B, st);
+}
+
+cudaError_t launch_learned_theta(const LearnedArgs& a, cudaStream_t st) {
+    if (!a.theta) return cudaErrorInvalidValue;
+    return launch_learned_kernel(a, 2, a.n_chains, st);
 }
 
 cudaError_t launch_record(const uint32_t* spins, int n_chains, int spc, int j, uint32_t* samples, cudaStream_t st) {
@@ -2057,6 +2106,12 @@ cudaError_t ensure_dynamic_smem(const void* fn, int bytes) {
     const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess) cur = bytes;
     return e;
+}
+
+// The FP32 expanded-table (one chain per warp) and gather paths store
+// theta_out; the FP64, Pfaffian and two-chain paths do not.
+bool sampler_writes_theta(const MachineDev& m, int fp64, const SamplerShape& sh) {
+    return !fp64 && m.pf.n == 0 && !sh.plan.pair && (sh.plan.use_u || sh.plan.gather);
 }
 
 cudaError_t launch_sampler(const SamplerArgs& a0, int fp64, const SamplerShape& sh, cudaStream_t st) {

@@ -83,6 +83,11 @@ struct SamplerArgs {
     // all), recording samples only when record != 0; chains start fresh only
     // in the segment at sweep 0, and the counters accumulate over segments
     int sweep0 = 0, nsweeps = 0, record = 1;
+    // [n_chains][padded T] FP32 theta of each chain's final configuration
+    // (after the launch's last FP64 recompute), entry t of chain c at
+    // c * padded T + t; written only by the FP32 table and gather paths
+    // (sampler_writes_theta), null: not written
+    float2* theta_out = nullptr;
 };
 
 // The Hamiltonian regrouped by transition for the FP32 evaluation kernel
@@ -151,10 +156,16 @@ struct LearnedArgs {
     float eps;              // uniform part of the proposal
     float* targets;         // [B][D] training targets (targets kernel)
     int B;
+    // [n_chains][padded T] FP32 theta of spins, kept current by accept (an
+    // accepted move stores its theta'); null: accept recomputes theta from
+    // the configuration in FP64
+    float2* theta = nullptr;
 };
 cudaError_t launch_learned_propose(const LearnedArgs& a, cudaStream_t st);
 cudaError_t launch_learned_accept(const LearnedArgs& a, cudaStream_t st);
 cudaError_t launch_learned_targets(const LearnedArgs& a, cudaStream_t st);
+// a.theta <- FP32 theta of a.spins (FP64 recompute from the configuration)
+cudaError_t launch_learned_theta(const LearnedArgs& a, cudaStream_t st);
 // chains from Philox stream 1 (as the sweep kernel's fresh start) when ctl[1] is set
 cudaError_t launch_init_chains(uint32_t* spins, int n, int n_chains, const uint32_t* ctl, uint64_t seed,
                                cudaStream_t st);
@@ -182,6 +193,8 @@ struct SamplerShape {
 cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bonds, SamplerShape* out,
                          int max_wpb = 0, int pair_mode = -1);
 cudaError_t launch_sampler(const SamplerArgs& a, int fp64, const SamplerShape& shape, cudaStream_t st);
+// whether the sweep path of this shape writes SamplerArgs::theta_out
+bool sampler_writes_theta(const MachineDev& m, int fp64, const SamplerShape& shape);
 cudaError_t launch_eval(const EvalArgs& a, int fp64, int warps_per_block, cudaStream_t st);
 // The FP32 evaluation kernel (E_loc and O_k from the term table, no Pfaffian
 // factor).  cudaErrorNotSupported when the machine or the table does not fit

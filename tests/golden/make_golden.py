@@ -1,7 +1,7 @@
 """Generate tests/golden/reference_golden.json from the reference's own files.
 
-Run once in a container that has the reference checkout (path given as the
-first argument, default /root/reference).  The GPU tests and the CPU suite
+Run once in a container that has the reference checkout; its path is the
+required first argument (``python make_golden.py <reference checkout>``).  The GPU tests and the CPU suite
 only read the committed JSON; nothing at test time reads the reference.
 
 Pins extracted (all produced by the reference project itself):
@@ -95,4 +95,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path of the rbm-nqs reference checkout>")
+    main(sys.argv[1])
