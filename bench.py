@@ -380,6 +380,8 @@ def run_batch(args, rank, world, local):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    if args.profile_region:
+        torch.cuda.profiler.start()
     with ClockSampler(local) as clk:
         for k in range(args.steps):
             with torch.cuda.stream(stream):
@@ -389,6 +391,8 @@ def run_batch(args, rank, world, local):
             ev[k][1].record(stream)
             neff += sum(s.N / (1.0 + 2.0 * x["tau"]) for s, x in zip(sessions, st))
         torch.cuda.synchronize()
+    if args.profile_region:
+        torch.cuda.profiler.stop()
     t_ms = sum(a.elapsed_time(b) for a, b in ev)
     # end to end: every session's weights in and out through the C ABI, each step
     ws = [s.get_weights() for s in sessions]

@@ -314,6 +314,15 @@ struct rbmnqs_handle {
     bool coop_dense = false;  // formed S too large for the cluster CG: cooperative grid CG
     rbmnqs::MfreePlan mfp{};
     rbmnqs::MfreeWork mfw{};
+    // matrix-free CG (solver 0) by the multi-system kernel: this session's
+    // descriptor, its tile partial sums and grid size; a batch merges the
+    // descriptors of its sessions into one launch
+    bool multi_cg = false;
+    DevBuf<rbmnqs::CgMultiProb> cgm;
+    DevBuf<double2> cgm_t2;
+    DevBuf<double> cgm_t1;
+    rbmnqs::CgMultiScratch cgms{};
+    int cgm_blocks = 0;
     DevBuf<unsigned char> mfbuf;
     // evaluation-mode observables, their per-sample values and statistics
     std::vector<std::unique_ptr<ObsDev>> obs;
@@ -630,6 +639,52 @@ struct rbmnqs_handle {
         ck(rbmnqs::launch_unpack(params.p, n, n_vb, nh, vb.p, hb.p, W64.p, W32.p, st), "unpack");
         mark(6);
     }
+    // the CG limits of cg_solver.cpp:260-334 (cg1)
+    int cg_max_it() const {
+        const int m = std::min(2 * P, cfg.max_iterations);
+        return m == 0 ? 2 * P : m;
+    }
+    double cg_rtol() const { return cfg.rtol == 0 ? 1e-16 : cfg.rtol; }
+    // this session's system for the multi-system matrix-free CG
+    rbmnqs::CgMultiProb cg_prob() const {
+        rbmnqs::CgMultiProb p{};
+        p.O = O.p;
+        p.d = full ? dzero.p : d.p;
+        p.F = F.p;
+        p.x = x.p;
+        p.diag = diag.p;
+        p.max_diag = maxdiag.p;
+        p.sch = sched.p;
+        p.res = cgres.p;
+        p.r = mfw.r;
+        p.p0 = mfw.p;
+        p.p1 = mfw.R1;
+        p.Ap = mfw.Ap;
+        p.v = mfw.tmpN;
+        p.norm = (double)N;
+        p.rtol = cg_rtol();
+        p.N = N;
+        p.P = P;
+        p.n_neural = P_neural;
+        p.max_it = cg_max_it();
+        return p;
+    }
+    // a batch solves this session's system in its merged launch: the SR
+    // step (not SGD, not the two solves of Heun) by matrix-free CG
+    bool batch_cg() const { return multi_cg && cfg.plugin != 3 && cfg.optimizer_type == 0 && !full; }
+    // the SR step around a solve that the batch launches: schedules and
+    // var(O) before it, the update after it
+    void enqueue_optimize_pre() {
+        ck(rbmnqs::launch_schedule(sched.p, st), "schedule");
+        ck(rbmnqs::launch_var_diag(O.p, fp64, d.p, N, P, mfp, mfw, diag.p, maxdiag.p, st, nullptr), "var diag");
+        mark(4);
+    }
+    void enqueue_optimize_post() {
+        mark(5);
+        ck(rbmnqs::launch_update(params.p, x.p, P, sched.p, cgres.p, plug.p, st), "update");
+        ck(rbmnqs::launch_unpack(params.p, n, n_vb, nh, vb.p, hb.p, W64.p, W32.p, st), "unpack");
+        mark(6);
+    }
     // solves that are cooperative launches (ordered one after another in a batch graph)
     bool coop_solve() const { return mfree || coop_dense || cfg.solver == 2; }
     // the step direction x: SR solve (warm start x) or the SGD gradient
@@ -662,9 +717,12 @@ struct rbmnqs_handle {
             ck(rbmnqs::launch_var_diag(O.p, fp64, dS, N, P, mfp, mfw, diag.p, maxdiag.p, st, vf), "var diag");
             mk(4);
             if (cg_after) ck(cudaStreamWaitEvent(st, cg_after, 0), "cg order");
-            ck(rbmnqs::launch_cg_mfree(O.p, fp64, dS, (double)N, N, P, P_neural, F.p, x.p, diag.p, maxdiag.p,
-                                       sched.p, 0, 0, 0, max_it, rtol, mfp, mfw, cgres.p, st),
-               "matrix-free cg");
+            if (multi_cg)
+                ck(rbmnqs::launch_cg_multi(cgm.p, 1, fp64, cgms, cgm_blocks, st), "matrix-free cg");
+            else
+                ck(rbmnqs::launch_cg_mfree(O.p, fp64, dS, (double)N, N, P, P_neural, F.p, x.p, diag.p, maxdiag.p,
+                                           sched.p, 0, 0, 0, max_it, rtol, mfp, mfw, cgres.p, st),
+                   "matrix-free cg");
             if (cg_done) ck(cudaEventRecord(cg_done, st), "cg order");
             mk(5);
         } else {
@@ -1133,6 +1191,7 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         h->maxdiag.alloc(1);
         h->sched.alloc(1);
         h->cgres.alloc(1);
+        h->multi_cg = h->mfree && cfg->solver == 0;
         {
             require(cfg->optimizer_type == 0 || cfg->optimizer_type == 1, "optimizer.type must be 0 (SR) or 1 (SGD)");
             require(cfg->plugin >= 0 && cfg->plugin <= 3,
@@ -1259,6 +1318,22 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
             const rbmnqs::SmemPlan pl = h->eval_plan();
             while (h->wpb > 1 && rbmnqs::eval_smem_bytes(h->machine(), h->fp64, h->wpb, pl) > 200 * 1024)
                 h->wpb >>= 1;
+        }
+        if (h->multi_cg) {
+            rbmnqs::CgMultiProb pr = h->cg_prob();
+            long long rc = 0, tc = 0;
+            const int tiles = rbmnqs::cg_multi_units(&pr, 1, &rc, &tc);
+            h->cgm.alloc(1);
+            h->cgm_t2.alloc(2 * (size_t)tiles);
+            h->cgm_t1.alloc(tiles);
+            ck(cudaMemcpyAsync(h->cgm.p, &pr, sizeof(pr), cudaMemcpyHostToDevice, h->st), "copy");
+            h->cgms.tdb = h->cgm_t2.p;
+            h->cgms.tpap = h->cgm_t2.p + tiles;
+            h->cgms.trs = h->cgm_t1.p;
+            h->cgms.sync = h->mfw.sync;
+            h->cgms.row_cost = rc;
+            h->cgms.tile_cost = tc;
+            ck(rbmnqs::cg_multi_blocks(&h->cgm_blocks), "multi-system CG plan");
         }
         ck(cudaStreamSynchronize(h->st), "sync");
         *out = h.release();
@@ -2026,17 +2101,30 @@ int rbmnqs_get_sweep_shape(rbmnqs_handle* h, int32_t* warps_per_block, int32_t* 
 struct rbmnqs_batch {
     std::vector<rbmnqs_handle*> hs;
     cudaStream_t st = nullptr;
-    cudaEvent_t fork = nullptr;
-    std::vector<cudaEvent_t> joins, cg_done;
+    cudaEvent_t fork = nullptr, solved = nullptr;
+    std::vector<cudaEvent_t> joins, cg_done, joins2;
     cudaGraphExec_t graph = nullptr;
     int graph_kernels = 0;
+    // sessions whose matrix-free CG runs in the merged multi-system launches
+    // (one launch per precision and per kCgMultiMax systems)
+    std::vector<char> merged;
+    struct Group {
+        int fp64, nprob;
+        DevBuf<rbmnqs::CgMultiProb> probs;
+        DevBuf<double2> t2;
+        DevBuf<double> t1;
+        DevBuf<rbmnqs::MfreeSync> sync;
+        rbmnqs::CgMultiScratch sc{};
+    };
+    std::vector<std::unique_ptr<Group>> groups;
+    int cg_blocks = 0;
     ~rbmnqs_batch() {
         if (graph) cudaGraphExecDestroy(graph);
-        for (auto e : joins)
-            if (e) cudaEventDestroy(e);
-        for (auto e : cg_done)
-            if (e) cudaEventDestroy(e);
+        for (auto* v : {&joins, &cg_done, &joins2})
+            for (auto e : *v)
+                if (e) cudaEventDestroy(e);
         if (fork) cudaEventDestroy(fork);
+        if (solved) cudaEventDestroy(solved);
         if (st) cudaStreamDestroy(st);
     }
 };
@@ -2055,10 +2143,50 @@ int rbmnqs_batch_create(rbmnqs_handle* const* sessions, int32_t n, rbmnqs_batch*
         }
         ck(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking), "stream");
         ck(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming), "event");
+        ck(cudaEventCreateWithFlags(&b->solved, cudaEventDisableTiming), "event");
         b->joins.resize(n, nullptr);
         b->cg_done.resize(n, nullptr);
+        b->joins2.resize(n, nullptr);
         for (auto& e : b->joins) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
         for (auto& e : b->cg_done) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+        for (auto& e : b->joins2) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+        // matrix-free CG systems of the same precision share launches when
+        // there are at least two of them
+        b->merged.assign(n, 0);
+        for (int fp = 0; fp < 2; fp++) {
+            std::vector<int> idx;
+            for (int i = 0; i < n; i++)
+                if (b->hs[i]->batch_cg() && b->hs[i]->fp64 == fp) idx.push_back(i);
+            if (idx.size() < 2) continue;
+            for (size_t g0 = 0; g0 < idx.size(); g0 += rbmnqs::kCgMultiMax) {
+                auto g = std::make_unique<rbmnqs_batch::Group>();
+                std::vector<rbmnqs::CgMultiProb> pr;
+                for (size_t k = g0; k < std::min(idx.size(), g0 + rbmnqs::kCgMultiMax); k++) {
+                    pr.push_back(b->hs[idx[k]]->cg_prob());
+                    b->merged[idx[k]] = 1;
+                }
+                g->fp64 = fp;
+                g->nprob = (int)pr.size();
+                long long rc = 0, tc = 0;
+                const int tiles = rbmnqs::cg_multi_units(pr.data(), g->nprob, &rc, &tc);
+                g->probs.alloc(pr.size());
+                g->t2.alloc(2 * (size_t)tiles);
+                g->t1.alloc(tiles);
+                g->sync.alloc(1);
+                ck(cudaMemcpyAsync(g->probs.p, pr.data(), pr.size() * sizeof(rbmnqs::CgMultiProb),
+                                   cudaMemcpyHostToDevice, b->st),
+                   "copy");
+                g->sc.tdb = g->t2.p;
+                g->sc.tpap = g->t2.p + tiles;
+                g->sc.trs = g->t1.p;
+                g->sc.sync = g->sync.p;
+                g->sc.row_cost = rc;
+                g->sc.tile_cost = tc;
+                b->groups.push_back(std::move(g));
+            }
+        }
+        if (!b->groups.empty()) ck(rbmnqs::cg_multi_blocks(&b->cg_blocks), "multi-system CG plan");
+        ck(cudaStreamSynchronize(b->st), "sync");
         *out = b.release();
     });
 }
@@ -2072,12 +2200,14 @@ int rbmnqs_batch_epoch(rbmnqs_batch* b, rbmnqs_sample_stats* s, rbmnqs_sr_stats*
             ck(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal), "capture");
             try {
                 ck(cudaEventRecord(b->fork, b->st), "fork");
-                cudaEvent_t prev_cg = nullptr;  // matrix-free solves run one after another
+                cudaEvent_t prev_cg = nullptr;  // cooperative solves run one after another
                 for (size_t i = 0; i < b->hs.size(); i++) {
                     rbmnqs_handle* h = b->hs[i];
                     ck(cudaStreamWaitEvent(h->st, b->fork, 0), "fork wait");
                     h->enqueue_sample();
-                    if (h->coop_solve()) {
+                    if (b->merged[i]) {
+                        h->enqueue_optimize_pre();
+                    } else if (h->coop_solve()) {
                         h->enqueue_optimize(prev_cg, b->cg_done[i]);
                         prev_cg = b->cg_done[i];
                     } else {
@@ -2085,6 +2215,23 @@ int rbmnqs_batch_epoch(rbmnqs_batch* b, rbmnqs_sample_stats* s, rbmnqs_sr_stats*
                     }
                     ck(cudaEventRecord(b->joins[i], h->st), "join");
                     ck(cudaStreamWaitEvent(b->st, b->joins[i], 0), "join wait");
+                }
+                if (!b->groups.empty()) {
+                    // the merged matrix-free solves, after every session's
+                    // sample and var(O) (and after the other cooperative
+                    // solves), then each merged session's update
+                    for (auto& g : b->groups)
+                        ck(rbmnqs::launch_cg_multi(g->probs.p, g->nprob, g->fp64, g->sc, b->cg_blocks, b->st),
+                           "matrix-free cg");
+                    ck(cudaEventRecord(b->solved, b->st), "solved");
+                    for (size_t i = 0; i < b->hs.size(); i++) {
+                        if (!b->merged[i]) continue;
+                        rbmnqs_handle* h = b->hs[i];
+                        ck(cudaStreamWaitEvent(h->st, b->solved, 0), "solved wait");
+                        h->enqueue_optimize_post();
+                        ck(cudaEventRecord(b->joins2[i], h->st), "join");
+                        ck(cudaStreamWaitEvent(b->st, b->joins2[i], 0), "join wait");
+                    }
                 }
             } catch (...) {
                 cudaStreamEndCapture(b->st, &g);

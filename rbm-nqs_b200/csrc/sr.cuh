@@ -156,6 +156,42 @@ struct MfreeWork {
     MfreeSync* sync;
     int nseg, lseg;
 };
+// Several matrix-free CG systems (cg1 semantics) in one cooperative launch
+// (cg_multi.cu).  One descriptor per system; O is float2 or double2 (one
+// precision per launch); r, p0, p1, Ap hold P entries, v N entries.
+constexpr int kCgMultiMax = 64;
+struct CgMultiProb {
+    const void* O;
+    const double2* d;
+    const double2* F;
+    double2* x;
+    const double* diag;
+    const double* max_diag;
+    const ScheduleDev* sch;
+    CgResultDev* res;
+    double2 *r, *p0, *p1, *Ap, *v;
+    double norm, rtol;
+    int N, P, n_neural, max_it;
+    // filled by cg_multi_units: first unit costs and first tile of the system
+    long long row_cost0, tile_cost0;
+    int tile0, pad;
+};
+// per-tile partial sums (d . b, p^H A p, ||r||^2) of all systems and the
+// barrier state; row_cost / tile_cost from cg_multi_units
+struct CgMultiScratch {
+    double2* tdb;
+    double2* tpap;
+    double* trs;
+    MfreeSync* sync;
+    long long row_cost, tile_cost;
+};
+// Fills the unit offsets of the descriptors; returns the total tile count
+// (the length of each partial-sum array).
+int cg_multi_units(CgMultiProb* probs, int nprob, long long* row_cost, long long* tile_cost);
+// cooperative grid size of the multi-system kernel on this device
+cudaError_t cg_multi_blocks(int* blocks);
+cudaError_t launch_cg_multi(const CgMultiProb* probs_dev, int nprob, int fp64, const CgMultiScratch& s, int blocks,
+                            cudaStream_t st);
 cudaError_t mfree_plan(int N, int P, MfreePlan* pl);
 size_t mfree_work_bytes(int N, int P, const MfreePlan& pl);
 MfreeWork mfree_carve(void* base, int N, int P, const MfreePlan& pl);
