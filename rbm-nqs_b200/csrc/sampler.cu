@@ -44,6 +44,16 @@ __device__ __forceinline__ uint32_t lds_u8(uint32_t addr) {
     asm volatile("ld.shared.u8 %0, [%1];" : "=r"(v) : "r"(addr));
     return v;
 }
+// N / 4 words from a 4 N-byte aligned shared address (N = 4, 8, 16)
+template <int N> __device__ __forceinline__ void lds_words(uint32_t addr, uint32_t (&w)[N / 4]) {
+    if constexpr (N == 16) {
+        asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]) : "r"(addr));
+    } else if constexpr (N == 8) {
+        asm volatile("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(w[0]), "=r"(w[1]) : "r"(addr));
+    } else {
+        asm volatile("ld.shared.u32 %0, [%1];" : "=r"(w[0]) : "r"(addr));
+    }
+}
 
 // word i of the configuration with constant indices only (a runtime index
 // would place the array in local memory)
@@ -436,7 +446,10 @@ struct Smem {
     float* bre;     // [n+1] Re v[f mod n_vb] (Metropolis bias term), [n] = 0
     int2* bonds;    // proposal bonds
     float2* Wg;     // gather path: [n+1][nh] FP32 W, row n = 0 (shared or global)
-    uint8_t* Pg;    // gather path, symmetric: [n+1][S] P_s(f), row n = n
+    uint8_t* Pg;    // gather path, symmetric: [n+1][S] P_s(f), row n = n; with
+                    // lane_rows in lane order: [n+1][32 / nh][E], entry
+                    // [f][g][e] = P_{g + e 32 / nh}(f) (the rows of the
+                    // entries e of the lanes l with l / nh = g)
     unsigned char* ham;  // evaluation: staged Hamiltonian tables
     double2* base64;     // [TP] hb + sum_f W[P_s(f), k]: theta of the all-up configuration (FP64)
     unsigned char* warp0;
@@ -557,8 +570,17 @@ __device__ inline void load_tables(const MachineDev& m, const Smem& s, int fp64,
         for (int i = tid; i < n_bonds; i += nt) s.bonds[i] = bonds[i];
     if (pl.gather && pl.wg)
         for (int i = tid; i < (m.n + 1) * m.nh; i += nt) s.Wg[i] = i < m.n * m.nh ? m.W32[i] : make_float2(0.f, 0.f);
-    if (pl.gather && m.symmetric)
-        for (int i = tid; i < (m.n + 1) * m.S; i += nt) s.Pg[i] = i < m.n * m.S ? m.perm[i] : (uint8_t)m.n;
+    if (pl.gather && m.symmetric) {
+        if (pl.lane_rows) {
+            const int G = 32 / m.nh, E = m.T / 32;
+            for (int i = tid; i < (m.n + 1) * m.S; i += nt) {
+                const int f = i / m.S, j = i % m.S, g = j / E, e = j % E;
+                s.Pg[i] = f < m.n ? m.perm[f * m.S + g + e * G] : (uint8_t)m.n;
+            }
+        } else {
+            for (int i = tid; i < (m.n + 1) * m.S; i += nt) s.Pg[i] = i < m.n * m.S ? m.perm[i] : (uint8_t)m.n;
+        }
+    }
     if (pl.use_u || pl.u64)
         for (int i = tid; i < (m.n + 1) * TP; i += nt) {
             const int f = i / TP, t = i % TP;
@@ -1293,6 +1315,134 @@ __device__ __forceinline__ void run_chain_gather(const SamplerArgs& a, const Sme
     chain_finish(a, chain, lane, sp, nacc, prop);
 }
 
+// The gather sweep for symmetric machines whose theta fills every lane
+// entry (T = 32 E) with nh | 32: lane l holds the entries (k, s) = (l mod
+// nh, l / nh + e 32 / nh), so the rows P_s(f) of its E entries are E
+// consecutive bytes of the lane-ordered symmetry table; a flip costs one
+// E-byte shared load, then per entry a byte extract and the W element load
+// (no per-entry index arithmetic or validity selects).  The arithmetic is
+// run_chain_gather's, operation for operation.
+template <int E>
+__device__ __forceinline__ void run_chain_lanerows(const SamplerArgs& a, const Smem& sm, int chain, int lane) {
+    const MachineDev& m = a.m;
+    const int n = m.n, nh = m.nh;
+    const uint2 key = make_uint2((uint32_t)a.seed, (uint32_t)(a.seed >> 32));
+    const uint32_t epoch = a.ctl[0];
+    uint32_t sp[4];
+    chain_start(a, chain, key, epoch, sp);
+
+    const int k = lane % nh, g = lane / nh;
+    const uint32_t wk = smem_addr(sm.Wg) + 8u * (uint32_t)k;       // FP32 W row r: wk + 8 nh r
+    const uint32_t rowb = 8u * (uint32_t)nh;
+    const uint32_t pta = smem_addr(sm.Pg) + (uint32_t)(g * E);    // this lane group's rows of flip 0
+    const uint32_t fstride = (uint32_t)m.S;                        // bytes per flip
+    auto rowof = [](const uint32_t (&pw)[E / 4], int e) -> uint32_t { return (pw[e >> 2] >> (8 * (e & 3))) & 0xffu; };
+    const double2* W64 = sm.W64 ? sm.W64 : m.W64;
+
+    float2 th[E];
+    float SL = 0.f;
+    auto recompute = [&]() {
+        // FP64 theta = b + sum_f sigma_f W[P_s(f), k], four entries at a time
+#pragma unroll
+        for (int c = 0; c < E; c += 4) {
+            double2 acc[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[q] = sm.base64[lane + 32 * (c + q)];
+#pragma unroll
+            for (int wd = 0; wd < 4; wd++) {  // down spins in increasing order
+                uint32_t bits = spin_word(sp, wd);
+                while (bits) {
+                    const int f = 32 * wd + __ffs(bits) - 1;
+                    bits &= bits - 1;
+                    uint32_t pw[1];
+                    lds_words<4>(pta + (uint32_t)f * fstride + (uint32_t)c, pw);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const uint32_t r = (pw[0] >> (8 * q)) & 0xffu;
+                        const double2 w = W64[r * nh + k];
+                        acc[q].x = fma(-2.0, w.x, acc[q].x);
+                        acc[q].y = fma(-2.0, w.y, acc[q].y);
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) th[c + q] = make_float2((float)acc[q].x, (float)acc[q].y);
+        }
+        SL = lnc_sweep_sum<E>(th);
+    };
+    recompute();
+
+    const int2* bonds = sm.bonds ? sm.bonds : a.prop_bonds;
+    const int total = segment_sweeps(a);
+    const uint32_t thr = a.bond_thr24;
+    uint32_t prop = prop_base(a), nacc = 0, pcode = 0;
+    float plu = 0.f;
+    for (int st = 0; st < total; st++) {
+        int slot = 0;
+        while (slot < n) {
+            if ((prop & 31u) == 0) {
+                const uint4 r = philox4x32(make_uint4(prop + lane, epoch, (uint32_t)chain, 0), key);
+                uint32_t f0, f1, bond;
+                if ((r.x >> 8) < thr) {
+                    const int2 b = bonds[pick(r.y, (uint32_t)a.n_prop_bonds)];
+                    f0 = (uint32_t)b.x;
+                    f1 = (uint32_t)b.y;
+                    bond = 1;
+                } else {
+                    f0 = pick(r.y, (uint32_t)n);
+                    f1 = (uint32_t)n;
+                    bond = 0;
+                }
+                pcode = f0 | (f1 << 8) | (bond << 16);
+                plu = 0.346573590279972655f * lg2_ftz(unit24<float>(r.z));  // 0.5 ln u
+            }
+            const int src = prop & 31u;
+            const uint32_t code = __shfl_sync(kFull, pcode, src);
+            const float lu = __shfl_sync(kFull, plu, src);
+            prop++;
+            const int f0 = code & 255u, f1 = (code >> 8) & 255u;
+            const bool bond = (code >> 16) != 0;
+            slot += bond ? 2 : 1;
+            const float g0 = spin_bit(sp, f0) ? 2.f : -2.f;  // -2 sigma_f
+            const float g1 = (bond && spin_bit(sp, f1)) ? 2.f : -2.f;
+            const float2 G0 = make_float2(g0, g0), G1 = make_float2(g1, g1);
+            uint32_t p0[E / 4];
+            lds_words<E>(pta + (uint32_t)f0 * fstride, p0);
+            float2 tn[E];
+            if (bond) {
+                uint32_t p1[E / 4];
+                lds_words<E>(pta + (uint32_t)f1 * fstride, p1);
+#pragma unroll
+                for (int e = 0; e < E; e++)
+                    tn[e] = __ffma2_rn(G1, lds_f2(wk + rowof(p1, e) * rowb),
+                                       __ffma2_rn(G0, lds_f2(wk + rowof(p0, e) * rowb), th[e]));
+            } else {
+#pragma unroll
+                for (int e = 0; e < E; e++) tn[e] = __ffma2_rn(G0, lds_f2(wk + rowof(p0, e) * rowb), th[e]);
+            }
+            const float sp_new = lnc_sweep_sum<E>(tn);
+            float d = sweep_sum(sp_new - SL);
+            d = fmaf(g0, sm.bre[f0], d);
+            d = fmaf(g1, sm.bre[f1], d);
+            if (lu < d) {
+#pragma unroll
+                for (int e = 0; e < E; e++) th[e] = tn[e];
+                SL = sp_new;
+                flip_bit(sp, f0);
+                if (bond) flip_bit(sp, f1);
+                nacc++;
+            }
+        }
+        recompute();  // FP64 recompute of theta once per sweep
+        if (const int j = sample_slot(a, st); j >= 0) {
+            const size_t idx = (size_t)chain * a.spc + j;
+            if (lane < 4) a.samples[4 * idx + lane] = spin_word(sp, lane);
+        }
+    }
+    if (a.theta_out) store_theta<E>(a.theta_out, chain, lane, th);
+    chain_finish(a, chain, lane, sp, nacc, prop);
+}
+
 // Thread bound per entries-per-lane: 28 warps (896 threads, 72 registers)
 // keep 4096 chains resident on 148 SMs for E <= 4.
 template <int E, bool PF = false> struct MaxThreads {
@@ -1333,6 +1483,12 @@ __global__ void __launch_bounds__(FAST == 2 ? MaxThreads<E, PF>::gather
             else
                 run_chain_fast<E, 4>(a, sm, chain, lane);
         else if constexpr (FAST == 2) {
+            if constexpr (E >= 4) {
+                if (a.plan.lane_rows) {
+                    run_chain_lanerows<E>(a, sm, chain, lane);
+                    continue;
+                }
+            }
             if (a.m.symmetric) {
                 if (a.plan.wg)
                     run_chain_gather<E, true, true>(a, sm, chain, lane);
@@ -2039,6 +2195,7 @@ static cudaError_t plan_sampler_impl(const MachineDev& m, int fp64, int n_chains
     // row in shared memory when it fits, else from L2)
     pl.gather = !fp64 && !pf && !pl.use_u;
     pl.wg = pl.gather && (m.n + 1) * m.nh * 8 <= 64 * 1024;
+    pl.lane_rows = pl.gather && pl.wg && m.symmetric && 32 % m.nh == 0 && m.T == TP && E >= 4;
     pl.u64 = pl.use_u && m.n * TP * 16 <= 96 * 1024;
     pl.w32 = !fp64 && !pl.use_u && !pl.gather && m.n * m.nh * 8 <= 64 * 1024;
     pl.w64 = m.n * m.nh * 16 <= 32 * 1024;

@@ -51,6 +51,8 @@ struct SmemPlan {
     int bonds;  // proposal bond list
     int gather; // FP32 sweep with gathered flip rows (the expanded table does not fit)
     int wg;     // gather path: W32 with its zero pad row in shared memory
+    int lane_rows;  // gather path, symmetric, nh | 32, T = 32 E (E >= 4): the symmetry
+                    // table in lane order (one E-byte load gives a lane its rows)
     int pair;   // table path with two chains per warp
     int ham;    // evaluation: bytes of the Hamiltonian tables staged in shared memory (0: read from L2)
 };
