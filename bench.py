@@ -255,6 +255,8 @@ def run_ours(args, rank, world, local):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    if args.profile_region:
+        torch.cuda.profiler.start()
     with ClockSampler(local) as clk:
         for k in range(args.steps):
             l2_flush()
@@ -269,6 +271,8 @@ def run_ours(args, rank, world, local):
                 laccs.append(st["learned_acceptance"])
             its.append(sr["iterations"])
         torch.cuda.synchronize()
+    if args.profile_region:
+        torch.cuda.profiler.stop()
     if world > 1:
         dist.barrier()
     t_ms = sum(a.elapsed_time(b) for a, b in ev)

@@ -1172,13 +1172,13 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         if (h->mfree) {
         } else if (h->gram_tc) {
             ck(rbmnqs::gram_tc_plan(h->N, h->P, &h->gtc), "gram plan");
-            const size_t pf = h->gtc.plane_floats();
-            h->gplanes.alloc(2 * pf);
-            ck(cudaMemsetAsync(h->gplanes.p, 0, 2 * pf * sizeof(float), h->st), "memset");  // padding stays 0
+            const size_t gb = h->gtc.buffer_bytes();
+            h->gplanes.alloc((gb + 3) / 4);
+            ck(cudaMemsetAsync(h->gplanes.p, 0, gb, h->st), "memset");  // padding stays 0
             h->gpart.alloc(h->gtc.partial_bytes() / sizeof(float));
             h->gerr.alloc(1);
             ck(cudaMemsetAsync(h->gerr.p, 0, sizeof(int), h->st), "memset");
-            ck(rbmnqs::gram_tc_maps(&h->gtc, h->gplanes.p, h->gplanes.p + pf), "tensor map");
+            ck(rbmnqs::gram_tc_maps(&h->gtc, h->gplanes.p), "tensor map");
         } else {
             h->gram_ks = rbmnqs::gram_splits(h->N, h->P);
             h->part.alloc((size_t)h->gram_ks * h->P * h->P);

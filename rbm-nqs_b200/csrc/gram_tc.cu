@@ -1,27 +1,34 @@
 // gram_tc.cu -- the SR Gram S = <conj(O - d) (O - d)^T> on the 5th-generation
-// tensor cores (tcgen05, kind::tf32, accumulator in TMEM).
+// tensor cores (tcgen05, kind::f16, accumulator in TMEM).
 //
 // Real embedding: with X[n][2p] = Re(O - d)[n][p], X[n][2p+1] = Im(...), the
 // real Gram G = X^T X gives S_pq = (G[2p][2q] + G[2p+1][2q+1]
 //                                   + i (G[2p][2q+1] - G[2p+1][2q])) / N.
-// Split precision: X = Xh + Xl with Xh, Xl rounded to TF32;
-// G ~= Xh Xh^T + Xh Xl^T + Xl Xh^T accumulated in FP32 inside TMEM (the
-// dropped Xl Xl^T term is ~2^-22 relative), split-K partial tiles are
-// summed in FP64.
+// Split precision in FP16: every real row r of X is scaled by a power of two
+// s_r (max_n |X[n][r]| s_r in [2^13, 2^14), from a row-maximum pass, so that
+// no value overflows FP16 and, since max <= sqrt(N) rms, typical values stay
+// far from the FP16 subnormals); X s = Xh + Xl with Xh = fp16(X s), Xl =
+// fp16(X s - Xh).  G s_r s_c ~= Xh Xh^T + Xh Xl^T + Xl Xh^T accumulated in
+// FP32 inside TMEM (the dropped Xl Xl^T term is ~2^-22 relative: the same
+// 11 + 11 significant bits as a TF32 hi / lo split, at twice the tensor rate
+// and half the bytes); split-K partial tiles are summed in FP64 and the
+// scales divided out.
 //
-// Layout: Xh, Xl are K-major [R][K] fp32 (row r = real parameter 2p or
+// Layout: Xh, Xl are K-major [R][K] fp16 (row r = real parameter 2p or
 // 2p+1, K = samples, both zero-padded to tile multiples).  One CTA owns one
 // 128x128 tile (tp <= tq) of G and one range of K: TMA (128-byte swizzle,
-// box 32 x 128) fills a two-stage ring of {Ah, Al, Bh, Bl} tiles; one thread
-// issues three tcgen05.mma (M = N = 128, K = 8) per k-step and commits each
-// stage back to its "empty" barrier; four warps read the accumulator with
-// tcgen05.ld and store the FP32 partial tile.  Every wait is bounded: on
-// timeout the kernel records an error code, stops issuing, drains and frees
-// its TMEM.
+// box 64 x 128) fills a three-stage ring of {Ah, Al, Bh, Bl} tiles; one thread
+// issues three tcgen05.mma (M = N = 128, K = 16) per k-step, four k-steps per
+// stage, and commits each stage back to its "empty" barrier; four warps read
+// the accumulator with tcgen05.ld and store the FP32 partial tile.  Every
+// wait is bounded: on timeout the kernel records an error code, stops
+// issuing, drains and frees its TMEM.
 #include <cuda.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "common.cuh"
@@ -34,25 +41,34 @@ namespace {
 using namespace tc;
 
 constexpr int TILE = 128;                     // M = N tile (rows of G)
-constexpr int BK = 32;                        // K per stage (128 B of fp32)
-constexpr int STAGE_TILE_BYTES = TILE * BK * 4;  // 16 KB
+constexpr int BK = 64;                        // K per stage (128 B of fp16)
+constexpr int STAGE_TILE_BYTES = TILE * BK * 2;  // 16 KB
 constexpr int STAGE_BYTES = 4 * STAGE_TILE_BYTES;  // Ah, Al, Bh, Bl
 constexpr int STAGES = 3;
-constexpr int kMaxKbPerSplit = 8;             // FP32 accumulation length per CTA
+constexpr int kMaxKbPerSplit = 4;             // FP32 accumulation length per CTA (256 samples)
 constexpr long kMaxPartialBytes = 64L << 20;  // split-K partial tiles
 
-// kind::tf32 instruction descriptor: FP32 accumulate, TF32 A and B, both
-// K-major, N = 128, M = 128.
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TILE >> 3) << 17) |
+// kind::f16 instruction descriptor: FP32 accumulate, FP16 A and B (format
+// 0), both K-major, N = 128, M = 128.
+constexpr uint32_t kIdesc = (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(TILE >> 3) << 17) |
                             ((uint32_t)(TILE >> 4) << 24);
 
-__device__ __forceinline__ void mma_tf32(uint32_t tmem, uint64_t a, uint64_t b, uint32_t acc) {
+__device__ __forceinline__ void mma_f16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t acc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem),
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem),
         "l"(a), "l"(b), "r"(kIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
         : "memory");
+}
+
+// power-of-two scale of a real row from its maximum |value|: max s in
+// [2^13, 2^14) (1 for an all-zero row)
+__device__ __forceinline__ float row_scale(float mx) {
+    if (!(mx > 0.f)) return 1.f;
+    int e;
+    frexpf(mx, &e);  // mx = f 2^e, f in [0.5, 1)
+    return ldexpf(1.f, 14 - e);
 }
 
 __global__ void __launch_bounds__(128, 1)
@@ -118,13 +134,13 @@ __global__ void __launch_bounds__(128, 1)
             if (!(ok = mbar_wait(smem_u32(&full_bar[s]), (i / STAGES) & 1))) break;
             asm volatile("tcgen05.fence::after_thread_sync;");
 #pragma unroll
-            for (int k = 0; k < BK / 8; k++) {
-                const uint32_t off = k * 32;  // 8 tf32 = 32 B along K inside the swizzled row
+            for (int k = 0; k < BK / 16; k++) {
+                const uint32_t off = k * 32;  // 16 fp16 = 32 B along K inside the swizzled row
                 const uint64_t ah = desc_sw128(stage_addr(s, 0) + off), al = desc_sw128(stage_addr(s, 1) + off);
                 const uint64_t bh = desc_sw128(stage_addr(s, 2) + off), bl = desc_sw128(stage_addr(s, 3) + off);
-                mma_tf32(tmem, ah, bh, (i > 0 || k > 0) ? 1u : 0u);
-                mma_tf32(tmem, ah, bl, 1u);
-                mma_tf32(tmem, al, bh, 1u);
+                mma_f16(tmem, ah, bh, (i > 0 || k > 0) ? 1u : 0u);
+                mma_f16(tmem, ah, bl, 1u);
+                mma_f16(tmem, al, bh, 1u);
             }
             mma_commit(smem_u32(&empty_bar[s]));
             consumed = i + 1;
@@ -178,12 +194,39 @@ __global__ void __launch_bounds__(128, 1)
     }
 }
 
-// O (N x P complex, fp32 or fp64), d -> K-major TF32 hi / lo planes
-// Xh[r][n], Xl[r][n] with r = 2p (real) / 2p+1 (imag); 32 x 32 transpose
-// tiles through shared memory.
+// Row maxima: rmax[2p] = max_n |Re(O - d)[n][p]|, rmax[2p+1] the same for
+// Im (rmax zeroed before; non-negative floats compare as their bit patterns).
 template <typename TO>
-__global__ void gram_prep(const TO* __restrict__ O, const double2* __restrict__ d, int N, int P, int ld,
-                          float* __restrict__ Xh, float* __restrict__ Xl) {
+__global__ void gram_rowmax(const TO* __restrict__ O, const double2* __restrict__ d, int N, int P,
+                            unsigned int* __restrict__ rmax) {
+    const int p = blockIdx.x * 32 + (threadIdx.x & 31);
+    if (p >= P) return;
+    const double2 dd = d[p];
+    float mr = 0.f, mi = 0.f;
+    for (int n = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5); n < N; n += gridDim.y * (blockDim.x >> 5)) {
+        float vr, vi;
+        if constexpr (sizeof(TO) == 8) {
+            const float2 o = reinterpret_cast<const float2*>(O)[(size_t)n * P + p];
+            vr = (float)((double)o.x - dd.x);
+            vi = (float)((double)o.y - dd.y);
+        } else {
+            const double2 o = reinterpret_cast<const double2*>(O)[(size_t)n * P + p];
+            vr = (float)(o.x - dd.x);
+            vi = (float)(o.y - dd.y);
+        }
+        mr = fmaxf(mr, fabsf(vr));
+        mi = fmaxf(mi, fabsf(vi));
+    }
+    atomicMax(rmax + 2 * p, __float_as_uint(mr));
+    atomicMax(rmax + 2 * p + 1, __float_as_uint(mi));
+}
+
+// O (N x P complex, fp32 or fp64), d, row maxima -> K-major FP16 hi / lo
+// planes Xh[r][n], Xl[r][n] of the scaled rows, r = 2p (real) / 2p+1 (imag);
+// 32 x 32 transpose tiles through shared memory.
+template <typename TO>
+__global__ void gram_prep(const TO* __restrict__ O, const double2* __restrict__ d, const float* __restrict__ rmax,
+                          int N, int P, int ld, __half* __restrict__ Xh, __half* __restrict__ Xl) {
     __shared__ float2 tile[32][33];
     const int n0 = blockIdx.x * 32, p0 = blockIdx.y * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
@@ -210,20 +253,18 @@ __global__ void gram_prep(const TO* __restrict__ O, const double2* __restrict__ 
         const float c[2] = {v.x, v.y};
 #pragma unroll
         for (int q = 0; q < 2; q++) {
-            uint32_t hi;
-            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(c[q]));
-            const float h = __uint_as_float(hi);
-            uint32_t lo;
-            asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(c[q] - h));
+            const float x = c[q] * row_scale(rmax[2 * p + q]);
+            const __half h = __float2half_rn(x);
             Xh[(size_t)(2 * p + q) * ld + n] = h;
-            Xl[(size_t)(2 * p + q) * ld + n] = __uint_as_float(lo);
+            Xl[(size_t)(2 * p + q) * ld + n] = __float2half_rn(x - __half2float(h));
         }
     }
 }
 
-// S[p][q] (p <= q) from the split partial tiles of G; Hermitian mirror.
-__global__ void gram_tc_finalize(const float* __restrict__ part, int ntile, int nsplit, int N, int P,
-                                 double2* __restrict__ S) {
+// S[p][q] (p <= q) from the split partial tiles of G, the row scales divided
+// out; Hermitian mirror.
+__global__ void gram_tc_finalize(const float* __restrict__ part, const float* __restrict__ rmax, int ntile,
+                                 int nsplit, int N, int P, double2* __restrict__ S) {
     const int nup = ntile * (ntile + 1) / 2;
     const size_t total = (size_t)P * P;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
@@ -241,6 +282,12 @@ __global__ void gram_tc_finalize(const float* __restrict__ part, int ntile, int 
             g01 += T[lr * TILE + lc + 1];
             g10 += T[(lr + 1) * TILE + lc];
         }
+        const double sr0 = row_scale(rmax[rr]), sr1 = row_scale(rmax[rr + 1]);
+        const double sc0 = row_scale(rmax[cc]), sc1 = row_scale(rmax[cc + 1]);
+        g00 /= sr0 * sc0;
+        g11 /= sr1 * sc1;
+        g01 /= sr0 * sc1;
+        g10 /= sr1 * sc0;
         double2 v = make_double2((g00 + g11) / N, (g01 - g10) / N);
         if (p == q) v.y = 0;
         S[i] = v;
@@ -277,18 +324,22 @@ cudaError_t gram_tc_plan(int N, int P, GramTC* g) {
     return cudaSuccess;
 }
 
-cudaError_t gram_tc_maps(GramTC* g, float* Xh, float* Xl) {
+cudaError_t gram_tc_maps(GramTC* g, void* buf) {
     auto fn = encode_fn();
     if (!fn) return cudaErrorNotSupported;
-    g->Xh = Xh;
-    g->Xl = Xl;
+    const size_t pe = g->plane_elems();
+    g->Xh = reinterpret_cast<__half*>(buf);
+    g->Xl = g->Xh + pe;
+    g->rmax = reinterpret_cast<float*>(g->Xl + pe);
+    __half* Xh = g->Xh;
+    __half* Xl = g->Xl;
     for (int which = 0; which < 2; which++) {
         CUtensorMap* m = reinterpret_cast<CUtensorMap*>(which == 0 ? g->map_h : g->map_l);
         const cuuint64_t dims[2] = {(cuuint64_t)g->K, (cuuint64_t)g->R};
-        const cuuint64_t strides[1] = {(cuuint64_t)g->K * 4};
+        const cuuint64_t strides[1] = {(cuuint64_t)g->K * 2};
         const cuuint32_t box[2] = {BK, TILE};
         const cuuint32_t estr[2] = {1, 1};
-        CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, which == 0 ? (void*)Xh : (void*)Xl, dims, strides, box,
+        CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, which == 0 ? (void*)Xh : (void*)Xl, dims, strides, box,
                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
@@ -298,11 +349,18 @@ cudaError_t gram_tc_maps(GramTC* g, float* Xh, float* Xl) {
 
 cudaError_t launch_gram_tc(const GramTC& g, const void* O, int fp64, const double2* d, float* part, int* err,
                            double2* S, cudaStream_t st) {
+    cudaError_t e0 = cudaMemsetAsync(g.rmax, 0, (size_t)g.R * sizeof(float), st);
+    if (e0 != cudaSuccess) return e0;
+    unsigned int* rmu = reinterpret_cast<unsigned int*>(g.rmax);
+    const dim3 mg((g.P + 31) / 32, std::max(1, std::min(64, (g.N + 255) / 256)));
     dim3 pg((g.N + 31) / 32, (g.P + 31) / 32);
-    if (fp64)
-        gram_prep<double2><<<pg, 256, 0, st>>>((const double2*)O, d, g.N, g.P, g.K, g.Xh, g.Xl);
-    else
-        gram_prep<float2><<<pg, 256, 0, st>>>((const float2*)O, d, g.N, g.P, g.K, g.Xh, g.Xl);
+    if (fp64) {
+        gram_rowmax<double2><<<mg, 256, 0, st>>>((const double2*)O, d, g.N, g.P, rmu);
+        gram_prep<double2><<<pg, 256, 0, st>>>((const double2*)O, d, g.rmax, g.N, g.P, g.K, g.Xh, g.Xl);
+    } else {
+        gram_rowmax<float2><<<mg, 256, 0, st>>>((const float2*)O, d, g.N, g.P, rmu);
+        gram_prep<float2><<<pg, 256, 0, st>>>((const float2*)O, d, g.rmax, g.N, g.P, g.K, g.Xh, g.Xl);
+    }
     const int smem = STAGES * STAGE_BYTES + 1024;
     cudaError_t e = ensure_dynamic_smem(reinterpret_cast<const void*>(gram_tc_kernel), smem);
     if (e != cudaSuccess) return e;
@@ -310,7 +368,7 @@ cudaError_t launch_gram_tc(const GramTC& g, const void* O, int fp64, const doubl
     const CUtensorMap* mh = reinterpret_cast<const CUtensorMap*>(g.map_h);
     const CUtensorMap* ml = reinterpret_cast<const CUtensorMap*>(g.map_l);
     gram_tc_kernel<<<dim3(nup, g.nsplit), 128, smem, st>>>(*mh, *ml, g.ntile, g.K / BK, part, err);
-    gram_tc_finalize<<<296, 256, 0, st>>>(part, g.ntile, g.nsplit, g.N, g.P, S);
+    gram_tc_finalize<<<296, 256, 0, st>>>(part, g.rmax, g.ntile, g.nsplit, g.N, g.P, S);
     return cudaGetLastError();
 }
 
