@@ -479,6 +479,12 @@ def time_form(sess, graph, steps, warmup, l2_flush, stream, clk=None, profile=Fa
     session's stream (L2 flushed between epochs, outside the events);
     `profile` brackets the timed epochs with cudaProfilerStart/Stop."""
     import torch
+    tuned = None
+    if graph:
+        # the solver-stage choices (Gram split count, CG kernel) tuned on
+        # the form's own O
+        sess.epoch()
+        tuned = sess.autotune_sr()
     for _ in range(max(1, warmup)):
         sess.epoch() if graph else (sess.sample(), sess.optimize())
     sess.timing_reset(True)
@@ -507,6 +513,9 @@ def time_form(sess, graph, steps, warmup, l2_flush, stream, clk=None, profile=Fa
         torch.cuda.profiler.stop()
     t_ms = [a.elapsed_time(b) for a, b in ev]
     ms, cnt = sess.timing()
+    if tuned is not None:
+        stats[0][1]["sr_tuning"] = {"gram_splits": tuned[0], "cg_kernel": ["cluster", "cooperative"][tuned[1]]
+                                    if tuned[1] >= 0 else None, "ms": tuned[2]}
     return t_ms, stats, [float(m / max(1, c)) for m, c in zip(ms, cnt)]
 
 
@@ -533,6 +542,8 @@ def form_summary(N, n, t_ms, stats, stage_ms):
          "epochs_timed": len(stats),
          "stage_ms_per_epoch": {nm: stage_ms[i] for i, nm in enumerate(
              ["sampler", "eval", "moments+stats", "gram+regularise", "cg", "update"])}}
+    if "sr_tuning" in stats[0][1]:
+        d["sr_tuning"] = stats[0][1]["sr_tuning"]
     if any(st["learned_acceptance"] for st, _ in stats):
         d["learned_acceptance"] = float(np.mean([st["learned_acceptance"] for st, _ in stats]))
     return d

@@ -294,6 +294,19 @@ int rbmnqs_timing_reset(rbmnqs_handle* h, int32_t enable);
 int rbmnqs_autotune(rbmnqs_handle* h, int32_t sweeps, int32_t* sampler_warps_per_block,
                     int32_t* eval_warps_per_block, double* sampler_ms);
 
+/* Solver-stage autotuner (no reference counterpart): on the session's
+ * current O (sample first), times the tensor-core Gram for the cheapest split-K
+ * counts of its cost model and keeps the fastest, and, where S is formed and
+ * the cluster CG holds it, times one CG solve each with the cluster kernel
+ * and the cooperative one-barrier kernel and keeps the faster.  Both CG
+ * kernels follow cg1 (the same iterates up to rounding); a different split
+ * count changes S only by FP32 rounding (within the 1e-5 of the FP32 path).
+ * x, the chains and the weights are left as they were; the epoch graph is
+ * re-captured.  Outputs (may be NULL): the split count (0 without the
+ * tensor-core Gram), the CG kernel (0 cluster, 1 cooperative, -1 not tuned)
+ * and the best Gram + CG milliseconds. */
+int rbmnqs_autotune_sr(rbmnqs_handle* h, int32_t* gram_splits, int32_t* cg_kernel, double* sr_ms);
+
 /* Sets the sweep launch shape: warps per block (0 = planned) and chains per
  * warp (1, or 2 for the FP32 expanded-table path with n <= 32 sites, whose
  * two-chain sweep is bit-identical to the one-chain sweep).  The epoch

@@ -2070,6 +2070,99 @@ int rbmnqs_autotune(rbmnqs_handle* h, int32_t sweeps, int32_t* sampler_wpb, int3
     });
 }
 
+int rbmnqs_autotune_sr(rbmnqs_handle* h, int32_t* gram_splits, int32_t* cg_kernel, double* sr_ms) {
+    return guard([&] {
+        require(h != nullptr, "rbmnqs_autotune_sr: null handle");
+        cudaEvent_t a, b;
+        ck(cudaEventCreate(&a), "event");
+        ck(cudaEventCreate(&b), "event");
+        auto timed = [&](auto&& launch) {
+            launch();  // warm-up
+            ck(cudaEventRecord(a, h->st), "event");
+            launch();
+            ck(cudaEventRecord(b, h->st), "event");
+            ck(cudaEventSynchronize(b), "sync");
+            float ms = 0;
+            ck(cudaEventElapsedTime(&ms, a, b), "elapsed");
+            return (double)ms;
+        };
+        const double2* dS = h->full ? h->dzero.p : h->d.p;
+        double total = 0;
+        int32_t splits = 0, kernel = -1;
+        // split-K count of the tensor-core Gram
+        if (h->gram_tc) {
+            int cand[6];
+            const int nc = rbmnqs::gram_tc_split_candidates(h->gtc, cand, 6);
+            double best = -1;
+            int bs = h->gtc.nsplit;
+            for (int i = 0; i < nc; i++) {
+                ck(rbmnqs::gram_tc_set_splits(&h->gtc, cand[i]), "gram splits");
+                const double ms = timed([&] {
+                    ck(rbmnqs::launch_gram_tc(h->gtc, h->O.p, h->fp64, dS, h->gpart.p, h->gerr.p, h->Sm.p, h->st),
+                       "tensor-core gram");
+                });
+                if (best < 0 || ms < best) {
+                    best = ms;
+                    bs = cand[i];
+                }
+            }
+            ck(rbmnqs::gram_tc_set_splits(&h->gtc, bs), "gram splits");
+            splits = bs;
+            total += best;
+        }
+        // CG kernel on the formed S: the cluster CG against the cooperative
+        // one-barrier CG (x restored after each trial)
+        if (!h->mfree && h->cfg.solver == 0 && h->cfg.optimizer_type == 0 && rbmnqs::cg_cluster_fits(h->P)) {
+            if (!h->mfbuf.p) {
+                ck(rbmnqs::mfree_plan(1, h->P, &h->mfp), "cooperative CG plan");
+                h->mfbuf.alloc(rbmnqs::mfree_work_bytes(1, h->P, h->mfp));
+                h->mfw = rbmnqs::mfree_carve(h->mfbuf.p, 1, h->P, h->mfp);
+                h->mfw.minres = 0;
+            }
+            if (h->gram_tc)
+                ck(rbmnqs::launch_gram_tc(h->gtc, h->O.p, h->fp64, dS, h->gpart.p, h->gerr.p, h->Sm.p, h->st),
+                   "tensor-core gram");
+            else
+                ck(rbmnqs::launch_gram_fp64(h->O.p, h->fp64, dS, h->N, h->P, h->gram_ks, h->part.p, h->Sm.p, h->st),
+                   "gram");
+            ck(rbmnqs::launch_regularize(h->Sm.p, h->P, h->P_neural, h->N, h->sched.p, h->diag.p, h->Sreg.p,
+                                         h->maxdiag.p, h->st, 0, h->full ? h->fstat_vfac() : nullptr),
+               "regularize");
+            DevBuf<double2> x0;
+            x0.alloc(h->P);
+            ck(cudaMemcpyAsync(x0.p, h->x.p, h->P * sizeof(double2), cudaMemcpyDeviceToDevice, h->st), "save x");
+            const int max_it = h->cg_max_it();
+            const double rtol = h->cg_rtol();
+            double ms[2];
+            for (int k = 0; k < 2; k++)
+                ms[k] = timed([&] {
+                    ck(cudaMemcpyAsync(h->x.p, x0.p, h->P * sizeof(double2), cudaMemcpyDeviceToDevice, h->st),
+                       "restore x");
+                    if (k == 0)
+                        ck(rbmnqs::launch_cg(h->Sreg.p, h->F.p, h->x.p, h->P, max_it, rtol, h->cgres.p, h->st), "cg");
+                    else
+                        ck(rbmnqs::launch_cg_dense_coop(h->Sreg.p, h->F.p, h->x.p, h->P, max_it, rtol, h->mfp, h->mfw,
+                                                        h->cgres.p, h->st),
+                           "cooperative solve");
+                });
+            ck(cudaMemcpyAsync(h->x.p, x0.p, h->P * sizeof(double2), cudaMemcpyDeviceToDevice, h->st), "restore x");
+            kernel = ms[1] < ms[0] ? 1 : 0;
+            h->coop_dense = kernel == 1;
+            total += std::min(ms[0], ms[1]);
+        }
+        ck(cudaStreamSynchronize(h->st), "sync");
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        if (h->graph) {  // re-capture with the new choices
+            cudaGraphExecDestroy(h->graph);
+            h->graph = nullptr;
+        }
+        if (gram_splits) *gram_splits = splits;
+        if (cg_kernel) *cg_kernel = kernel;
+        if (sr_ms) *sr_ms = total;
+    });
+}
+
 int rbmnqs_set_sweep_shape(rbmnqs_handle* h, int32_t warps_per_block, int32_t chains_per_warp) {
     return guard([&] {
         require(h && warps_per_block >= 0 && (chains_per_warp == 1 || chains_per_warp == 2), "bad arguments");

@@ -29,6 +29,8 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <utility>
+#include <vector>
 #include <cstdint>
 
 #include "common.cuh"
@@ -45,8 +47,8 @@ constexpr int BK = 64;                        // K per stage (128 B of fp16)
 constexpr int STAGE_TILE_BYTES = TILE * BK * 2;  // 16 KB
 constexpr int STAGE_BYTES = 4 * STAGE_TILE_BYTES;  // Ah, Al, Bh, Bl
 constexpr int STAGES = 3;
-constexpr int kMaxKbPerSplit = 4;             // FP32 accumulation length per CTA (256 samples)
-constexpr long kMaxPartialBytes = 64L << 20;  // split-K partial tiles
+constexpr long kMaxPartialBytes = 256L << 20;  // split-K partial tiles
+constexpr int kMaxAccumKb = 128;               // preferred longest FP32 accumulation per CTA (8192 samples)
 
 // kind::f16 instruction descriptor: FP32 accumulate, FP16 A and B (format
 // 0), both K-major, N = 128, M = 128.
@@ -297,7 +299,40 @@ __global__ void gram_tc_finalize(const float* __restrict__ part, const float* __
 
 }  // namespace
 
-size_t GramTC::partial_bytes() const { return (size_t)nsplit * (ntile * (ntile + 1) / 2) * TILE * TILE * 4; }
+size_t GramTC::partial_bytes() const { return (size_t)max_splits * (ntile * (ntile + 1) / 2) * TILE * TILE * 4; }
+
+// Modelled time of a split count: CTAs run in waves of one per SM (the
+// shared-memory ring takes most of an SM), each CTA streams its k-blocks and
+// pays a fixed set-up and epilogue of about kOverheadKb k-blocks.
+static double gram_cost(int nup, int nkb, int ns, int sms) {
+    constexpr double kOverheadKb = 8.0;
+    const long ctas = (long)nup * ns;
+    const long waves = (ctas + sms - 1) / sms;
+    return (double)waves * ((double)((nkb + ns - 1) / ns) + kOverheadKb);
+}
+
+int gram_tc_split_candidates(const GramTC& g, int* out, int max_out) {
+    // the split counts within the partial-buffer bound, ordered by modelled cost
+    const int nup = g.ntile * (g.ntile + 1) / 2, nkb = g.K / BK;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    std::vector<std::pair<double, int>> c;
+    for (int ns = 1; ns <= g.max_splits; ns++) c.push_back({gram_cost(nup, nkb, ns, sms), ns});
+    std::stable_sort(c.begin(), c.end());
+    int n = 0;
+    for (const auto& e : c) {
+        if (n >= max_out) break;
+        out[n++] = e.second;
+    }
+    return n;
+}
+
+cudaError_t gram_tc_set_splits(GramTC* g, int ns) {
+    if (ns < 1 || ns > g->max_splits) return cudaErrorInvalidValue;
+    g->nsplit = ns;
+    return cudaSuccess;
+}
 
 cudaError_t gram_tc_plan(int N, int P, GramTC* g) {
     g->N = N;
@@ -310,17 +345,27 @@ cudaError_t gram_tc_plan(int N, int P, GramTC* g) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    // enough CTAs for the SMs, and FP32 accumulation runs of at most
-    // kMaxKbPerSplit k-blocks (256 samples) while the partial tiles stay
-    // within kMaxPartialBytes; splits are summed in FP64
-    int ns = sms / nup;
-    int acc_splits = (nkb + kMaxKbPerSplit - 1) / kMaxKbPerSplit;
-    const long cap = kMaxPartialBytes / ((long)nup * TILE * TILE * 4);
-    if (acc_splits > cap) acc_splits = (int)(cap < 1 ? 1 : cap);
-    if (ns < acc_splits) ns = acc_splits;
-    if (ns < 1) ns = 1;
-    if (ns > nkb) ns = nkb;
-    g->nsplit = ns;
+    // split counts: at most one k-block per split and partial tiles within
+    // kMaxPartialBytes (splits are summed in FP64).  The default is the
+    // lowest modelled cost (gram_cost) among the counts whose FP32
+    // accumulation runs are at most kMaxAccumKb k-blocks, or the largest
+    // allowed count when none is that short; rbmnqs_autotune_sr times the
+    // cheapest candidates on the device.
+    long cap = kMaxPartialBytes / ((long)nup * TILE * TILE * 4);
+    if (cap < 1) cap = 1;
+    if (cap > nkb) cap = nkb;
+    g->max_splits = (int)cap;
+    const int ns_min = std::min((int)cap, std::max(1, (nkb + kMaxAccumKb - 1) / kMaxAccumKb));
+    int best = ns_min;
+    double best_cost = gram_cost(nup, nkb, ns_min, sms);
+    for (int ns = ns_min + 1; ns <= cap; ns++) {
+        const double c = gram_cost(nup, nkb, ns, sms);
+        if (c < best_cost) {
+            best_cost = c;
+            best = ns;
+        }
+    }
+    g->nsplit = best;
     return cudaSuccess;
 }
 

@@ -12,13 +12,13 @@ namespace rbmnqs {
 // K = N rounded up to 64; Xh / Xl are the FP16 hi / lo planes [R][K] of the
 // scaled rows, rmax the R row maxima the scales come from.
 struct GramTC {
-    int N = 0, P = 0, R = 0, K = 0, ntile = 0, nsplit = 1;
+    int N = 0, P = 0, R = 0, K = 0, ntile = 0, nsplit = 1, max_splits = 1;
     __half* Xh = nullptr;
     __half* Xl = nullptr;
     float* rmax = nullptr;
     alignas(64) unsigned char map_h[128];
     alignas(64) unsigned char map_l[128];
-    // bytes of the FP32 split-K partial tiles
+    // bytes of the FP32 split-K partial tiles for the largest split count
     size_t partial_bytes() const;
     // elements of one plane
     size_t plane_elems() const { return (size_t)R * K; }
@@ -27,6 +27,9 @@ struct GramTC {
 };
 
 cudaError_t gram_tc_plan(int N, int P, GramTC* g);
+// up to max_out split counts (1..max_splits) in order of modelled cost
+int gram_tc_split_candidates(const GramTC& g, int* out, int max_out);
+cudaError_t gram_tc_set_splits(GramTC* g, int ns);
 // buf: buffer_bytes(), zero-filled once (the padding rows / columns of the
 // planes are never written); carves the planes and encodes the two tensor
 // maps.

@@ -120,6 +120,7 @@ def _declare(L):
         "rbmnqs_timing_reset": [VP, C.c_int32],
         "rbmnqs_graph_kernels": [VP, P_I],
         "rbmnqs_autotune": [VP, C.c_int32, P_I, P_I, P_D],
+        "rbmnqs_autotune_sr": [VP, P_I, P_I, P_D],
         "rbmnqs_save": [VP, C.c_char_p],
         "rbmnqs_load": [VP, C.c_char_p],
         "rbmnqs_n_updates": [VP, P_I64],
@@ -500,6 +501,14 @@ class Session:
         sw, ew, ms = C.c_int32(), C.c_int32(), C.c_double()
         _ck(lib().rbmnqs_autotune(self._h, sweeps, C.byref(sw), C.byref(ew), C.byref(ms)))
         return sw.value, ew.value, ms.value
+
+    def autotune_sr(self):
+        """Solver-stage autotuning (rbmnqs_autotune_sr) on the current O:
+        (Gram split count or 0, CG kernel 0 cluster / 1 cooperative / -1,
+        best Gram + CG ms)."""
+        gs, ck_, ms = C.c_int32(), C.c_int32(), C.c_double()
+        _ck(lib().rbmnqs_autotune_sr(self._h, C.byref(gs), C.byref(ck_), C.byref(ms)))
+        return gs.value, ck_.value, ms.value
 
 
 class Batch:

@@ -64,3 +64,24 @@ def test_autotune_keeps_the_trajectory():
         b.epoch()
     assert np.array_equal(a.get_weights(), b.get_weights())
     assert np.array_equal(a.spins(), b.spins())
+
+
+def test_autotune_sr_keeps_S_within_tolerance():
+    """The solver-stage autotuner (Gram split count, CG kernel) on the
+    32-spin symmetric machine: the tuned tensor-core Gram still matches the
+    oracle's S on the same samples at the FP32-path tolerance, and the
+    session keeps training with the tuned choices."""
+    spec = ("kitaev", 4, 1, 4, 0, 1024, 4)
+    a = make(spec, 11)
+    a.epoch()
+    gs, kern, ms = a.autotune_sr()
+    assert gs >= 1 and kern in (0, 1) and ms > 0
+    a.sample()
+    a.optimize()
+    Eg, Og = a.samples()
+    d, F, diag, S = a.sr_moments()
+    So = O.sr_matrix(Og, O.sr_moments(Og, Eg)[0])
+    assert np.linalg.norm(S - So) / np.linalg.norm(So) < 1e-5
+    for _ in range(2):
+        st, sr = a.epoch()
+        assert sr["status"] == 0
