@@ -65,8 +65,12 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem, uint64_t a, uint64_t b, 
         : "memory");
 }
 
-// grid (M / 128, nsplit); K range of this CTA: [blockIdx.y * nchunks * 64, +nchunks * 64)
-__global__ void __launch_bounds__(128, 1)
+// grid (M / 128, nsplit, output tiles); K range of this CTA: [blockIdx.y *
+// nchunks * 64, +nchunks * 64); output columns [blockIdx.z * N, +N) (N is
+// the tile width, at most 128 when the output is split).  Eight warps: warp
+// w reads TMEM lanes 32 (w mod 4) .. +31 and the 16-column chunks of parity
+// w / 4 in the epilogue.
+__global__ void __launch_bounds__(256, 1)
     gemm_bf16_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int N,
                      int nchunks, Epi epi, int* __restrict__ err) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -76,7 +80,7 @@ __global__ void __launch_bounds__(128, 1)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
     const uint32_t a_base = base, b_base = base + nchunks * (kRows * 128);
-    const int m0 = blockIdx.x * kRows, k0 = blockIdx.y * nchunks * kChunk;
+    const int m0 = blockIdx.x * kRows, k0 = blockIdx.y * nchunks * kChunk, n0 = blockIdx.z * N;
     const uint32_t ncols = N <= 32 ? 32u : (N <= 64 ? 64u : (N <= 128 ? 128u : 256u));
 
     if (tid == 0) {
@@ -102,7 +106,7 @@ __global__ void __launch_bounds__(128, 1)
             mbar_expect_tx(fb, (uint32_t)nchunks * (kRows * 128 + N * 128));
             for (int c = 0; c < nchunks; c++) {
                 tma_load_2d(a_base + c * (kRows * 128), &mapA, fb, k0 + c * kChunk, m0);
-                tma_load_2d(b_base + c * (N * 128), &mapB, fb, k0 + c * kChunk, 0);
+                tma_load_2d(b_base + c * (N * 128), &mapB, fb, k0 + c * kChunk, n0);
             }
         }
         // under the test fault no copy is in flight and nothing arrives:
@@ -131,18 +135,20 @@ __global__ void __launch_bounds__(128, 1)
     if (!have && tid == 0 && ok_load) atomicExch(err, 2);
     asm volatile("tcgen05.fence::after_thread_sync;");
 
-    const int row = m0 + 32 * warp + lane;
+    const int quarter = warp & 3;
+    const int row = m0 + 32 * quarter + lane;
     __syncwarp();
-    for (int c0 = 0; c0 < N; c0 += 16) {
+    for (int cl = 16 * (warp >> 2); cl < N; cl += 32) {
         uint32_t r[16];
         __syncwarp();
         if (have) {
-            tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, r);
+            tmem_ld16(tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)cl, r);
         } else {
 #pragma unroll
             for (int j = 0; j < 16; j++) r[j] = 0u;
         }
         if (row >= epi.mtot) continue;
+        const int c0 = n0 + cl;  // output column
         const size_t o = (size_t)row * epi.ld + c0;
         if (epi.mode == kStoreF32) {
             float* dst = epi.f32 + (size_t)blockIdx.y * epi.mtot * epi.ld + o;
@@ -334,6 +340,10 @@ __global__ void init_normal(float* w, size_t n, float std, uint64_t seed, uint32
     }
 }
 
+// rows of a B operand's TMA box for an output of N columns: 128-column
+// output tiles when N is a larger multiple of 128
+static int b_tile(int N) { return (N > 128 && N % 128 == 0) ? 128 : N; }
+
 cudaError_t encode_map(void* dst, const void* base, int rows, int cols, int box_rows) {
     auto fn = encode_fn();
     if (!fn) return cudaErrorNotSupported;
@@ -357,16 +367,18 @@ static cudaError_t gemm(const void* mapA, const void* mapB, int M, int N, int K,
                         cudaStream_t st) {
     Epi e = e0;
     e.stall = test_fault() == 2 ? 1 : 0;
-    // M multiple of 128, N multiple of 16 (<= 256), K = nsplit * nchunks * 64
+    // M multiple of 128, N multiple of 16 (<= 256), K = nsplit * nchunks * 64;
+    // outputs wider than 128 columns (multiples of 128) in 128-column tiles
+    // (the B map's box is b_tile(N) rows)
     const int nchunks = K / (kChunk * nsplit);
     if (M % kRows || N % 16 || N > kMaxN || nchunks < 1 || nchunks > kMaxChunks || nchunks * kChunk * nsplit != K)
         return cudaErrorInvalidValue;
-    const int smem = nchunks * (kRows * 128 + N * 128) + 1024;
+    const int NT = b_tile(N);
+    const int smem = nchunks * (kRows * 128 + NT * 128) + 1024;
     cudaError_t r = ensure_dynamic_smem(reinterpret_cast<const void*>(gemm_bf16_kernel), smem);
     if (r != cudaSuccess) return r;
-    gemm_bf16_kernel<<<dim3(M / kRows, nsplit), 128, smem, st>>>(*reinterpret_cast<const CUtensorMap*>(mapA),
-                                                                  *reinterpret_cast<const CUtensorMap*>(mapB), N,
-                                                                  nchunks, e, err);
+    gemm_bf16_kernel<<<dim3(M / kRows, nsplit, N / NT), 256, smem, st>>>(
+        *reinterpret_cast<const CUtensorMap*>(mapA), *reinterpret_cast<const CUtensorMap*>(mapB), NT, nchunks, e, err);
     return cudaGetLastError();
 }
 
@@ -425,18 +437,18 @@ Mlp::Mlp(const MlpDims& d, int max_batch, cudaStream_t st) : d_(d), st_(st) {
     chk(encode_map(mA2_.m, A2_, Bm, H2, kRows));
     chk(encode_map(mG3_.m, G3_, Bm, Oo, kRows));
     chk(encode_map(mG2_.m, G2_, Bm, H2, kRows));
-    chk(encode_map(mW1_.m, W1_, H1, I, H1));
-    chk(encode_map(mW2_.m, W2_, H2, H1, H2));
-    chk(encode_map(mW3_.m, W3_, Oo, H2, Oo));
-    chk(encode_map(mW3t_.m, W3t_, H2, Oo, H2));
-    chk(encode_map(mW2t_.m, W2t_, H1, H2, H1));
+    chk(encode_map(mW1_.m, W1_, H1, I, b_tile(H1)));
+    chk(encode_map(mW2_.m, W2_, H2, H1, b_tile(H2)));
+    chk(encode_map(mW3_.m, W3_, Oo, H2, b_tile(Oo)));
+    chk(encode_map(mW3t_.m, W3t_, H2, Oo, b_tile(H2)));
+    chk(encode_map(mW2t_.m, W2t_, H1, H2, b_tile(H1)));
     // weight-gradient GEMMs: A = G^T [out][B] (128-row tiles), B = X^T [in][B] (box = in rows)
     chk(encode_map(mG3t_.m, G3t_, r128(Oo), Bm, kRows));
     chk(encode_map(mG2t_.m, G2t_, r128(H2), Bm, kRows));
     chk(encode_map(mG1t_.m, G1t_, r128(H1), Bm, kRows));
-    chk(encode_map(mA2t_.m, A2t_, H2, Bm, H2));
-    chk(encode_map(mA1t_.m, A1t_, H1, Bm, H1));
-    chk(encode_map(mX0t_.m, X0t_, I, Bm, I));
+    chk(encode_map(mA2t_.m, A2t_, H2, Bm, b_tile(H2)));
+    chk(encode_map(mA1t_.m, A1t_, H1, Bm, b_tile(H1)));
+    chk(encode_map(mX0t_.m, X0t_, I, Bm, b_tile(I)));
     if (e != cudaSuccess) throw e;
 }
 
