@@ -10,7 +10,7 @@ a checkpoint is trained first (plain FP32 SR from seeded complex Gaussian
 weights of std 1e-4, 600 epochs of 4096 chains; saved with rbmnqs_save and
 loaded by every form), then each form runs its epochs from it:
   * learned  -- the headline `value`: mixed precision (FP32 psi ratios,
-    FP64 theta recompute, TF32x3 tensor-core Gram, FP64 CG), the whole epoch
+    FP64 theta recompute, FP16x3 split-precision tensor-core Gram, FP64 CG), the whole epoch
     as one CUDA graph, one learned move per sample after each sweep (the
     proposal network trained every epoch);
   * plain_fp32 -- the same without the learned moves;
@@ -52,7 +52,7 @@ WORKLOADS = {
                             train=dict(n_chains=4096, warmup=15, bond_flips=0.5, epochs=600),
                             learned=dict(proposal=1, learned_steps=1, learned_train=2, learned_lr=1e-3)),
     # Kitaev 32 spins, symmetric RBM alpha=4, 4096 chains x 64 sweeps,
-    # FP32 sweep / FP64 theta recompute, TF32x3 tensor-core Gram, FP64 CG
+    # FP32 sweep / FP64 theta recompute, FP16x3 split-precision tensor-core Gram, FP64 CG
     "kitaev32_symm_a4": dict(model="kitaev", n_cells=4, rbm_type=1, alpha=4, symmetry=0.5, n_chains=4096,
                              samples_per_chain=1, warmup=63, step=1, bond_flips=0.5, std=1e-4,
                              reg2=(1e-4, 1e-4, 1.0), precision=0, gram=0),
@@ -153,7 +153,7 @@ def describe(wl, P):
                                                       if wl.get("pfaffian") else "") + f", {P} params",
          "n_chains": wl["n_chains"], "sweeps_per_epoch": wl["warmup"] + wl["samples_per_chain"] * wl["step"],
          "samples_per_epoch": wl["n_chains"] * wl["samples_per_chain"], "bond_flips": wl["bond_flips"],
-         "gram": "TF32x3 tcgen05" if wl["gram"] == 0 and wl["precision"] == 0 else "FP64",
+         "gram": "FP16x3 split-precision tcgen05" if wl["gram"] == 0 and wl["precision"] == 0 else "FP64",
          "sr": "CG reg2=1e-4 reg1=(1,1e-4,0.9) lr=1e-2"}
     if wl.get("pfaffian"):
         d["pfaffian_refresh"] = wl["pf_refresh"]
@@ -661,7 +661,7 @@ def run_forms(args, rank, world, local):
     res = {
         "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_learned_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 psi ratios / fp64 theta+CG / tf32x3 Gram",
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 psi ratios / fp64 theta+CG / fp16x3 split-precision Gram",
         "data": "synthetic (checkpoint trained here from seeded complex Gaussian weights std 1e-4, Philox chains)",
         "config": {"workload": args.workload, "model": f"kitaev honeycomb n_cells={wl['n_cells']} ({n} spins) J=-1",
                    "machine": f"symmetric RBM alpha={wl['alpha']}, {P} params",

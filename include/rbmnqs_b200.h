@@ -112,10 +112,10 @@ typedef struct {
     int32_t max_iterations;    /* optimizer.sr.max_iterations (0 = 2P) */
     double rtol;               /* optimizer.sr.rtol (0 = 1e-16) */
     int32_t precision;         /* 0: FP32 psi-ratio math with FP64 theta
-                                     recompute, TF32x3 tensor-core Gram;
+                                     recompute, FP16x3 split-precision tensor-core Gram;
                                   1: FP64 throughout */
     int32_t n_updates;         /* rbm n_updates_ (decay_t offset on resume) */
-    int32_t gram;              /* S build: 0 = by precision (TF32x3 tensor
+    int32_t gram;              /* S build: 0 = by precision (FP16x3 tensor
                                   cores when precision is 0, FP64 when 1);
                                   1 = FP64 CUDA cores in either precision */
     /* Learned proposals (no reference counterpart): 0 = plain Metropolis;

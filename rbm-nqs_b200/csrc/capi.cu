@@ -346,7 +346,7 @@ struct rbmnqs_handle {
     DevBuf<int> pf_ptr;
     DevBuf<uint32_t> pf_pairs;
     DevBuf<double2> pf_scratch;
-    // tensor-core Gram (mixed precision): TF32 hi / lo planes, FP32 split-K
+    // tensor-core Gram (mixed precision): FP16 hi / lo planes, FP32 split-K
     // partial tiles, pipeline error flag
     bool gram_tc = false;
     rbmnqs::GramTC gtc;

@@ -1,7 +1,7 @@
 """Parity at the benchmark shapes.
 
 * The mixed-precision SR epoch of the 32-spin Kitaev benchmark (4096 chains,
-  symmetric RBM alpha=4, FP32 sweep, TF32x3 tensor-core Gram, cluster CG):
+  symmetric RBM alpha=4, FP32 sweep, FP16x3 split-precision tensor-core Gram, cluster CG):
   the step dw = lr x of every epoch against the oracle's CG
   (cg_solver.cpp:260-334) on the GPU's own samples, FP32-path tolerance.
 * The toric-code shapes of the batched benchmark at L = 5 and 8 (basic RBM

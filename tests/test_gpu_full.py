@@ -133,7 +133,7 @@ def test_full_state_vector_matches_eval_and_ed():
 
 
 def test_full_fp32_tracks_fp64():
-    """Mixed precision (FP32 ratios, TF32x3 tensor-core Gram) on the full
+    """Mixed precision (FP32 ratios, FP16x3 split-precision tensor-core Gram) on the full
     sampler follows the FP64 training within the FP32 tolerance."""
     _, _, a = make(model="kitaev", L=2, kind=1, alpha=2, precision=0, std=0.05)
     _, _, b = make(model="kitaev", L=2, kind=1, alpha=2, precision=1, std=0.05)

@@ -197,7 +197,7 @@ def test_gather_sweep_fp32_follows_fp64_chains(L, kind, alpha, model):
 @pytest.mark.parametrize("precision,gram", [(1, 0), (0, 1), (0, 0)])
 def test_sr_moments_and_gram_match_oracle(case, precision, gram):
     """precision 1 and gram 1: FP64 Gram (1e-10); precision 0 with gram 0:
-    TF32x3 tensor-core Gram with FP32 accumulation (1e-5)."""
+    FP16x3 split-precision tensor-core Gram with FP32 accumulation (1e-5)."""
     om, mach, s, rng = make_pair(case, precision=precision, chains=16, spc=32, warmup=2, std=0.2, gram=gram)
     s.sample()
     s.optimize()
@@ -221,7 +221,7 @@ def test_sr_moments_and_gram_match_oracle(case, precision, gram):
     ("kitaev4_symm_a4", 256, 16),    # the 32-spin symmetric alpha=4 shape, P = 133
 ])
 def test_tensor_core_gram_matches_oracle(case, chains, spc):
-    """S from the tcgen05 TF32x3 Gram against the FP64 oracle on the GPU's own
+    """S from the tcgen05 FP16x3 split-precision Gram against the FP64 oracle on the GPU's own
     O samples: Frobenius-relative error below 1e-5, element-wise error
     below 1e-5 of max|S|, exactly Hermitian with a real diagonal."""
     om, mach, s, rng = make_pair(case, precision=0, chains=chains, spc=spc, warmup=2, std=0.2)
