@@ -173,7 +173,19 @@ __global__ void __launch_bounds__(kThreads) cg_multi_kernel(const CgMultiProb* _
                     if (k < nch) {
                         unsigned char* sg = ring + (k % kStages) * kStageBytes;
                         const int cs = k * CW, cw = min(CW, P - cs);
-                        if (vec) {
+                        if (vec && cw == CW) {
+                            // full chunk: SEGS 16-byte segments per row, RPP rows per pass
+                            constexpr int SEGS = CW * ES / 16, RPP = kThreads / SEGS;
+                            const int h = tid % SEGS, r0 = tid / SEGS;
+                            const char* src = reinterpret_cast<const char*>(O + (size_t)(n0 + r0) * P + cs) + 16 * h;
+                            const size_t rstep = (size_t)RPP * P * ES;
+                            uint32_t dst = saddr(sg + r0 * (CW * ES) + 16 * h);
+                            for (int r = r0; r < nr; r += RPP) {
+                                cp16(dst, src);
+                                src += rstep;
+                                dst += RPP * (CW * ES);
+                            }
+                        } else if (vec) {
                             const int segs = cw * ES / 16;
                             for (int r = 0; r < nr; r++) {
                                 const char* src = reinterpret_cast<const char*>(O + (size_t)(n0 + r) * P + cs);
@@ -199,9 +211,12 @@ __global__ void __launch_bounds__(kThreads) cg_multi_kernel(const CgMultiProb* _
                 for (int r = 0; r < kRows; r++) ax[r] = ay[r] = 0.0;
                 for (int k = 0; k < kAhead; k++) issue(k);
                 for (int k = 0; k < nch; k++) {
-                    issue(k + kAhead);
-                    cp_wait<kAhead>();
+                    // chunk k landed (this thread's copies), then everyone's
+                    // copies are visible and everyone is done with chunk k - 1,
+                    // whose stage takes chunk k + kAhead
+                    cp_wait<kAhead - 1>();
                     __syncthreads();
+                    issue(k + kAhead);
                     const unsigned char* sg = ring + (k % kStages) * kStageBytes;
                     const TO* Os = reinterpret_cast<const TO*>(sg);
                     const double2* bs = reinterpret_cast<const double2*>(sg + kStageO);
@@ -216,7 +231,6 @@ __global__ void __launch_bounds__(kThreads) cg_multi_kernel(const CgMultiProb* _
                         for (int r = 0; r < kRows; r++)
                             if (r < nr) cmac(ax[r], ay[r], to_d2(Os[r * CW + c]), b);
                     }
-                    __syncthreads();
                 }
 #pragma unroll
                 for (int r = 0; r < kRows; r++) {
@@ -312,7 +326,19 @@ __global__ void __launch_bounds__(kThreads) cg_multi_kernel(const CgMultiProb* _
                     if (k < nch) {
                         unsigned char* sg = ring + (k % kStages) * kStageBytes;
                         const int ns = k * RB, rows = min(RB, N - ns);
-                        if (vec) {
+                        if (vec && tw == kTile) {
+                            // full tile: SEGS 16-byte segments per row, RPP rows per pass
+                            constexpr int SEGS = kTile * ES / 16, RPP = kThreads / SEGS;
+                            const int h = tid % SEGS, r0 = tid / SEGS;
+                            const char* src = reinterpret_cast<const char*>(O + (size_t)(ns + r0) * P + qs) + 16 * h;
+                            const size_t rstep = (size_t)RPP * P * ES;
+                            uint32_t dst = saddr(sg + r0 * (kTile * ES) + 16 * h);
+                            for (int r = r0; r < rows; r += RPP) {
+                                cp16(dst, src);
+                                src += rstep;
+                                dst += RPP * (kTile * ES);
+                            }
+                        } else if (vec) {
                             const int segs = tw * ES / 16;  // per row
                             for (int g = tid; g < rows * segs; g += kThreads) {
                                 const int r = g / segs, h = g - r * segs;
@@ -333,9 +359,9 @@ __global__ void __launch_bounds__(kThreads) cg_multi_kernel(const CgMultiProb* _
                 double a0x = 0, a0y = 0, a1x = 0, a1y = 0;
                 for (int k = 0; k < kAhead; k++) issue(k);
                 for (int k = 0; k < nch; k++) {
-                    issue(k + kAhead);
-                    cp_wait<kAhead>();
+                    cp_wait<kAhead - 1>();  // as in phase A: one barrier per chunk
                     __syncthreads();
+                    issue(k + kAhead);
                     const unsigned char* sg = ring + (k % kStages) * kStageBytes;
                     const TO* Os = reinterpret_cast<const TO*>(sg);
                     const double2* vs = reinterpret_cast<const double2*>(sg + kStageO);
@@ -358,7 +384,6 @@ __global__ void __launch_bounds__(kThreads) cg_multi_kernel(const CgMultiProb* _
                     } else if (2 * c < tw) {
                         for (int rr = rg; rr < rows; rr += kGroups) cmacc(a0x, a0y, to_d2(Os[rr * kTile + 2 * c]), vs[rr]);
                     }
-                    __syncthreads();
                 }
                 colred[0][tid] = make_double2(a0x, a0y);
                 colred[1][tid] = make_double2(a1x, a1y);
