@@ -543,6 +543,9 @@ struct rbmnqs_handle {
             if (cfg.step > 0) {
                 a.sweep0 = cfg.warmup + j * cfg.step;
                 a.nsweeps = cfg.step;
+                // after the sample loop's first sweep launch theta is current
+                // for every chain (written by that launch, kept by the moves)
+                a.theta_in = (sweep_theta && j > 0) ? lth.p : nullptr;
                 ck(rbmnqs::launch_sampler(a, fp64, shape, st), "sampler kernel");
             } else if (l.theta && cfg.learned_steps > 0) {
                 ck(rbmnqs::launch_learned_theta(l, st), "learned theta");

@@ -1370,7 +1370,14 @@ __device__ __forceinline__ void run_chain_lanerows(const SamplerArgs& a, const S
         }
         SL = lnc_sweep_sum<E>(th);
     };
-    recompute();
+    if (a.theta_in) {
+        const float2* src = a.theta_in + (size_t)chain * (32 * E) + lane;
+#pragma unroll
+        for (int e = 0; e < E; e++) th[e] = src[32 * e];
+        SL = lnc_sweep_sum<E>(th);
+    } else {
+        recompute();
+    }
 
     const int2* bonds = sm.bonds ? sm.bonds : a.prop_bonds;
     const int total = segment_sweeps(a);

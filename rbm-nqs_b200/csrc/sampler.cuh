@@ -90,6 +90,11 @@ struct SamplerArgs {
     // c * padded T + t; written only by the FP32 table and gather paths
     // (sampler_writes_theta), null: not written
     float2* theta_out = nullptr;
+    // the same layout read at chain start instead of the FP64 theta
+    // recompute, when the caller keeps it current for the configurations
+    // (learned moves between sweep launches); used by the lane-ordered
+    // gather path, the others recompute; null: recomputed
+    const float2* theta_in = nullptr;
 };
 
 // The Hamiltonian regrouped by transition for the FP32 evaluation kernel
