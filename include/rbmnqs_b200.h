@@ -143,8 +143,9 @@ typedef struct {
                                   ||r|| / (||A|| ||x|| + ||b||), max_iterations
                                   defaults to 4 n_params), 2 = direct
                                   (direct_solver.cpp:31-59: multiplicative
-                                  diagonal regularisation, exact solve;
-                                  n_params <= 2048) */
+                                  diagonal regularisation, exact solve; above
+                                  2048 parameters in sample space, at most
+                                  4096 samples per epoch) */
     int32_t optimizer_type;    /* optimizer.type: 0 = SR, 1 = SGD
                                   (gradient_descent.cpp:42-60) */
     double sgd_real_factor;    /* optimizer.sgd.real_factor */

@@ -324,6 +324,9 @@ struct rbmnqs_handle {
     rbmnqs::CgMultiScratch cgms{};
     int cgm_blocks = 0;
     DevBuf<unsigned char> mfbuf;
+    // direct solver above the formed-S sizes: the sample-space (Woodbury) work
+    DevBuf<unsigned char> wbbuf;
+    rbmnqs::WoodburyWork wbw{};
     // evaluation-mode observables, their per-sample values and statistics
     std::vector<std::unique_ptr<ObsDev>> obs;
     DevBuf<double2> obsE, obsMean;
@@ -720,7 +723,11 @@ struct rbmnqs_handle {
             ck(rbmnqs::launch_var_diag(O.p, fp64, dS, N, P, mfp, mfw, diag.p, maxdiag.p, st, vf), "var diag");
             mk(4);
             if (cg_after) ck(cudaStreamWaitEvent(st, cg_after, 0), "cg order");
-            if (multi_cg)
+            if (cfg.solver == 2)
+                ck(rbmnqs::launch_woodbury_solve(O.p, fp64, dS, N, P, P_neural, (double)N, F.p, x.p, maxdiag.p,
+                                                 sched.p, 0, 0, 0, wbw, cgres.p, st),
+                   "direct solve (sample space)");
+            else if (multi_cg)
                 ck(rbmnqs::launch_cg_multi(cgm.p, 1, fp64, cgms, cgm_blocks, st), "matrix-free cg");
             else
                 ck(rbmnqs::launch_cg_mfree(O.p, fp64, dS, (double)N, N, P, P_neural, F.p, x.p, diag.p, maxdiag.p,
@@ -1157,9 +1164,14 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
         }
         h->gram_tc = !h->fp64 && cfg->gram == 0 && !h->mfree;
         require(cfg->solver >= 0 && cfg->solver <= 2, "solver must be 0 (cg), 1 (minresqlp) or 2 (direct)");
-        require(cfg->solver != 2 || !h->mfree,
-                "the direct solver needs the formed S (at most " + std::to_string(kDenseMax) + " parameters)",
+        require(cfg->solver != 2 || !h->mfree || h->N <= rbmnqs::kWoodburyMaxN,
+                "the direct solver above " + std::to_string(kDenseMax) + " parameters solves in sample space: at most " +
+                    std::to_string(rbmnqs::kWoodburyMaxN) + " samples per epoch",
                 RBMNQS_ERR_UNSUPPORTED);
+        if (cfg->solver == 2 && h->mfree) {
+            h->wbbuf.alloc(rbmnqs::woodbury_work_bytes(h->N, h->P));
+            h->wbw = rbmnqs::woodbury_carve(h->wbbuf.p, h->N, h->P);
+        }
         h->coop_dense = !h->mfree && cfg->solver != 2 && (!rbmnqs::cg_cluster_fits(h->P) || cfg->solver == 1);
         if (cfg->solver == 2) {
             h->dsync.alloc(1);
@@ -1706,8 +1718,22 @@ int rbmnqs_sr_solve(rbmnqs_handle* h, const double* O, int32_t N, const double* 
             max_it = h->cfg.max_iterations > 0 ? h->cfg.max_iterations : 4 * P;
             rtol = h->cfg.rtol > 0 ? h->cfg.rtol : 1e-16;
         }
-        require(!direct || P <= kDenseMax, "the direct solver needs the formed S", RBMNQS_ERR_UNSUPPORTED);
-        if (P > kDenseMax) {
+        require(!direct || P <= kDenseMax || N <= rbmnqs::kWoodburyMaxN,
+                "the direct solver above " + std::to_string(kDenseMax) + " parameters solves in sample space: at most " +
+                    std::to_string(rbmnqs::kWoodburyMaxN) + " samples",
+                RBMNQS_ERR_UNSUPPORTED);
+        if (P > kDenseMax && direct) {
+            // the sample-space form of the direct solve (woodbury.cu)
+            DevBuf<unsigned char> wb;
+            wb.alloc(rbmnqs::woodbury_work_bytes(N, P));
+            const rbmnqs::WoodburyWork ww = rbmnqs::woodbury_carve(wb.p, N, P);
+            dmax.alloc(1);
+            ck(rbmnqs::launch_max_diag(ddiag.p, P, dmax.p, h->st), "max diag");
+            ck(rbmnqs::launch_woodbury_solve(dO.p, 1, dd.p, N, P, h->P_neural, norm, dF.p, dx.p, dmax.p, nullptr, r1,
+                                             r2, rd, ww, res.p, h->st),
+               "direct solve (sample space)");
+            ck(cudaStreamSynchronize(h->st), "sync");  // before wb goes out of scope
+        } else if (P > kDenseMax) {
             // the operator form (cg_solver.cpp aprod) on the given O, d, norm
             rbmnqs::MfreePlan pl{};
             ck(rbmnqs::mfree_plan(N, P, &pl), "matrix-free plan");

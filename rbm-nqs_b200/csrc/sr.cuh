@@ -192,6 +192,25 @@ int cg_multi_units(CgMultiProb* probs, int nprob, long long* row_cost, long long
 cudaError_t cg_multi_blocks(int* blocks);
 cudaError_t launch_cg_multi(const CgMultiProb* probs_dev, int nprob, int fp64, const CgMultiScratch& s, int blocks,
                             cudaStream_t st);
+// The direct solver above the formed-S sizes (woodbury.cu): S_reg x = F
+// through the N x N system K = N I + Abar Lambda^-1 Abar^H of the Woodbury
+// identity, K factored by launch_direct_solve.
+struct WoodburyWork {
+    double2* K;  // [N][N]
+    double2 *y, *u, *z, *work;
+    double *winv, *spp;
+    MfreeSync* sync;
+};
+constexpr int kWoodburyMaxN = 4096;
+size_t woodbury_work_bytes(int N, int P);
+WoodburyWork woodbury_carve(void* base, int N, int P);
+// x = S_reg^-1 F; the regularisation from sch (device schedules) or, when
+// sch is null, r1, r2, rd; S_pp from O itself, the r2 shift from max_diag
+// (the maximum of the variance diagonal)
+cudaError_t launch_woodbury_solve(const void* O, int fp64, const double2* d, int N, int P, int n_neural,
+                                  double norm, const double2* F, double2* x, const double* max_diag,
+                                  const ScheduleDev* sch, double r1, double r2, double rd, const WoodburyWork& w,
+                                  CgResultDev* res, cudaStream_t st);
 cudaError_t mfree_plan(int N, int P, MfreePlan* pl);
 size_t mfree_work_bytes(int N, int P, const MfreePlan& pl);
 MfreeWork mfree_carve(void* base, int N, int P, const MfreePlan& pl);
