@@ -318,6 +318,9 @@ struct rbmnqs_handle {
     // descriptor, its tile partial sums and grid size; a batch merges the
     // descriptors of its sessions into one launch
     bool multi_cg = false;
+    // set while a batch captures its graph: this session's sweep runs in the
+    // batch's sweep launch, enqueue_sample skips its own
+    bool batch_swept = false;
     DevBuf<rbmnqs::CgMultiProb> cgm;
     DevBuf<double2> cgm_t2;
     DevBuf<double> cgm_t1;
@@ -601,7 +604,7 @@ struct rbmnqs_handle {
         if (tm) mark(0);
         if (net)
             enqueue_learned_sampling();
-        else
+        else if (!batch_swept)
             ck(rbmnqs::launch_sampler(a, fp64, shape, st), "sampler kernel");
         if (tm) mark(1);
         // E_loc and O_k of every sample (local_op::evaluate, derivative)
@@ -2240,6 +2243,20 @@ struct rbmnqs_batch {
     };
     std::vector<std::unique_ptr<Group>> groups;
     int cg_blocks = 0;
+    // sessions whose sweeps run in the batch's sweep launches (one per
+    // entries-per-lane class with at least two sessions)
+    std::vector<char> swept;
+    struct SweepGroup {
+        int E, nprob, blocks, smem;
+        int first;  // the group's first session: its stream runs the launch
+        cudaEvent_t done = nullptr;
+        DevBuf<rbmnqs::BatchSweepDesc> desc;
+        ~SweepGroup() {
+            if (done) cudaEventDestroy(done);
+        }
+    };
+    std::vector<int> sweep_group;  // per session: its sweep group, -1 none
+    std::vector<std::unique_ptr<SweepGroup>> sweeps;
     ~rbmnqs_batch() {
         if (graph) cudaGraphExecDestroy(graph);
         for (auto* v : {&joins, &cg_done, &joins2})
@@ -2308,6 +2325,44 @@ int rbmnqs_batch_create(rbmnqs_handle* const* sessions, int32_t n, rbmnqs_batch*
             }
         }
         if (!b->groups.empty()) ck(rbmnqs::cg_multi_blocks(&b->cg_blocks), "multi-system CG plan");
+        // sweeps: the plain FP32 Metropolis sessions grouped by entries per lane
+        b->swept.assign(n, 0);
+        b->sweep_group.assign(n, -1);
+        for (int E = 1; E <= 8; E *= 2) {
+            std::vector<rbmnqs::BatchSweepDesc> ds;
+            std::vector<int> idx;
+            int smem = 0, blocks = 0;
+            for (int i = 0; i < n; i++) {
+                rbmnqs_handle* h = b->hs[i];
+                if (h->fp64 || h->pf_n || h->net || h->full || rbmnqs::elements_per_lane(h->T) != E) continue;
+                rbmnqs::BatchSweepDesc d{};
+                d.a = h->sampler_args();
+                int sm = 0;
+                if (!rbmnqs::sampler_batch_plan(h->machine(), 0, h->cfg.n_chains, h->n_prop_bonds, &d, &sm)) continue;
+                d.block0 = blocks;
+                blocks += d.blocks;
+                smem = std::max(smem, sm);
+                ds.push_back(d);
+                idx.push_back(i);
+            }
+            if (ds.size() < 2) continue;
+            auto g = std::make_unique<rbmnqs_batch::SweepGroup>();
+            g->E = E;
+            g->nprob = (int)ds.size();
+            g->blocks = blocks;
+            g->smem = smem;
+            g->desc.alloc(ds.size());
+            ck(cudaMemcpyAsync(g->desc.p, ds.data(), ds.size() * sizeof(rbmnqs::BatchSweepDesc),
+                               cudaMemcpyHostToDevice, b->st),
+               "copy");
+            g->first = idx[0];
+            ck(cudaEventCreateWithFlags(&g->done, cudaEventDisableTiming), "event");
+            for (int i : idx) {
+                b->swept[i] = 1;
+                b->sweep_group[i] = (int)b->sweeps.size();
+            }
+            b->sweeps.push_back(std::move(g));
+        }
         ck(cudaStreamSynchronize(b->st), "sync");
         *out = b.release();
     });
@@ -2322,11 +2377,23 @@ int rbmnqs_batch_epoch(rbmnqs_batch* b, rbmnqs_sample_stats* s, rbmnqs_sr_stats*
             ck(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal), "capture");
             try {
                 ck(cudaEventRecord(b->fork, b->st), "fork");
+                // the batched sweeps, each class on the stream of its first
+                // session, concurrently; the sessions of a class continue
+                // after its launch
+                for (auto& g : b->sweeps) {
+                    cudaStream_t gs = b->hs[g->first]->st;
+                    ck(cudaStreamWaitEvent(gs, b->fork, 0), "fork wait");
+                    ck(rbmnqs::launch_sampler_batch(g->E, g->desc.p, g->nprob, g->blocks, g->smem, gs), "batch sweep");
+                    ck(cudaEventRecord(g->done, gs), "swept");
+                }
                 cudaEvent_t prev_cg = nullptr;  // cooperative solves run one after another
                 for (size_t i = 0; i < b->hs.size(); i++) {
                     rbmnqs_handle* h = b->hs[i];
                     ck(cudaStreamWaitEvent(h->st, b->fork, 0), "fork wait");
+                    if (b->sweep_group[i] >= 0) ck(cudaStreamWaitEvent(h->st, b->sweeps[b->sweep_group[i]]->done, 0), "swept wait");
+                    h->batch_swept = b->swept[i] != 0;
                     h->enqueue_sample();
+                    h->batch_swept = false;
                     if (b->merged[i]) {
                         h->enqueue_optimize_pre();
                     } else if (h->coop_solve()) {
@@ -2356,6 +2423,7 @@ int rbmnqs_batch_epoch(rbmnqs_batch* b, rbmnqs_sample_stats* s, rbmnqs_sr_stats*
                     }
                 }
             } catch (...) {
+                for (auto* h : b->hs) h->batch_swept = false;
                 cudaStreamEndCapture(b->st, &g);
                 throw;
             }

@@ -1450,6 +1450,71 @@ __device__ __forceinline__ void run_chain_lanerows(const SamplerArgs& a, const S
     chain_finish(a, chain, lane, sp, nacc, prop);
 }
 
+// ---------------------------------------------------------------------------
+// The sweeps of several sessions (independent trainings of a batch) in one
+// launch.  Every problem gets a contiguous range of blocks; a block stages
+// its problem's tables (the problem's own shared-memory plan for the
+// launch's warps per block) and its warps take the problem's chains,
+// chain = warp * blocks + local block (one chain per warp and pass).  The
+// per-chain sweep is the per-session kernel's function for the problem's
+// entries per lane and path, so every chain's samples, counters and final
+// configuration are bit-identical to the session's own launch.
+template <int E>
+__device__ __forceinline__ void batch_chain(const SamplerArgs& a, const Smem& sm, int chain, int lane, int path) {
+    if (path == 0) {  // expanded flip table
+        if (a.m.n <= 32)
+            run_chain_fast<E, 1>(a, sm, chain, lane);
+        else
+            run_chain_fast<E, 4>(a, sm, chain, lane);
+        return;
+    }
+    if constexpr (E >= 4) {
+        if (a.plan.lane_rows) {
+            run_chain_lanerows<E>(a, sm, chain, lane);
+            return;
+        }
+    }
+    if (a.m.symmetric) {
+        if (a.plan.wg)
+            run_chain_gather<E, true, true>(a, sm, chain, lane);
+        else
+            run_chain_gather<E, true, false>(a, sm, chain, lane);
+    } else {
+        if (a.plan.wg)
+            run_chain_gather<E, false, true>(a, sm, chain, lane);
+        else
+            run_chain_gather<E, false, false>(a, sm, chain, lane);
+    }
+}
+
+template <int E>
+__global__ void __launch_bounds__(32 * kBatchSweepWarps)
+    sampler_batch_kernel(const BatchSweepDesc* __restrict__ desc, int nprob) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(16) unsigned char sa_raw[sizeof(SamplerArgs)];
+    __shared__ int pidx;
+    if (threadIdx.x == 0) {
+        int i = 0;
+        while (i + 1 < nprob && desc[i + 1].block0 <= (int)blockIdx.x) i++;
+        pidx = i;
+    }
+    __syncthreads();
+    {  // the problem's arguments into shared memory, word by word
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&desc[pidx].a);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(sa_raw);
+        for (int w = threadIdx.x; w < (int)(sizeof(SamplerArgs) / 4); w += blockDim.x) dst[w] = src[w];
+    }
+    __syncthreads();
+    const SamplerArgs& a = *reinterpret_cast<const SamplerArgs*>(sa_raw);
+    const int lb = blockIdx.x - desc[pidx].block0, nb = desc[pidx].blocks;
+    const int path = desc[pidx].path;
+    Smem sm = carve(smem, a.m, 0, a.plan, a.n_prop_bonds, sweep_warp_bytes(a.m.T, 4, 0));
+    load_tables(a.m, sm, 0, a.plan, a.prop_bonds, a.n_prop_bonds);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int chain = warp * nb + lb; chain < a.n_chains; chain += kBatchSweepWarps * nb)
+        batch_chain<E>(a, sm, chain, lane, path);
+}
+
 // Thread bound per entries-per-lane: 28 warps (896 threads, 72 registers)
 // keep 4096 chains resident on 148 SMs for E <= 4.
 template <int E, bool PF = false> struct MaxThreads {
@@ -2340,6 +2405,54 @@ cudaError_t launch_eval(const EvalArgs& a, int fp64, int wpb, cudaStream_t st) {
         if (e != cudaErrorNotSupported) return e;
     }
     return launch_eval_warp(a, fp64, wpb, st);
+}
+
+
+// ---------------------------------------------------------------------------
+// Batch sweep (several sessions, one launch)
+bool sampler_batch_plan(const MachineDev& m, int fp64, int n_chains, int n_bonds, BatchSweepDesc* d, int* smem) {
+    const int E = elements_per_lane(m.T);
+    if (fp64 || m.pf.n > 0 || E > 8) return false;
+    SamplerShape sh{};
+    if (plan_sampler(m, 0, n_chains, n_bonds, &sh, kBatchSweepWarps, 0) != cudaSuccess) return false;
+    SmemPlan pl = sh.plan;
+    pl.pair = 0;
+    if (!pl.use_u && !pl.gather) return false;
+    int dev = 0, smem_max = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const int budget = smem_max - 8 * 1024 - (int)sizeof(SamplerArgs);
+    int bytes = sampler_smem_bytes(m, 0, kBatchSweepWarps, pl, n_bonds);
+    if (bytes > budget && pl.u64) {  // without the FP64 expanded table
+        pl.u64 = 0;
+        bytes = sampler_smem_bytes(m, 0, kBatchSweepWarps, pl, n_bonds);
+    }
+    if (bytes > budget) return false;
+    d->a.plan = pl;
+    d->E = E;
+    d->path = pl.use_u ? 0 : 1;
+    d->blocks = (n_chains + kBatchSweepWarps - 1) / kBatchSweepWarps;
+    *smem = bytes;
+    return true;
+}
+
+cudaError_t launch_sampler_batch(int E, const BatchSweepDesc* desc_dev, int nprob, int blocks, int smem,
+                                 cudaStream_t st) {
+    if (nprob < 1 || blocks < 1) return cudaErrorInvalidValue;
+    const void* fn = nullptr;
+    switch (E) {
+        case 1: fn = reinterpret_cast<const void*>(sampler_batch_kernel<1>); break;
+        case 2: fn = reinterpret_cast<const void*>(sampler_batch_kernel<2>); break;
+        case 4: fn = reinterpret_cast<const void*>(sampler_batch_kernel<4>); break;
+        case 8: fn = reinterpret_cast<const void*>(sampler_batch_kernel<8>); break;
+        default: return cudaErrorInvalidValue;
+    }
+    cudaError_t e = ensure_dynamic_smem(fn, smem);
+    if (e != cudaSuccess) return e;
+    const BatchSweepDesc* d = desc_dev;
+    int np = nprob;
+    void* args[] = {&d, &np};
+    return cudaLaunchKernel(fn, dim3(blocks), dim3(32 * kBatchSweepWarps), args, smem, st);
 }
 
 }  // namespace rbmnqs

@@ -200,6 +200,23 @@ struct SamplerShape {
 cudaError_t plan_sampler(const MachineDev& m, int fp64, int n_chains, int n_bonds, SamplerShape* out,
                          int max_wpb = 0, int pair_mode = -1);
 cudaError_t launch_sampler(const SamplerArgs& a, int fp64, const SamplerShape& shape, cudaStream_t st);
+// The sweeps of several sessions in one launch per entries-per-lane class
+// (a batch): one descriptor per session, its blocks [block0, block0 +
+// blocks) of the launch.
+constexpr int kBatchSweepWarps = 8;
+struct BatchSweepDesc {
+    SamplerArgs a;  // the session's arguments with its plan for kBatchSweepWarps warps
+    int block0, blocks;
+    int E;          // entries per lane
+    int path;       // 0 expanded flip table, 1 gathered rows
+};
+// Fills d->a.plan, E, path and blocks (d->a must hold the session's other
+// arguments) and the shared-memory bytes; false when the session's sweep
+// cannot run in the batch launch (FP64, Pfaffian, more than 8 entries per
+// lane, or tables that do not fit with kBatchSweepWarps warps).
+bool sampler_batch_plan(const MachineDev& m, int fp64, int n_chains, int n_bonds, BatchSweepDesc* d, int* smem);
+cudaError_t launch_sampler_batch(int E, const BatchSweepDesc* desc_dev, int nprob, int blocks, int smem,
+                                 cudaStream_t st);
 // whether the sweep path of this shape writes SamplerArgs::theta_out
 bool sampler_writes_theta(const MachineDev& m, int fp64, const SamplerShape& shape);
 cudaError_t launch_eval(const EvalArgs& a, int fp64, int warps_per_block, cudaStream_t st);

@@ -1,7 +1,8 @@
 """Batched independent trainings (one CUDA-graph launch for several sessions
-of different lattices and sizes, the matrix-free CG systems of one precision
-solved by one multi-system launch) and the launch-shape autotuner: both must
-leave every session's trajectory bit-for-bit what its own epochs produce."""
+of different lattices and sizes; the FP32 sweeps of one entries-per-lane
+class in one launch, the matrix-free CG systems of one precision in one
+multi-system launch) and the launch-shape autotuner: both must leave every
+session's trajectory bit-for-bit what its own epochs produce."""
 import numpy as np
 import pytest
 
@@ -24,6 +25,11 @@ PROBLEMS = [
 # each session's own epoch graph has two kernels for its solve (barrier
 # reset, CG), the batch two for all three
 MERGED = 3
+# FP32 sweeps in the batch's sweep launches, one per entries-per-lane class:
+# toric L = 3, 4, 4 (2 entries per lane) and the 32-spin symmetric Kitaev
+# machine with toric L = 5 (4 entries per lane): five session sweeps, two
+# launches
+SWEPT, SWEEP_LAUNCHES = 5, 2
 
 
 def make(spec, seed):
@@ -51,7 +57,8 @@ def test_batch_epochs_equal_individual_epochs():
     for x, y in zip(a, b):
         assert np.array_equal(x.get_weights(), y.get_weights())
         assert np.array_equal(x.spins(), y.spins())
-    assert batch.graph_kernels() == sum(s.graph_kernels() for s in b) - 2 * (MERGED - 1)
+    assert batch.graph_kernels() == (sum(s.graph_kernels() for s in b) - 2 * (MERGED - 1) - SWEPT
+                                     + SWEEP_LAUNCHES)
 
 
 def test_autotune_keeps_the_trajectory():
