@@ -675,9 +675,13 @@ template <typename TO> const void* cg_fn() { return reinterpret_cast<const void*
 // iteration ahead writes the other buffer while slower blocks still read).
 __global__ void __launch_bounds__(kThreads) cg_dense1_kernel(const double2* __restrict__ S,
                                                              const double2* __restrict__ F, double2* x, int P,
-                                                             int max_it, double rtol, MfreeWork w, CgResultDev* res) {
+                                                             int max_it, double rtol, MfreeWork w, CgResultDev* res,
+                                                             int cache_rows) {
     extern __shared__ double2 sv[];
     double2 *p = sv, *r = sv + P, *xs = sv + 2 * P;
+    // cache_rows: every warp owns at most one row of S (the grid has at
+    // least P warps) and keeps it in shared memory for the whole solve
+    double2* srow = sv + 3 * P + (size_t)(threadIdx.x >> 5) * P;
     __shared__ double redd[kThreads / 32];
     __shared__ double2 redz[kThreads / 32];
     const int tid = threadIdx.x, lane = tid & 31, G = gridDim.x, blk = blockIdx.x;
@@ -688,17 +692,19 @@ __global__ void __launch_bounds__(kThreads) cg_dense1_kernel(const double2* __re
         res->qlp_iterations = 0;
         res->acond = 0;
     }
+    if (cache_rows && gw < P)
+        for (int q = lane; q < P; q += 32) srow[q] = __ldg(S + (size_t)gw * P + q);
     // rows of S times a shared-memory vector into a global buffer
     auto matvec = [&](const double2* v, double2* out) {
         for (int row = gw; row < P; row += nwarps) {
-            const double2* Sr = S + (size_t)row * P;
+            const double2* Sr = cache_rows ? srow : S + (size_t)row * P;
             double ax = 0, ay = 0;
             int q = lane;
             for (; q + 96 < P; q += 128) {
                 double2 a[4], b[4];
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
-                    a[u] = __ldg(Sr + q + 32 * u);
+                    a[u] = cache_rows ? Sr[q + 32 * u] : __ldg(Sr + q + 32 * u);
                     b[u] = v[q + 32 * u];
                 }
 #pragma unroll
@@ -708,7 +714,7 @@ __global__ void __launch_bounds__(kThreads) cg_dense1_kernel(const double2* __re
                 }
             }
             for (; q < P; q += 32) {
-                const double2 a = __ldg(Sr + q), b = v[q];
+                const double2 a = cache_rows ? Sr[q] : __ldg(Sr + q), b = v[q];
                 ax = fma(a.x, b.x, fma(-a.y, b.y, ax));
                 ay = fma(a.x, b.y, fma(a.y, b.x, ay));
             }
@@ -867,25 +873,38 @@ cudaError_t launch_cg_dense_coop(const double2* A, const double2* b, double2* x,
     cudaError_t e = launch_init_sync(w.sync, st);
     if (e != cudaSuccess) return e;
     if (!w.minres) {
-        // CG: the one-barrier kernel, p, r and x of every block in shared memory
-        const int smem = 3 * P * (int)sizeof(double2);
+        // CG: the one-barrier kernel, p, r and x of every block in shared
+        // memory, and each warp's row of S too when the rows fit
+        const int base_smem = 3 * P * (int)sizeof(double2);
+        const int row_smem = (kThreads / 32) * P * (int)sizeof(double2);
         const void* fn = reinterpret_cast<const void*>(cg_dense1_kernel);
-        if ((e = ensure_dynamic_smem(fn, smem)) != cudaSuccess) return e;
-        int dev = 0, sms = 148, per_sm = 0;
+        int dev = 0, sms = 148, per_sm = 0, smem_max = 0;
         if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        const int rows_blocks = (P + kThreads / 32 - 1) / (kThreads / 32);  // one row per warp
+        int cache = base_smem + row_smem <= smem_max - 8 * 1024 ? 1 : 0;
+        int smem = base_smem + (cache ? row_smem : 0);
+        if ((e = ensure_dynamic_smem(fn, smem)) != cudaSuccess) return e;
         if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_dense1_kernel, kThreads, smem)) !=
             cudaSuccess)
             return e;
+        if (cache && rows_blocks > sms * per_sm) {  // not every row gets its own warp
+            cache = 0;
+            smem = base_smem;
+            if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_dense1_kernel, kThreads, smem)) !=
+                cudaSuccess)
+                return e;
+        }
         if (per_sm < 1) return cudaErrorInvalidConfiguration;
-        int blocks = std::min(sms * per_sm, (P + kThreads / 32 - 1) / (kThreads / 32));
+        int blocks = std::min(sms * per_sm, rows_blocks);
         blocks = std::max(1, blocks);
         MfreeWork wk = w;
         const double2* S = A;
         const double2* F = b;
         double2* xo = x;
         CgResultDev* r = res;
-        void* args[] = {&S, &F, &xo, &P, &max_it, &rtol, &wk, &r};
+        void* args[] = {&S, &F, &xo, &P, &max_it, &rtol, &wk, &r, &cache};
         return cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(kThreads), args, smem, st);
     }
     MfreeWork wk = w;
