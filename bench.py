@@ -136,6 +136,18 @@ def init_dist(world, backend):
     return dist
 
 
+def max_over_ranks(values, world, device="cuda"):
+    """Device times of every rank reduced to their maximum (the job's time
+    is the slowest replica's); unchanged with one rank."""
+    if world <= 1:
+        return list(values)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(list(values), device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def make_weights(P, std, seed, n_neural=None, pf_std=None):
     """complex Gaussian weights; pair parameters (index >= n_neural) with pf_std"""
     rng = np.random.default_rng(seed)
@@ -294,10 +306,7 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize()
     t2_ms = sum(a.elapsed_time(b) for a, b in ev2)
 
-    if world > 1:
-        t = torch.tensor([t_ms, t2_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms, t2_ms = t.tolist()
+    t_ms, t2_ms = max_over_ranks([t_ms, t2_ms], world)
     tau = float(np.mean(taus))
     neff_epoch = N / (1.0 + 2.0 * tau)
     value = world * args.steps * neff_epoch / (t_ms * 1e-3)
@@ -411,10 +420,7 @@ def run_batch(args, rank, world, local):
         ev2[k][1].record(stream)
     torch.cuda.synchronize()
     t2_ms = sum(a.elapsed_time(b) for a, b in ev2)
-    if world > 1:
-        t = torch.tensor([t_ms, t2_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms, t2_ms = t.tolist()
+    t_ms, t2_ms = max_over_ranks([t_ms, t2_ms], world)
     its = [x["iterations"] for x in sr]
     Pmax = max(s.n_params for s in sessions)
     hb = sum(s.n_params for s in sessions) * 16
@@ -637,10 +643,7 @@ def run_forms(args, rank, world, local):
     out["plain_fp64"] = form_summary(p64.N, n, t_ms, stats, stage)
     del p64
 
-    if world > 1:
-        t = torch.tensor([t_learned_ms, t2_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_learned_ms, t2_ms = t.tolist()
+    t_learned_ms, t2_ms = max_over_ranks([t_learned_ms, t2_ms], world)
     if rank != 0:
         return None
     L = out["learned"]
