@@ -474,15 +474,14 @@ __global__ void __launch_bounds__(32 * eloc_warps(KB* NG), eloc_min_blocks(KB* N
                     if (ti >= n_terms) continue;  // uniform
                     const TermDev tm = sTerms[ti];
                     const int nf = term_nf(tm);
+                    // theta' = theta - 2 sigma_f W[..] over the flips; an
+                    // off-diagonal term flips at least one site, so the
+                    // first flip reads theta and writes theta' directly
+                    // (no per-term copy of the lane's theta registers)
                     float2 tr[NP], tq[NP];
 #pragma unroll
-                    for (int p = 0; p < NP; p++) {
-                        tr[p] = thr[p];
-                        tq[p] = thi[p];
-                    }
-#pragma unroll
                     for (int q = 0; q < NFM; q++) {
-                        if (q >= nf) break;  // uniform
+                        if (q > 0 && q >= nf) break;  // uniform
                         const int f = term_flip(tm, q);
                         const float g = sbit(sp, f) ? 2.f : -2.f;  // -2 sigma_f
                         const float2 g2 = make_float2(g, g);
@@ -501,8 +500,9 @@ __global__ void __launch_bounds__(32 * eloc_warps(KB* NG), eloc_min_blocks(KB* N
                                 }
 #pragma unroll
                                 for (int h = 0; h < KB / 2; h++) {
-                                    tr[j * (KB / 2) + h] = __ffma2_rn(g2, ur[h], tr[j * (KB / 2) + h]);
-                                    tq[j * (KB / 2) + h] = __ffma2_rn(g2, ui[h], tq[j * (KB / 2) + h]);
+                                    const int pi = j * (KB / 2) + h;
+                                    tr[pi] = __ffma2_rn(g2, ur[h], q == 0 ? thr[pi] : tr[pi]);
+                                    tq[pi] = __ffma2_rn(g2, ui[h], q == 0 ? thi[pi] : tq[pi]);
                                 }
                             }
                         } else {
@@ -523,8 +523,8 @@ __global__ void __launch_bounds__(32 * eloc_warps(KB* NG), eloc_min_blocks(KB* N
                                         w[h] = __ldg(m.W32 + (ok ? f : n) * nh + (ok ? g_k(j) : 0));
                                     }
                                 }
-                                tr[p] = __ffma2_rn(g2, make_float2(w[0].x, w[1].x), tr[p]);
-                                tq[p] = __ffma2_rn(g2, make_float2(w[0].y, w[1].y), tq[p]);
+                                tr[p] = __ffma2_rn(g2, make_float2(w[0].x, w[1].x), q == 0 ? thr[p] : tr[p]);
+                                tq[p] = __ffma2_rn(g2, make_float2(w[0].y, w[1].y), q == 0 ? thi[p] : tq[p]);
                             }
                         }
                     }

@@ -100,43 +100,53 @@ __device__ __forceinline__ int warp_argmax(double v) {
     return who;
 }
 
-// Fresh context (pfaffian::get_context): A <- the antisymmetrised X^{-1} of
-// configuration `bits`.  A: the warp's n x n shared-memory matrix (leading
-// dimension kPfLd); scr: a second per-warp n x n buffer (global or shared,
-// leading dimension sld) for the unscramble.  Gauss-Jordan with lane =
-// column for the row operations and lane = row for the pivot search.
-// Warp-collective.
-__device__ __forceinline__ void pf_fresh(const PfDev& p, uint32_t bits, int lane, double2* A, PfStage& st,
-                                         double2* scr, int sld) {
+// Gauss-Jordan inverse of X (configuration `bits`) in the n x n workspace A
+// (leading dimension ld; shared or global memory), partial (row) pivoting
+// with rows kept in place: afterwards row piv[k] of A holds X^{-1}[k][piv[j]]
+// in column j.  Lane = column for the row operations, lane = row for the
+// pivot search.  The full 32 x 32 block is written (rows / columns >= n
+// zero).  LD is a compile-time constant so that the row updates of a step
+// can be issued back to back.  Warp-collective.
+template <int LD>
+__device__ __forceinline__ void pf_gauss_jordan(const PfDev& p, uint32_t bits, int lane, double2* A, int* piv) {
+    constexpr int ld = LD;
     const int n = p.n;
-    // the full 32 x 32 block: rows / columns >= n stay zero for the
-    // fixed-length matrix-vector loops of pf_ratio
     for (int i = 0; i < kPfMaxSites; i++)
-        A[i * kPfLd + lane] = (i < n && lane < n) ? pf_elem(p, bits, i, lane, 0, 0) : make_double2(0.0, 0.0);
+        A[i * ld + lane] = (i < n && lane < n) ? pf_elem(p, bits, i, lane, 0, 0) : make_double2(0.0, 0.0);
     __syncwarp();
     uint32_t used = 0;
     for (int k = 0; k < n; k++) {
-        const double2 fcol = lane < n ? A[lane * kPfLd + k] : make_double2(0.0, 0.0);
+        const double2 fcol = lane < n ? A[lane * ld + k] : make_double2(0.0, 0.0);
         const bool cand = lane < n && !((used >> lane) & 1u);
         const int pr = warp_argmax(cand ? zabs2(fcol) : -1.0);
         used |= 1u << pr;
-        if (lane == 0) st.piv[k] = pr;
+        if (lane == 0) piv[k] = pr;
         const double2 ip = zrcp(zshfl(fcol, pr));
         double2 rp = make_double2(0.0, 0.0);
         if (lane < n) {
-            rp = lane == k ? ip : zmul(A[pr * kPfLd + lane], ip);
-            A[pr * kPfLd + lane] = rp;
+            rp = lane == k ? ip : zmul(A[pr * ld + lane], ip);
+            A[pr * ld + lane] = rp;
         }
         for (int i = 0; i < n; i++) {
             if (i == pr) continue;
             const double2 f = zshfl(fcol, i);
             if (lane < n) {
-                const double2 a = lane == k ? make_double2(0.0, 0.0) : A[i * kPfLd + lane];
-                A[i * kPfLd + lane] = zsub(a, zmul(f, rp));
+                const double2 a = lane == k ? make_double2(0.0, 0.0) : A[i * ld + lane];
+                A[i * ld + lane] = zsub(a, zmul(f, rp));
             }
         }
         __syncwarp();
     }
+}
+
+// Fresh context (pfaffian::get_context): A <- the antisymmetrised X^{-1} of
+// configuration `bits`.  A: the warp's n x n shared-memory matrix (leading
+// dimension kPfLd); scr: a second per-warp n x n buffer (global or shared,
+// leading dimension sld) for the unscramble.  Warp-collective.
+__device__ __forceinline__ void pf_fresh(const PfDev& p, uint32_t bits, int lane, double2* A, PfStage& st,
+                                         double2* scr, int sld) {
+    const int n = p.n;
+    pf_gauss_jordan<kPfLd>(p, bits, lane, A, st.piv);
     // unscramble: row p_k of A holds X^{-1}[k][p_j] in column j
     if (lane < n) {
         const int pj = st.piv[lane];
@@ -408,6 +418,212 @@ __device__ __forceinline__ void pf_derivative(const PfDev& p, uint32_t bits, int
                 out[a + p.n_indep * c] = make_float2((float)acc[c].x, (float)acc[c].y);
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Sweep form.  The Metropolis sweep keeps X^{-1} (antisymmetric) as its
+// circulant half, Cx[(d - 1) * 32 + i] = X^{-1}[i][(i + d) & 31] for
+// d = 1..16: 8 KB per warp instead of the 16.9 KB square, so that a block
+// holds about twice the chains.  Lane i walks its row in offset order (the
+// entries (i, i + d) from Cx[d][i], the entries (i, i - d) as -Cx[d][i - d]),
+// both conflict-free across the warp.  The pair (i, i + 16) is held twice,
+// once per orientation, and each copy is updated by its own row's formula.
+// Rows and columns >= n are zero and stay zero.
+constexpr int kPfCircBytes = 16 * kPfMaxSites * 16;
+constexpr int kPfSweepFlips = 2;  // sweep proposals: one spin or one bond
+
+struct PfSweepStage {
+    double2 BT[kPfSweepFlips][kPfMaxSites];      // dense columns of B, column-major
+    double2 IB[2 * kPfSweepFlips][kPfMaxSites];  // X^{-1} B, column-major
+    int piv[kPfMaxSites];                        // Gauss-Jordan pivot row of each column
+    int qinv[kPfMaxSites];                       // inverse of piv
+};
+
+// X^{-1}[i][j] from the circulant half (branch-free: the entries (i, i + d),
+// d <= 16, are held by row i, the others as -X^{-1}[j][i] by row j)
+__device__ __forceinline__ double2 pf_circ_at(const double2* Cx, int i, int j) {
+    const int d = (j - i) & 31;
+    const bool fw = d <= 16;
+    const double2 v = Cx[d == 0 ? 0 : (fw ? (d - 1) * kPfMaxSites + i : (31 - d) * kPfMaxSites + j)];
+    const double s = d == 0 ? 0.0 : (fw ? 1.0 : -1.0);
+    return make_double2(s * v.x, s * v.y);
+}
+
+// Unscramble and antisymmetrise the Gauss-Jordan result A (leading dimension
+// LD) into the circulant half: Cx(i, j) = (X^{-1}[i][j] - X^{-1}[j][i]) / 2
+// with X^{-1}[k][m] = A[piv[k]][qinv[m]].
+template <int LD>
+__device__ __forceinline__ void pf_unscramble_circ(int n, int lane, const double2* A, const PfSweepStage& st,
+                                                   double2* Cx) {
+    const int pi = lane < n ? st.piv[lane] : 0, qi = lane < n ? st.qinv[lane] : 0;
+#pragma unroll 4
+    for (int d = 1; d <= 16; d++) {
+        const int j = (lane + d) & 31;
+        double2 v = make_double2(0.0, 0.0);
+        if (lane < n && j < n) {
+            const double2 a = A[pi * LD + st.qinv[j]], b = A[st.piv[j] * LD + qi];
+            v = make_double2(0.5 * (a.x - b.x), 0.5 * (a.y - b.y));
+        }
+        Cx[(d - 1) * kPfMaxSites + lane] = v;
+    }
+}
+
+// Fresh context in circulant form: Gauss-Jordan in the warp's global
+// scratch gscr (leading dimension 32; it stays in L1, which a square
+// workspace in shared memory would shrink for every warp of the block), then
+// X^{-1} unscrambled and antisymmetrised straight into Cx:
+// Cx(i, j) = (X^{-1}[i][j] - X^{-1}[j][i]) / 2 with X^{-1}[k][m] =
+// A[piv[k]][qinv[m]] (pfaffian.cpp:284-297).  Warp-collective.
+__device__ __forceinline__ void pf_fresh_circ(const PfDev& p, uint32_t bits, int lane, double2* Cx, PfSweepStage& st,
+                                              double2* gscr) {
+    const int n = p.n;
+    pf_gauss_jordan<kPfMaxSites>(p, bits, lane, gscr, st.piv);
+    if (lane < n) st.qinv[st.piv[lane]] = lane;
+    __syncwarp();
+    pf_unscramble_circ<kPfMaxSites>(n, lane, gscr, st, Cx);
+    __syncwarp();
+}
+
+// Butterfly warp sum of a complex value (every lane gets the same result:
+// IEEE addition is commutative).
+__device__ __forceinline__ double2 zwarp_sum(double2 v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, off);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, off);
+    }
+    return v;
+}
+
+// Pairs of the 2 NF x 2 NF matrix C^{-1} (r < q), every lane: NF = 1: c[0]
+// = (0, 1); NF = 2: c = (0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3).
+template <int NF> struct PfPairs {
+    double2 c[NF == 1 ? 1 : 6];
+};
+
+// psi ratio factor of the Pfaffian for flipping sites fl[0..NF) with X^{-1}
+// in circulant form (the same rank-2m formula as pf_ratio).  Lane t holds
+// row t of B and of X^{-1} B (ib), so each entry of C^{-1} is one warp sum
+// of lane products plus entries of X^{-1} B on the flipped sites' lanes.
+// Leaves X^{-1} B in st.IB (and this lane's row in ib) and C^{-1} in cp for
+// pf_accept_circ.  Warp-collective.
+template <int NF>
+__device__ __forceinline__ double2 pf_ratio_circ(const PfDev& p, uint32_t bits, const int* fl, int lane,
+                                                 PfSweepStage& st, const double2* Cx, double2 (&ib)[2 * NF],
+                                                 PfPairs<NF>& cp) {
+    static_assert(NF == 1 || NF == 2, "sweep proposals flip one or two sites");
+    const int n = p.n;
+    uint32_t fm = 0;
+#pragma unroll
+    for (int q = 0; q < NF; q++) fm |= 1u << fl[q];
+    double2 b[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+        b[k] = make_double2(0.0, 0.0);
+        if (lane < n && lane != fl[k]) {
+            const double2 a1 = pf_elem(p, bits, lane, fl[k], (fm >> lane) & 1u, 1);
+            const double2 a0 = pf_elem(p, bits, lane, fl[k], 0, 0);
+            b[k] = zsub(a1, a0);
+        }
+        st.BT[k][lane] = b[k];
+    }
+    __syncwarp();
+    // this lane's row of X^{-1} B: the entries (i, i + d) and (i, i - d)
+    double2 up[NF], dn[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) up[k] = dn[k] = make_double2(0.0, 0.0);
+#pragma unroll 4
+    for (int d = 1; d <= 16; d++) {
+        const int j = (lane + d) & 31;
+        const double2 x = Cx[(d - 1) * kPfMaxSites + lane];
+#pragma unroll
+        for (int k = 0; k < NF; k++) up[k] = zfma(x, st.BT[k][j], up[k]);
+    }
+#pragma unroll 5
+    for (int d = 1; d <= 15; d++) {
+        const int j = (lane - d) & 31;
+        const double2 x = Cx[(d - 1) * kPfMaxSites + j];
+#pragma unroll
+        for (int k = 0; k < NF; k++) dn[k] = zfma(x, st.BT[k][j], dn[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < NF; k++) {
+        ib[k] = zsub(up[k], dn[k]);
+        ib[NF + k] = pf_circ_at(Cx, lane, fl[k]);
+    }
+#pragma unroll
+    for (int q = 0; q < 2 * NF; q++) st.IB[q][lane] = ib[q];
+    // X^{-1} B entries on the flipped sites' lanes
+    auto at = [&](int q, int site) { return zshfl(ib[q], site); };
+    if constexpr (NF == 1) {
+        // (0, 1): (sum_t B_t0 IB_t1 - IB_{f0,0}) / 2 - 1
+        const double2 s = zwarp_sum(zmul(b[0], ib[1]));
+        double2 c = zscale(zsub(s, at(0, fl[0])), 0.5);
+        c.x -= 1.0;
+        cp.c[0] = c;
+        return make_double2(-c.x, -c.y);  // (-1)^{m(m+1)/2}, m = 1
+    } else {
+        const double2 s01 = zwarp_sum(zsub(zmul(b[0], ib[1]), zmul(b[1], ib[0])));
+        const double2 s02 = zwarp_sum(zmul(b[0], ib[2]));
+        const double2 s03 = zwarp_sum(zmul(b[0], ib[3]));
+        const double2 s12 = zwarp_sum(zmul(b[1], ib[2]));
+        const double2 s13 = zwarp_sum(zmul(b[1], ib[3]));
+        const double2 i00 = at(0, fl[0]), i01 = at(1, fl[0]), i03 = at(3, fl[0]);
+        const double2 i10 = at(0, fl[1]), i11 = at(1, fl[1]), i12 = at(2, fl[1]);
+        // C0: C(k, l) = a(f_k, f_l) - a'(f_k, f_l) below the diagonal block
+        const double2 d01 = zsub(pf_elem(p, bits, fl[1], fl[0], 0, 0), pf_elem(p, bits, fl[1], fl[0], 1, 1));
+        cp.c[0] = zsub(zscale(s01, 0.5), d01);
+        cp.c[1] = zscale(zsub(s02, i00), 0.5);
+        cp.c[1].x -= 1.0;
+        cp.c[2] = zscale(zsub(s03, i10), 0.5);
+        cp.c[3] = zscale(zsub(s12, i01), 0.5);
+        cp.c[4] = zscale(zsub(s13, i11), 0.5);
+        cp.c[4].x -= 1.0;
+        cp.c[5] = zscale(zsub(i03, i12), 0.5);
+        const double2 pf = zadd(zsub(zmul(cp.c[0], cp.c[5]), zmul(cp.c[1], cp.c[4])), zmul(cp.c[2], cp.c[3]));
+        return make_double2(-pf.x, -pf.y);  // (-1)^{m(m+1)/2}, m = 2
+    }
+}
+
+// X^{-1} update after an accepted move (pf_accept in circulant form): with
+// Ca = (C^{-1})^{-1}, t1 = (row i of X^{-1} B) Ca and
+// X^{-1}(i, i + d) += t1 . (row i + d of X^{-1} B), d = 1..16.
+template <int NF>
+__device__ __forceinline__ void pf_accept_circ(int lane, const PfSweepStage& st, const double2 (&ib)[2 * NF],
+                                               const PfPairs<NF>& cp, double2* Cx, int n) {
+    double2 t1[2 * NF];
+    if constexpr (NF == 1) {
+        // Ca = [[0, -1/c], [1/c, 0]]
+        const double2 ic = zrcp(cp.c[0]);
+        t1[0] = zmul(ib[1], ic);
+        t1[1] = zmul(ib[0], make_double2(-ic.x, -ic.y));
+    } else {
+        const double2 c01 = cp.c[0], c02 = cp.c[1], c03 = cp.c[2], c12 = cp.c[3], c13 = cp.c[4], c23 = cp.c[5];
+        const double2 ip = zrcp(zadd(zsub(zmul(c01, c23), zmul(c02, c13)), zmul(c03, c12)));
+        // Ca = adj / Pf: Ca[t][q] for t != q (antisymmetric)
+        const double2 a01 = zmul(c23, ip), a02 = zmul(c13, ip), a03 = zmul(c12, ip);
+        const double2 a12 = zmul(c03, ip), a13 = zmul(c02, ip), a23 = zmul(c01, ip);
+        // Ca[0][1] = -a01, Ca[0][2] = a02, Ca[0][3] = -a03, Ca[1][2] = -a12,
+        // Ca[1][3] = a13, Ca[2][3] = -a23; Ca[q][t] = -Ca[t][q]
+        // t1[q] = sum_t ib[t] Ca[t][q]
+        t1[0] = zsub(zsub(zmul(ib[1], a01), zmul(ib[2], a02)), zmul(ib[3], make_double2(-a03.x, -a03.y)));
+        t1[1] = zsub(zadd(zmul(ib[0], make_double2(-a01.x, -a01.y)), zmul(ib[2], a12)), zmul(ib[3], a13));
+        t1[2] = zadd(zadd(zmul(ib[0], a02), zmul(ib[1], make_double2(-a12.x, -a12.y))), zmul(ib[3], a23));
+        t1[3] = zadd(zadd(zmul(ib[0], make_double2(-a03.x, -a03.y)), zmul(ib[1], a13)),
+                     zmul(ib[2], make_double2(-a23.x, -a23.y)));
+    }
+    __syncwarp();  // st.IB of every lane
+    if (lane < n) {
+#pragma unroll 4
+        for (int d = 1; d <= 16; d++) {
+            const int j = (lane + d) & 31;
+            double2 acc = Cx[(d - 1) * kPfMaxSites + lane];
+#pragma unroll
+            for (int q = 0; q < 2 * NF; q++) acc = zfma(t1[q], st.IB[q][j], acc);
+            Cx[(d - 1) * kPfMaxSites + lane] = acc;
+        }
+    }
+    __syncwarp();
 }
 
 }  // namespace rbmnqs

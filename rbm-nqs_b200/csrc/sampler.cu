@@ -468,15 +468,19 @@ __host__ __device__ inline int padded_T(int T) {
 // per-warp scratch.  Evaluation: spins (16 B) | theta [T] | ln cosh re [T] |
 // phase [T] | tanh theta [T] (evaluated in FP64 from the FP64 theta, so
 // O_k keep FP32 accuracy next to the poles of tanh).  Sweeps: proposal ln|cosh| [TP].
-// With the Pfaffian factor: + the PfStage staging and the n x n FP64 matrix
-// X^{-1} (both), + the evaluation's unscramble buffer.
+// With the Pfaffian factor: evaluation + the PfStage staging, the n x n FP64
+// matrix X^{-1} and its unscramble buffer; sweeps: the PfSweepStage staging
+// and X^{-1} as its circulant half only (the proposal ln cosh values stay in
+// registers, the fresh inverse runs in global scratch), so that the 14
+// chains per SM of 2048 chains on 148 SMs fit the 164 KB carve-out and
+// leave 92 KB of L1.
 __host__ __device__ inline int eval_rbm_bytes(int T, int rsize) { return align16(16 + T * 7 * rsize); }
 __host__ __device__ inline int sweep_rbm_bytes(int T, int rsize) { return align16(padded_T(T) * rsize); }
 __host__ __device__ inline int eval_warp_bytes(int T, int rsize, int pf) {
     return eval_rbm_bytes(T, rsize) + (pf ? (int)sizeof(PfStage) + 2 * kPfMatBytes : 0);
 }
 __host__ __device__ inline int sweep_warp_bytes(int T, int rsize, int pf) {
-    return sweep_rbm_bytes(T, rsize) + (pf ? (int)sizeof(PfStage) + kPfMatBytes : 0);
+    return pf ? (int)sizeof(PfSweepStage) + kPfCircBytes : sweep_rbm_bytes(T, rsize);
 }
 
 __host__ __device__ inline int table_bytes(const MachineDev& m, int fp64, const SmemPlan& pl, int n_bonds) {
@@ -682,11 +686,13 @@ __device__ __forceinline__ void chain_finish(const SamplerArgs& a, int chain, in
 // PF: the Pfaffian factor rides along (pfaffian.cuh): fresh X^{-1} at chain
 // start, ratio of every proposal by the rank-2m formula, X^{-1} updated on
 // acceptance and rebuilt every pf.refresh accepted moves
-// (abstract_sampler.cpp:103-113).  pst / pA: the warp's staging and X^{-1}
-// in shared memory; pscr: its unscramble buffer in global memory.
+// (abstract_sampler.cpp:103-113).  pst / Cx: the warp's staging and X^{-1}
+// (circulant half) in shared memory; pscr: its Gauss-Jordan workspace in
+// global memory.  With PF the proposal's ln cosh values stay in registers
+// (wlp unused).
 template <int E, typename R, bool PF>
 __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, int chain, int lane, R* wlp,
-                                          PfStage* pst, double2* pA, double2* pscr) {
+                                          PfSweepStage* pst, double2* Cx, double2* pscr) {
     const MachineDev& m = a.m;
     const C2<R>* W = Wsel<R>::get(m, sm.W32 ? sm.W32 : m.W32);
     const double2* W64 = sm.W64 ? sm.W64 : m.W64;
@@ -697,17 +703,20 @@ __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, 
     chain_start(a, chain, key, epoch, sp);
 
     C2<R> th[E];
-    R L[E];
+    R L[E], lpn[E];  // lpn: the proposal's ln|cosh| (PF; else in wlp)
     theta_fp64<E, R>(m, W64, sm.perm, lane, sp, th);
 #pragma unroll
     for (int e = 0; e < E; e++) L[e] = slot_valid(lane, e, m.T) ? lnc_re<R>(th[e].x, th[e].y) : (R)0;
 
     // Pfaffian context (pfaffian.cpp:284-297)
-    double2 ib[2 * kPfMaxFlips];
+    double2 ib1[2], ib2[4];
+    PfPairs<1> cp1;
+    PfPairs<2> cp2;
     int ar = 0;  // accepted moves since the chain start (refresh counter)
-    if constexpr (PF) pf_fresh(m.pf, sp[0], lane, pA, *pst, pscr, kPfMaxSites);
-    auto xi = [&](int t) { return pA[lane * kPfLd + t]; };
-    auto xcol = [&](int f) { return pA[lane * kPfLd + f]; };
+    // the fresh context is built before the next proposal (one inlined copy
+    // for the chain start and every refresh; a refresh due after the chain's
+    // last proposal changes nothing that the chain outputs)
+    bool fresh = true;
 
     // U(f, e): the flip row of site f for this lane's entry e
     auto U = [&](int f, int e) -> C2<R> {
@@ -746,6 +755,11 @@ __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, 
                 f0 = (int)pick(r1, (uint32_t)n);
                 slot += 1;
             }
+            if constexpr (PF)
+                if (fresh) {
+                    pf_fresh_circ(m.pf, sp[0], lane, Cx, *pst, pscr);
+                    fresh = false;
+                }
             const bool s0 = spin_bit(sp, f0), s1 = f1 >= 0 && spin_bit(sp, f1);
             const R g0 = s0 ? (R)2 : (R)-2;  // -2 sigma_f
             const R g1 = s1 ? (R)2 : (R)-2;
@@ -763,7 +777,10 @@ __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, 
                     t.y = fma(g1, u1.y, t.y);
                 }
                 const R lp = lnc_re<R>(t.x, t.y);
-                wlp[lane + 32 * e] = lp;  // read back only if accepted
+                if constexpr (PF)
+                    lpn[e] = lp;
+                else
+                    wlp[lane + 32 * e] = lp;  // read back only if accepted
                 d += lp - L[e];
             }
             d = warp_sum(d);
@@ -777,8 +794,8 @@ __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, 
             bool accept;
             if constexpr (PF) {
                 const int fl[2] = {f0, f1};
-                const double2 c2 = f1 >= 0 ? pf_ratio<2>(m.pf, sp[0], fl, lane, *pst, xi, xcol, ib)
-                                           : pf_ratio<1>(m.pf, sp[0], fl, lane, *pst, xi, xcol, ib);
+                const double2 c2 = f1 >= 0 ? pf_ratio_circ<2>(m.pf, sp[0], fl, lane, *pst, Cx, ib2, cp2)
+                                           : pf_ratio_circ<1>(m.pf, sp[0], fl, lane, *pst, Cx, ib1, cp1);
                 accept = (double)unit24<R>(r2) < exp(2.0 * (double)d) * zabs2(c2);
             } else {
                 accept = unit24<R>(r2) < exp_r((R)2 * d);
@@ -795,7 +812,7 @@ __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, 
                         th[e].x = fma(g1, u1.x, th[e].x);
                         th[e].y = fma(g1, u1.y, th[e].y);
                     }
-                    L[e] = wlp[lane + 32 * e];
+                    L[e] = PF ? lpn[e] : wlp[lane + 32 * e];
                 }
                 flip_bit(sp, f0);
                 if (f1 >= 0) flip_bit(sp, f1);
@@ -803,9 +820,11 @@ __device__ __forceinline__ void run_chain(const SamplerArgs& a, const Smem& sm, 
                 if constexpr (PF) {
                     ar++;
                     if (m.pf.refresh && ar % m.pf.refresh == 0)
-                        pf_fresh(m.pf, sp[0], lane, pA, *pst, pscr, kPfMaxSites);
+                        fresh = true;
+                    else if (f1 >= 0)
+                        pf_accept_circ<2>(lane, *pst, ib2, cp2, Cx, m.pf.n);
                     else
-                        pf_accept(f1 >= 0 ? 2 : 1, lane, *pst, ib, pA, m.pf.n);
+                        pf_accept_circ<1>(lane, *pst, ib1, cp1, Cx, m.pf.n);
                 }
             }
         }
@@ -1518,7 +1537,7 @@ __global__ void __launch_bounds__(32 * kBatchSweepWarps)
 // Thread bound per entries-per-lane: 28 warps (896 threads, 72 registers)
 // keep 4096 chains resident on 148 SMs for E <= 4.
 template <int E, bool PF = false> struct MaxThreads {
-    static constexpr int v = PF ? 256 : (E <= 2 ? 1024 : (E <= 4 ? 896 : (E <= 8 ? 512 : 256)));
+    static constexpr int v = PF ? 512 : (E <= 2 ? 1024 : (E <= 4 ? 896 : (E <= 8 ? 512 : 256)));
     static constexpr int gather = E <= 4 ? 896 : (E <= 8 ? 640 : 384);
     static constexpr int pair = E <= 1 ? 1024 : (E <= 2 ? 768 : 512);  // 2 E entries per lane
 };
@@ -1537,8 +1556,8 @@ __global__ void __launch_bounds__(FAST == 2 ? MaxThreads<E, PF>::gather
     load_tables(a.m, sm, fp64, a.plan, a.prop_bonds, a.n_prop_bonds);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     R* wlp = reinterpret_cast<R*>(sm.warp0 + warp * sm.warp_bytes);
-    PfStage* pst = reinterpret_cast<PfStage*>(sm.warp0 + warp * sm.warp_bytes + sweep_rbm_bytes(a.m.T, sizeof(R)));
-    double2* pA = reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(pst) + sizeof(PfStage));
+    PfSweepStage* pst = reinterpret_cast<PfSweepStage*>(sm.warp0 + warp * sm.warp_bytes);
+    double2* Cx = reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(pst) + sizeof(PfSweepStage));
     double2* pscr = PF ? a.m.pf.scratch + (size_t)(blockIdx.x * (blockDim.x >> 5) + warp) * kPfMaxSites * kPfMaxSites
                        : nullptr;
     const int total_warps = (blockDim.x >> 5) * gridDim.x;
@@ -1573,7 +1592,7 @@ __global__ void __launch_bounds__(FAST == 2 ? MaxThreads<E, PF>::gather
                     run_chain_gather<E, false, false>(a, sm, chain, lane);
             }
         } else
-            run_chain<E, R, PF>(a, sm, chain, lane, wlp, pst, pA, pscr);
+            run_chain<E, R, PF>(a, sm, chain, lane, wlp, pst, Cx, pscr);
     }
 }
 
@@ -2309,6 +2328,23 @@ static cudaError_t plan_sampler_impl(const MachineDev& m, int fp64, int n_chains
     if (per_sm < 1) per_sm = 1;
     long blocks = ((long)units + wpb - 1) / wpb;
     if (blocks > (long)sms * per_sm) blocks = (long)sms * per_sm;
+    if (pf) {
+        // the Pfaffian sweep's Gauss-Jordan scratch, tables and spills live
+        // in L1: ask for no more shared memory than the resident blocks use
+        // (1 KB reserved per block), the rest of the SM's 256 KB stays L1.
+        // The hint is a whole percentage, rounded down: the driver raises it
+        // to the smallest carve-out that the launch needs (rounding up can
+        // step past a carve-out that fits, e.g. 164 KB at 72 %).
+        int sm_max = 0;
+        cudaDeviceGetAttribute(&sm_max, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        const long resident = std::min<long>(per_sm, (blocks + sms - 1) / sms);
+        const long need = resident * (smem + 1024);
+        if (sm_max > 0) {
+            const int pct = (int)std::min<long>(100, need * 100 / sm_max);
+            err = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+            if (err != cudaSuccess) return err;
+        }
+    }
     out->plan = pl;
     out->warps_per_block = wpb;
     out->blocks = (int)blocks;
