@@ -101,28 +101,88 @@ __device__ __forceinline__ int warp_argmax(double v) {
 }
 
 // Gauss-Jordan inverse of X (configuration `bits`) in the n x n workspace A
-// (leading dimension ld; shared or global memory), partial (row) pivoting
+// (leading dimension LD; shared or global memory), partial (row) pivoting
 // with rows kept in place: afterwards row piv[k] of A holds X^{-1}[k][piv[j]]
 // in column j.  Lane = column for the row operations, lane = row for the
 // pivot search.  The full 32 x 32 block is written (rows / columns >= n
-// zero).  LD is a compile-time constant so that the row updates of a step
-// can be issued back to back.  Warp-collective.
+// zero).  Two elimination steps share one pass over the rows: the second
+// pivot column is updated by the first step in registers, and each row takes
+// both rank-1 updates between one load and one store -- the operations and
+// their order are those of two single steps, so the result is the same to
+// the bit, with half the row traffic (the workspace of the sweep is global
+// memory, whose stores go through to L2).  The two pivot columns reach the
+// row loop through fb (2 x 32 entries of per-warp shared memory, read as
+// broadcasts), the column-(k + 1) special case through the multiplier of the
+// first update.  LD is a compile-time constant so that the row updates can
+// be issued back to back.  The loops stay rolled: the elimination runs
+// between proposals of the other warps of the SM, whose loop must stay in
+// the instruction cache.  Warp-collective.
 template <int LD>
-__device__ __forceinline__ void pf_gauss_jordan(const PfDev& p, uint32_t bits, int lane, double2* A, int* piv) {
+__device__ __forceinline__ void pf_gauss_jordan(const PfDev& p, uint32_t bits, int lane, double2* A, int* piv,
+                                                double2* fb) {
     constexpr int ld = LD;
     const int n = p.n;
+    const double2 zero = make_double2(0.0, 0.0);
+#pragma unroll 2
     for (int i = 0; i < kPfMaxSites; i++)
-        A[i * ld + lane] = (i < n && lane < n) ? pf_elem(p, bits, i, lane, 0, 0) : make_double2(0.0, 0.0);
+        A[i * ld + lane] = (i < n && lane < n) ? pf_elem(p, bits, i, lane, 0, 0) : zero;
     __syncwarp();
     uint32_t used = 0;
-    for (int k = 0; k < n; k++) {
-        const double2 fcol = lane < n ? A[lane * ld + k] : make_double2(0.0, 0.0);
-        const bool cand = lane < n && !((used >> lane) & 1u);
-        const int pr = warp_argmax(cand ? zabs2(fcol) : -1.0);
+    int k = 0;
+#pragma unroll 1
+    for (; k + 1 < n; k += 2) {
+        // step k: pivot row p1 of column k (c0), normalised row rp1
+        const double2 c0 = lane < n ? A[lane * ld + k] : zero;
+        const double2 c1 = lane < n ? A[lane * ld + k + 1] : zero;
+        const int p1 = warp_argmax((lane < n && !((used >> lane) & 1u)) ? zabs2(c0) : -1.0);
+        used |= 1u << p1;
+        if (lane == 0) piv[k] = p1;
+        const double2 ip1 = zrcp(zshfl(c0, p1));
+        double2 rp1 = zero;
+        if (lane < n) rp1 = lane == k ? ip1 : zmul(A[p1 * ld + lane], ip1);
+        // column k + 1 after step k (row p1 holds rp1)
+        const double2 r1k1 = zshfl(rp1, k + 1);
+        const double2 c1u = lane == p1 ? r1k1 : zsub(c1, zmul(c0, r1k1));
+        fb[lane] = c0;
+        fb[kPfMaxSites + lane] = c1u;
+        // step k + 1: pivot row p2 of the updated column, normalised row rp2
+        const int p2 = warp_argmax((lane < n && !((used >> lane) & 1u)) ? zabs2(c1u) : -1.0);
+        used |= 1u << p2;
+        if (lane == 0) piv[k + 1] = p2;
+        const double2 ip2 = zrcp(zshfl(c1u, p2));
+        const double2 f1p2 = zshfl(c0, p2), f2p1 = zshfl(c1u, p1);
+        double2 rp2 = zero, r1p = zero;
+        if (lane < n) {
+            const double2 a1 = zsub(lane == k ? zero : A[p2 * ld + lane], zmul(f1p2, rp1));
+            rp2 = lane == k + 1 ? ip2 : zmul(a1, ip2);
+            r1p = zsub(lane == k + 1 ? zero : rp1, zmul(f2p1, rp2));
+        }
+        __syncwarp();
+        // the other rows: a - f1 rp1 - f2 rp2, with a = 0 in columns k and
+        // k + 1 and, in column k + 1, the first update's result discarded
+        // (rp1 there taken as 0: 0 - f1 0 = +0, as the discarded value)
+        const bool keep = lane != k && lane != k + 1;
+        const double2 rp1e = lane == k + 1 ? zero : rp1;
+        if (lane < n) {
+#pragma unroll 2
+            for (int i = 0; i < n; i++) {
+                if (i == p1 || i == p2) continue;  // uniform
+                const double2 f1 = fb[i], f2 = fb[kPfMaxSites + i];
+                const double2 a = keep ? A[i * ld + lane] : zero;
+                A[i * ld + lane] = zsub(zsub(a, zmul(f1, rp1e)), zmul(f2, rp2));
+            }
+            A[p2 * ld + lane] = rp2;
+            A[p1 * ld + lane] = r1p;
+        }
+        __syncwarp();
+    }
+    if (k < n) {  // odd n: one single step
+        const double2 fcol = lane < n ? A[lane * ld + k] : zero;
+        const int pr = warp_argmax((lane < n && !((used >> lane) & 1u)) ? zabs2(fcol) : -1.0);
         used |= 1u << pr;
         if (lane == 0) piv[k] = pr;
         const double2 ip = zrcp(zshfl(fcol, pr));
-        double2 rp = make_double2(0.0, 0.0);
+        double2 rp = zero;
         if (lane < n) {
             rp = lane == k ? ip : zmul(A[pr * ld + lane], ip);
             A[pr * ld + lane] = rp;
@@ -130,10 +190,7 @@ __device__ __forceinline__ void pf_gauss_jordan(const PfDev& p, uint32_t bits, i
         for (int i = 0; i < n; i++) {
             if (i == pr) continue;
             const double2 f = zshfl(fcol, i);
-            if (lane < n) {
-                const double2 a = lane == k ? make_double2(0.0, 0.0) : A[i * ld + lane];
-                A[i * ld + lane] = zsub(a, zmul(f, rp));
-            }
+            if (lane < n) A[i * ld + lane] = zsub(lane == k ? zero : A[i * ld + lane], zmul(f, rp));
         }
         __syncwarp();
     }
@@ -146,7 +203,7 @@ __device__ __forceinline__ void pf_gauss_jordan(const PfDev& p, uint32_t bits, i
 __device__ __forceinline__ void pf_fresh(const PfDev& p, uint32_t bits, int lane, double2* A, PfStage& st,
                                          double2* scr, int sld) {
     const int n = p.n;
-    pf_gauss_jordan<kPfLd>(p, bits, lane, A, st.piv);
+    pf_gauss_jordan<kPfLd>(p, bits, lane, A, st.piv, &st.IB[0][0]);
     // unscramble: row p_k of A holds X^{-1}[k][p_j] in column j
     if (lane < n) {
         const int pj = st.piv[lane];
@@ -477,7 +534,7 @@ __device__ __forceinline__ void pf_unscramble_circ(int n, int lane, const double
 __device__ __forceinline__ void pf_fresh_circ(const PfDev& p, uint32_t bits, int lane, double2* Cx, PfSweepStage& st,
                                               double2* gscr) {
     const int n = p.n;
-    pf_gauss_jordan<kPfMaxSites>(p, bits, lane, gscr, st.piv);
+    pf_gauss_jordan<kPfMaxSites>(p, bits, lane, gscr, st.piv, &st.BT[0][0]);
     if (lane < n) st.qinv[st.piv[lane]] = lane;
     __syncwarp();
     pf_unscramble_circ<kPfMaxSites>(n, lane, gscr, st, Cx);
