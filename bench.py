@@ -105,6 +105,8 @@ def parse():
     ap.add_argument("--cpu-baseline", type=int, default=1, help="time the CPU restatement beside our arm")
     ap.add_argument("--chains", type=int, default=0, help="override the workload's chain count (profiling)")
     ap.add_argument("--sweeps", type=int, default=0, help="override the sweeps per epoch (profiling)")
+    ap.add_argument("--pf-refresh", type=int, default=-1,
+                    help="override the Pfaffian workloads' refresh period in accepted moves (0: never; profiling)")
     ap.add_argument("--forms", default="learned,plain_fp32,plain_fp64",
                     help="forms of the 128-spin workload to run (profiling runs a subset; the metric line needs all)")
     ap.add_argument("--profile-region", type=int, default=0,
@@ -118,6 +120,8 @@ def workload(args):
         wl["n_chains"] = args.chains
     if args.sweeps:
         wl["warmup"] = args.sweeps - wl["samples_per_chain"] * wl["step"]
+    if args.pf_refresh >= 0 and wl.get("pfaffian"):
+        wl["pf_refresh"] = args.pf_refresh
     return wl
 
 

@@ -59,8 +59,9 @@ cudaError_t launch_eloc_fast(const EvalArgs& a, cudaStream_t st) {
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
     const int warps = eloc::eloc_warps(kb * ng);
-    // small blocks share the SM three ways: keep their tables to a third
-    if (kb * ng <= 4) budget = std::min(budget, 72 * 1024);
+    // small blocks share the SM seven ways: keep their tables to a seventh
+    // where they fit (basic machines read W from L2 otherwise)
+    if (kb * ng <= 4) budget = std::min(budget, 32 * 1024 - 1024);
     const ElocLayout L = eloc::eloc_layout(m, a.tt, kb, warps, a.O != nullptr, budget);
     if (L.total > budget) return cudaErrorNotSupported;
     if ((e = ensure_dynamic_smem(fn, L.total)) != cudaSuccess) return e;

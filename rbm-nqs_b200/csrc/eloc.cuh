@@ -41,10 +41,11 @@ namespace rbmnqs {
 namespace eloc {
 
 // Warps per block and resident blocks per SM by entries per lane: up to 4
-// entries, 8-warp blocks at up to 85 registers (3 blocks, 24 warps per SM);
-// above, 16-warp blocks at up to 128 registers.
-__host__ __device__ constexpr int eloc_warps(int E) { return E <= 4 ? 8 : 16; }
-__host__ __device__ constexpr int eloc_min_blocks(int E) { return E <= 4 ? 3 : 1; }
+// entries, 4-warp blocks at up to 72 registers (7 blocks, 28 warps per SM:
+// 4096 samples, one per warp, in one wave of 148 SMs); above, 16-warp
+// blocks at up to 128 registers.
+__host__ __device__ constexpr int eloc_warps(int E) { return E <= 4 ? 4 : 16; }
+__host__ __device__ constexpr int eloc_min_blocks(int E) { return E <= 4 ? 7 : 1; }
 
 __host__ __device__ inline int a16(int x) { return (x + 15) & ~15; }
 
@@ -601,7 +602,37 @@ __global__ void __launch_bounds__(32 * eloc_warps(KB* NG), eloc_min_blocks(KB* N
                     acc.y = warp_sum(acc.y);
                     if (lane == 0) Orow[n_vb + k] = acc;
                 }
-                // W[j, k]: sum_s sigma_{P_s^{-1}(j)} tanh theta[k, s]
+                // W[j, k]: sum_s sigma_{P_s^{-1}(j)} tanh theta[k, s].  With
+                // n a multiple of 128 and nh of 4, each lane takes four
+                // consecutive sites: one 32-bit load gives their four
+                // inverse-symmetry bytes, two 16-byte loads the four tanh
+                // values they share (same sums, same order per output)
+                if (n % 128 == 0 && nh % 4 == 0) {
+                    for (int jb = 4 * lane; jb < n; jb += 128) {
+                        for (int k0 = 0; k0 < nh; k0 += 4) {
+                            float2 acc[4][4] = {};
+                            for (int s = 0; s < S; s++) {
+                                const uint32_t iv = *reinterpret_cast<const uint32_t*>(sInv + s * n + jb);
+                                const float4 t01 = *reinterpret_cast<const float4*>(tn + k0 + nh * s);
+                                const float4 t23 = *reinterpret_cast<const float4*>(tn + k0 + 2 + nh * s);
+                                const float2 t[4] = {make_float2(t01.x, t01.y), make_float2(t01.z, t01.w),
+                                                     make_float2(t23.x, t23.y), make_float2(t23.z, t23.w)};
+#pragma unroll
+                                for (int jj = 0; jj < 4; jj++) {
+                                    const float sg = sgn[(iv >> (8 * jj)) & 0xffu];
+                                    const float2 G2 = make_float2(sg, sg);
+#pragma unroll
+                                    for (int i = 0; i < 4; i++) acc[jj][i] = __ffma2_rn(G2, t[i], acc[jj][i]);
+                                }
+                            }
+#pragma unroll
+                            for (int i = 0; i < 4; i++)
+#pragma unroll
+                                for (int jj = 0; jj < 4; jj++)
+                                    Orow[n_vb + nh + jb + jj + n * (k0 + i)] = acc[jj][i];
+                        }
+                    }
+                } else
                 for (int j = lane; j < n; j += 32) {
                     for (int k0 = 0; k0 < nh; k0 += 4) {
                         float2 acc[4] = {};
