@@ -88,7 +88,7 @@ SAMPLER_DRAM_BYTES = {"kitaev32_symm_a4": 136704.0}
 # FP32 complex); the capture of 32768 samples wrote 78.9 MB (the rest of its
 # 135.5 MB still in L2 when the kernel ended), scaled by 8 to the 262144
 # samples of one launch
-ELOC_DRAM_BYTES = {"kitaev128_forms": 8 * 78.9e6}
+ELOC_DRAM_BYTES = {"kitaev128_forms": 8 * 79.5e6}
 ELOC_TRAFFIC_SOURCE = ("dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of 32768 samples "
                        "(profiles/eloc_kernel_kitaev128_symm_a4.md), scaled to 262144 samples")
 L2_FLUSH_BYTES = 256 << 20
