@@ -2019,13 +2019,25 @@ __global__ void __launch_bounds__(256) learned_targets(const LearnedArgs a, int 
         float lg[8];  // min(0, 2 ln|psi'/psi|) of moves lane + 32 i
 #pragma unroll
         for (int i = 0; i < 8; i++) lg[i] = -INFINITY;
-        for (int mv = 0; mv < D; mv++) {
-            float2 tp[E];
-            const float d =
-                sweep_sum(move_partial<E>(a.m, L, le, th, s0, sp, a.mflip[2 * mv], a.mflip[2 * mv + 1], lane, tp));
+        // moves in groups of MG: their partial sums are independent, so the
+        // transcendentals and the warp reductions of a group overlap (the
+        // same per-move arithmetic and reduction)
+        constexpr int MG = 4;
+        for (int mv0 = 0; mv0 < D; mv0 += MG) {
+            float d[MG];
 #pragma unroll
-            for (int i = 0; i < 8; i++)
-                if (mv == lane + 32 * i) lg[i] = fminf(0.f, 2.f * d);
+            for (int g = 0; g < MG; g++) {
+                const int mv = min(mv0 + g, D - 1);
+                float2 tp[E];
+                d[g] = move_partial<E>(a.m, L, le, th, s0, sp, a.mflip[2 * mv], a.mflip[2 * mv + 1], lane, tp);
+            }
+#pragma unroll
+            for (int g = 0; g < MG; g++) {
+                const float dg = sweep_sum(d[g]);
+#pragma unroll
+                for (int i = 0; i < 8; i++)
+                    if (mv0 + g == lane + 32 * i) lg[i] = fminf(0.f, 2.f * dg);
+            }
         }
         float mx = -INFINITY;
 #pragma unroll
