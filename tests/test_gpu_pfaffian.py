@@ -119,6 +119,38 @@ def test_pf_metropolis_fp32_statistics_agree():
     assert same > 0.9
 
 
+def test_pf_metropolis_fp64_at_bench_shape_reproduces_oracle_chains():
+    """The 2048-chain shape of the 32-spin Pfaffian benchmark: 14 chains per
+    block sharing the tables, X^{-1} in circulant form, the fresh inverse
+    every 4 accepted moves in each warp's global scratch.  Every chain's
+    configurations, E_loc and the acceptance match the FP64 oracle."""
+    chains, spc, warm = 2048, 2, 3
+    om, mach, s, rng = make_pair("kitaev4_symm_a2_pf05", precision=1, chains=chains, spc=spc, warmup=warm,
+                                 bond_flips=0.5, std=0.1, refresh=4)
+    st = s.sample()
+    Eg, _ = s.samples(with_O=False)
+    Eo, _, acc, spo = O.metropolis(mach, om, chains, spc, warmup=warm, bond_flips=0.5, seed=123, epoch=0,
+                                   pf_refresh=4, with_O=False)
+    assert np.array_equal(s.spins(), spo)
+    assert rel(Eg, Eo) < TOL64
+    assert abs(st["acceptance"] - acc.mean()) < 1e-12
+
+
+def test_pf_metropolis_fp32_at_bench_shape_follows_oracle():
+    """The benchmark's own path at its shape (FP32 RBM ratios, FP64 Pfaffian,
+    2048 chains, refresh every 32 accepted moves): the samples follow the
+    FP64 oracle's except after acceptance ties."""
+    chains, spc, warm = 2048, 2, 3
+    om, mach, s, rng = make_pair("kitaev4_symm_a2_pf05", precision=0, chains=chains, spc=spc, warmup=warm,
+                                 bond_flips=0.5, std=0.1, refresh=32)
+    s.sample()
+    Eg, _ = s.samples(with_O=False)
+    Eo, _, _, _ = O.metropolis(mach, om, chains, spc, warmup=warm, bond_flips=0.5, seed=123, epoch=0,
+                               pf_refresh=32, with_O=False)
+    same = np.mean(np.abs(Eg - Eo) < 1e-4 * np.maximum(1, np.abs(Eo)))
+    assert same > 0.9
+
+
 @pytest.mark.parametrize("case", ["kitaev2_basic_a1_pf0", "kitaev3_symm_a2_pf05"])
 def test_pf_full_enumeration_matches_oracle_and_ed(case):
     om, mach, s, rng = make_pair(case, precision=1, std=0.3)
