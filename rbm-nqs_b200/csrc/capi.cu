@@ -309,6 +309,7 @@ struct rbmnqs_handle {
     DevBuf<rbmnqs::MfreeSync> dsync;
     DevBuf<double2> dwork;
     DevBuf<rbmnqs::EpochStatsDev> stats;
+    DevBuf<double> estat;  // per-bin partials and ticket of the energy statistics
     // matrix-free SR (n_params above the dense limit): no S is formed
     bool mfree = false;
     bool coop_dense = false;  // formed S too large for the cluster CG: cooperative grid CG
@@ -612,7 +613,7 @@ struct rbmnqs_handle {
         if (tm) mark(2);
         ck(rbmnqs::launch_moments(O.p, fp64, E.p, N, P, mom_blocks, pd.p, pf.p, pe.p, d.p, F.p, emean.p, st),
            "moments");
-        ck(rbmnqs::launch_energy_stats(E.p, N, n_bins, emean.p, nacc.p, nprop.p, cfg.n_chains, stats.p, st),
+        ck(rbmnqs::launch_energy_stats(E.p, N, n_bins, emean.p, nacc.p, nprop.p, cfg.n_chains, estat.p, stats.p, st),
            "energy stats");
         if (net) enqueue_learned_training();
         ck(rbmnqs::launch_advance(ctl.p, cfg.reinit_chains, st), "advance");
@@ -1246,6 +1247,8 @@ int rbmnqs_create(const rbmnqs_model* mdl, const rbmnqs_config* cfg, rbmnqs_hand
             ck(cudaMemcpyAsync(h->plug.p, &pd, sizeof(pd), cudaMemcpyHostToDevice, h->st), "copy");
         }
         h->stats.alloc(1);
+        h->estat.alloc(rbmnqs::energy_stats_scratch_doubles(h->n_bins));
+        ck(cudaMemsetAsync(h->estat.p, 0, h->estat.n * sizeof(double), h->st), "memset");
         // decay_t schedules with the n_updates offset
         h->n_updates = cfg->n_updates;
         set_schedules(h.get(), h->n_updates);
@@ -1929,7 +1932,7 @@ int rbmnqs_get_observables(rbmnqs_handle* h, double* values) {
             }
             ck(rbmnqs::launch_mean(h->obsE.p, h->N, h->obsMean.p + i, h->st), "observable mean");
             ck(rbmnqs::launch_energy_stats(h->obsE.p, h->N, h->n_bins, h->obsMean.p + i, h->nacc.p, h->nprop.p,
-                                           h->cfg.n_chains, h->obsStats.p + i, h->st),
+                                           h->cfg.n_chains, h->estat.p, h->obsStats.p + i, h->st),
                "observable statistics");
         }
         std::vector<rbmnqs::EpochStatsDev> st(no);

@@ -136,43 +136,67 @@ __global__ void moments_final(const double2* pd, const double2* pf, const double
 // aggregator::finalize for a_h_ with n_bins bins (aggregator.cpp:84-164,
 // 233-239): mean, M2, binned M2, tau, unbiased variances, binned stddev; and
 // the mean acceptance over chains (metropolis_sampler.cpp:89-91).
-__global__ void energy_stats(const double2* E, int N, int n_bins, const double2* emean, const uint32_t* nacc,
-                             const uint32_t* nprop, int n_chains, EpochStatsDev* out) {
+// E_loc statistics of the epoch in one launch: block j of the n_bins blocks
+// reads bin j (contiguous, coalesced) for its sum and its share of
+// sum |e - mu|^2; the last block to finish adds the partials in bin order
+// (deterministic) and writes the statistics.  part: 4 doubles per bin, then
+// the ticket counter (zero between launches: the last block resets it).
+__global__ void __launch_bounds__(256) energy_stats(const double2* E, int N, int n_bins, const double2* emean,
+                                                    const uint32_t* nacc, const uint32_t* nprop, int n_chains,
+                                                    double* part, EpochStatsDev* out) {
     __shared__ double red[32];
+    __shared__ int last;
+    unsigned int* ticket = reinterpret_cast<unsigned int*>(part + 4 * n_bins);
     const double2 mu = *emean;
-    double m2 = 0;
+    const int bs = N / n_bins;
+    const double2* Eb = E + (size_t)blockIdx.x * bs;
+    double m2 = 0, sx = 0, sy = 0;
     int finite = 1;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) {
-        const double2 e = E[i];
+    for (int i = threadIdx.x; i < bs; i += blockDim.x) {
+        const double2 e = Eb[i];
         if (!isfinite(e.x) || !isfinite(e.y)) finite = 0;
         const double dx = e.x - mu.x, dy = e.y - mu.y;
         m2 += dx * dx + dy * dy;
+        sx += e.x;
+        sy += e.y;
     }
     m2 = block_sum(m2, red);
-    const int bs = N / n_bins;
-    double m2b = 0;
-    for (int b = threadIdx.x; b < n_bins; b += blockDim.x) {
-        double sx = 0, sy = 0;
-        for (int i = 0; i < bs; i++) {
-            sx += E[(size_t)b * bs + i].x;
-            sy += E[(size_t)b * bs + i].y;
-        }
-        const double dx = sx / bs - mu.x, dy = sy / bs - mu.y;
-        m2b += bs * (dx * dx + dy * dy);
+    sx = block_sum(sx, red);
+    sy = block_sum(sy, red);
+    const double nf = block_sum((double)finite, red);
+    if (threadIdx.x == 0) {
+        double* pp = part + 4 * blockIdx.x;
+        pp[0] = m2;
+        pp[1] = sx;
+        pp[2] = sy;
+        pp[3] = nf == (double)blockDim.x ? 1.0 : 0.0;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == (unsigned int)(n_bins - 1);
     }
-    m2b = block_sum(m2b, red);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
     double acc = 0;
     for (int c = threadIdx.x; c < n_chains; c += blockDim.x) acc += nprop[c] ? (double)nacc[c] / nprop[c] : 0.0;
     acc = block_sum(acc, red);
-    const double nf = block_sum((double)finite, red);
     if (threadIdx.x == 0) {
+        const volatile double* vp = part;
+        double M2 = 0, M2b = 0;
+        int fin = 1;
+        for (int b = 0; b < n_bins; b++) {
+            M2 += vp[4 * b];
+            const double dx = vp[4 * b + 1] / bs - mu.x, dy = vp[4 * b + 2] / bs - mu.y;
+            M2b += bs * (dx * dx + dy * dy);
+            if (vp[4 * b + 3] == 0.0) fin = 0;
+        }
+        *ticket = 0u;
         double tau = 0;
-        if (n_bins > 1 && !(m2 == 0 && m2b == 0)) {
-            double r = bs * m2b / m2;
+        if (n_bins > 1 && !(M2 == 0 && M2b == 0)) {
+            const double r = bs * M2b / M2;
             tau = 0.5 * ((r < 1 ? 1 : r) - 1);
         }
         const double den = (double)N - 1.0;
-        double v = m2 / den, vb = m2b / den;
+        double v = M2 / den, vb = M2b / den;
         v = v < 0 ? 0 : v;
         vb = vb < 0 ? 0 : vb;
         out->energy = mu;
@@ -181,7 +205,7 @@ __global__ void energy_stats(const double2* E, int N, int n_bins, const double2*
         out->tau = tau;
         out->stddev = n_bins > 1 ? sqrt(vb / n_bins) : sqrt(v / N);
         out->acceptance = acc / n_chains;
-        out->finite = nf == (double)blockDim.x ? 1 : 0;
+        out->finite = fin;
     }
 }
 
@@ -1034,8 +1058,10 @@ cudaError_t launch_mean(const double2* E, int N, double2* mu, cudaStream_t st) {
 }
 
 cudaError_t launch_energy_stats(const double2* E, int N, int n_bins, const double2* emean, const uint32_t* nacc,
-                                const uint32_t* nprop, int n_chains, EpochStatsDev* out, cudaStream_t st) {
-    energy_stats<<<1, 1024, 0, st>>>(E, N, n_bins, emean, nacc, nprop, n_chains, out);
+                                const uint32_t* nprop, int n_chains, double* scratch, EpochStatsDev* out,
+                                cudaStream_t st) {
+    if (n_bins < 1 || n_bins > kMaxBins || N % n_bins) return cudaErrorInvalidValue;
+    energy_stats<<<n_bins, 256, 0, st>>>(E, N, n_bins, emean, nacc, nprop, n_chains, scratch, out);
     return cudaGetLastError();
 }
 

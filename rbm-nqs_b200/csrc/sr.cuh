@@ -39,8 +39,14 @@ struct CgResultDev {
 cudaError_t launch_moments(const void* O, int fp64, const double2* E, int N, int P, int nblk, double2* pd,
                            double2* pf, double2* pe, double2* d, double2* F, double2* emean, cudaStream_t st,
                            const double* w = nullptr, const double* wsum = nullptr);
+// E_loc statistics (one block per bin; n_bins <= kMaxBins and divides N).
+// scratch: energy_stats_scratch_doubles(n_bins) doubles, zero before the
+// first launch (each launch leaves it zero).
+constexpr int kMaxBins = 64;
+inline size_t energy_stats_scratch_doubles(int n_bins) { return 4 * (size_t)n_bins + 1; }
 cudaError_t launch_energy_stats(const double2* E, int N, int n_bins, const double2* emean, const uint32_t* nacc,
-                                const uint32_t* nprop, int n_chains, EpochStatsDev* out, cudaStream_t st);
+                                const uint32_t* nprop, int n_chains, double* scratch, EpochStatsDev* out,
+                                cudaStream_t st);
 cudaError_t launch_mean(const double2* E, int N, double2* mu, cudaStream_t st);
 int gram_splits(int N, int P);
 cudaError_t launch_gram_fp64(const void* O, int fp64, const double2* d, int N, int P, int nks, double2* part,
