@@ -290,19 +290,42 @@ __global__ void transpose_bf16(const __nv_bfloat16* __restrict__ in, int R, int 
 }
 
 // gradient of a layer: dW = sum over splits (FP32), db = column sums of G
-__global__ void finish_grads(const float* __restrict__ part, int nsplit, int out, int in,
-                             const __nv_bfloat16* __restrict__ G, int rows, float* __restrict__ dW,
-                             float* __restrict__ db) {
-    const size_t total = (size_t)out * in;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-        float s = 0.f;
-        for (int k = 0; k < nsplit; k++) s += part[(size_t)k * total + i];
-        dW[i] = s;
+// dW = the sum of the split-K partials (blocks [0, wblocks), grid-stride);
+// db = the column sums of G over the rows (blocks from wblocks on, 32
+// columns each: the block's warps take interleaved rows with four
+// accumulators, then the warp partials are added in warp order)
+__global__ void __launch_bounds__(256) finish_grads(const float* __restrict__ part, int nsplit, int out, int in,
+                                                    const __nv_bfloat16* __restrict__ G, int rows,
+                                                    float* __restrict__ dW, float* __restrict__ db, int wblocks) {
+    if ((int)blockIdx.x < wblocks) {
+        const size_t total = (size_t)out * in;
+        for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)wblocks * blockDim.x) {
+            float s = 0.f;
+            for (int k = 0; k < nsplit; k++) s += part[(size_t)k * total + i];
+            dW[i] = s;
+        }
+        return;
     }
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < out; c += gridDim.x * blockDim.x) {
-        float s = 0.f;
-        for (int b = 0; b < rows; b++) s += __bfloat162float(G[(size_t)b * out + c]);
-        db[c] = s;
+    __shared__ float red[8][33];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int c = (blockIdx.x - wblocks) * 32 + lane;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    if (c < out) {
+        int b = w;
+        for (; b + 3 * nw < rows; b += 4 * nw) {
+            a0 += __bfloat162float(G[(size_t)b * out + c]);
+            a1 += __bfloat162float(G[(size_t)(b + nw) * out + c]);
+            a2 += __bfloat162float(G[(size_t)(b + 2 * nw) * out + c]);
+            a3 += __bfloat162float(G[(size_t)(b + 3 * nw) * out + c]);
+        }
+        for (; b < rows; b += nw) a0 += __bfloat162float(G[(size_t)b * out + c]);
+    }
+    red[w][lane] = (a0 + a1) + (a2 + a3);
+    __syncthreads();
+    if (w == 0 && c < out) {
+        float t = red[0][lane];
+        for (int j = 1; j < nw; j++) t += red[j][lane];
+        db[c] = t;
     }
 }
 
@@ -619,8 +642,9 @@ cudaError_t Mlp::backward_step(int B, float lr, cudaStream_t st, bool apply) {
         p.mtot = l.out;
         const int mrows = (l.out + kRows - 1) / kRows * kRows;
         if ((r = gemm(l.a, l.b, mrows, l.in, M, ns, p, err_, st)) != cudaSuccess) return r;
-        finish_grads<<<grid_for((size_t)l.out * l.in), 256, 0, st>>>(part_, ns, l.out, l.in, l.G, M,
-                                                                     grad_ + off_W(l.layer), grad_ + off_b(l.layer));
+        const int wb = grid_for((size_t)l.out * l.in), cb = (l.out + 31) / 32;
+        finish_grads<<<wb + cb, 256, 0, st>>>(part_, ns, l.out, l.in, l.G, M, grad_ + off_W(l.layer),
+                                              grad_ + off_b(l.layer), wb);
     }
     if (!apply) return cudaGetLastError();
     step_++;
