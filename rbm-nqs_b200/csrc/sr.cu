@@ -176,18 +176,20 @@ __global__ void __launch_bounds__(256) energy_stats(const double2* E, int N, int
     __syncthreads();
     if (!last) return;
     __threadfence();
+    // the partials into shared memory in parallel, then added in bin order
+    __shared__ double sp[4 * kMaxBins];
+    for (int i = threadIdx.x; i < 4 * n_bins; i += blockDim.x) sp[i] = reinterpret_cast<volatile double*>(part)[i];
     double acc = 0;
     for (int c = threadIdx.x; c < n_chains; c += blockDim.x) acc += nprop[c] ? (double)nacc[c] / nprop[c] : 0.0;
-    acc = block_sum(acc, red);
+    acc = block_sum(acc, red);  // (its barriers also publish sp)
     if (threadIdx.x == 0) {
-        const volatile double* vp = part;
         double M2 = 0, M2b = 0;
         int fin = 1;
         for (int b = 0; b < n_bins; b++) {
-            M2 += vp[4 * b];
-            const double dx = vp[4 * b + 1] / bs - mu.x, dy = vp[4 * b + 2] / bs - mu.y;
+            M2 += sp[4 * b];
+            const double dx = sp[4 * b + 1] / bs - mu.x, dy = sp[4 * b + 2] / bs - mu.y;
             M2b += bs * (dx * dx + dy * dy);
-            if (vp[4 * b + 3] == 0.0) fin = 0;
+            if (sp[4 * b + 3] == 0.0) fin = 0;
         }
         *ticket = 0u;
         double tau = 0;
