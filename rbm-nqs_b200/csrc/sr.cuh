@@ -102,7 +102,7 @@ cudaError_t launch_update(double2* params, double2* x, int P, const ScheduleDev*
                           cudaStream_t st);
 // Matrix-free CG (cg_mfree.cu) for parameter counts without a formed S.
 struct MfreeSync {
-    uint32_t count, gen;
+    uint32_t count, gen;  // count: arrivals so far (grows by the grid's blocks per barrier); gen unused
     int bad;
     uint32_t extra;     // arrivals beyond the grid's blocks a barrier waits for (0; 1 under test fault 1)
     uint32_t spin_cap;  // polls before a waiting block gives up (0: kBarrierSpin)
