@@ -66,8 +66,7 @@ __global__ void moments_partial(const TO* O, const double2* E, int N, int P, dou
     const int n0 = (int)((long)N * blockIdx.x / nb), n1 = (int)((long)N * (blockIdx.x + 1) / nb);
     for (int p = threadIdx.x; p < P; p += blockDim.x) {
         double sx = 0, sy = 0, fx = 0, fy = 0;
-        for (int n = n0; n < n1; n++) {
-            double2 o = ld2(O, (size_t)n * P + p);
+        auto add = [&](double2 o, int n) {
             if (w) {
                 const double wn = w[n];
                 o = make_double2(wn * o.x, wn * o.y);
@@ -77,7 +76,17 @@ __global__ void moments_partial(const TO* O, const double2* E, int N, int P, dou
             sy += o.y;
             fx += e.x * o.x + e.y * o.y;  // E * conj(O)
             fy += e.y * o.x - e.x * o.y;
+        };
+        // four rows' loads in flight before their (ordered) sums
+        int n = n0;
+        for (; n + 3 < n1; n += 4) {
+            double2 o[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) o[u] = ld2(O, (size_t)(n + u) * P + p);
+#pragma unroll
+            for (int u = 0; u < 4; u++) add(o[u], n + u);
         }
+        for (; n < n1; n++) add(ld2(O, (size_t)n * P + p), n);
         pd[(size_t)blockIdx.x * P + p] = make_double2(sx, sy);
         pf[(size_t)blockIdx.x * P + p] = make_double2(fx, fy);
     }
@@ -1037,10 +1046,13 @@ __global__ void unpack_weights(const double2* params, int n, int n_vb, int nh, d
 cudaError_t launch_moments(const void* O, int fp64, const double2* E, int N, int P, int nblk, double2* pd,
                            double2* pf, double2* pe, double2* d, double2* F, double2* emean, cudaStream_t st,
                            const double* w, const double* wsum) {
+    // one column per thread (a single pass over the block's rows) up to 1024
+    // parameters
+    const int thr = std::min(1024, std::max(32, (P + 31) / 32 * 32));
     if (fp64)
-        moments_partial<double2><<<nblk, 256, 0, st>>>((const double2*)O, E, N, P, pd, pf, pe, w);
+        moments_partial<double2><<<nblk, thr, 0, st>>>((const double2*)O, E, N, P, pd, pf, pe, w);
     else
-        moments_partial<float2><<<nblk, 256, 0, st>>>((const float2*)O, E, N, P, pd, pf, pe, w);
+        moments_partial<float2><<<nblk, thr, 0, st>>>((const float2*)O, E, N, P, pd, pf, pe, w);
     moments_final<<<(P + 7) / 8, 256, 0, st>>>(pd, pf, pe, nblk, N, P, d, F, emean, wsum);
     return cudaGetLastError();
 }
