@@ -205,20 +205,29 @@ __global__ void gram_rowmax(const TO* __restrict__ O, const double2* __restrict_
     if (p >= P) return;
     const double2 dd = d[p];
     float mr = 0.f, mi = 0.f;
-    for (int n = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5); n < N; n += gridDim.y * (blockDim.x >> 5)) {
+    auto take = [&](TO o) {
         float vr, vi;
         if constexpr (sizeof(TO) == 8) {
-            const float2 o = reinterpret_cast<const float2*>(O)[(size_t)n * P + p];
             vr = (float)((double)o.x - dd.x);
             vi = (float)((double)o.y - dd.y);
         } else {
-            const double2 o = reinterpret_cast<const double2*>(O)[(size_t)n * P + p];
             vr = (float)(o.x - dd.x);
             vi = (float)(o.y - dd.y);
         }
         mr = fmaxf(mr, fabsf(vr));
         mi = fmaxf(mi, fabsf(vi));
+    };
+    // four rows' loads in flight before their maxima (order-free)
+    const int step = gridDim.y * (blockDim.x >> 5);
+    int n = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    for (; n + 3 * step < N; n += 4 * step) {
+        TO o[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) o[u] = O[(size_t)(n + u * step) * P + p];
+#pragma unroll
+        for (int u = 0; u < 4; u++) take(o[u]);
     }
+    for (; n < N; n += step) take(O[(size_t)n * P + p]);
     atomicMax(rmax + 2 * p, __float_as_uint(mr));
     atomicMax(rmax + 2 * p + 1, __float_as_uint(mi));
 }
