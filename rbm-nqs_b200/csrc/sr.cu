@@ -335,25 +335,30 @@ __global__ void regularize(const double2* S, int P, int n_neural, int N, const S
     const double r1 = sch->value[1], r2 = sch->value[2], rd = sch->value[3];
     // unbiased variance factor: N / (N - 1), or W / (W - W2 / W) for weights
     const double vf = vfac ? *vfac : (double)N / ((double)N - 1.0);
+    // every block forms max(diag) itself (order-free); block 0 stores diag
     double mx = 0;
     for (int p = threadIdx.x; p < P; p += blockDim.x) {
         const double v = S[(size_t)p * P + p].x * vf;
-        diag[p] = v;
+        if (blockIdx.x == 0) diag[p] = v;
         mx = fmax(mx, v);
     }
     mx = block_max(mx, red);
-    if (threadIdx.x == 0) *max_diag_out = mx;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *max_diag_out = mx;
+    // the copy over all blocks, the shift applied to the diagonal entries
+    // (index p (P + 1)) on the way
     const size_t total = (size_t)P * P;
-    for (size_t i = threadIdx.x; i < total; i += blockDim.x) Sreg[i] = S[i];
-    __syncthreads();
-    for (int p = threadIdx.x; p < P; p += blockDim.x) {
-        double2& s = Sreg[(size_t)p * P + p];
-        if (direct) {
-            const double g = p < n_neural ? 1.0 + r1 : (1.0 + r1) + rd;
-            s = make_double2(s.x * g + r2 * mx, s.y * g);
-        } else {
-            s.x += diag[p] * (p < n_neural ? r1 : r1 + rd) + mx * r2;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        double2 s = S[i];
+        if (i % (size_t)(P + 1) == 0) {
+            const int p = (int)(i / (size_t)(P + 1));
+            if (direct) {
+                const double g = p < n_neural ? 1.0 + r1 : (1.0 + r1) + rd;
+                s = make_double2(s.x * g + r2 * mx, s.y * g);
+            } else {
+                s.x += s.x * vf * (p < n_neural ? r1 : r1 + rd) + mx * r2;
+            }
         }
+        Sreg[i] = s;
     }
 }
 
@@ -1112,7 +1117,8 @@ cudaError_t launch_schedule_regs(ScheduleDev* s, cudaStream_t st) {
 
 cudaError_t launch_regularize(const double2* S, int P, int n_neural, int N, const ScheduleDev* sch, double* diag,
                               double2* Sreg, double* max_diag, cudaStream_t st, int direct, const double* vfac) {
-    regularize<<<1, 1024, 0, st>>>(S, P, n_neural, N, sch, diag, Sreg, max_diag, direct, vfac);
+    const int blocks = (int)std::max<long>(1, std::min<long>(296, ((long)P * P + 1023) / 1024));
+    regularize<<<blocks, 1024, 0, st>>>(S, P, n_neural, N, sch, diag, Sreg, max_diag, direct, vfac);
     return cudaGetLastError();
 }
 
